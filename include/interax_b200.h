@@ -1,0 +1,172 @@
+/*
+ * interax_b200.h -- C ABI of the B200 (sm_100a) kernels for the InteraxFF short-range path.
+ *
+ * The reference plugin reaches its GPU path through OpenMM's platform-kernel interface: the abstract kernels
+ * CalcInteraxDispersionForceKernel, CalcInteraxExchangeForceKernel, CalcInteraxShortRangeForceKernel and
+ * CalcInteraxThreeBodyForceKernel (openmmapi/include/InteraxKernels.h:51-189), each with
+ *   initialize(const System&, const <Force>&)
+ *   double execute(ContextImpl&, bool includeForces, bool includeEnergy)
+ *   copyParametersToContext(ContextImpl&, const <Force>&)
+ * implemented for CUDA by platforms/common/src/CommonInteraxKernels.cpp:139-646 and registered by
+ * platforms/cuda/src/CudaInteraxKernelFactory.cpp:45-87.  This header is the flat boundary those classes (or any
+ * FFI: ctypes, cgo, JNI) bind: plain pointers and sizes, no C++ or torch types.
+ *
+ * Conventions
+ *   - Every function returns IX_OK (0) or an error code; ix_last_error() returns the message, which repeats the
+ *     reference's OpenMMException text where the reference throws one.
+ *   - Lengths nm, energies kJ/mol, forces kJ/mol/nm, positions double precision, row-major N x 3.
+ *   - Box vectors: 9 doubles a, b, c in OpenMM's reduced form (a = (ax,0,0), b = (bx,by,0), c = (cx,cy,cz)).
+ *   - A context is used from one host thread at a time; independent contexts may run concurrently.
+ *   - The context owns all device memory it allocates; no caller pointer is kept after a call returns.
+ */
+#ifndef INTERAX_B200_H
+#define INTERAX_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define IX_OK 0
+#define IX_ERR_INVALID 1     /* illegal settings or arguments (OpenMMException in the reference) */
+#define IX_ERR_CUDA 2        /* a CUDA runtime error; the message names the call */
+#define IX_ERR_STATE 3       /* call made in the wrong order (e.g. compute before positions) */
+#define IX_ERR_NO_DEVICE 4   /* no CUDA device, or the requested device is missing */
+
+/* Nonbonded methods (InteraxPairForce.h:79-96) */
+#define IX_NO_CUTOFF 0
+#define IX_CUTOFF_NON_PERIODIC 1
+#define IX_CUTOFF_PERIODIC 2
+
+/* Overlap methods (InteraxExchangeForce.h:66-79) */
+#define IX_OVERLAP_EXACT 0
+#define IX_OVERLAP_INTERAX_ORDER2 2
+
+/* Three-body damping methods (InteraxThreeBodyForce.h:85-96) */
+#define IX_NO_DAMPING 0
+#define IX_TANG_TOENNIES 1
+
+/* Term indices of the per-term energy array */
+#define IX_TERM_DISPERSION 0
+#define IX_TERM_EXCHANGE 1
+#define IX_TERM_SHORT_RANGE 2
+#define IX_TERM_THREE_BODY 3
+#define IX_NUM_TERMS 4
+
+typedef struct ix_ctx ix_ctx;
+
+/* Settings every pair force has (InteraxPairForce.h:70-239).  The three pair forces of one context are evaluated
+ * in one fused pass over one neighbor list, so, as on the reference's CUDA platform (InteraxPairForce.h:50-53,
+ * CommonInteraxKernels.h:42-46), they must have identical nonbonded methods, cutoffs and exclusions. */
+typedef struct {
+    int nonbonded_method;          /* IX_NO_CUTOFF, IX_CUTOFF_NON_PERIODIC, IX_CUTOFF_PERIODIC */
+    double cutoff;                 /* nm */
+    int use_switching_function;
+    double switching_distance;     /* nm */
+    double softcore_radius;        /* nm, 0 disables the soft core */
+    int force_group;               /* 0..31 */
+    const char* alchemical_parameter;   /* name of the context parameter; NULL = "lambda_sterics" */
+    int num_exclusions;
+    const int32_t* exclusions;     /* 2 x num_exclusions particle indices */
+} ix_pair_settings;
+
+/* Create a context for a System of num_particles particles on CUDA device `device`.  `box` (9 doubles) is the
+ * System's default periodic box, used to validate CutoffPeriodic cutoffs as checkPairForce does
+ * (openmmapi/src/InteraxPairForce.cpp:113-136); it may be NULL for non-periodic systems. */
+int ix_ctx_create(int num_particles, int device, const double* default_box, ix_ctx** out);
+
+/* Destroy a context and free its device memory. */
+void ix_ctx_destroy(ix_ctx* ctx);
+
+/* Message of the last error of `ctx`, or of the last failed ix_ctx_create when ctx is NULL. */
+const char* ix_last_error(const ix_ctx* ctx);
+
+/* Add the pair forces.  Replaces CalcInterax{Dispersion,Exchange,ShortRange}ForceKernel::initialize
+ * (InteraxKernels.h:64-67, 99-102, 134-137; CUDA: CommonInteraxKernels.cpp:221-249, 304-313, 345-354).
+ *   dispersion params: num_particles x 5 (m1, m2, m3, alpha, width)       InteraxDispersionForce.h:103
+ *   exchange params:   num_particles x 2 (amplitude, width)                InteraxExchangeForce.h:108
+ *   short range:       num_particles x 3 (k, l, width)                     InteraxShortRangeForce.h:109
+ *   is_alchemical:     num_particles bytes (0/1) */
+int ix_add_dispersion(ix_ctx* ctx, const ix_pair_settings* settings, const double* params,
+                      const uint8_t* is_alchemical, double damping_scale, int use_long_range_correction);
+int ix_add_exchange(ix_ctx* ctx, const ix_pair_settings* settings, const double* params,
+                    const uint8_t* is_alchemical, int overlap_method);
+int ix_add_short_range(ix_ctx* ctx, const ix_pair_settings* settings, const double* params,
+                       const uint8_t* is_alchemical, int overlap_method);
+
+/* Add the three-body force.  Replaces CalcInteraxThreeBodyForceKernel::initialize (InteraxKernels.h:169-172;
+ * CUDA: CommonInteraxKernels.cpp:437-571).  Site s is the unweighted centroid of
+ * site_particles[site_offsets[s] .. site_offsets[s+1]); site_params is num_sites x 3 (alpha, frequency, width);
+ * molecule < 0 puts a site in a molecule of its own (InteraxThreeBodyForce.h:116-130). */
+int ix_add_three_body(ix_ctx* ctx, int num_sites, const int32_t* site_offsets, const int32_t* site_particles,
+                      const double* site_params, const int32_t* molecule, const uint8_t* is_alchemical,
+                      double cutoff, double scale_factor, int damping_method, double damping_scale,
+                      double centroid_damping_radius, int periodic, const char* alchemical_parameter,
+                      int force_group);
+
+/* Replace copyParametersToContext (InteraxKernels.h:84-85, 119-120, 154-155, 187-188; Reference semantics
+ * ReferenceInteraxKernels.cpp:98-198, CUDA CommonInteraxKernels.cpp:261-375, 618-629).  The particle count, the
+ * alchemical flags, the exclusions, the nonbonded method, the cutoff and the overlap method cannot change. */
+int ix_update_dispersion(ix_ctx* ctx, const double* params, double damping_scale);
+int ix_update_exchange(ix_ctx* ctx, const double* params, int overlap_method);
+int ix_update_short_range(ix_ctx* ctx, const double* params, int overlap_method);
+int ix_update_three_body(ix_ctx* ctx, const double* site_params, double scale_factor, double damping_scale,
+                         double centroid_damping_radius);
+
+/* Set a context parameter (the alchemical parameters; ContextImpl::setParameter in OpenMM).  Parameters that no
+ * force uses are accepted and ignored. */
+int ix_set_parameter(ix_ctx* ctx, const char* name, double value);
+
+/* Copy positions (num_particles x 3, host memory) and, for periodic systems, the box (9 doubles, may be NULL to keep
+ * the previous box) to the device. */
+int ix_set_positions(ix_ctx* ctx, const double* positions, const double* box);
+
+/* Evaluate the forces whose force group is in the bit mask `groups` (execute() of every selected kernel,
+ * InteraxPairForceImpl.h:84-88, InteraxThreeBodyForceImpl.cpp:64-68).  `term_energies` (may be NULL) receives the
+ * energy of each term (IX_TERM_*, 0 for terms not evaluated), `energy` (may be NULL) their sum, and `forces`
+ * (num_particles x 3 host doubles, may be NULL) the total force of the selected terms (overwritten). */
+int ix_compute(ix_ctx* ctx, int groups, int include_forces, int include_energy, double* term_energies,
+               double* energy, double* forces);
+
+/* Device-resident variant for integration into a GPU engine: evaluate on the context's stream using the positions
+ * already on the device, and ADD the forces to d_force_fixed, an int64 fixed-point buffer (scale 2^32,
+ * layout x[0..stride), y[stride..2 stride), z[...]) as OpenMM's CUDA platform keeps them
+ * (platforms/common/src/kernels/interaxThreeBody.cc:644-652), in original particle order.  d_term_energies
+ * (device, IX_NUM_TERMS doubles, may be NULL) receives the term energies.  Nothing is copied to the host and the
+ * call does not synchronize. */
+int ix_compute_device(ix_ctx* ctx, int groups, long long* d_force_fixed, int force_stride,
+                      double* d_term_energies);
+
+/* Device positions in and device forces out, for callers that keep their state on the GPU: d_positions is
+ * num_particles x 3 doubles on the device (copied device-to-device on the context's stream), d_forces receives
+ * num_particles x 3 doubles (overwritten) and d_term_energies IX_NUM_TERMS doubles.  Does not synchronize. */
+int ix_compute_device_f64(ix_ctx* ctx, int groups, const double* d_positions, const double* box,
+                          double* d_forces, double* d_term_energies);
+
+/* Counts of the last evaluation: interacting pairs (non-excluded, within the cutoff, gate true, counted once) and
+ * interacting triples.  Counting costs an extra reduction, so it is done only after ix_set_counting(ctx, 1). */
+int ix_set_counting(ix_ctx* ctx, int enable);
+int ix_get_counts(ix_ctx* ctx, long long* num_pairs, long long* num_triples);
+
+/* Velocity-Verlet MD on the device with the context's forces (all groups): `num_steps` steps of `dt` ps, masses
+ * in amu.  Velocities (N x 3, nm/ps) are read from and written back to `velocities`; positions are written back
+ * to `positions` (both may be NULL to keep the state on the device; the first call must pass both).  Returns the
+ * final potential energy in *energy if not NULL. */
+int ix_md_set_masses(ix_ctx* ctx, const double* masses);
+int ix_md_run(ix_ctx* ctx, int num_steps, double dt, double* positions, double* velocities, double* energy);
+
+/* The CUDA stream the context launches on (as a void*), so callers can order their own work around it. */
+void* ix_get_stream(ix_ctx* ctx);
+
+/* Synchronize the context's stream and report any asynchronous error. */
+int ix_synchronize(ix_ctx* ctx);
+
+/* Library version string. */
+const char* ix_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* INTERAX_B200_H */
