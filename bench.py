@@ -1,0 +1,317 @@
+"""Benchmark of the InteraxFF short-range path on B200: the plain drop-in at size (24,000-atom water box).
+
+One step = one velocity-Verlet MD step of 1 fs on the device: the fused pair pass (dispersion + exchange + short
+range over one neighbor list, with the list maintenance it needs) and the three-body (ATM) pass over 8,000 molecular
+sites, plus the integration.  Metric: interactions/s, the interacting pairs plus interacting triples evaluated per
+second (the pair and triple counts come from the kernels, per step); ns/day follows from the step time.
+
+  value      device-resident: per-step CUDA-event time on the context's stream, L2 flushed between steps
+  e2e        through the C ABI with host buffers: positions host->device, evaluation, forces device->host, per step
+  roofline   the pair kernel (the dominant kernel): algorithmic operations per launch (pairs x F_PAIR) over its
+             event-timed duration, against the device's FP32 issue peak measured live by ix_measure_fp32_peak
+  cpu_baseline  the FP64 oracle (restatement of the reference's Reference platform) on one full evaluation
+
+--impl reference times the reference's own CPU implementation of the path (its restatement, since the plugin cannot
+be built without OpenMM) on the same workload, one evaluation per step.
+"""
+import argparse
+import ctypes
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path[:0] = [str(ROOT / "openmm-interax-plugin_b200"), str(ROOT / "oracle")]
+
+import numpy as np  # noqa: E402
+
+# Algorithmic operations per interacting pair and per interacting triple of the reference algorithm, counted once by
+# running the FP64 oracle on counting values over the 24,000-atom box (oracle/count_ops.py): the three pair terms'
+# functions (order-6 Taylor overlap for equal widths, closed form otherwise, full Tang-Toennies series) plus the pair
+# driver, and the ATM triple with C9.
+F_PAIR = 612.4
+F_TRIPLE = 151.0
+METRIC = "interactions/s"
+WORKLOAD = "water box 24,000 atoms (8,000 rigid-geometry waters, 6.208 nm periodic, cutoff 1.0 nm) + ATM on " \
+           "8,000 molecular sites (cutoff 0.6 nm); velocity-Verlet 1 fs"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--config", default="24k")
+    p.add_argument("--seed", type=int, default=1)
+    return p.parse_args()
+
+
+def dist_init(args):
+    """One process per GPU under torchrun; returns (rank, world)."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return rank, world
+
+
+def build_system(args, rank):
+    from interaxplugin import workloads as W
+    cfg = W.CONFIGS[args.config]
+    # every rank runs an independent replica (a single box does not shard; see the design notes)
+    return W.water_box(cfg["num_waters"], cfg["box_length"], cfg["cutoff"], seed=args.seed + rank,
+                       three_body_cutoff=cfg["three_body_cutoff"])
+
+
+def relax(ctx, system, positions, iterations=60, max_step=0.01):
+    """Steepest descent with a capped step, so that 1 fs velocity Verlet starts without the lattice's hot contacts."""
+    pos = positions.copy()
+    for _ in range(iterations):
+        ctx.setPositions(pos)
+        f = ctx.getState(getEnergy=False).getForces()
+        fmax = np.sqrt((f ** 2).sum(1)).max()
+        pos = pos + f * (max_step / max(fmax, 1e-12))
+    ctx.setPositions(pos)
+    return pos
+
+
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(system, pos, box):
+    """The FP64 oracle (restated Reference platform, one thread) on one full evaluation of the workload."""
+    import pyoracle
+    counts = []
+    t0 = time.perf_counter()
+    for force in system._forces:
+        term = pyoracle.term_of(force)
+        if term == 3:
+            pyoracle.three_body(force, pos, box, counts=counts)
+        elif term == 0:
+            pyoracle.pair_force(term, force, pos, box, counts=counts)
+        else:
+            pyoracle.pair_force(term, force, pos, box)
+    dt = time.perf_counter() - t0
+    interactions = sum(counts)
+    return {"value": interactions / dt, "unit": METRIC, "cores": 1, "kind": "port",
+            "sample": f"one evaluation of the four terms of the 24,000-atom box by the FP64 oracle "
+                      f"({interactions} interactions, {dt:.1f} s)"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    system, pos, box = build_system(args, 0)
+    times, inter = [], []
+    for step in range(args.warmup + args.steps):
+        r = cpu_baseline(system, pos, box)
+        if step >= args.warmup:
+            inter.append(r["value"])
+            times.append(float(r["sample"].split("(")[-1].split(",")[1].split("s")[0]))
+    value = float(np.mean(inter))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * float(np.mean(times)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD + " (one energy+force evaluation per step)"},
+            "cpu_baseline": {"value": value, "unit": METRIC, "cores": 1, "kind": "port",
+                             "sample": "one evaluation of the four terms of the 24,000-atom box per step"},
+            "e2e": {"value": value, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def run_ours(args, rank, world):
+    import torch
+    from interaxplugin import Context, _capi
+    from interaxplugin import workloads as W
+
+    device = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(device)
+    system, pos0, box = build_system(args, rank)
+    ctx = Context(system, properties={"DeviceIndex": device})
+    L = _capi.lib()
+    pos = relax(ctx, system, pos0)
+    vel = W.initial_velocities(system, 300.0, seed=rank)
+    dt_ps = 0.001
+    # masses, velocities and the first forces
+    masses = np.array([system.getParticleMass(i) for i in range(system.getNumParticles())])
+    ctx._check(L.ix_md_set_masses(ctx._ctx, _capi.ptr(masses)))
+    vel = np.ascontiguousarray(vel)
+    ctx._check(L.ix_md_run(ctx._ctx, 1, dt_ps, None, _capi.ptr(vel), None))
+    ctx._check(L.ix_set_profiling(ctx._ctx, 1))
+    stream = torch.cuda.ExternalStream(L.ix_get_stream(ctx._ctx))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")   # 256 MB > 126 MB L2
+    peak = ctypes.c_double()
+    ctx._check(L.ix_measure_fp32_peak(device, ctypes.byref(peak)))
+
+    def md_step():
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        ctx._check(L.ix_md_steps_async(ctx._ctx, 1, dt_ps))
+        end.record(stream)
+        rc = L.ix_md_finish(ctx._ctx, None, None, None)
+        if rc != 0:
+            raise RuntimeError(L.ix_last_error(ctx._ctx).decode())
+        pair_ms, atm_ms = ctypes.c_double(), ctypes.c_double()
+        ctx._check(L.ix_get_kernel_times(ctx._ctx, ctypes.byref(pair_ms), ctypes.byref(atm_ms)))
+        pairs, triples = ctx.getCounts()
+        return start.elapsed_time(end), pair_ms.value, atm_ms.value, pairs, triples
+
+    for _ in range(args.warmup):
+        md_step()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    rows = []
+    launches0 = ctypes.c_longlong()
+    ctx._check(L.ix_get_launch_count(ctx._ctx, ctypes.byref(launches0)))
+    with ClockSampler(device) as clocks:
+        for _ in range(args.steps):
+            rows.append(md_step())
+    torch.cuda.synchronize()
+    launches1 = ctypes.c_longlong()
+    ctx._check(L.ix_get_launch_count(ctx._ctx, ctypes.byref(launches1)))
+    rows = np.array(rows)
+    step_ms = rows[:, 0].sum()
+    interactions = rows[:, 3].sum() + rows[:, 4].sum()
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([step_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+        c = torch.tensor([interactions], dtype=torch.float64, device="cuda")
+        dist.all_reduce(c, op=dist.ReduceOp.SUM)
+        interactions = float(c.item())
+    value = interactions / (step_ms * 1e-3)
+    ms_per_step = step_ms / args.steps
+
+    # e2e: the same configurations through the host API (positions in, forces out, pinned host buffers)
+    n = system.getNumParticles()
+    hpos = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    hfor = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    cur = np.empty((n, 3))
+    ctx._check(L.ix_md_finish(ctx._ctx, _capi.ptr(cur), None, None))
+    hpos.numpy()[:] = cur
+    terms = np.zeros(4)
+    energy = ctypes.c_double()
+    e2e_t, e2e_inter = 0.0, 0
+    for step in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        ctx._check(L.ix_set_positions(ctx._ctx, ctypes.c_void_p(hpos.data_ptr()), None))
+        ctx._check(L.ix_compute(ctx._ctx, -1, 1, 1, _capi.ptr(terms), ctypes.byref(energy),
+                                ctypes.c_void_p(hfor.data_ptr())))
+        t1 = time.perf_counter()
+        if step >= args.warmup:
+            e2e_t += t1 - t0
+            p, tr = ctx.getCounts()
+            e2e_inter += p + tr
+    e2e_value = e2e_inter / e2e_t
+
+    if rank != 0:
+        return
+    pair_ms = float(np.mean(rows[:, 1]))
+    pairs_per_launch = float(np.mean(rows[:, 3]))
+    achieved = pairs_per_launch * F_PAIR / (pair_ms * 1e-3) / 1e12
+    base = cpu_baseline(system, cur, box)
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "atoms": n, "sites": system.getForce(3).getNumSites(),
+                   "pairs_per_step": float(np.mean(rows[:, 3])), "triples_per_step": float(np.mean(rows[:, 4])),
+                   "ns_per_day": 86400 * dt_ps * 1e-3 / (ms_per_step * 1e-3),
+                   "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                     "frac": achieved / peak.value, "traffic": None,
+                     "kernel": "kPairTiles", "kernel_ms": pair_ms, "ops_per_pair": F_PAIR,
+                     "peak_source": "measured live: FMA-chain kernel on every SM (ix_measure_fp32_peak)",
+                     "three_body_ms": float(np.mean(rows[:, 2])), "ops_per_triple": F_TRIPLE},
+        "cpu_baseline": base,
+        "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": n * 3 * 8,
+                "d2h_bytes_per_step": n * 3 * 8 + 4 * 8 + 8},
+        "gpu_launches": int(launches1.value - launches0.value),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    rank, world = dist_init(args)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -156,11 +156,33 @@ int ix_get_counts(ix_ctx* ctx, long long* num_pairs, long long* num_triples);
 int ix_md_set_masses(ix_ctx* ctx, const double* masses);
 int ix_md_run(ix_ctx* ctx, int num_steps, double dt, double* positions, double* velocities, double* energy);
 
+/* The same split in two: ix_md_steps_async enqueues `num_steps` steps on the context's stream and returns at once
+ * (ix_md_run or ix_md_set_masses plus a first ix_md_run must have set the masses and velocities); ix_md_finish
+ * synchronizes, checks the neighbor lists (an overflow during the steps makes it return IX_ERR_STATE after growing
+ * them: the steps must be rerun) and copies the state out (any pointer may be NULL). */
+int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt);
+int ix_md_finish(ix_ctx* ctx, double* positions, double* velocities, double* energy);
+
+/* Kernel timing for measurement: with profiling enabled, CUDA events bracket the pair and three-body kernels of each
+ * evaluation; ix_get_kernel_times returns the durations (ms) of the last evaluation's kernels.  A measurement tool
+ * with no counterpart in the reference. */
+int ix_set_profiling(ix_ctx* ctx, int enable);
+int ix_get_kernel_times(ix_ctx* ctx, double* pair_ms, double* three_body_ms);
+
+/* Number of kernels of this library launched on the context so far (a measurement aid; no counterpart in the
+ * reference). */
+int ix_get_launch_count(ix_ctx* ctx, long long* launches);
+
 /* The CUDA stream the context launches on (as a void*), so callers can order their own work around it. */
 void* ix_get_stream(ix_ctx* ctx);
 
 /* Synchronize the context's stream and report any asynchronous error. */
 int ix_synchronize(ix_ctx* ctx);
+
+/* FP32 issue peak of CUDA device `device` in TFLOP/s (an FMA counts two operations), measured by a kernel of
+ * independent FMA chains on every SM: the roofline denominator of the pair and three-body kernels.  A measurement
+ * tool with no counterpart in the reference. */
+int ix_measure_fp32_peak(int device, double* tflops);
 
 /* Library version string. */
 const char* ix_version(void);

@@ -1,0 +1,1256 @@
+// Context and C ABI of the B200 kernels (include/interax_b200.h).
+//
+// A context holds one System's short-range forces on one GPU: the settings and parameters of the three pair forces
+// (evaluated together by the fused pair kernel) and of the three-body force, the device buffers, and the CUDA stream
+// every launch goes to.  The host logic mirrors the reference's ForceImpl/kernel classes: validation as
+// checkPairForce (openmmapi/src/InteraxPairForce.cpp:113-136) and InteraxThreeBodyForceImpl::initialize
+// (openmmapi/src/InteraxThreeBodyForceImpl.cpp:42-62), force-group gating as calcForcesAndEnergy
+// (InteraxPairForceImpl.h:84-88), parameter updates as copyParametersToContext (ReferenceInteraxKernels.cpp:98-198).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <set>
+#include <string>
+#include <vector>
+
+#include "../../include/interax_b200.h"
+#include "ix_atm.cuh"
+#include "ix_common.cuh"
+#include "ix_host_math.h"
+#include "ix_md.cuh"
+#include "ix_nblist.cuh"
+#include "ix_pair.cuh"
+#include "ix_probe.cuh"
+
+using namespace ix;
+
+namespace {
+
+thread_local std::string g_createError;
+
+const char* kTermNames[3] = {"InteraxDispersionForce", "InteraxExchangeForce", "InteraxShortRangeForce"};
+
+struct PairTerm {
+    bool present = false;
+    int group = 0;
+    std::string alchName = "lambda_sterics";
+    bool useSwitch = false;
+    double switchDistance = -1.0, softcoreRadius = 0.0;
+    std::vector<double> params;          // n x stride
+    std::vector<unsigned char> alch;
+    bool anyAlch = false;
+    int overlapMethod = 0;
+    double dampingScale = 1.0;
+    bool useLrc = false;
+    double lrcCoef = 0.0, lrcAlchCoef = 0.0;
+};
+
+struct DeviceBuffer {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+}  // namespace
+
+struct ix_ctx {
+    int n = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int numSMs = 148;
+    std::string error;
+    double defaultBox[9] = {2, 0, 0, 0, 2, 0, 0, 0, 2};
+    double box[9] = {2, 0, 0, 0, 2, 0, 0, 0, 2};
+    bool havePositions = false;
+    std::map<std::string, double> parameters;
+    bool counting = false;
+    long long lastPairs = 0, lastTriples = 0;
+
+    // pair forces
+    PairTerm term[3];
+    bool pairShared = false;             // method, cutoff and exclusions recorded
+    int method = 0;
+    double cutoff = 1.0;
+    std::vector<std::pair<int, int>> exclusions;   // normalized (min, max), sorted unique
+    bool pairDirty = true;               // parameters must be re-uploaded
+    bool pairAllocated = false;
+
+    // three-body force
+    bool atmPresent = false;
+    int atmGroup = 0;
+    std::string atmAlchName = "lambda_sterics";
+    std::vector<int> siteOffsets, siteParticles, molecule;
+    std::vector<double> siteParams;      // numSites x 3
+    std::vector<unsigned char> siteAlch;
+    bool atmAnyAlch = false;
+    double atmCutoff = 1.2, atmScale = 1.0, atmDampingScale = 1.0, atmCentroidRadius = 0.0;
+    int atmDamping = 0;
+    bool atmPeriodic = false;
+    bool atmDirty = true;
+    bool atmAllocated = false;
+    int atmCap = 0;
+
+    // device memory
+    std::map<std::string, DeviceBuffer> buffers;
+    double* dPos = nullptr;              // n x 3
+    long long* dEnergyFixed = nullptr;   // 4
+    unsigned long long* dCounts = nullptr;   // pairs, triples
+    int* dFlags = nullptr;               // pair list flags [4], atm flags [2]
+    double* dOutForces = nullptr;        // n x 3
+    double* dOutEnergy = nullptr;        // 4
+    // pair list
+    ListBuffers L{};
+    ListGeometry G{};
+    PairBuffers P{};
+    float4 *dP0o = nullptr, *dP1o = nullptr, *dP2o = nullptr;
+    int* dFlagso = nullptr;
+    float4 *dP0 = nullptr, *dP1 = nullptr, *dP2 = nullptr;
+    int* dFlagsSorted = nullptr;
+    int tileCap = 0;
+    int pairGridBlocks = 0;
+    // three-body
+    AtmBuffers A{};
+    // MD
+    double* dVel = nullptr;
+    double* dInvMass = nullptr;
+    bool haveMasses = false;
+    bool mdForcesValid = false;          // dOutForces holds all-group forces of the current positions
+    // optional CUDA-event timing of the pair and triple kernels (ix_set_profiling)
+    bool profiling = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    bool evPair = false, evAtm = false;
+    long long launches = 0;              // kernels of this library launched on the context
+};
+
+// ---------------------------------------------------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------------------------------------------------
+
+static int fail(ix_ctx* ctx, int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->error = buf;
+    else g_createError = buf;
+    return code;
+}
+
+#define IX_CUDA(ctx, call)                                                                                   \
+    do {                                                                                                     \
+        cudaError_t _e = (call);                                                                             \
+        if (_e != cudaSuccess) return fail(ctx, IX_ERR_CUDA, "%s failed: %s", #call, cudaGetErrorString(_e)); \
+    } while (0)
+
+template <class T>
+static int deviceAlloc(ix_ctx* ctx, const std::string& name, size_t count, T** out) {
+    DeviceBuffer& b = ctx->buffers[name];
+    size_t bytes = std::max<size_t>(count * sizeof(T), 16);
+    if (b.p && b.bytes >= bytes) {
+        *out = reinterpret_cast<T*>(b.p);
+        return IX_OK;
+    }
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) return fail(ctx, IX_ERR_CUDA, "cudaMalloc of %zu bytes (%s) failed: %s", bytes, name.c_str(),
+                                      cudaGetErrorString(e));
+    b.bytes = bytes;
+    *out = reinterpret_cast<T*>(b.p);
+    return IX_OK;
+}
+
+#define IX_TRY(expr)                \
+    do {                            \
+        int _rc = (expr);           \
+        if (_rc != IX_OK) return _rc; \
+    } while (0)
+
+static Box makeBox(const double* b) {
+    Box box;
+    for (int k = 0; k < 3; k++) {
+        box.a[k] = b[k];
+        box.b[k] = b[3 + k];
+        box.c[k] = b[6 + k];
+    }
+    box.inv[0] = 1.0 / b[0];
+    box.inv[1] = 1.0 / b[4];
+    box.inv[2] = 1.0 / b[8];
+    box.triclinic = (b[3] != 0 || b[6] != 0 || b[7] != 0);
+    return box;
+}
+
+static BoxF makeBoxF(const Box& b) {
+    BoxF f;
+    for (int k = 0; k < 3; k++) {
+        f.a[k] = (float)b.a[k];
+        f.b[k] = (float)b.b[k];
+        f.c[k] = (float)b.c[k];
+        f.inv[k] = (float)b.inv[k];
+    }
+    return f;
+}
+
+static double lambdaOf(const ix_ctx* ctx, const std::string& name, bool anyAlch) {
+    if (!anyAlch) return 1.0;
+    auto it = ctx->parameters.find(name);
+    return it == ctx->parameters.end() ? 1.0 : it->second;
+}
+
+static unsigned mortonCode(unsigned x, unsigned y, unsigned z) {
+    auto spread = [](unsigned v) {
+        unsigned r = 0;
+        for (int b = 0; b < 10; b++) r |= ((v >> b) & 1u) << (3 * b);
+        return r;
+    };
+    return spread(x) | (spread(y) << 1) | (spread(z) << 2);
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// pair force setup
+// ---------------------------------------------------------------------------------------------------------------------
+
+static int addPairForce(ix_ctx* ctx, int t, const ix_pair_settings* s, const double* params, const uint8_t* alch,
+                        int stride) {
+    const char* name = kTermNames[t];
+    if (!ctx) return IX_ERR_INVALID;
+    if (!s || !params || !alch) return fail(ctx, IX_ERR_INVALID, "%s: null argument", name);
+    if (ctx->term[t].present) return fail(ctx, IX_ERR_INVALID, "%s: the context already has this force", name);
+    // checkPairForce (InteraxPairForce.cpp:113-136)
+    if (s->nonbonded_method < 0 || s->nonbonded_method > 2)
+        return fail(ctx, IX_ERR_INVALID, "InteraxPairForce: Illegal value for nonbonded method");
+    for (int i = 0; i < s->num_exclusions; i++) {
+        int p1 = s->exclusions[2 * i], p2 = s->exclusions[2 * i + 1];
+        if (p1 < 0 || p1 >= ctx->n || p2 < 0 || p2 >= ctx->n)
+            return fail(ctx, IX_ERR_INVALID, "%s: Illegal particle index for an exclusion", name);
+    }
+    if (s->softcore_radius < 0)
+        return fail(ctx, IX_ERR_INVALID, "InteraxPairForce: The soft-core radius cannot be negative");
+    if (s->force_group < 0 || s->force_group > 31)
+        return fail(ctx, IX_ERR_INVALID, "%s: Force group must be between 0 and 31", name);
+    if (s->nonbonded_method != IX_NO_CUTOFF) {
+        if (s->cutoff <= 0) return fail(ctx, IX_ERR_INVALID, "%s: The cutoff distance must be positive", name);
+        if (s->use_switching_function && (s->switching_distance < 0 || s->switching_distance >= s->cutoff))
+            return fail(ctx, IX_ERR_INVALID, "%s: Switching distance must satisfy 0 <= r_switch < r_cutoff", name);
+        if (s->nonbonded_method == IX_CUTOFF_PERIODIC) {
+            const double* b = ctx->defaultBox;
+            if (s->cutoff > 0.5 * b[0] || s->cutoff > 0.5 * b[4] || s->cutoff > 0.5 * b[8])
+                return fail(ctx, IX_ERR_INVALID,
+                            "%s: The cutoff distance cannot be greater than half the periodic box size.", name);
+        }
+    }
+    // exclusions, normalized
+    std::vector<std::pair<int, int>> ex;
+    ex.reserve(s->num_exclusions);
+    for (int i = 0; i < s->num_exclusions; i++) {
+        int p1 = s->exclusions[2 * i], p2 = s->exclusions[2 * i + 1];
+        if (p1 != p2) ex.push_back({std::min(p1, p2), std::max(p1, p2)});
+    }
+    std::sort(ex.begin(), ex.end());
+    ex.erase(std::unique(ex.begin(), ex.end()), ex.end());
+    double cutoff = s->nonbonded_method == IX_NO_CUTOFF ? 0.0 : s->cutoff;
+    if (ctx->pairShared) {
+        // one fused pass over one list, as the reference's CUDA platform requires (InteraxPairForce.h:50-53)
+        if (ctx->method != s->nonbonded_method || ctx->cutoff != cutoff || ctx->exclusions != ex)
+            return fail(ctx, IX_ERR_INVALID,
+                        "%s: all Interax pair forces of a Context must have identical nonbonded methods, cutoffs and "
+                        "exclusions (they are evaluated in one pass over one neighbor list)",
+                        name);
+    }
+    else {
+        ctx->pairShared = true;
+        ctx->method = s->nonbonded_method;
+        ctx->cutoff = cutoff;
+        ctx->exclusions = std::move(ex);
+    }
+    PairTerm& T = ctx->term[t];
+    T.present = true;
+    T.group = s->force_group;
+    T.alchName = s->alchemical_parameter ? s->alchemical_parameter : "lambda_sterics";
+    T.useSwitch = s->nonbonded_method != IX_NO_CUTOFF && s->use_switching_function;
+    T.switchDistance = s->switching_distance;
+    T.softcoreRadius = s->softcore_radius;
+    T.params.assign(params, params + (size_t)ctx->n * stride);
+    T.alch.assign(alch, alch + ctx->n);
+    T.anyAlch = std::any_of(T.alch.begin(), T.alch.end(), [](unsigned char a) { return a != 0; });
+    ctx->pairDirty = true;
+    ctx->pairAllocated = false;
+    return IX_OK;
+}
+
+static void computeLrc(ix_ctx* ctx) {
+    PairTerm& T = ctx->term[0];
+    T.lrcCoef = T.lrcAlchCoef = 0.0;
+    if (!T.present || !T.useLrc || ctx->method != IX_CUTOFF_PERIODIC) return;
+    ixhost::longRangeCorrection(ctx->n, T.params.data(), T.alch.data(), ctx->cutoff, T.useSwitch, T.switchDistance,
+                                T.dampingScale, T.lrcCoef, T.lrcAlchCoef);
+}
+
+// Per-particle float parameters in original order, with the term flags.
+static int uploadPairParams(ix_ctx* ctx) {
+    const int n = ctx->n;
+    std::vector<float4> p0(n), p1(n), p2(n);
+    std::vector<int> flags(n);
+    std::vector<bool> equalWidths(n, true);
+    for (int i = 0; i < n; i++) {
+        float4 a = make_float4(0, 0, 0, 0), b = make_float4(0, 0, 0, 0), c = make_float4(0, 0, 0, 0);
+        int f = kFlagReal;
+        if (ctx->term[0].present) {
+            const double* p = &ctx->term[0].params[5 * i];
+            a = make_float4((float)p[0], (float)p[1], (float)p[2], (float)p[3]);
+            b.x = (float)p[4];
+            if (p[3] != 0) f |= kFlagGateDisp;
+            if (ctx->term[0].alch[i]) f |= 1;
+        }
+        double wx = 0, ws = 0;
+        if (ctx->term[1].present) {
+            const double* p = &ctx->term[1].params[2 * i];
+            b.y = (float)p[0];
+            wx = p[1];
+            c.x = (float)wx;
+            c.y = wx != 0 ? (float)(1.0 / wx) : 0.0f;
+            if (wx != 0) f |= kFlagGateExch;
+            if (ctx->term[1].alch[i]) f |= 2;
+        }
+        if (ctx->term[2].present) {
+            const double* p = &ctx->term[2].params[3 * i];
+            b.z = (float)p[0];
+            b.w = (float)p[1];
+            ws = p[2];
+            c.z = (float)ws;
+            c.w = ws != 0 ? (float)(1.0 / ws) : 0.0f;
+            if (ws != 0) f |= kFlagGateSr;
+            if (ctx->term[2].alch[i]) f |= 4;
+        }
+        p0[i] = a;
+        p1[i] = b;
+        p2[i] = c;
+        flags[i] = f;
+        equalWidths[i] = (wx == ws);
+    }
+    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP0o, p0.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP1o, p1.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP2o, p2.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dFlagso, flags.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    computeLrc(ctx);
+    ctx->pairDirty = false;
+    // a rebuild gathers the parameters into sorted order
+    int one = 1;
+    IX_CUDA(ctx, cudaMemcpyAsync(ctx->L.flag, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    return IX_OK;
+}
+
+__global__ void kGatherParams(ListBuffers L, const float4* p0o, const float4* p1o, const float4* p2o,
+                              const int* flagso, float4* p0, float4* p1, float4* p2, int* flags) {
+    if (!rebuildRequested(L)) return;
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= L.np) return;
+    int i = L.sortedAtom[s];
+    if (i >= 0) {
+        p0[s] = p0o[i];
+        p1[s] = p1o[i];
+        p2[s] = p2o[i];
+        flags[s] = flagso[i];
+    }
+    else {
+        p0[s] = make_float4(0, 0, 0, 0);
+        p1[s] = make_float4(0, 0, 0, 0);
+        p2[s] = make_float4(0, 0, 0, 0);
+        flags[s] = 0;
+    }
+}
+
+__global__ void kClearFlag(int* flag) { *flag = 0; }
+
+// Estimated number of tiles of the list (the build reports overflows, and the host then grows the buffers).
+static long long estimateTiles(const ix_ctx* ctx, int nb) {
+    if (ctx->method == IX_NO_CUTOFF) return (long long)nb * (nb + 1) / 2 + nb;
+    double volume;
+    if (ctx->method == IX_CUTOFF_PERIODIC) volume = ctx->box[0] * ctx->box[4] * ctx->box[8];
+    else volume = std::max(1.0, ctx->n / 100.0);   // unknown extent: assume liquid density
+    double rho = ctx->n / volume;
+    double e = std::cbrt(32.0 / rho);
+    double c = ctx->cutoff + kPairSkin;
+    double dil = e * e * e + 6 * e * e * c + 3 * M_PI * e * c * c + 4.0 / 3.0 * M_PI * c * c * c;
+    double perBlock = std::min<double>(rho * dil, ctx->n) / 32.0 / 2.0 + 2.0;
+    long long est = (long long)(1.5 * nb * perBlock) + 64;
+    long long full = (long long)nb * (nb + 1) / 2 + nb;
+    return std::min(est, full);
+}
+
+static int allocatePair(ix_ctx* ctx, long long tileCap) {
+    const int n = ctx->n;
+    const int nb = (n + 31) / 32, np = nb * 32;
+    ListBuffers& L = ctx->L;
+    L.n = n;
+    L.nb = nb;
+    L.np = np;
+    // cell grid
+    ListGeometry& G = ctx->G;
+    G.periodic = ctx->method == IX_CUTOFF_PERIODIC;
+    G.useCutoff = ctx->method != IX_NO_CUTOFF;
+    G.listCutoff = (float)(ctx->cutoff + kPairSkin);
+    int nc[3];
+    if (G.periodic) {
+        double volume = ctx->box[0] * ctx->box[4] * ctx->box[8];
+        double cell = std::cbrt(4.0 * volume / n);
+        const double len[3] = {ctx->box[0], ctx->box[4], ctx->box[8]};
+        for (int d = 0; d < 3; d++) nc[d] = std::min(1024, std::max(1, (int)(len[d] / cell)));
+    }
+    else {
+        int m = std::min(1024, std::max(1, (int)std::lround(std::cbrt(n / 4.0))));
+        nc[0] = nc[1] = nc[2] = m;
+    }
+    for (int d = 0; d < 3; d++) G.nc[d] = nc[d];
+    const int numCells = nc[0] * nc[1] * nc[2];
+    std::vector<std::pair<unsigned, int>> order(numCells);
+    for (int z = 0; z < nc[2]; z++)
+        for (int y = 0; y < nc[1]; y++)
+            for (int x = 0; x < nc[0]; x++) {
+                int c = (z * nc[1] + y) * nc[0] + x;
+                order[c] = {mortonCode(x, y, z), c};
+            }
+    std::sort(order.begin(), order.end());
+    std::vector<int> rank(numCells);
+    for (int k = 0; k < numCells; k++) rank[order[k].second] = k;
+    L.numCells = numCells;
+
+    int* cellRank;
+    IX_TRY(deviceAlloc(ctx, "cellRank", numCells, &cellRank));
+    IX_CUDA(ctx, cudaMemcpyAsync(cellRank, rank.data(), numCells * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    L.cellRank = cellRank;
+    IX_TRY(deviceAlloc(ctx, "cellKey", n, &L.cellKey));
+    IX_TRY(deviceAlloc(ctx, "cellCount", numCells, &L.cellCount));
+    IX_TRY(deviceAlloc(ctx, "cellStart", numCells + 1, &L.cellStart));
+    IX_TRY(deviceAlloc(ctx, "cellFill", numCells, &L.cellFill));
+    IX_TRY(deviceAlloc(ctx, "order", n, &L.order));
+    IX_TRY(deviceAlloc(ctx, "bboxMinMax", 8, &L.bboxMinMax));
+    IX_TRY(deviceAlloc(ctx, "refPos", 3 * (size_t)n, &L.refPos));
+    IX_TRY(deviceAlloc(ctx, "sortedAtom", np, &L.sortedAtom));
+    IX_TRY(deviceAlloc(ctx, "slotOf", n, &L.slotOf));
+    IX_TRY(deviceAlloc(ctx, "shift", 3 * (size_t)np, &L.shift));
+    IX_TRY(deviceAlloc(ctx, "spos", 3 * (size_t)np, &L.spos));
+    IX_TRY(deviceAlloc(ctx, "sposf", np, &L.sposf));
+    IX_TRY(deviceAlloc(ctx, "bbox", 2 * (size_t)nb, &L.bbox));
+    IX_TRY(deviceAlloc(ctx, "blockTiles", nb + 1, &L.blockTiles));
+    IX_TRY(deviceAlloc(ctx, "blockTasks", nb + 1, &L.blockTasks));
+    if (tileCap > (long long)1 << 28) return fail(ctx, IX_ERR_INVALID, "neighbor list too large (%lld tiles)", tileCap);
+    ctx->tileCap = (int)tileCap;
+    L.tileCap = (int)tileCap;
+    L.exclCap = (int)std::min<long long>(tileCap, 8LL * nb + 256);
+    L.taskCap = (int)(tileCap / kTaskTiles + nb + 1);
+    IX_TRY(deviceAlloc(ctx, "tileJ", 32 * (size_t)L.tileCap, &L.tileJ));
+    IX_TRY(deviceAlloc(ctx, "tileIBlock", L.tileCap, &L.tileIBlock));
+    IX_TRY(deviceAlloc(ctx, "tileExcl", L.tileCap, &L.tileExcl));
+    IX_TRY(deviceAlloc(ctx, "exclMasks", 32 * (size_t)L.exclCap, &L.exclMasks));
+    IX_TRY(deviceAlloc(ctx, "exclCounter", 1, &L.exclCounter));
+    IX_TRY(deviceAlloc(ctx, "tasks", L.taskCap, &L.tasks));
+    IX_TRY(deviceAlloc(ctx, "numTasks", 1, &L.numTasks));
+    IX_CUDA(ctx, cudaMemsetAsync(L.numTasks, 0, sizeof(int), ctx->stream));
+    L.flag = ctx->dFlags;
+    L.pos = ctx->dPos;
+    // exclusions CSR
+    std::vector<std::vector<int>> part(n);
+    for (auto& e : ctx->exclusions) {
+        part[e.first].push_back(e.second);
+        part[e.second].push_back(e.first);
+    }
+    std::vector<int> start(n + 1, 0), list;
+    std::vector<int2> range(n);
+    for (int i = 0; i < n; i++) {
+        std::sort(part[i].begin(), part[i].end());
+        start[i] = (int)list.size();
+        list.insert(list.end(), part[i].begin(), part[i].end());
+        range[i] = part[i].empty() ? make_int2(1, 0) : make_int2(part[i].front(), part[i].back());
+    }
+    start[n] = (int)list.size();
+    int *dStart, *dList;
+    int2* dRange;
+    IX_TRY(deviceAlloc(ctx, "exclStart", n + 1, &dStart));
+    IX_TRY(deviceAlloc(ctx, "exclList", std::max<size_t>(list.size(), 1), &dList));
+    IX_TRY(deviceAlloc(ctx, "exclRange", n, &dRange));
+    IX_CUDA(ctx, cudaMemcpyAsync(dStart, start.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    if (!list.empty())
+        IX_CUDA(ctx, cudaMemcpyAsync(dList, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    IX_CUDA(ctx, cudaMemcpyAsync(dRange, range.data(), n * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+    L.exclStart = dStart;
+    L.exclList = dList;
+    L.exclRange = dRange;
+    // parameters
+    IX_TRY(deviceAlloc(ctx, "p0o", n, &ctx->dP0o));
+    IX_TRY(deviceAlloc(ctx, "p1o", n, &ctx->dP1o));
+    IX_TRY(deviceAlloc(ctx, "p2o", n, &ctx->dP2o));
+    IX_TRY(deviceAlloc(ctx, "flagso", n, &ctx->dFlagso));
+    IX_TRY(deviceAlloc(ctx, "p0", np, &ctx->dP0));
+    IX_TRY(deviceAlloc(ctx, "p1", np, &ctx->dP1));
+    IX_TRY(deviceAlloc(ctx, "p2", np, &ctx->dP2));
+    IX_TRY(deviceAlloc(ctx, "flagsSorted", np, &ctx->dFlagsSorted));
+    IX_TRY(deviceAlloc(ctx, "forceFixed", 3 * (size_t)np, &ctx->P.forceFixed));
+    ctx->P.p0 = ctx->dP0;
+    ctx->P.p1 = ctx->dP1;
+    ctx->P.p2 = ctx->dP2;
+    ctx->P.flags = ctx->dFlagsSorted;
+    ctx->P.energyFixed = ctx->dEnergyFixed;
+    ctx->P.pairCount = ctx->dCounts;
+    int perSM = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kPairTiles, 32 * kPairWarps, 0);
+    ctx->pairGridBlocks = std::max(1, perSM) * ctx->numSMs;
+    ctx->pairAllocated = true;
+    IX_TRY(uploadPairParams(ctx));
+    return IX_OK;
+}
+
+static void updateGeometry(ix_ctx* ctx) {
+    ListGeometry& G = ctx->G;
+    G.box = makeBox(ctx->box);
+    G.boxf = makeBoxF(G.box);
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// three-body setup
+// ---------------------------------------------------------------------------------------------------------------------
+
+static int allocateAtm(ix_ctx* ctx) {
+    const int ns = (int)ctx->siteParams.size() / 3;
+    AtmBuffers& A = ctx->A;
+    int *dOff, *dPart, *dMol;
+    float4* dParams;
+    IX_TRY(deviceAlloc(ctx, "siteOffsets", ns + 1, &dOff));
+    IX_TRY(deviceAlloc(ctx, "siteParticles", std::max<size_t>(ctx->siteParticles.size(), 1), &dPart));
+    IX_TRY(deviceAlloc(ctx, "siteMolecule", ns, &dMol));
+    IX_TRY(deviceAlloc(ctx, "siteParams", ns, &dParams));
+    IX_CUDA(ctx, cudaMemcpyAsync(dOff, ctx->siteOffsets.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    IX_CUDA(ctx, cudaMemcpyAsync(dPart, ctx->siteParticles.data(), ctx->siteParticles.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, ctx->stream));
+    std::vector<int> mol(ns);
+    for (int i = 0; i < ns; i++) mol[i] = ctx->molecule[i] < 0 ? -1 - i : ctx->molecule[i];
+    IX_CUDA(ctx, cudaMemcpyAsync(dMol, mol.data(), ns * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    A.siteOffsets = dOff;
+    A.siteParticles = dPart;
+    A.molecule = dMol;
+    A.siteParams = dParams;
+    IX_TRY(deviceAlloc(ctx, "sitePos", 3 * (size_t)ns, &A.sitePos));
+    IX_TRY(deviceAlloc(ctx, "siteRef", 3 * (size_t)ns, &A.siteRef));
+    IX_TRY(deviceAlloc(ctx, "nbrCount", ns, &A.nbrCount));
+    IX_TRY(deviceAlloc(ctx, "siteForce", 3 * (size_t)ns, &A.siteForce));
+    IX_TRY(deviceAlloc(ctx, "atmParticleForce", 3 * (size_t)ctx->n, &A.particleForce));
+    // neighbor capacity: twice the expected half list at the site density, at least 64, at most all sites
+    if (ctx->atmCap == 0) {
+        double volume = ctx->atmPeriodic ? ctx->box[0] * ctx->box[4] * ctx->box[8] : std::max(1.0, ns / 30.0);
+        double rho = ns / volume;
+        double c = ctx->atmCutoff + kSiteSkin;
+        double expect = rho * 4.0 / 3.0 * M_PI * c * c * c / 2.0;
+        int cap = (int)std::max(64.0, 2.0 * expect + 32.0);
+        cap = std::min(((cap + 31) / 32) * 32, std::max(32, ((ns + 31) / 32) * 32));
+        ctx->atmCap = cap;
+    }
+    A.cap = ctx->atmCap;
+    IX_TRY(deviceAlloc(ctx, "nbr", (size_t)ns * A.cap, &A.nbr));
+    A.flag = ctx->dFlags + 4;
+    A.numParticles = ctx->n;
+    A.energyFixed = ctx->dEnergyFixed + 3;
+    A.tripleCount = ctx->dCounts + 1;
+    ctx->atmAllocated = true;
+    ctx->atmDirty = true;
+    return IX_OK;
+}
+
+static int uploadAtmParams(ix_ctx* ctx) {
+    const int ns = (int)ctx->siteParams.size() / 3;
+    std::vector<float4> p(ns);
+    for (int i = 0; i < ns; i++)
+        p[i] = make_float4((float)ctx->siteParams[3 * i], (float)ctx->siteParams[3 * i + 1],
+                           (float)ctx->siteParams[3 * i + 2], ctx->siteAlch[i] ? 1.0f : 0.0f);
+    IX_CUDA(ctx, cudaMemcpyAsync((void*)ctx->A.siteParams, p.data(), ns * sizeof(float4), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    int one = 1;
+    IX_CUDA(ctx, cudaMemcpyAsync(ctx->A.flag, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->atmDirty = false;
+    return IX_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// evaluation
+// ---------------------------------------------------------------------------------------------------------------------
+
+__global__ void kFinalize(int n, int np, const int* slotOf, const long long* pairForce, const long long* atmForce,
+                          const long long* energyFixed, double lrcEnergy, double* outForces, double* outEnergy,
+                          long long* addFixed, int stride) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        long long f[3] = {0, 0, 0};
+        if (pairForce) {
+            int s = slotOf[i];
+            f[0] = pairForce[s];
+            f[1] = pairForce[np + s];
+            f[2] = pairForce[2 * np + s];
+        }
+        if (atmForce) {
+            f[0] += atmForce[i];
+            f[1] += atmForce[n + i];
+            f[2] += atmForce[2 * n + i];
+        }
+        if (outForces) {
+            const double inv = 1.0 / kFixedScale;
+            outForces[3 * i] = (double)f[0] * inv;
+            outForces[3 * i + 1] = (double)f[1] * inv;
+            outForces[3 * i + 2] = (double)f[2] * inv;
+        }
+        if (addFixed) {
+            atomicAddFixed(addFixed + i, f[0]);
+            atomicAddFixed(addFixed + stride + i, f[1]);
+            atomicAddFixed(addFixed + 2 * stride + i, f[2]);
+        }
+    }
+    if (i == 0 && outEnergy) {
+        for (int t = 0; t < 4; t++) outEnergy[t] = (double)energyFixed[t] / kFixedScale;
+        outEnergy[0] += lrcEnergy;
+    }
+}
+
+// Which terms of the context are selected by a force-group mask.
+static unsigned selectedTerms(const ix_ctx* ctx, int groups) {
+    unsigned mask = 0;
+    for (int t = 0; t < 3; t++)
+        if (ctx->term[t].present && ((groups >> ctx->term[t].group) & 1)) mask |= 1u << t;
+    if (ctx->atmPresent && ((groups >> ctx->atmGroup) & 1)) mask |= 8u;
+    return mask;
+}
+
+static PairTermConfig pairConfig(const ix_ctx* ctx, unsigned terms) {
+    PairTermConfig C{};
+    C.termMask = (int)(terms & 7u);
+    for (int t = 0; t < 3; t++) {
+        const PairTerm& T = ctx->term[t];
+        double lam = lambdaOf(ctx, T.alchName, T.anyAlch);
+        C.lambda[t] = (float)lam;
+        C.softShift[t] = (T.anyAlch && T.softcoreRadius > 0) ? (float)((1.0 - lam) * std::pow(T.softcoreRadius, 6.0)) : 0.0f;
+        C.useSwitch[t] = T.useSwitch;
+        C.switchDist[t] = (float)T.switchDistance;
+        C.invSwitchWidth[t] = T.useSwitch ? (float)(1.0 / (ctx->cutoff - T.switchDistance)) : 0.0f;
+        C.overlapMethod[t] = T.overlapMethod;
+    }
+    C.twoBeta = (float)(2.0 * ctx->term[0].dampingScale);
+    // the exchange and short-range terms share one overlap when their widths and methods agree for every particle
+    C.shareOverlap = 0;
+    if (ctx->term[1].present && ctx->term[2].present && ctx->term[1].overlapMethod == ctx->term[2].overlapMethod) {
+        bool same = true;
+        for (int i = 0; i < ctx->n && same; i++) same = ctx->term[1].params[2 * i + 1] == ctx->term[2].params[3 * i + 2];
+        C.shareOverlap = same;
+    }
+    C.useCutoff = ctx->method != IX_NO_CUTOFF;
+    C.periodic = ctx->method == IX_CUTOFF_PERIODIC;
+    C.cutoff = ctx->cutoff;
+    C.cutoff2 = (float)(ctx->cutoff * ctx->cutoff);
+    double tc = ctx->cutoff * (1.0 + 1e-5) + 1e-5;
+    C.testCutoff2 = (float)(tc * tc);
+    C.box = ctx->G.box;
+    C.boxf = ctx->G.boxf;
+    return C;
+}
+
+// Launch the whole evaluation on the context's stream.  Forces go to outForces (device, n x 3 doubles) and/or are
+// added to addFixed; energies to outEnergy (device, 4 doubles).
+static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, double* outEnergy, long long* addFixed,
+                            int stride) {
+    const int n = ctx->n;
+    cudaStream_t st = ctx->stream;
+    const bool doPair = (terms & 7u) != 0;
+    const bool doAtm = (terms & 8u) != 0;
+    updateGeometry(ctx);
+    IX_CUDA(ctx, cudaMemsetAsync(ctx->dEnergyFixed, 0, 4 * sizeof(long long), st));
+    IX_CUDA(ctx, cudaMemsetAsync(ctx->dCounts, 0, 2 * sizeof(unsigned long long), st));
+    double lrcEnergy = 0.0;
+    if (doPair) {
+        if (ctx->pairDirty) IX_TRY(uploadPairParams(ctx));
+        ListBuffers& L = ctx->L;
+        const int tpb = 256;
+        const int gN = (n + tpb - 1) / tpb, gNp = (L.np + tpb - 1) / tpb;
+        const int gCells = (L.numCells + tpb - 1) / tpb;
+        kCheckDisplacement<<<gN, tpb, 0, st>>>(L, 0.25f * kPairSkin * kPairSkin);
+        kResetCells<<<std::max(1, std::min(gCells, 1024)), tpb, 0, st>>>(L);
+        if (!ctx->G.periodic) kParticleBounds<<<gN, tpb, 0, st>>>(L);
+        kCellKeys<<<gN, tpb, 0, st>>>(L, ctx->G);
+        kScanCells<<<1, 1024, 0, st>>>(L);
+        kScatterCells<<<gN, tpb, 0, st>>>(L);
+        kSortWithinCells<<<gCells, tpb, 0, st>>>(L);
+        kSortedAtoms<<<gNp, tpb, 0, st>>>(L, ctx->G);
+        kGatherParams<<<gNp, tpb, 0, st>>>(L, ctx->dP0o, ctx->dP1o, ctx->dP2o, ctx->dFlagso, ctx->dP0, ctx->dP1,
+                                           ctx->dP2, ctx->dFlagsSorted);
+        kUpdateSortedPositions<<<gNp, tpb, 0, st>>>(L);
+        kBlockBounds<<<(L.nb * 32 + tpb - 1) / tpb, tpb, 0, st>>>(L);
+        const int warpsPerBlock = 8;
+        const int gB = (L.nb + warpsPerBlock - 1) / warpsPerBlock;
+        kBuildTiles<0><<<gB, 32 * warpsPerBlock, 0, st>>>(L, ctx->G);
+        kScanBlocks<<<1, 1024, 0, st>>>(L);
+        kBuildTiles<1><<<gB, 32 * warpsPerBlock, 0, st>>>(L, ctx->G);
+        kClearFlag<<<1, 1, 0, st>>>(L.flag);
+        IX_CUDA(ctx, cudaMemsetAsync(ctx->P.forceFixed, 0, 3 * (size_t)L.np * sizeof(long long), st));
+        PairTermConfig C = pairConfig(ctx, terms);
+        if (ctx->profiling) cudaEventRecord(ctx->ev[0], st);
+        kPairTiles<<<ctx->pairGridBlocks, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        ctx->launches += ctx->G.periodic ? 15 : 16;
+        if (ctx->profiling) cudaEventRecord(ctx->ev[1], st);
+        ctx->evPair = ctx->profiling;
+        IX_CUDA(ctx, cudaGetLastError());
+        const PairTerm& D = ctx->term[0];
+        if ((terms & 1u) && (D.lrcCoef != 0 || D.lrcAlchCoef != 0)) {
+            double lam = lambdaOf(ctx, D.alchName, D.anyAlch);
+            lrcEnergy = (D.lrcCoef + lam * D.lrcAlchCoef) / (ctx->box[0] * ctx->box[4] * ctx->box[8]);
+        }
+    }
+    if (doAtm) {
+        if (ctx->atmDirty) IX_TRY(uploadAtmParams(ctx));
+        AtmBuffers& A = ctx->A;
+        AtmConfig C{};
+        C.numSites = (int)ctx->siteParams.size() / 3;
+        C.periodic = ctx->atmPeriodic;
+        C.box = makeBox(ctx->box);
+        C.boxf = makeBoxF(C.box);
+        C.cutoff2 = (float)(ctx->atmCutoff * ctx->atmCutoff);
+        double lc = ctx->atmCutoff + kSiteSkin;
+        C.listCutoff2 = (float)(lc * lc);
+        C.scale = (float)ctx->atmScale;
+        C.lambda = (float)lambdaOf(ctx, ctx->atmAlchName, ctx->atmAnyAlch);
+        C.useTangToennies = ctx->atmDamping == IX_TANG_TOENNIES;
+        C.twoBeta = (float)(2.0 * ctx->atmDampingScale);
+        C.invCentroidRadius = ctx->atmCentroidRadius > 0 ? (float)(1.0 / ctx->atmCentroidRadius) : 0.0f;
+        C.maxMove2 = 0.25f * kSiteSkin * kSiteSkin;
+        const int tpb = 256;
+        const int gS = (C.numSites + tpb - 1) / tpb;
+        IX_CUDA(ctx, cudaMemsetAsync(A.siteForce, 0, 3 * (size_t)C.numSites * sizeof(long long), st));
+        IX_CUDA(ctx, cudaMemsetAsync(A.particleForce, 0, 3 * (size_t)n * sizeof(long long), st));
+        kSiteCentroids<<<gS, tpb, 0, st>>>(A, C, ctx->dPos);
+        kSiteNeighbors<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, st>>>(A, C);
+        kClearFlag<<<1, 1, 0, st>>>(A.flag);
+        const size_t smem = sizeof(AtmWarpStorage) * kAtmWarps;
+        int blocks = std::min((C.numSites + kAtmWarps - 1) / kAtmWarps, ctx->numSMs * 8);
+        if (ctx->profiling) cudaEventRecord(ctx->ev[2], st);
+        kTriples<<<std::max(1, blocks), 32 * kAtmWarps, smem, st>>>(A, C);
+        if (ctx->profiling) cudaEventRecord(ctx->ev[3], st);
+        ctx->evAtm = ctx->profiling;
+        kSpreadSiteForces<<<gS, tpb, 0, st>>>(A, C);
+        ctx->launches += 5;
+        IX_CUDA(ctx, cudaGetLastError());
+    }
+    kFinalize<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->L.np, ctx->L.slotOf, doPair ? ctx->P.forceFixed : nullptr,
+                                              doAtm ? ctx->A.particleForce : nullptr, ctx->dEnergyFixed, lrcEnergy,
+                                              outForces, outEnergy, addFixed, stride);
+    ctx->launches += 1;
+    IX_CUDA(ctx, cudaGetLastError());
+    return IX_OK;
+}
+
+// Make sure buffers exist for the selected terms.
+static int prepare(ix_ctx* ctx, unsigned terms) {
+    if (!ctx->havePositions) return fail(ctx, IX_ERR_STATE, "positions have not been set");
+    if ((terms & 7u) && !ctx->pairAllocated) {
+        updateGeometry(ctx);
+        const int nb = (ctx->n + 31) / 32;
+        IX_TRY(allocatePair(ctx, estimateTiles(ctx, nb)));
+    }
+    if ((terms & 8u) && !ctx->atmAllocated) IX_TRY(allocateAtm(ctx));
+    return IX_OK;
+}
+
+// After a synchronized evaluation: grow the lists that overflowed.  Returns true if the evaluation must be redone.
+static int checkOverflow(ix_ctx* ctx, unsigned terms, bool& redo) {
+    redo = false;
+    int flags[6];
+    IX_CUDA(ctx, cudaMemcpy(flags, ctx->dFlags, sizeof(flags), cudaMemcpyDeviceToHost));
+    if ((terms & 7u) && (flags[1] || flags[2] || flags[3])) {
+        long long tiles = 0;
+        int cnt = 0;
+        IX_CUDA(ctx, cudaMemcpy(&cnt, ctx->L.blockTiles + ctx->L.nb, sizeof(int), cudaMemcpyDeviceToHost));
+        tiles = std::max<long long>(2LL * ctx->tileCap, (long long)(1.3 * cnt) + 64);
+        int zero[4] = {1, 0, 0, 0};
+        IX_CUDA(ctx, cudaMemcpy(ctx->dFlags, zero, sizeof(zero), cudaMemcpyHostToDevice));
+        ctx->pairAllocated = false;
+        IX_TRY(allocatePair(ctx, tiles));
+        if (flags[2]) ctx->L.exclCap = std::min(ctx->L.tileCap, 4 * ctx->L.exclCap);
+        IX_TRY(deviceAlloc(ctx, "exclMasks", 32 * (size_t)ctx->L.exclCap, &ctx->L.exclMasks));
+        redo = true;
+    }
+    if ((terms & 8u) && flags[5]) {
+        ctx->atmCap = std::min(2 * ctx->atmCap, (((int)ctx->siteParams.size() / 3 + 31) / 32) * 32 + 32);
+        if (flags[5] & 2) ctx->atmCap = std::max(ctx->atmCap, 256);
+        int f[2] = {1, 0};
+        IX_CUDA(ctx, cudaMemcpy(ctx->dFlags + 4, f, sizeof(f), cudaMemcpyHostToDevice));
+        IX_TRY(allocateAtm(ctx));
+        IX_TRY(uploadAtmParams(ctx));
+        if (flags[5] & 2) return fail(ctx, IX_ERR_INVALID,
+                                      "InteraxThreeBodyForce: more than 256 sites within the cutoff of one site");
+        redo = true;
+    }
+    return IX_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------------------------------------------------
+
+extern "C" {
+
+const char* ix_version(void) { return "interax-b200 0.1 (sm_100a)"; }
+
+int ix_measure_fp32_peak(int device, double* tflops) {
+    if (!tflops) return fail(nullptr, IX_ERR_INVALID, "ix_measure_fp32_peak: tflops is NULL");
+    cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(nullptr, IX_ERR_NO_DEVICE, "cudaSetDevice(%d) failed: %s", device, cudaGetErrorString(e));
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    int perSM = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kFmaPeak, 256, 0);
+    const int blocks = prop.multiProcessorCount * std::max(1, perSM) * 4;
+    float* sink = nullptr;
+    if (cudaMalloc(&sink, 256 * sizeof(float)) != cudaSuccess) return fail(nullptr, IX_ERR_CUDA, "cudaMalloc failed");
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    double best = 0.0;
+    for (int rep = 0; rep < 5; rep++) {
+        cudaEventRecord(a);
+        kFmaPeak<<<blocks, 256>>>(sink, 1.0f + rep);
+        cudaEventRecord(b);
+        cudaEventSynchronize(b);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, a, b);
+        double flops = 2.0 * (double)blocks * 256 * kProbeIters * kProbeChains;
+        if (rep > 0) best = std::max(best, flops / (ms * 1e-3) / 1e12);
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(nullptr, IX_ERR_CUDA, "FMA probe failed: %s", cudaGetErrorString(e));
+    *tflops = best;
+    return IX_OK;
+}
+
+int ix_ctx_create(int num_particles, int device, const double* default_box, ix_ctx** out) {
+    if (!out) return fail(nullptr, IX_ERR_INVALID, "ix_ctx_create: out is NULL");
+    *out = nullptr;
+    if (num_particles <= 0) return fail(nullptr, IX_ERR_INVALID, "ix_ctx_create: the System has no particles");
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+        return fail(nullptr, IX_ERR_NO_DEVICE, "no CUDA device available (%s)", cudaGetErrorString(e));
+    if (device < 0 || device >= count)
+        return fail(nullptr, IX_ERR_NO_DEVICE, "CUDA device %d does not exist (%d devices)", device, count);
+    e = cudaSetDevice(device);
+    if (e != cudaSuccess) return fail(nullptr, IX_ERR_CUDA, "cudaSetDevice(%d) failed: %s", device, cudaGetErrorString(e));
+    cudaDeviceProp prop;
+    cudaGetDeviceProperties(&prop, device);
+    if (prop.major < 10)
+        return fail(nullptr, IX_ERR_NO_DEVICE, "device %d (%s, sm_%d%d) is not a Blackwell (sm_100) GPU", device,
+                    prop.name, prop.major, prop.minor);
+    ix_ctx* ctx = new ix_ctx();
+    ctx->n = num_particles;
+    ctx->device = device;
+    ctx->numSMs = prop.multiProcessorCount;
+    if (default_box) {
+        std::memcpy(ctx->defaultBox, default_box, sizeof(ctx->defaultBox));
+        std::memcpy(ctx->box, default_box, sizeof(ctx->box));
+    }
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return fail(nullptr, IX_ERR_CUDA, "cudaStreamCreate failed");
+    }
+    int rc = IX_OK;
+    if ((rc = deviceAlloc(ctx, "pos", 3 * (size_t)num_particles, &ctx->dPos)) != IX_OK ||
+        (rc = deviceAlloc(ctx, "energyFixed", 4, &ctx->dEnergyFixed)) != IX_OK ||
+        (rc = deviceAlloc(ctx, "counts", 2, &ctx->dCounts)) != IX_OK ||
+        (rc = deviceAlloc(ctx, "flags", 8, &ctx->dFlags)) != IX_OK ||
+        (rc = deviceAlloc(ctx, "outForces", 3 * (size_t)num_particles, &ctx->dOutForces)) != IX_OK ||
+        (rc = deviceAlloc(ctx, "outEnergy", 4, &ctx->dOutEnergy)) != IX_OK) {
+        g_createError = ctx->error;
+        ix_ctx_destroy(ctx);
+        return rc;
+    }
+    int init[8] = {1, 0, 0, 0, 1, 0, 0, 0};
+    cudaMemcpy(ctx->dFlags, init, sizeof(init), cudaMemcpyHostToDevice);
+    *out = ctx;
+    return IX_OK;
+}
+
+void ix_ctx_destroy(ix_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    for (auto& kv : ctx->buffers)
+        if (kv.second.p) cudaFree(kv.second.p);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+const char* ix_last_error(const ix_ctx* ctx) { return ctx ? ctx->error.c_str() : g_createError.c_str(); }
+
+int ix_add_dispersion(ix_ctx* ctx, const ix_pair_settings* settings, const double* params, const uint8_t* alch,
+                      double damping_scale, int use_lrc) {
+    IX_TRY(addPairForce(ctx, 0, settings, params, alch, 5));
+    ctx->term[0].dampingScale = damping_scale;
+    ctx->term[0].useLrc = use_lrc != 0;
+    return IX_OK;
+}
+
+int ix_add_exchange(ix_ctx* ctx, const ix_pair_settings* settings, const double* params, const uint8_t* alch,
+                    int overlap_method) {
+    if (ctx && overlap_method != 0 && overlap_method != 2)
+        return fail(ctx, IX_ERR_INVALID, "InteraxExchangeForce: Illegal value for overlap method");
+    IX_TRY(addPairForce(ctx, 1, settings, params, alch, 2));
+    ctx->term[1].overlapMethod = overlap_method;
+    return IX_OK;
+}
+
+int ix_add_short_range(ix_ctx* ctx, const ix_pair_settings* settings, const double* params, const uint8_t* alch,
+                       int overlap_method) {
+    if (ctx && overlap_method != 0 && overlap_method != 2)
+        return fail(ctx, IX_ERR_INVALID, "InteraxShortRangeForce: Illegal value for overlap method");
+    IX_TRY(addPairForce(ctx, 2, settings, params, alch, 3));
+    ctx->term[2].overlapMethod = overlap_method;
+    return IX_OK;
+}
+
+int ix_add_three_body(ix_ctx* ctx, int num_sites, const int32_t* site_offsets, const int32_t* site_particles,
+                      const double* site_params, const int32_t* molecule, const uint8_t* alch, double cutoff,
+                      double scale_factor, int damping_method, double damping_scale, double centroid_radius,
+                      int periodic, const char* alch_name, int force_group) {
+    if (!ctx) return IX_ERR_INVALID;
+    if (ctx->atmPresent) return fail(ctx, IX_ERR_INVALID, "InteraxThreeBodyForce: the context already has this force");
+    if (num_sites < 0 || (num_sites > 0 && (!site_offsets || !site_particles || !site_params || !molecule || !alch)))
+        return fail(ctx, IX_ERR_INVALID, "InteraxThreeBodyForce: null argument");
+    if (damping_method != IX_NO_DAMPING && damping_method != IX_TANG_TOENNIES)
+        return fail(ctx, IX_ERR_INVALID, "InteraxThreeBodyForce: Illegal value for damping method");
+    if (centroid_radius < 0)
+        return fail(ctx, IX_ERR_INVALID, "InteraxThreeBodyForce: The centroid damping radius cannot be negative");
+    // InteraxThreeBodyForceImpl::initialize (InteraxThreeBodyForceImpl.cpp:42-59)
+    for (int s = 0; s < num_sites; s++) {
+        if (site_offsets[s + 1] <= site_offsets[s])
+            return fail(ctx, IX_ERR_INVALID, "InteraxThreeBodyForce: A site must contain at least one particle");
+        for (int k = site_offsets[s]; k < site_offsets[s + 1]; k++)
+            if (site_particles[k] < 0 || site_particles[k] >= ctx->n)
+                return fail(ctx, IX_ERR_INVALID, "InteraxThreeBodyForce: Illegal particle index for a site");
+        if (damping_method == IX_TANG_TOENNIES && site_params[3 * s + 2] <= 0)
+            return fail(ctx, IX_ERR_INVALID,
+                        "InteraxThreeBodyForce: The Tang-Toennies damping requires a positive width for every site");
+    }
+    if (cutoff <= 0) return fail(ctx, IX_ERR_INVALID, "InteraxThreeBodyForce: The cutoff distance must be positive");
+    if (force_group < 0 || force_group > 31)
+        return fail(ctx, IX_ERR_INVALID, "InteraxThreeBodyForce: Force group must be between 0 and 31");
+    ctx->atmPresent = num_sites > 0;
+    ctx->atmGroup = force_group;
+    ctx->atmAlchName = alch_name ? alch_name : "lambda_sterics";
+    ctx->siteOffsets.assign(site_offsets, site_offsets + num_sites + 1);
+    ctx->siteParticles.assign(site_particles, site_particles + site_offsets[num_sites]);
+    ctx->siteParams.assign(site_params, site_params + 3 * (size_t)num_sites);
+    ctx->molecule.assign(molecule, molecule + num_sites);
+    ctx->siteAlch.assign(alch, alch + num_sites);
+    ctx->atmAnyAlch = std::any_of(ctx->siteAlch.begin(), ctx->siteAlch.end(), [](unsigned char a) { return a != 0; });
+    ctx->atmCutoff = cutoff;
+    ctx->atmScale = scale_factor;
+    ctx->atmDamping = damping_method;
+    ctx->atmDampingScale = damping_scale;
+    ctx->atmCentroidRadius = centroid_radius;
+    ctx->atmPeriodic = periodic != 0;
+    ctx->atmAllocated = false;
+    ctx->atmDirty = true;
+    return IX_OK;
+}
+
+static int updatePair(ix_ctx* ctx, int t, const double* params, int stride) {
+    if (!ctx) return IX_ERR_INVALID;
+    ctx->mdForcesValid = false;
+    if (!ctx->term[t].present) return fail(ctx, IX_ERR_STATE, "%s: the context has no such force", kTermNames[t]);
+    if (!params) return fail(ctx, IX_ERR_INVALID, "%s: null argument", kTermNames[t]);
+    ctx->term[t].params.assign(params, params + (size_t)ctx->n * stride);
+    ctx->pairDirty = true;
+    return IX_OK;
+}
+
+int ix_update_dispersion(ix_ctx* ctx, const double* params, double damping_scale) {
+    IX_TRY(updatePair(ctx, 0, params, 5));
+    ctx->term[0].dampingScale = damping_scale;
+    return IX_OK;
+}
+
+int ix_update_exchange(ix_ctx* ctx, const double* params, int overlap_method) {
+    if (ctx && ctx->term[1].present && overlap_method != ctx->term[1].overlapMethod)
+        return fail(ctx, IX_ERR_INVALID, "updateParametersInContext: The overlap method has changed");
+    return updatePair(ctx, 1, params, 2);
+}
+
+int ix_update_short_range(ix_ctx* ctx, const double* params, int overlap_method) {
+    if (ctx && ctx->term[2].present && overlap_method != ctx->term[2].overlapMethod)
+        return fail(ctx, IX_ERR_INVALID, "updateParametersInContext: The overlap method has changed");
+    return updatePair(ctx, 2, params, 3);
+}
+
+int ix_update_three_body(ix_ctx* ctx, const double* site_params, double scale_factor, double damping_scale,
+                         double centroid_radius) {
+    if (!ctx) return IX_ERR_INVALID;
+    ctx->mdForcesValid = false;
+    if (!ctx->atmPresent) return fail(ctx, IX_ERR_STATE, "InteraxThreeBodyForce: the context has no such force");
+    // the centroid damping cannot be switched on or off (CommonInteraxKernels.cpp:621-623)
+    if ((centroid_radius > 0) != (ctx->atmCentroidRadius > 0))
+        return fail(ctx, IX_ERR_INVALID,
+                    "updateParametersInContext: The centroid damping cannot be switched on or off");
+    if (centroid_radius < 0)
+        return fail(ctx, IX_ERR_INVALID, "InteraxThreeBodyForce: The centroid damping radius cannot be negative");
+    const int ns = (int)ctx->siteParams.size() / 3;
+    if (ctx->atmDamping == IX_TANG_TOENNIES)
+        for (int s = 0; s < ns; s++)
+            if (site_params[3 * s + 2] <= 0)
+                return fail(ctx, IX_ERR_INVALID,
+                            "InteraxThreeBodyForce: The Tang-Toennies damping requires a positive width for every site");
+    ctx->siteParams.assign(site_params, site_params + 3 * (size_t)ns);
+    ctx->atmScale = scale_factor;
+    ctx->atmDampingScale = damping_scale;
+    ctx->atmCentroidRadius = centroid_radius;
+    ctx->atmDirty = true;
+    return IX_OK;
+}
+
+int ix_set_parameter(ix_ctx* ctx, const char* name, double value) {
+    if (!ctx || !name) return IX_ERR_INVALID;
+    ctx->mdForcesValid = false;
+    ctx->parameters[name] = value;
+    return IX_OK;
+}
+
+int ix_set_positions(ix_ctx* ctx, const double* positions, const double* box) {
+    if (!ctx) return IX_ERR_INVALID;
+    ctx->mdForcesValid = false;
+    if (!positions) return fail(ctx, IX_ERR_INVALID, "ix_set_positions: positions is NULL");
+    for (size_t i = 0; i < 3 * (size_t)ctx->n; i++)
+        if (!std::isfinite(positions[i]))
+            return fail(ctx, IX_ERR_INVALID, "Particle coordinate is NaN or infinite (particle %zu)", i / 3);
+    if (box) {
+        if (box[0] <= 0 || box[4] <= 0 || box[8] <= 0)
+            return fail(ctx, IX_ERR_INVALID, "Illegal periodic box vectors");
+        std::memcpy(ctx->box, box, sizeof(ctx->box));
+    }
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dPos, positions, 3 * (size_t)ctx->n * sizeof(double), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    ctx->havePositions = true;
+    return IX_OK;
+}
+
+int ix_compute(ix_ctx* ctx, int groups, int include_forces, int include_energy, double* term_energies,
+               double* energy, double* forces) {
+    if (!ctx) return IX_ERR_INVALID;
+    ctx->mdForcesValid = false;
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    unsigned terms = selectedTerms(ctx, groups);
+    if (terms) IX_TRY(prepare(ctx, terms));
+    double e[4] = {0, 0, 0, 0};
+    for (int attempt = 0; attempt < 4; attempt++) {
+        if (terms) IX_TRY(launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0));
+        IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        bool redo = false;
+        if (terms) IX_TRY(checkOverflow(ctx, terms, redo));
+        if (!redo) break;
+    }
+    if (terms) {
+        IX_CUDA(ctx, cudaMemcpy(e, ctx->dOutEnergy, sizeof(e), cudaMemcpyDeviceToHost));
+        unsigned long long c[2];
+        IX_CUDA(ctx, cudaMemcpy(c, ctx->dCounts, sizeof(c), cudaMemcpyDeviceToHost));
+        ctx->lastPairs = (terms & 7u) ? (long long)c[0] : 0;
+        ctx->lastTriples = (terms & 8u) ? (long long)c[1] : 0;
+    }
+    for (int t = 0; t < 4; t++)
+        if (!((terms >> t) & 1u)) e[t] = 0.0;
+    if (term_energies) std::memcpy(term_energies, e, sizeof(e));
+    if (energy) *energy = e[0] + e[1] + e[2] + e[3];
+    if (forces) {
+        if (terms && include_forces)
+            IX_CUDA(ctx, cudaMemcpy(forces, ctx->dOutForces, 3 * (size_t)ctx->n * sizeof(double), cudaMemcpyDeviceToHost));
+        else std::memset(forces, 0, 3 * (size_t)ctx->n * sizeof(double));
+    }
+    (void)include_energy;
+    return IX_OK;
+}
+
+int ix_compute_device(ix_ctx* ctx, int groups, long long* d_force_fixed, int force_stride, double* d_term_energies) {
+    if (!ctx) return IX_ERR_INVALID;
+    if (force_stride < ctx->n) return fail(ctx, IX_ERR_INVALID, "ix_compute_device: stride smaller than the particle count");
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    unsigned terms = selectedTerms(ctx, groups);
+    if (!terms) return IX_OK;
+    IX_TRY(prepare(ctx, terms));
+    return launchEvaluation(ctx, terms, nullptr, d_term_energies, d_force_fixed, force_stride);
+}
+
+int ix_compute_device_f64(ix_ctx* ctx, int groups, const double* d_positions, const double* box, double* d_forces,
+                          double* d_term_energies) {
+    if (!ctx) return IX_ERR_INVALID;
+    ctx->mdForcesValid = false;
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (box) std::memcpy(ctx->box, box, sizeof(ctx->box));
+    if (d_positions) {
+        IX_CUDA(ctx, cudaMemcpyAsync(ctx->dPos, d_positions, 3 * (size_t)ctx->n * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, ctx->stream));
+        ctx->havePositions = true;
+    }
+    unsigned terms = selectedTerms(ctx, groups);
+    if (!terms) {
+        if (d_forces) IX_CUDA(ctx, cudaMemsetAsync(d_forces, 0, 3 * (size_t)ctx->n * sizeof(double), ctx->stream));
+        if (d_term_energies) IX_CUDA(ctx, cudaMemsetAsync(d_term_energies, 0, 4 * sizeof(double), ctx->stream));
+        return IX_OK;
+    }
+    IX_TRY(prepare(ctx, terms));
+    return launchEvaluation(ctx, terms, d_forces, d_term_energies, nullptr, 0);
+}
+
+int ix_set_counting(ix_ctx* ctx, int enable) {
+    if (!ctx) return IX_ERR_INVALID;
+    ctx->counting = enable != 0;
+    return IX_OK;
+}
+
+int ix_get_counts(ix_ctx* ctx, long long* num_pairs, long long* num_triples) {
+    if (!ctx) return IX_ERR_INVALID;
+    if (num_pairs) *num_pairs = ctx->lastPairs;
+    if (num_triples) *num_triples = ctx->lastTriples;
+    return IX_OK;
+}
+
+void* ix_get_stream(ix_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+
+int ix_synchronize(ix_ctx* ctx) {
+    if (!ctx) return IX_ERR_INVALID;
+    IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    IX_CUDA(ctx, cudaGetLastError());
+    return IX_OK;
+}
+
+int ix_md_set_masses(ix_ctx* ctx, const double* masses) {
+    if (!ctx || !masses) return IX_ERR_INVALID;
+    std::vector<double> inv(ctx->n);
+    for (int i = 0; i < ctx->n; i++) {
+        if (!(masses[i] >= 0)) return fail(ctx, IX_ERR_INVALID, "Illegal mass for particle %d", i);
+        inv[i] = masses[i] > 0 ? 1.0 / masses[i] : 0.0;
+    }
+    IX_TRY(deviceAlloc(ctx, "invMass", ctx->n, &ctx->dInvMass));
+    IX_TRY(deviceAlloc(ctx, "vel", 3 * (size_t)ctx->n, &ctx->dVel));
+    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dInvMass, inv.data(), ctx->n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    ctx->haveMasses = true;
+    return IX_OK;
+}
+
+int ix_set_profiling(ix_ctx* ctx, int enable) {
+    if (!ctx) return IX_ERR_INVALID;
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (enable && !ctx->ev[0])
+        for (auto& e : ctx->ev) IX_CUDA(ctx, cudaEventCreate(&e));
+    ctx->profiling = enable != 0;
+    ctx->evPair = ctx->evAtm = false;
+    return IX_OK;
+}
+
+int ix_get_kernel_times(ix_ctx* ctx, double* pair_ms, double* three_body_ms) {
+    if (!ctx) return IX_ERR_INVALID;
+    float ms = 0.0f;
+    if (pair_ms) {
+        *pair_ms = 0.0;
+        if (ctx->evPair) {
+            IX_CUDA(ctx, cudaEventSynchronize(ctx->ev[1]));
+            IX_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]));
+            *pair_ms = ms;
+        }
+    }
+    if (three_body_ms) {
+        *three_body_ms = 0.0;
+        if (ctx->evAtm) {
+            IX_CUDA(ctx, cudaEventSynchronize(ctx->ev[3]));
+            IX_CUDA(ctx, cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]));
+            *three_body_ms = ms;
+        }
+    }
+    return IX_OK;
+}
+
+// Enqueue velocity-Verlet steps without synchronizing (masses and velocities must have been set by ix_md_run or
+// ix_md_set_state).
+int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt) {
+    if (!ctx) return IX_ERR_INVALID;
+    if (!ctx->haveMasses) return fail(ctx, IX_ERR_STATE, "ix_md_steps_async: masses have not been set");
+    if (!ctx->havePositions) return fail(ctx, IX_ERR_STATE, "positions have not been set");
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    unsigned terms = selectedTerms(ctx, -1);
+    if (terms) IX_TRY(prepare(ctx, terms));
+    const int n = ctx->n;
+    const int g = (n + 255) / 256;
+    if (!ctx->mdForcesValid) {
+        if (terms) IX_TRY(launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0));
+        else IX_CUDA(ctx, cudaMemsetAsync(ctx->dOutForces, 0, 3 * (size_t)n * sizeof(double), ctx->stream));
+        ctx->mdForcesValid = true;
+    }
+    for (int step = 0; step < num_steps; step++) {
+        kVerletFirstHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos);
+        if (terms) IX_TRY(launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0));
+        kVerletSecondHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel);
+        ctx->launches += 2;
+    }
+    IX_CUDA(ctx, cudaGetLastError());
+    return IX_OK;
+}
+
+int ix_get_launch_count(ix_ctx* ctx, long long* launches) {
+    if (!ctx || !launches) return IX_ERR_INVALID;
+    *launches = ctx->launches;
+    return IX_OK;
+}
+
+// Finish enqueued MD steps: synchronize, check the neighbor lists (an overflow during the steps invalidates them:
+// the lists are grown and IX_ERR_STATE is returned), record the counts of the last evaluation, copy the state out.
+int ix_md_finish(ix_ctx* ctx, double* positions, double* velocities, double* energy) {
+    if (!ctx) return IX_ERR_INVALID;
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    unsigned terms = selectedTerms(ctx, -1);
+    bool redo = false;
+    if (terms) IX_TRY(checkOverflow(ctx, terms, redo));
+    if (redo) {
+        ctx->mdForcesValid = false;
+        return fail(ctx, IX_ERR_STATE, "neighbor list overflow during MD; the lists were grown, rerun the steps");
+    }
+    unsigned long long c[2] = {0, 0};
+    IX_CUDA(ctx, cudaMemcpy(c, ctx->dCounts, sizeof(c), cudaMemcpyDeviceToHost));
+    ctx->lastPairs = (terms & 7u) ? (long long)c[0] : 0;
+    ctx->lastTriples = (terms & 8u) ? (long long)c[1] : 0;
+    const int n = ctx->n;
+    if (positions)
+        IX_CUDA(ctx, cudaMemcpy(positions, ctx->dPos, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (velocities)
+        IX_CUDA(ctx, cudaMemcpy(velocities, ctx->dVel, 3 * (size_t)n * sizeof(double), cudaMemcpyDeviceToHost));
+    if (energy) {
+        double e[4] = {0, 0, 0, 0};
+        if (terms) IX_CUDA(ctx, cudaMemcpy(e, ctx->dOutEnergy, sizeof(e), cudaMemcpyDeviceToHost));
+        *energy = e[0] + e[1] + e[2] + e[3];
+    }
+    return IX_OK;
+}
+
+int ix_md_run(ix_ctx* ctx, int num_steps, double dt, double* positions, double* velocities, double* energy) {
+    if (!ctx) return IX_ERR_INVALID;
+    if (!ctx->haveMasses) return fail(ctx, IX_ERR_STATE, "ix_md_run: masses have not been set");
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (velocities)
+        IX_CUDA(ctx, cudaMemcpyAsync(ctx->dVel, velocities, 3 * (size_t)ctx->n * sizeof(double), cudaMemcpyHostToDevice,
+                                     ctx->stream));
+    IX_TRY(ix_md_steps_async(ctx, num_steps, dt));
+    return ix_md_finish(ctx, positions, velocities, energy);
+}
+
+}  // extern "C"

@@ -1,0 +1,163 @@
+// Pair energies of the InteraxFF dispersion, exchange and short-range terms in single precision.
+//
+// Same functions as the reference (openmmapi/include/internal/InteraxPairTerms.h:167-337; CUDA snippets
+// platforms/common/src/kernels/interaxDispersion.cc, interaxSlaterOverlap.cc, interaxExchange.cc,
+// interaxShortRange.cc), evaluated in a form chosen for float arithmetic:
+//
+//  * The Slater overlap S(r; a, b) uses no Taylor/closed-form switch for the Exact method.  With a <= b,
+//    h = b - a, s = a + b and delta = r h / (a b) >= 0 the closed form can be rewritten without cancellation as
+//        8 pi S = e^(-r/a) [ 1/s^3 + r/(a s^3) + r^2/(2 a^2 b s^2) + phi3(delta) r^2 (r h/(a^3 b^2 s^2) - 4/(a b s^3)) ]
+//    with phi_k(z) = sum_n z^n/(n+k)! (phi3 = (e^z - 1 - z - z^2/2)/z^3), which is positive and smooth in delta.
+//    For equal widths it reduces to the limit e^(-x)(1 + x + x^2/3)/(64 pi a^3).  Evaluated in float it is exact to
+//    a few ulp for all widths and distances, where the reference's float switch loses up to ~1e-2 near t = 0.2.
+//  * The InteraxOrder2 method reproduces the export's order-2 expansion about the width of the particle with the
+//    lower original index where the widths differ by less than 0.01 bohr (InteraxPairTerms.h:151-159), and is the
+//    exact overlap elsewhere, which is what the reference's closed form computes there.
+//  * Tang-Toennies damping keeps the reference's series/closed-form switch at x = (n+1)/2
+//    (InteraxPairTerms.h:223-253), with the series truncated at k = 28, which is exact to float rounding for
+//    x < 5.5.
+#pragma once
+
+#include "ix_common.cuh"
+#include "overlap_taylor_table.h"
+
+namespace ix {
+
+constexpr float kInv8Pi = 0.0397887357729738339422f;   // 1/(8 pi)
+constexpr float kInvPi = 0.318309886183790671538f;
+constexpr float kOrder2MaxDelta = 0.01f * 0.0529177210903f;   // 0.01 bohr in nm
+
+// e^(-r/a) phi3 and phi4 parts of the overlap, returns 8 pi S and d(8 pi S)/dr.  a <= b, ia = 1/a, ib = 1/b.
+__device__ __forceinline__ void overlapExact(float r, float a, float ia, float b, float ib, float& s8pi,
+                                             float& ds8pi) {
+    const float h = b - a;
+    const float s = a + b;
+    float is = rcpApprox(s);
+    is = fmaf(is, fmaf(-s, is, 1.0f), is);
+    const float is2 = is * is;
+    const float is3 = is2 * is;
+    const float ea = expNeg(r * ia);
+    const float hab = h * ia * ib;          // d delta / dr
+    const float d = r * hab;                 // delta >= 0
+    float eP3, eP4;                          // e^(-r/a) phi3(delta), e^(-r/a) phi4(delta)
+    if (d < 2.0f) {
+        // phi4(d) = sum_{n=0}^{11} d^n/(n+4)!; the omitted terms are below 1e-8 relative for d < 2
+        float p4 = 1.0f / 1307674368000.0f;                 // 1/15!
+        p4 = fmaf(p4, d, 1.0f / 87178291200.0f);            // 1/14!
+        p4 = fmaf(p4, d, 1.0f / 6227020800.0f);             // 1/13!
+        p4 = fmaf(p4, d, 1.0f / 479001600.0f);              // 1/12!
+        p4 = fmaf(p4, d, 1.0f / 39916800.0f);               // 1/11!
+        p4 = fmaf(p4, d, 1.0f / 3628800.0f);                // 1/10!
+        p4 = fmaf(p4, d, 1.0f / 362880.0f);                 // 1/9!
+        p4 = fmaf(p4, d, 1.0f / 40320.0f);                  // 1/8!
+        p4 = fmaf(p4, d, 1.0f / 5040.0f);                   // 1/7!
+        p4 = fmaf(p4, d, 1.0f / 720.0f);                    // 1/6!
+        p4 = fmaf(p4, d, 1.0f / 120.0f);                    // 1/5!
+        p4 = fmaf(p4, d, 1.0f / 24.0f);                     // 1/4!
+        const float p3 = fmaf(d, p4, 1.0f / 6.0f);
+        eP3 = ea * p3;
+        eP4 = ea * p4;
+    }
+    else {
+        // no cancellation worth the series here: e_b - e_a (1 + d + d^2/2) loses at most a factor 3 at d = 2
+        const float eb = expNeg(r * ib);
+        float id = rcpApprox(d);
+        id = fmaf(id, fmaf(-d, id, 1.0f), id);
+        eP3 = (eb - ea * fmaf(d, fmaf(0.5f, d, 1.0f), 1.0f)) * id * id * id;
+        eP4 = fmaf(ea, -1.0f / 6.0f, eP3) * id;
+    }
+    const float c2 = ia * is3;
+    const float c3 = 0.5f * ia * ia * ib * is2;
+    const float k1 = h * ia * ia * ia * ib * ib * is2;
+    const float k2 = 4.0f * ia * ib * is3;
+    const float rk1 = r * k1;
+    const float br = r * r * (rk1 - k2);
+    const float dbr = r * fmaf(3.0f, rk1, -2.0f * k2);
+    const float poly = fmaf(r, fmaf(r, c3, c2), is3);
+    const float dpoly = fmaf(2.0f * r, c3, c2);
+    const float eg = fmaf(eP3, br, ea * poly);
+    const float egp = fmaf(eP3, dbr, fmaf(fmaf(-3.0f, eP4, eP3) * hab, br, ea * dpoly));
+    s8pi = eg;
+    ds8pi = fmaf(-eg, ia, egp);
+}
+
+// Order-2 Taylor expansion of InteraxFF about width l (l = the width of the lower-index particle), returns
+// 8 pi S and its derivative.
+__device__ __forceinline__ void overlapOrder2Taylor(float r, float l, float il, float other, float& s8pi,
+                                                    float& ds8pi) {
+    const float t = (other - l) * il;
+    const float x = r * il;
+    float sv = 0.0f, sd = 0.0f;
+#pragma unroll
+    for (int n = 2; n >= 0; n--) {
+        float v = 0.0f, dv = 0.0f;
+#pragma unroll
+        for (int k = n + 2; k >= 0; k--) {
+            v = fmaf(v, x, kOverlapTaylorValue[n][k]);
+            dv = fmaf(dv, x, kOverlapTaylorDeriv[n][k]);
+        }
+        sv = fmaf(sv, t, v);
+        sd = fmaf(sd, t, dv);
+    }
+    const float pre = expNeg(x) * il * il * il * (8.0f);   // 8 pi S = 8 e^-x / l^3 sum ...
+    s8pi = pre * sv;
+    ds8pi = pre * il * sd;
+}
+
+// 8 pi S(r) and its derivative for the widths of particles i and j, with the overlap method of the force.
+// firstIsI: particle i has the lower original index (InteraxOrder2 expands about its width).
+__device__ __forceinline__ void overlap8pi(float r, float wi, float iwi, float wj, float iwj, int method,
+                                           bool firstIsI, float& s8pi, float& ds8pi) {
+    if (method == 2 && fabsf(wi - wj) < kOrder2MaxDelta) {
+        if (firstIsI) overlapOrder2Taylor(r, wi, iwi, wj, s8pi, ds8pi);
+        else overlapOrder2Taylor(r, wj, iwj, wi, s8pi, ds8pi);
+        return;
+    }
+    if (wi <= wj) overlapExact(r, wi, iwi, wj, iwj, s8pi, ds8pi);
+    else overlapExact(r, wj, iwj, wi, iwi, s8pi, ds8pi);
+}
+
+// Tang-Toennies damped C6/C8/C10 dispersion (InteraxPairTerms.h:267-293).  p = (m1, m2, m3, alpha), w the widths.
+__device__ __forceinline__ void dispersionEnergy(float r, float invR, float4 pi, float4 pj, float wi, float wj,
+                                                 float twoBeta, float& energy, float& dEdR) {
+    const float denom = fmaxf(fmaf(pi.w, pj.x, pj.w * pi.x), 1e-30f);
+    const float pref = pi.w * pj.w * __fdividef(1.0f, denom);
+    const float c6 = pref * pi.x * pj.x;
+    const float c8 = 1.5f * pref * fmaf(pi.x, pj.y, pi.y * pj.x);
+    const float c10 = pref * fmaf(2.0f, fmaf(pi.x, pj.z, pi.z * pj.x), 4.2f * pi.y * pj.y);
+    const float dxdr = twoBeta * __fdividef(1.0f, wi + wj);
+    const float x = dxdr * r;
+    const float expX = expNeg(x);
+    float t[11];
+    t[0] = 1.0f;
+#pragma unroll
+    for (int k = 1; k <= 10; k++) t[k] = t[k - 1] * x * (1.0f / k);
+    const float s6 = (((((1.0f + t[1]) + t[2]) + t[3]) + t[4]) + t[5]) + t[6];
+    const float s8 = (s6 + t[7]) + t[8];
+    const float s10 = (s8 + t[9]) + t[10];
+    float f6 = fmaf(-expX, s6, 1.0f), f8 = fmaf(-expX, s8, 1.0f), f10 = fmaf(-expX, s10, 1.0f);
+    if (x < 5.5f) {
+        // f_n = exp(-x) sum_{k>n} x^k/k! where the closed form cancels
+        float term = t[10], tail = 0.0f;
+#pragma unroll 1
+        for (int k = 11; k <= 28; k++) {
+            term = term * x * __fdividef(1.0f, (float)k);
+            tail += term;
+        }
+        const float tail10 = tail;
+        const float tail8 = (tail10 + t[10]) + t[9];
+        const float tail6 = (tail8 + t[8]) + t[7];
+        f10 = expX * tail10;
+        if (x < 4.5f) f8 = expX * tail8;
+        if (x < 3.5f) f6 = expX * tail6;
+    }
+    const float invR2 = invR * invR;
+    const float invR6 = invR2 * invR2 * invR2;
+    const float e6 = c6 * invR6, e8 = c8 * invR6 * invR2, e10 = c10 * invR6 * invR2 * invR2;
+    energy = -fmaf(f6, e6, fmaf(f8, e8, f10 * e10));
+    const float g = expX * dxdr;
+    dEdR = -(e6 * fmaf(g, t[6], -6.0f * f6 * invR) + e8 * fmaf(g, t[8], -8.0f * f8 * invR) +
+             e10 * fmaf(g, t[10], -10.0f * f10 * invR));
+}
+
+}  // namespace ix

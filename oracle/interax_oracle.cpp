@@ -96,7 +96,7 @@ void candidatePairs(int n, const std::vector<Vec3>& pos, const Vec3* box, const 
 
 double computePairForce(PairTerm term, const std::vector<Vec3>& pos, const Vec3* box, const PairSettings& s,
                         const PairParams& params, double lambda, std::vector<Vec3>& forces,
-                        int64_t* numInteracting) {
+                        int64_t* numInteracting, OpCounter* ops) {
     int n = int(pos.size());
     bool periodic = (s.method == 2);
     bool useCutoff = (s.method != 0);
@@ -143,6 +143,19 @@ double computePairForce(PairTerm term, const std::vector<Vec3>& pos, const Vec3*
             shortRangePair(rEff, a[0], a[1], a[2], b[0], b[1], b[2], scheme, e, dEdR);
         }
         count++;
+        if (ops) {
+            // the same term evaluated on counting values
+            OpCounter& oc = opCounter();
+            oc = OpCounter();
+            Counted ce, cd;
+            if (term == kDispersion)
+                dispersionPair<Counted>(rEff, a[0], a[1], a[2], a[3], a[4], b[0], b[1], b[2], b[3], b[4],
+                                        params.dampingScale, ce, cd);
+            else if (term == kExchange) exchangePair<Counted>(rEff, a[0], a[1], b[0], b[1], scheme, ce, cd);
+            else shortRangePair<Counted>(rEff, a[0], a[1], a[2], b[0], b[1], b[2], scheme, ce, cd);
+            ops->arith += oc.arith;
+            ops->transcendental += oc.transcendental;
+        }
         if (rEff != r) dEdR *= std::pow(r / rEff, 5);
         if (useSwitch && r > s.switchDistance) {
             double t = (r - s.switchDistance) / (s.cutoff - s.switchDistance);
@@ -250,74 +263,93 @@ void longRangeCorrection(const PairSettings& s, const PairParams& params, double
 // ------------------------------------------------------------------------------------------------------------------
 
 // Tang-Toennies f_3: InteraxThreeBodyTerms.h:51-65.
-static void tangToennies3(double x, double& f, double& df) {
-    double e = std::exp(-x);
-    double t3 = x * x * x / 6;
+template <class T>
+static void tangToennies3(T x, T& f, T& df) {
+    T e = vexp(-x);
+    T t3 = x * x * x / T(6.0);
     df = e * t3;
-    if (x < 2) {
-        double term = t3, tail = 0;
+    if (vval(x) < 2) {
+        T term = t3, tail = T(0.0);
         for (int k = 4; k <= 30; k++) {
-            term *= x / k;
-            tail += term;
+            term = term * (x / T(double(k)));
+            tail = tail + term;
         }
         f = e * tail;
     }
-    else f = 1 - e * (1 + x + x * x / 2 + t3);
+    else f = T(1.0) - e * (T(1.0) + x + x * x / T(2.0) + t3);
 }
 
 // g(r) = 1 - exp(-(r/R0)^6): InteraxThreeBodyTerms.h:71-77.
-static void centroidDamping(double r, double invR0, double& g, double& dg) {
-    double x = r * invR0;
-    double x6 = x * x * x;
-    x6 *= x6;
-    g = -std::expm1(-x6);
-    dg = 6 * x6 * std::exp(-x6) / r;
+template <class T>
+static void centroidDamping(T r, T invR0, T& g, T& dg) {
+    T x = r * invR0;
+    T x6 = x * x * x;
+    x6 = x6 * x6;
+    g = T(-std::expm1(-vval(x6)));
+    dg = T(6.0) * x6 * vexp(-x6) / r;
 }
 
-// One triple: InteraxThreeBodyTerms.h:97-146.
-static double computeTriple(const Vec3& a, const Vec3& b, const Vec3& c, double c9, const double* rates, Vec3& fA,
-                            Vec3& fB, Vec3& fC, double radius) {
-    double u = a.dot(a), v = b.dot(b), w = c.dot(c);
-    double p = a.dot(b), q = a.dot(c), s = b.dot(c);
-    double invP = 1 / (u * v * w);
-    double invP32 = invP * std::sqrt(invP);
-    double invP52 = invP32 * invP;
-    double pqs = p * q * s;
-    double energy = c9 * (invP32 - 3 * pqs * invP52);
-    double radial = c9 * (-3 * invP32 + 15 * pqs * invP52);
-    double cross = -3 * c9 * invP52;
-    Vec3 dEda = a * (radial / u) + (b * (q * s) + c * (p * s)) * cross;
-    Vec3 dEdb = b * (radial / v) + (a * (q * s) + c * (p * q)) * cross;
-    Vec3 dEdc = c * (radial / w) + (a * (p * s) + b * (p * q)) * cross;
-    if (rates != nullptr || radius > 0) {
-        double len[3] = {std::sqrt(u), std::sqrt(v), std::sqrt(w)};
-        double f[3], dfdr[3];
+// One triple: InteraxThreeBodyTerms.h:97-146.  T is double, or the counting type (then the returned forces are
+// discarded).
+template <class T>
+static double computeTripleT(const Vec3& av, const Vec3& bv, const Vec3& cv, double c9d, const double* ratesd,
+                             Vec3& fA, Vec3& fB, Vec3& fC, double radius) {
+    T a[3] = {T(av.x), T(av.y), T(av.z)}, b[3] = {T(bv.x), T(bv.y), T(bv.z)}, c[3] = {T(cv.x), T(cv.y), T(cv.z)};
+    T c9 = T(c9d);
+    auto dot = [](const T* x, const T* y) { return x[0] * y[0] + x[1] * y[1] + x[2] * y[2]; };
+    T u = dot(a, a), v = dot(b, b), w = dot(c, c);
+    T p = dot(a, b), q = dot(a, c), s = dot(b, c);
+    T invP = T(1.0) / (u * v * w);
+    T invP32 = invP * vsqrt(invP);
+    T invP52 = invP32 * invP;
+    T pqs = p * q * s;
+    T energy = c9 * (invP32 - T(3.0) * pqs * invP52);
+    T radial = c9 * (T(-3.0) * invP32 + T(15.0) * pqs * invP52);
+    T cross = T(-3.0) * c9 * invP52;
+    T dEda[3], dEdb[3], dEdc[3];
+    for (int k = 0; k < 3; k++) {
+        dEda[k] = a[k] * (radial / u) + (b[k] * (q * s) + c[k] * (p * s)) * cross;
+        dEdb[k] = b[k] * (radial / v) + (a[k] * (q * s) + c[k] * (p * q)) * cross;
+        dEdc[k] = c[k] * (radial / w) + (a[k] * (p * s) + b[k] * (p * q)) * cross;
+    }
+    if (ratesd != nullptr || radius > 0) {
+        T len[3] = {vsqrt(u), vsqrt(v), vsqrt(w)};
+        T f[3], dfdr[3];
         for (int i = 0; i < 3; i++) {
-            if (rates != nullptr) {
-                tangToennies3(rates[i] * len[i], f[i], dfdr[i]);
-                dfdr[i] *= rates[i];
+            if (ratesd != nullptr) {
+                T rate = T(ratesd[i]);
+                tangToennies3<T>(rate * len[i], f[i], dfdr[i]);
+                dfdr[i] = dfdr[i] * rate;
             }
             else {
-                f[i] = 1;
-                dfdr[i] = 0;
+                f[i] = T(1.0);
+                dfdr[i] = T(0.0);
             }
             if (radius > 0) {
-                double g, dg;
-                centroidDamping(len[i], 1 / radius, g, dg);
+                T g, dg;
+                centroidDamping<T>(len[i], T(1.0) / T(radius), g, dg);
                 dfdr[i] = dfdr[i] * g + f[i] * dg;
-                f[i] *= g;
+                f[i] = f[i] * g;
             }
         }
-        double damping = f[0] * f[1] * f[2];
-        dEda = dEda * damping + a * (energy * dfdr[0] * f[1] * f[2] / len[0]);
-        dEdb = dEdb * damping + b * (energy * f[0] * dfdr[1] * f[2] / len[1]);
-        dEdc = dEdc * damping + c * (energy * f[0] * f[1] * dfdr[2] / len[2]);
-        energy *= damping;
+        T damping = f[0] * f[1] * f[2];
+        T sa = energy * dfdr[0] * f[1] * f[2] / len[0];
+        T sb = energy * f[0] * dfdr[1] * f[2] / len[1];
+        T sc = energy * f[0] * f[1] * dfdr[2] / len[2];
+        for (int k = 0; k < 3; k++) {
+            dEda[k] = dEda[k] * damping + a[k] * sa;
+            dEdb[k] = dEdb[k] * damping + b[k] * sb;
+            dEdc[k] = dEdc[k] * damping + c[k] * sc;
+        }
+        energy = energy * damping;
     }
-    fA += dEda + dEdb;
-    fB += dEdc - dEda;
-    fC -= dEdb + dEdc;
-    return energy;
+    Vec3 ga(vval(dEda[0]), vval(dEda[1]), vval(dEda[2]));
+    Vec3 gb(vval(dEdb[0]), vval(dEdb[1]), vval(dEdb[2]));
+    Vec3 gc(vval(dEdc[0]), vval(dEdc[1]), vval(dEdc[2]));
+    fA += ga + gb;
+    fB += gc - ga;
+    fC -= gb + gc;
+    return vval(energy);
 }
 
 static double computeC9(double a1, double w1, double a2, double w2, double a3, double w3) {
@@ -328,7 +360,7 @@ static double computeC9(double a1, double w1, double a2, double w2, double a3, d
 // N x N neighbor matrix and loops over i < j < k; here each site keeps the sorted list of its neighbors above it and
 // the triples are enumerated in the same i, j, k order, so the energies and forces are summed in the same order.
 double computeThreeBody(const std::vector<Vec3>& pos, const Vec3* box, const ThreeBodySettings& s, double lambda,
-                        std::vector<Vec3>& forces, int64_t* numTriples) {
+                        std::vector<Vec3>& forces, int64_t* numTriples, OpCounter* ops) {
     int ns = int(s.siteParticles.size());
     bool anyAlch = false;
     for (auto a : s.alch) anyAlch |= (a != 0);
@@ -384,8 +416,19 @@ double computeThreeBody(const std::vector<Vec3>& pos, const Vec3* box, const Thr
                 double rates[3] = {2 * s.dampingScale / (s.width[i] + s.width[j]),
                                    2 * s.dampingScale / (s.width[i] + s.width[k]),
                                    2 * s.dampingScale / (s.width[j] + s.width[k])};
-                energy += computeTriple(delta(i, j), delta(i, k), delta(j, k), c9, useDamping ? rates : nullptr,
-                                        siteForces[i], siteForces[j], siteForces[k], s.centroidRadius);
+                energy += computeTripleT<double>(delta(i, j), delta(i, k), delta(j, k), c9,
+                                                 useDamping ? rates : nullptr, siteForces[i], siteForces[j],
+                                                 siteForces[k], s.centroidRadius);
+                if (ops) {
+                    OpCounter& oc = opCounter();
+                    oc = OpCounter();
+                    Vec3 dummy[3];
+                    computeTripleT<Counted>(delta(i, j), delta(i, k), delta(j, k), c9, useDamping ? rates : nullptr,
+                                            dummy[0], dummy[1], dummy[2], s.centroidRadius);
+                    // C9 (12 operations, InteraxThreeBodyForceImpl.h:69-72) and the three displacements (9)
+                    ops->arith += oc.arith + 12 + 9;
+                    ops->transcendental += oc.transcendental;
+                }
             }
         }
     }
@@ -526,6 +569,70 @@ double ox_three_body(int n, const double* xyz, const double* box9, int num_sites
         std::snprintf(g_error, sizeof(g_error), "%s", ex.what());
         return NAN;
     }
+}
+
+// Operations of the reference algorithm per interacting pair of one pair term (only the term's own function; the
+// geometry, switch and force accumulation shared by the fused terms are ox_pair_driver_ops()).  out[0] arithmetic,
+// out[1] transcendental, out[2] number of pairs.
+void ox_pair_ops(int term, int n, const double* xyz, const double* box9, const ox_pair_settings* settings,
+                 const double* params, const unsigned char* alch, double damping_scale, int overlap_method,
+                 double lambda, double* out) {
+    std::vector<Vec3> pos, f(n);
+    Vec3 box[3];
+    toVectors(n, xyz, box9, pos, box);
+    PairParams p;
+    p.stride = term == 0 ? 5 : (term == 1 ? 2 : 3);
+    p.p.assign(params, params + size_t(n) * p.stride);
+    p.alch.assign(alch, alch + n);
+    p.dampingScale = damping_scale;
+    p.overlapMethod = overlap_method;
+    int64_t cnt = 0;
+    OpCounter ops;
+    computePairForce(PairTerm(term), pos, box, toSettings(settings), p, lambda, f, &cnt, &ops);
+    out[0] = double(ops.arith);
+    out[1] = double(ops.transcendental);
+    out[2] = double(cnt);
+}
+
+// Per-pair operations of the pair driver (ReferenceInteraxPairIxn.h:89-126) once per pair: displacement (3),
+// r^2 (5), sqrt (1 transcendental), cutoff test (1), scale and dE/dr / r (2), force vector (3), accumulation into
+// both particles (6).  out[0] arithmetic, out[1] transcendental.
+void ox_pair_driver_ops(double* out) {
+    out[0] = 3 + 5 + 1 + 2 + 3 + 6;
+    out[1] = 1;
+}
+
+// Operations per interacting triple (computeTriple, C9, displacements).  out as ox_pair_ops.
+void ox_three_body_ops(int n, const double* xyz, const double* box9, int num_sites, const int* site_offsets,
+                       const int* site_particles, const double* site_params, const int* molecule,
+                       const unsigned char* alch, double cutoff, double scale, int damping_method,
+                       double damping_scale, double centroid_radius, int periodic, double lambda, double* out) {
+    std::vector<Vec3> pos, f(n);
+    Vec3 box[3];
+    toVectors(n, xyz, box9, pos, box);
+    ThreeBodySettings s;
+    s.siteParticles.resize(num_sites);
+    for (int i = 0; i < num_sites; i++)
+        s.siteParticles[i].assign(site_particles + site_offsets[i], site_particles + site_offsets[i + 1]);
+    for (int i = 0; i < num_sites; i++) {
+        s.alpha.push_back(site_params[3 * i]);
+        s.frequency.push_back(site_params[3 * i + 1]);
+        s.width.push_back(site_params[3 * i + 2]);
+    }
+    s.molecule.assign(molecule, molecule + num_sites);
+    s.alch.assign(alch, alch + num_sites);
+    s.cutoff = cutoff;
+    s.scale = scale;
+    s.dampingMethod = damping_method;
+    s.dampingScale = damping_scale;
+    s.centroidRadius = centroid_radius;
+    s.periodic = periodic != 0;
+    int64_t cnt = 0;
+    OpCounter ops;
+    computeThreeBody(pos, box, s, lambda, f, &cnt, &ops);
+    out[0] = double(ops.arith);
+    out[1] = double(ops.transcendental);
+    out[2] = double(cnt);
 }
 
 // Slater overlap and its derivative (for the known-answer tests).  method: 0 Exact (double precision switch),

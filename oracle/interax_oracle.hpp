@@ -31,6 +31,30 @@ inline double vabs(double v) { return std::fabs(v); }
 inline double vpow(double a, double b) { return std::pow(a, b); }
 inline double vval(double v) { return v; }
 
+// A double that counts the operations performed on it: +, -, *, / and negation as arithmetic, exp, sqrt and pow as
+// transcendental.  Used to fix the algorithmic work per pair and per triple.
+struct OpCounter {
+    long long arith = 0, transcendental = 0;
+};
+inline OpCounter& opCounter() {
+    static thread_local OpCounter c;
+    return c;
+}
+struct Counted {
+    double v;
+    Counted() : v(0) {}
+    Counted(double x) : v(x) {}
+};
+inline Counted operator+(Counted a, Counted b) { opCounter().arith++; return Counted(a.v + b.v); }
+inline Counted operator-(Counted a, Counted b) { opCounter().arith++; return Counted(a.v - b.v); }
+inline Counted operator*(Counted a, Counted b) { opCounter().arith++; return Counted(a.v * b.v); }
+inline Counted operator/(Counted a, Counted b) { opCounter().arith++; return Counted(a.v / b.v); }
+inline Counted operator-(Counted a) { opCounter().arith++; return Counted(-a.v); }
+inline Counted vexp(Counted a) { opCounter().transcendental++; return Counted(std::exp(a.v)); }
+inline Counted vsqrt(Counted a) { opCounter().transcendental++; return Counted(std::sqrt(a.v)); }
+inline Counted vpow(Counted a, Counted b) { opCounter().transcendental++; return Counted(std::pow(a.v, b.v)); }
+inline double vval(Counted a) { return a.v; }
+
 // ------------------------------------------------------------------------------------------------------------------
 // Taylor coefficients of the Slater overlap integral about the width l (openmmapi/include/internal/InteraxPairTerms.h
 // :87-113).  They are not copied: they are derived here from the closed form by series arithmetic.  With a = l,
@@ -150,6 +174,33 @@ struct SlaterTaylorScheme {
 template <class T>
 inline void slaterOverlap(T r, T a, T b, const SlaterTaylorScheme& scheme, T& overlap, T& dOverlapdR) {
     const double pi = M_PI;
+    // Where the Taylor expansion about l applies (the reference evaluates both branches and selects one; only the
+    // selected one is evaluated here, with the same result)
+    T l = scheme.aboutSmallerWidth ? (vval(a) < vval(b) ? a : b) : a;
+    T invL = T(1.0) / l;
+    T delta = a + b - l - l;
+    T t = delta * invL;
+    T x = r * invL;
+    double absT = std::fabs(vval(t));
+    bool nearAbsolute = std::fabs(vval(delta)) < scheme.maxDelta;
+    bool nearRelative = (absT < scheme.maxT) && (absT * vval(x) < scheme.maxTX);
+    if (nearAbsolute || nearRelative) {
+        const OverlapTaylorTable& table = overlapTaylorTable();
+        T sumValue = T(0.0), sumDeriv = T(0.0);
+        for (int n = scheme.order; n >= 0; n--) {
+            T value = T(0.0), deriv = T(0.0);
+            for (int k = kTaylorTerms - 1; k >= 0; k--) {
+                value = value * x + T(table.value[n][k]);
+                deriv = deriv * x + T(table.deriv[n][k]);
+            }
+            sumValue = sumValue * t + value;
+            sumDeriv = sumDeriv * t + deriv;
+        }
+        T prefactor = vexp(-x) * invL * invL * invL / T(pi);
+        overlap = prefactor * sumValue;
+        dOverlapdR = prefactor * invL * sumDeriv;
+        return;
+    }
     // closed form: S = F / (8 pi r)
     T aa = a * a, bb = b * b;
     T d = bb - aa;
@@ -159,34 +210,8 @@ inline void slaterOverlap(T r, T a, T b, const SlaterTaylorScheme& scheme, T& ov
     T f = c * (expA - expB) + r * invD2 * (a * expA + b * expB);
     T dfdr = c * (expB / b - expA / a) + invD2 * (a * expA + b * expB - r * (expA + expB));
     T invR = T(1.0) / r;
-    T closedOverlap = f * invR / (T(8.0) * T(pi));
-    T closedDeriv = (r * dfdr - f) * invR * invR / (T(8.0) * T(pi));
-    // Taylor expansion about l
-    T l = scheme.aboutSmallerWidth ? (vval(a) < vval(b) ? a : b) : a;
-    T invL = T(1.0) / l;
-    T delta = a + b - l - l;
-    T t = delta * invL;
-    T x = r * invL;
-    const OverlapTaylorTable& table = overlapTaylorTable();
-    T sumValue = T(0.0), sumDeriv = T(0.0);
-    for (int n = scheme.order; n >= 0; n--) {
-        T value = T(0.0), deriv = T(0.0);
-        for (int k = kTaylorTerms - 1; k >= 0; k--) {
-            value = value * x + T(table.value[n][k]);
-            deriv = deriv * x + T(table.deriv[n][k]);
-        }
-        sumValue = sumValue * t + value;
-        sumDeriv = sumDeriv * t + deriv;
-    }
-    T prefactor = vexp(-x) * invL * invL * invL / T(pi);
-    T taylorOverlap = prefactor * sumValue;
-    T taylorDeriv = prefactor * invL * sumDeriv;
-    double absT = std::fabs(vval(t));
-    bool nearAbsolute = std::fabs(vval(delta)) < scheme.maxDelta;
-    bool nearRelative = (absT < scheme.maxT) && (absT * vval(x) < scheme.maxTX);
-    bool useTaylor = nearAbsolute || nearRelative;
-    overlap = useTaylor ? taylorOverlap : closedOverlap;
-    dOverlapdR = useTaylor ? taylorDeriv : closedDeriv;
+    overlap = f * invR / (T(8.0) * T(pi));
+    dOverlapdR = (r * dfdr - f) * invR * invR / (T(8.0) * T(pi));
 }
 
 // Tang-Toennies f_6, f_8, f_10 and their derivatives: InteraxPairTerms.h:223-253.
@@ -329,7 +354,7 @@ struct PairParams {
 
 double computePairForce(PairTerm term, const std::vector<Vec3>& pos, const Vec3* box, const PairSettings& s,
                         const PairParams& params, double lambda, std::vector<Vec3>& forces,
-                        int64_t* numInteracting = nullptr);
+                        int64_t* numInteracting = nullptr, OpCounter* ops = nullptr);
 
 // Long range correction coefficients: openmmapi/src/InteraxDispersionForceImpl.cpp:49-149.
 void longRangeCorrection(const PairSettings& s, const PairParams& params, double& coefficient,
@@ -349,6 +374,6 @@ struct ThreeBodySettings {
 };
 
 double computeThreeBody(const std::vector<Vec3>& pos, const Vec3* box, const ThreeBodySettings& s, double lambda,
-                        std::vector<Vec3>& forces, int64_t* numTriples = nullptr);
+                        std::vector<Vec3>& forces, int64_t* numTriples = nullptr, OpCounter* ops = nullptr);
 
 }  // namespace ixo
