@@ -47,7 +47,7 @@ struct AtmBuffers {
     long long* siteForce;        // 3 x numSites, SoA fixed point
     long long* particleForce;    // 3 x numParticles, SoA fixed point (original order)
     int numParticles;
-    long long* energyFixed;      // one value
+    double* energyPartials;      // one per warp of the triple kernel's grid
     unsigned long long* tripleCount;
 };
 
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(32 * kAtmWarps) kTriples(AtmBuffers A, AtmConf
         __syncwarp();
     }
     const double sum = warpSumD(eAcc);
-    if (lane == 0 && sum != 0.0) atomicAddFixed(A.energyFixed, toFixedD(sum));
+    if (lane == 0) A.energyPartials[blockIdx.x * kAtmWarps + (threadIdx.x >> 5)] = sum;
     for (int o = 16; o > 0; o >>= 1) triples += __shfl_xor_sync(0xffffffffu, triples, o);
     if (lane == 0 && triples) atomicAdd(A.tripleCount, triples);
 }

@@ -45,6 +45,27 @@ __device__ __forceinline__ float expNeg(float x) {
     return fmaf(p, yLo * 0.693147180559945309f, p);            // 2^yLo ~ 1 + yLo ln 2
 }
 
+// exp(-(xHi + xLo)) for a float-float argument (|xLo| << xHi).
+__device__ __forceinline__ float expNegDF(float xHi, float xLo) {
+    const float kLog2eHi = 1.44269502162933349609375f;
+    const float kLog2eLo = 1.925963033500011079834e-8f;
+    float yHi = -xHi * kLog2eHi;
+    float yLo = fmaf(-xHi, kLog2eHi, -yHi);
+    yLo = fmaf(-xHi, kLog2eLo, yLo);
+    yLo = fmaf(-xLo, kLog2eHi, yLo);
+    float p = ex2Approx(yHi);
+    return fmaf(p, yLo * 0.693147180559945309f, p);
+}
+
+// exp(-r (invHi + invLo)), the exponent formed with a compensated product: the rounding of the reciprocal width
+// to float, which the exponential would amplify by r/width (10 to 40 for interacting pairs) into a systematic error,
+// is carried in invLo.
+__device__ __forceinline__ float expNegScaled(float r, float invHi, float invLo) {
+    const float xHi = r * invHi;
+    const float xLo = fmaf(r, invHi, -xHi) + r * invLo;
+    return expNegDF(xHi, xLo);
+}
+
 // sqrt(r2) to ~0.5 ulp: approximate reciprocal square root followed by one Newton correction of the root.
 __device__ __forceinline__ float sqrtRefined(float r2, float& invR) {
     float y = rsqrtApprox(r2);

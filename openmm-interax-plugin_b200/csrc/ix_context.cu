@@ -106,7 +106,11 @@ struct ix_ctx {
     ListBuffers L{};
     ListGeometry G{};
     PairBuffers P{};
-    float4 *dP0o = nullptr, *dP1o = nullptr, *dP2o = nullptr;
+    float4 *dP0o = nullptr, *dP1o = nullptr, *dP2o = nullptr, *dP3o = nullptr;
+    float4* dP3 = nullptr;
+    double* dPairPartials = nullptr;     // per-warp energies of the pair kernel (3 per warp)
+    double* dAtmPartials = nullptr;      // per-warp energies of the triple kernel
+    int atmGridBlocks = 0;
     int* dFlagso = nullptr;
     float4 *dP0 = nullptr, *dP1 = nullptr, *dP2 = nullptr;
     int* dFlagsSorted = nullptr;
@@ -295,7 +299,7 @@ static void computeLrc(ix_ctx* ctx) {
 // Per-particle float parameters in original order, with the term flags.
 static int uploadPairParams(ix_ctx* ctx) {
     const int n = ctx->n;
-    std::vector<float4> p0(n), p1(n), p2(n);
+    std::vector<float4> p0(n), p1(n), p2(n), p3(n);
     std::vector<int> flags(n);
     std::vector<bool> equalWidths(n, true);
     for (int i = 0; i < n; i++) {
@@ -333,10 +337,16 @@ static int uploadPairParams(ix_ctx* ctx) {
         p2[i] = c;
         flags[i] = f;
         equalWidths[i] = (wx == ws);
+        // float remainders of the widths and their reciprocals (float-float values for the kernel)
+        const double wide[4] = {wx, wx != 0 ? 1.0 / wx : 0.0, ws, ws != 0 ? 1.0 / ws : 0.0};
+        float lo[4];
+        for (int k = 0; k < 4; k++) lo[k] = (float)(wide[k] - (double)(float)wide[k]);
+        p3[i] = make_float4(lo[0], lo[1], lo[2], lo[3]);
     }
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP0o, p0.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP1o, p1.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP2o, p2.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP3o, p3.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dFlagso, flags.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     computeLrc(ctx);
@@ -348,7 +358,8 @@ static int uploadPairParams(ix_ctx* ctx) {
 }
 
 __global__ void kGatherParams(ListBuffers L, const float4* p0o, const float4* p1o, const float4* p2o,
-                              const int* flagso, float4* p0, float4* p1, float4* p2, int* flags) {
+                              const float4* p3o, const int* flagso, float4* p0, float4* p1, float4* p2, float4* p3,
+                              int* flags) {
     if (!rebuildRequested(L)) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= L.np) return;
@@ -357,12 +368,14 @@ __global__ void kGatherParams(ListBuffers L, const float4* p0o, const float4* p1
         p0[s] = p0o[i];
         p1[s] = p1o[i];
         p2[s] = p2o[i];
+        p3[s] = p3o[i];
         flags[s] = flagso[i];
     }
     else {
         p0[s] = make_float4(0, 0, 0, 0);
         p1[s] = make_float4(0, 0, 0, 0);
         p2[s] = make_float4(0, 0, 0, 0);
+        p3[s] = make_float4(0, 0, 0, 0);
         flags[s] = 0;
     }
 }
@@ -487,6 +500,8 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
     IX_TRY(deviceAlloc(ctx, "p0o", n, &ctx->dP0o));
     IX_TRY(deviceAlloc(ctx, "p1o", n, &ctx->dP1o));
     IX_TRY(deviceAlloc(ctx, "p2o", n, &ctx->dP2o));
+    IX_TRY(deviceAlloc(ctx, "p3o", n, &ctx->dP3o));
+    IX_TRY(deviceAlloc(ctx, "p3", np, &ctx->dP3));
     IX_TRY(deviceAlloc(ctx, "flagso", n, &ctx->dFlagso));
     IX_TRY(deviceAlloc(ctx, "p0", np, &ctx->dP0));
     IX_TRY(deviceAlloc(ctx, "p1", np, &ctx->dP1));
@@ -496,12 +511,14 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
     ctx->P.p0 = ctx->dP0;
     ctx->P.p1 = ctx->dP1;
     ctx->P.p2 = ctx->dP2;
+    ctx->P.p3 = ctx->dP3;
     ctx->P.flags = ctx->dFlagsSorted;
-    ctx->P.energyFixed = ctx->dEnergyFixed;
     ctx->P.pairCount = ctx->dCounts;
     int perSM = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kPairTiles, 32 * kPairWarps, 0);
     ctx->pairGridBlocks = std::max(1, perSM) * ctx->numSMs;
+    IX_TRY(deviceAlloc(ctx, "pairPartials", 3 * (size_t)ctx->pairGridBlocks * kPairWarps, &ctx->dPairPartials));
+    ctx->P.energyPartials = ctx->dPairPartials;
     ctx->pairAllocated = true;
     IX_TRY(uploadPairParams(ctx));
     return IX_OK;
@@ -555,7 +572,9 @@ static int allocateAtm(ix_ctx* ctx) {
     IX_TRY(deviceAlloc(ctx, "nbr", (size_t)ns * A.cap, &A.nbr));
     A.flag = ctx->dFlags + 4;
     A.numParticles = ctx->n;
-    A.energyFixed = ctx->dEnergyFixed + 3;
+    ctx->atmGridBlocks = std::max(1, std::min((ns + kAtmWarps - 1) / kAtmWarps, ctx->numSMs * 8));
+    IX_TRY(deviceAlloc(ctx, "atmPartials", (size_t)ctx->atmGridBlocks * kAtmWarps, &ctx->dAtmPartials));
+    A.energyPartials = ctx->dAtmPartials;
     A.tripleCount = ctx->dCounts + 1;
     ctx->atmAllocated = true;
     ctx->atmDirty = true;
@@ -582,8 +601,7 @@ static int uploadAtmParams(ix_ctx* ctx) {
 // ---------------------------------------------------------------------------------------------------------------------
 
 __global__ void kFinalize(int n, int np, const int* slotOf, const long long* pairForce, const long long* atmForce,
-                          const long long* energyFixed, double lrcEnergy, double* outForces, double* outEnergy,
-                          long long* addFixed, int stride) {
+                          double* outForces, long long* addFixed, int stride) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         long long f[3] = {0, 0, 0};
@@ -610,8 +628,29 @@ __global__ void kFinalize(int n, int np, const int* slotOf, const long long* pai
             atomicAddFixed(addFixed + 2 * stride + i, f[2]);
         }
     }
-    if (i == 0 && outEnergy) {
-        for (int t = 0; t < 4; t++) outEnergy[t] = (double)energyFixed[t] / kFixedScale;
+}
+
+// Term energies from the per-warp partials: each thread sums a fixed strided subset, then a fixed reduction tree,
+// so the result is identical on every run.  lrcEnergy (the long range correction, from the host) joins term 0.
+__global__ void kReduceEnergies(const double* pairPartials, int numPairWarps, const double* atmPartials,
+                                int numAtmWarps, double lrcEnergy, double* outEnergy) {
+    __shared__ double red[4][256];
+    const int t = threadIdx.x;
+    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    if (pairPartials)
+        for (int w = t; w < numPairWarps; w += 256)
+            for (int k = 0; k < 3; k++) s[k] += pairPartials[3 * w + k];
+    if (atmPartials)
+        for (int w = t; w < numAtmWarps; w += 256) s[3] += atmPartials[w];
+    for (int k = 0; k < 4; k++) red[k][t] = s[k];
+    __syncthreads();
+    for (int half = 128; half > 0; half >>= 1) {
+        if (t < half)
+            for (int k = 0; k < 4; k++) red[k][t] += red[k][t + half];
+        __syncthreads();
+    }
+    if (t == 0 && outEnergy) {
+        for (int k = 0; k < 4; k++) outEnergy[k] = red[k][0];
         outEnergy[0] += lrcEnergy;
     }
 }
@@ -683,8 +722,8 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         kScatterCells<<<gN, tpb, 0, st>>>(L);
         kSortWithinCells<<<gCells, tpb, 0, st>>>(L);
         kSortedAtoms<<<gNp, tpb, 0, st>>>(L, ctx->G);
-        kGatherParams<<<gNp, tpb, 0, st>>>(L, ctx->dP0o, ctx->dP1o, ctx->dP2o, ctx->dFlagso, ctx->dP0, ctx->dP1,
-                                           ctx->dP2, ctx->dFlagsSorted);
+        kGatherParams<<<gNp, tpb, 0, st>>>(L, ctx->dP0o, ctx->dP1o, ctx->dP2o, ctx->dP3o, ctx->dFlagso, ctx->dP0,
+                                           ctx->dP1, ctx->dP2, ctx->dP3, ctx->dFlagsSorted);
         kUpdateSortedPositions<<<gNp, tpb, 0, st>>>(L);
         kBlockBounds<<<(L.nb * 32 + tpb - 1) / tpb, tpb, 0, st>>>(L);
         const int warpsPerBlock = 8;
@@ -732,7 +771,7 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         kSiteNeighbors<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, st>>>(A, C);
         kClearFlag<<<1, 1, 0, st>>>(A.flag);
         const size_t smem = sizeof(AtmWarpStorage) * kAtmWarps;
-        int blocks = std::min((C.numSites + kAtmWarps - 1) / kAtmWarps, ctx->numSMs * 8);
+        int blocks = ctx->atmGridBlocks;
         if (ctx->profiling) cudaEventRecord(ctx->ev[2], st);
         kTriples<<<std::max(1, blocks), 32 * kAtmWarps, smem, st>>>(A, C);
         if (ctx->profiling) cudaEventRecord(ctx->ev[3], st);
@@ -742,9 +781,11 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         IX_CUDA(ctx, cudaGetLastError());
     }
     kFinalize<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->L.np, ctx->L.slotOf, doPair ? ctx->P.forceFixed : nullptr,
-                                              doAtm ? ctx->A.particleForce : nullptr, ctx->dEnergyFixed, lrcEnergy,
-                                              outForces, outEnergy, addFixed, stride);
-    ctx->launches += 1;
+                                              doAtm ? ctx->A.particleForce : nullptr, outForces, addFixed, stride);
+    kReduceEnergies<<<1, 256, 0, st>>>(doPair ? ctx->dPairPartials : nullptr, ctx->pairGridBlocks * kPairWarps,
+                                       doAtm ? ctx->dAtmPartials : nullptr, ctx->atmGridBlocks * kAtmWarps,
+                                       lrcEnergy, outEnergy);
+    ctx->launches += 2;
     IX_CUDA(ctx, cudaGetLastError());
     return IX_OK;
 }

@@ -46,17 +46,18 @@ struct PairBuffers {
     const float4* p0;            // sorted: m1, m2, m3, alpha
     const float4* p1;            // sorted: dispersion width, amplitude A, K, L
     const float4* p2;            // sorted: exchange width, 1/width, short-range width, 1/width
+    const float4* p3;            // sorted: the float remainders of p2's four values (float-float widths)
     const int* flags;            // sorted
     long long* forceFixed;       // 3 x np, sorted order, SoA
-    long long* energyFixed;      // 3 terms
+    double* energyPartials;      // 3 per warp of the grid, summed in a fixed order afterwards
     unsigned long long* pairCount;
 };
 
 // Every pair term of one pair.  r, invR: distance; fi, fj: flags.  Adds each term's scaled energy to e[] and returns
 // the scaled dE/dr of all terms.
 __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, float invR, float4 a0, float4 a1,
-                                           float4 a2, int fi, float4 b0, float4 b1, float4 b2, int fj,
-                                           bool iFirst, float e[3]) {
+                                           float4 a2, float4 a3, int fi, float4 b0, float4 b1, float4 b2,
+                                           float4 b3, int fj, bool iFirst, float e[3]) {
     float dTotal = 0.0f;
     float shared8pi = 0.0f, sharedD8pi = 0.0f, sharedR = -1.0f;
 #pragma unroll
@@ -87,13 +88,15 @@ __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, flo
                 ds8pi = sharedD8pi;
             }
             else if (t == 1) {
-                overlap8pi(rEff, a2.x, a2.y, b2.x, b2.y, C.overlapMethod[1], iFirst, s8pi, ds8pi);
+                overlap8pi(rEff, Width{a2.x, a3.x, a2.y, a3.y}, Width{b2.x, b3.x, b2.y, b3.y}, C.overlapMethod[1],
+                           iFirst, s8pi, ds8pi);
                 shared8pi = s8pi;
                 sharedD8pi = ds8pi;
                 sharedR = rEff;
             }
             else {
-                overlap8pi(rEff, a2.z, a2.w, b2.z, b2.w, C.overlapMethod[2], iFirst, s8pi, ds8pi);
+                overlap8pi(rEff, Width{a2.z, a3.z, a2.w, a3.w}, Width{b2.z, b3.z, b2.w, b3.w}, C.overlapMethod[2],
+                           iFirst, s8pi, ds8pi);
             }
             if (t == 1) {
                 // exchange A_i A_j S (InteraxPairTerms.h:305-312)
@@ -103,7 +106,7 @@ __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, flo
             }
             else {
                 // short range (K_i+K_j)/2 St + (L_i+L_j)/2 St^2, St = 8 pi (s_i+s_j)^3 S (InteraxPairTerms.h:325-337)
-                const float ws = a2.z + b2.z;
+                const float ws = (a2.z + b2.z) + (a3.z + b3.z);
                 const float norm = ws * ws * ws;
                 const float st = norm * s8pi;
                 const float k = 0.5f * (a1.z + b1.z);
@@ -130,7 +133,7 @@ __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, flo
 struct PairWarpStorage {
     double x[2][32], y[2][32], z[2][32];
     float4 pf[2][32];
-    float4 a0[2][32], a1[2][32], a2[2][32];
+    float4 a0[2][32], a1[2][32], a2[2][32], a3[2][32];
     int flags[2][32], orig[2][32], slot[2][32];
     float fx[2][32], fy[2][32], fz[2][32];
     unsigned short queue[1024];
@@ -148,6 +151,7 @@ __device__ __forceinline__ void stageParticle(PairWarpStorage& S, int side, int 
         S.a0[side][lane] = P.p0[s];
         S.a1[side][lane] = P.p1[s];
         S.a2[side][lane] = P.p2[s];
+        S.a3[side][lane] = P.p3[s];
         S.flags[side][lane] = P.flags[s];
         S.orig[side][lane] = L.sortedAtom[s];
         S.slot[side][lane] = s;
@@ -238,8 +242,8 @@ __global__ void __launch_bounds__(32 * kPairWarps) kPairTiles(ListBuffers L, Pai
                     if (inside && (fi & fj & (kFlagGateDisp | kFlagGateExch | kFlagGateSr))) {
                         float invR;
                         const float r = sqrtRefined(r2, invR);
-                        const float dEdR = pairTerms(C, r, invR, S.a0[0][i], S.a1[0][i], S.a2[0][i], fi,
-                                                     S.a0[1][j], S.a1[1][j], S.a2[1][j], fj,
+                        const float dEdR = pairTerms(C, r, invR, S.a0[0][i], S.a1[0][i], S.a2[0][i], S.a3[0][i],
+                                                     fi, S.a0[1][j], S.a1[1][j], S.a2[1][j], S.a3[1][j], fj,
                                                      S.orig[0][i] < S.orig[1][j], e);
                         const float fs = dEdR * invR;
                         const float fxv = dx * fs, fyv = dy * fs, fzv = dz * fs;
@@ -262,9 +266,12 @@ __global__ void __launch_bounds__(32 * kPairWarps) kPairTiles(ListBuffers L, Pai
         __syncwarp();
         flushForce(S, 0, lane, L.np, P.forceFixed);
     }
+    // each warp's energy, in a fixed order of its tasks and a fixed reduction tree; the partials of all warps are
+    // summed in a fixed order by kReduceEnergies, so the total is the same on every run
+    const int globalWarp = blockIdx.x * kPairWarps + warp;
     for (int t = 0; t < 3; t++) {
         const double sum = warpSumD(eAcc[t]);
-        if (lane == 0 && sum != 0.0) atomicAddFixed(P.energyFixed + t, toFixedD(sum));
+        if (lane == 0) P.energyPartials[3 * globalWarp + t] = sum;
     }
     for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
     if (lane == 0 && pairs) atomicAdd(P.pairCount, pairs);

@@ -27,16 +27,23 @@ constexpr float kInv8Pi = 0.0397887357729738339422f;   // 1/(8 pi)
 constexpr float kInvPi = 0.318309886183790671538f;
 constexpr float kOrder2MaxDelta = 0.01f * 0.0529177210903f;   // 0.01 bohr in nm
 
-// e^(-r/a) phi3 and phi4 parts of the overlap, returns 8 pi S and d(8 pi S)/dr.  a <= b, ia = 1/a, ib = 1/b.
-__device__ __forceinline__ void overlapExact(float r, float a, float ia, float b, float ib, float& s8pi,
-                                             float& ds8pi) {
-    const float h = b - a;
-    const float s = a + b;
+// A Slater width as float-float: the width w + wLo and its reciprocal iw + iwLo, each the double-precision value
+// split into a float and the float remainder.  The low parts keep the widths' rounding out of the exponentials.
+struct Width {
+    float w, wLo, iw, iwLo;
+};
+
+// 8 pi S and d(8 pi S)/dr for widths A <= B (the cancellation-free form above).
+__device__ __forceinline__ void overlapExact(float r, const Width& A, const Width& B, float& s8pi, float& ds8pi) {
+    const float a = A.w, ia = A.iw, ib = B.iw;
+    const float h = (B.w - A.w) + (B.wLo - A.wLo);
+    const float s = (A.w + B.w) + (A.wLo + B.wLo);
     float is = rcpApprox(s);
     is = fmaf(is, fmaf(-s, is, 1.0f), is);
     const float is2 = is * is;
     const float is3 = is2 * is;
-    const float ea = expNeg(r * ia);
+    const float ea = expNegScaled(r, A.iw, A.iwLo);
+    (void)a;
     const float hab = h * ia * ib;          // d delta / dr
     const float d = r * hab;                 // delta >= 0
     float eP3, eP4;                          // e^(-r/a) phi3(delta), e^(-r/a) phi4(delta)
@@ -60,7 +67,7 @@ __device__ __forceinline__ void overlapExact(float r, float a, float ia, float b
     }
     else {
         // no cancellation worth the series here: e_b - e_a (1 + d + d^2/2) loses at most a factor 3 at d = 2
-        const float eb = expNeg(r * ib);
+        const float eb = expNegScaled(r, B.iw, B.iwLo);
         float id = rcpApprox(d);
         id = fmaf(id, fmaf(-d, id, 1.0f), id);
         eP3 = (eb - ea * fmaf(d, fmaf(0.5f, d, 1.0f), 1.0f)) * id * id * id;
@@ -83,9 +90,10 @@ __device__ __forceinline__ void overlapExact(float r, float a, float ia, float b
 
 // Order-2 Taylor expansion of InteraxFF about width l (l = the width of the lower-index particle), returns
 // 8 pi S and its derivative.
-__device__ __forceinline__ void overlapOrder2Taylor(float r, float l, float il, float other, float& s8pi,
+__device__ __forceinline__ void overlapOrder2Taylor(float r, const Width& L, const Width& O, float& s8pi,
                                                     float& ds8pi) {
-    const float t = (other - l) * il;
+    const float il = L.iw;
+    const float t = ((O.w - L.w) + (O.wLo - L.wLo)) * il;
     const float x = r * il;
     float sv = 0.0f, sd = 0.0f;
 #pragma unroll
@@ -99,22 +107,22 @@ __device__ __forceinline__ void overlapOrder2Taylor(float r, float l, float il, 
         sv = fmaf(sv, t, v);
         sd = fmaf(sd, t, dv);
     }
-    const float pre = expNeg(x) * il * il * il * (8.0f);   // 8 pi S = 8 e^-x / l^3 sum ...
+    const float pre = expNegScaled(r, L.iw, L.iwLo) * il * il * il * (8.0f);   // 8 pi S = 8 e^-x / l^3 sum ...
     s8pi = pre * sv;
     ds8pi = pre * il * sd;
 }
 
 // 8 pi S(r) and its derivative for the widths of particles i and j, with the overlap method of the force.
 // firstIsI: particle i has the lower original index (InteraxOrder2 expands about its width).
-__device__ __forceinline__ void overlap8pi(float r, float wi, float iwi, float wj, float iwj, int method,
-                                           bool firstIsI, float& s8pi, float& ds8pi) {
-    if (method == 2 && fabsf(wi - wj) < kOrder2MaxDelta) {
-        if (firstIsI) overlapOrder2Taylor(r, wi, iwi, wj, s8pi, ds8pi);
-        else overlapOrder2Taylor(r, wj, iwj, wi, s8pi, ds8pi);
+__device__ __forceinline__ void overlap8pi(float r, const Width& Wi, const Width& Wj, int method, bool firstIsI,
+                                           float& s8pi, float& ds8pi) {
+    if (method == 2 && fabsf((Wi.w - Wj.w) + (Wi.wLo - Wj.wLo)) < kOrder2MaxDelta) {
+        if (firstIsI) overlapOrder2Taylor(r, Wi, Wj, s8pi, ds8pi);
+        else overlapOrder2Taylor(r, Wj, Wi, s8pi, ds8pi);
         return;
     }
-    if (wi <= wj) overlapExact(r, wi, iwi, wj, iwj, s8pi, ds8pi);
-    else overlapExact(r, wj, iwj, wi, iwi, s8pi, ds8pi);
+    if (Wi.w < Wj.w || (Wi.w == Wj.w && Wi.wLo <= Wj.wLo)) overlapExact(r, Wi, Wj, s8pi, ds8pi);
+    else overlapExact(r, Wj, Wi, s8pi, ds8pi);
 }
 
 // Tang-Toennies damped C6/C8/C10 dispersion (InteraxPairTerms.h:267-293).  p = (m1, m2, m3, alpha), w the widths.

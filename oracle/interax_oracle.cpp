@@ -11,6 +11,12 @@
 
 namespace ixo {
 
+// Sum of |pair or triple energies| of the last evaluation on this thread (reset at the start of each one).
+static double& lastAbsEnergy() {
+    static thread_local double value = 0.0;
+    return value;
+}
+
 static bool isRectangular(const Vec3* box) {
     return box[1].x == 0 && box[2].x == 0 && box[2].y == 0;
 }
@@ -98,6 +104,7 @@ double computePairForce(PairTerm term, const std::vector<Vec3>& pos, const Vec3*
                         const PairParams& params, double lambda, std::vector<Vec3>& forces,
                         int64_t* numInteracting, OpCounter* ops) {
     int n = int(pos.size());
+    lastAbsEnergy() = 0.0;
     bool periodic = (s.method == 2);
     bool useCutoff = (s.method != 0);
     bool useSwitch = useCutoff && s.useSwitch;
@@ -157,6 +164,8 @@ double computePairForce(PairTerm term, const std::vector<Vec3>& pos, const Vec3*
             ops->transcendental += oc.transcendental;
         }
         if (rEff != r) dEdR *= std::pow(r / rEff, 5);
+        // sum of |pair energies| before switching: the error scale of tests/TestInteraxPairForce.h:105-142
+        lastAbsEnergy() += std::fabs((alchPair ? lambda : 1.0) * e);
         if (useSwitch && r > s.switchDistance) {
             double t = (r - s.switchDistance) / (s.cutoff - s.switchDistance);
             double sv = 1 + t * t * t * (-10 + t * (15 - t * 6));
@@ -362,6 +371,7 @@ static double computeC9(double a1, double w1, double a2, double w2, double a3, d
 double computeThreeBody(const std::vector<Vec3>& pos, const Vec3* box, const ThreeBodySettings& s, double lambda,
                         std::vector<Vec3>& forces, int64_t* numTriples, OpCounter* ops) {
     int ns = int(s.siteParticles.size());
+    lastAbsEnergy() = 0.0;
     bool anyAlch = false;
     for (auto a : s.alch) anyAlch |= (a != 0);
     if (!anyAlch) lambda = 1.0;
@@ -416,9 +426,11 @@ double computeThreeBody(const std::vector<Vec3>& pos, const Vec3* box, const Thr
                 double rates[3] = {2 * s.dampingScale / (s.width[i] + s.width[j]),
                                    2 * s.dampingScale / (s.width[i] + s.width[k]),
                                    2 * s.dampingScale / (s.width[j] + s.width[k])};
-                energy += computeTripleT<double>(delta(i, j), delta(i, k), delta(j, k), c9,
-                                                 useDamping ? rates : nullptr, siteForces[i], siteForces[j],
-                                                 siteForces[k], s.centroidRadius);
+                const double et = computeTripleT<double>(delta(i, j), delta(i, k), delta(j, k), c9,
+                                                         useDamping ? rates : nullptr, siteForces[i], siteForces[j],
+                                                         siteForces[k], s.centroidRadius);
+                energy += et;
+                lastAbsEnergy() += std::fabs(et);
                 if (ops) {
                     OpCounter& oc = opCounter();
                     oc = OpCounter();
@@ -480,6 +492,9 @@ static PairSettings toSettings(const ox_pair_settings* s) {
 static char g_error[512];
 
 const char* ox_last_error() { return g_error; }
+
+// Sum of |pair energies| (before switching) or |triple energies| of the last ox_pair_force / ox_three_body call.
+double ox_last_abs_energy() { return lastAbsEnergy(); }
 
 // Energy of one pair force; forces (n x 3) are added to.  term: 0 dispersion (params n x 5: m1 m2 m3 alpha width),
 // 1 exchange (n x 2: amplitude width), 2 short range (n x 3: k l width).  Returns NaN on error.

@@ -39,6 +39,8 @@ def lib():
         L.ox_tang_toennies.argtypes = [ctypes.c_double, P, P]
         L.ox_overlap_taylor_table.argtypes = [P, P]
         L.ox_long_range_coefficients.argtypes = [ctypes.c_int, P, P, P, ctypes.c_double, ctypes.c_int, P, P]
+        L.ox_last_abs_energy.restype = ctypes.c_double
+        L.ox_last_abs_energy.argtypes = []
         _LIB = L
     return _LIB
 
@@ -110,9 +112,11 @@ def term_of(force):
     return None
 
 
-def evaluate(system, positions, box=None, parameters=None, groups=0xFFFFFFFF, per_force=False):
+def evaluate(system, positions, box=None, parameters=None, groups=0xFFFFFFFF, per_force=False, abs_energy=None):
     """The Reference-platform result for a System: total energy and forces of the forces in `groups`.
-    `parameters` maps context parameter names (the alchemical parameters) to values; missing ones default to 1."""
+    `parameters` maps context parameter names (the alchemical parameters) to values; missing ones default to 1.
+    If `abs_energy` is a list, the sum of |pair and triple energies| (before switching; the error scale of the
+    reference's tests, tests/TestInteraxPairForce.h:105-142) is appended to it."""
     parameters = parameters or {}
     if box is None:
         box = system.getDefaultPeriodicBoxVectors()
@@ -120,6 +124,7 @@ def evaluate(system, positions, box=None, parameters=None, groups=0xFFFFFFFF, pe
     energy = 0.0
     forces = np.zeros((n, 3))
     results = []
+    total_abs = 0.0
     for force in system._forces:
         term = term_of(force)
         if term is None or not (groups >> force.getForceGroup()) & 1:
@@ -129,9 +134,12 @@ def evaluate(system, positions, box=None, parameters=None, groups=0xFFFFFFFF, pe
             e, f = three_body(force, positions, box, lam)
         else:
             e, f = pair_force(term, force, positions, box, lam)
+        total_abs += lib().ox_last_abs_energy()
         energy += e
         forces += f
         results.append((force, e, f))
+    if abs_energy is not None:
+        abs_energy.append(total_abs)
     return (energy, forces, results) if per_force else (energy, forces)
 
 

@@ -38,8 +38,13 @@ def max_force_error(f, f_ref):
 
 
 def compare(system, positions, box=None, parameters=None, groups=0xFFFFFFFF, energy_tol=ENERGY_TOL,
-            force_tol=FORCE_RMS_TOL, abs_energy=None, context=None):
-    e_ref, f_ref = pyoracle.evaluate(system, positions, box, parameters, groups)
+            force_tol=FORCE_RMS_TOL, abs_energy=None, context=None, scale="total"):
+    """Compare with the oracle.  scale="total": energy error relative to |E|; scale="abs": relative to the sum of
+    |pair and triple energies|, the error scale of the reference's own tests (tests/TestInteraxPairForce.h:134-142)."""
+    absE = []
+    e_ref, f_ref = pyoracle.evaluate(system, positions, box, parameters, groups, abs_energy=absE)
+    if scale == "abs" and abs_energy is None:
+        abs_energy = max(absE[0], abs(e_ref))
     e, f, ctx = gpu_state(system, positions, box, parameters, groups, context)
     e_err, f_err = errors(e, f, e_ref, f_ref, abs_energy)
     assert np.all(np.isfinite(f))
