@@ -184,6 +184,30 @@ int ix_synchronize(ix_ctx* ctx);
  * tool with no counterpart in the reference. */
 int ix_measure_fp32_peak(int device, double* tflops);
 
+/* Three-body (ATM) energy and forces with no allocation at all; this entry point has no counterpart in the
+ * reference.  It is for callers that cannot call cudaMalloc where they need the forces: code running while a CUDA
+ * graph is being captured (allocation is not allowed inside stream capture), engines whose device memory belongs to
+ * their own pool, and step loops that must not allocate.  All working memory is one fixed file-scope __device__
+ * array (about 2.7 MB on every GPU that loads the library, held until the process exits) that every call shares:
+ * calls that overlap on the GPU race on it, so the caller must serialize them (one stream per device, or an event
+ * between them).  Limits: 16384 particles, 4096 sites, 128 sites above any site within the cutoff (more are dropped
+ * and reported by ix_three_body_noalloc_overflow); larger inputs are rejected with IX_ERR_INVALID.
+ * Inputs and outputs are device pointers on the current CUDA device: d_positions (num_particles x 3 doubles), the
+ * sites as in ix_add_three_body (site particle indices outside [0, num_particles) are ignored), d_forces
+ * (num_particles x 3 doubles, overwritten with the three-body forces) and d_energy (one double).  `box` is a host
+ * pointer (9 doubles, may be NULL when not periodic) and `stream` a cudaStream_t (NULL: the default stream).  The
+ * first call on a device looks up the array's device address (cudaGetSymbolAddress) once; make that first call
+ * before any stream capture.  The call is asynchronous on `stream`. */
+int ix_three_body_noalloc(int num_particles, const double* d_positions, const double* box, int num_sites,
+                          const int32_t* d_site_offsets, const int32_t* d_site_particles,
+                          const double* d_site_params, const int32_t* d_molecule, const uint8_t* d_is_alchemical,
+                          double cutoff, double scale_factor, int damping_method, double damping_scale,
+                          double centroid_damping_radius, int periodic, double lambda, double* d_forces,
+                          double* d_energy, void* stream);
+
+/* Whether the last ix_three_body_noalloc call on the current device dropped neighbors (synchronizes the device). */
+int ix_three_body_noalloc_overflow(int* overflow);
+
 /* Library version string. */
 const char* ix_version(void);
 

@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <set>
 #include <string>
 #include <vector>
@@ -1292,6 +1293,229 @@ int ix_md_run(ix_ctx* ctx, int num_steps, double dt, double* positions, double* 
                                      ctx->stream));
     IX_TRY(ix_md_steps_async(ctx, num_steps, dt));
     return ix_md_finish(ctx, positions, velocities, energy);
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Three-body evaluation without any allocation.
+//
+// Some callers cannot call cudaMalloc at the point where they need the forces: a CUDA graph being captured (an
+// allocation inside stream capture is not allowed), an engine whose device memory is owned by its own pool, or a
+// real-time loop that must not allocate.  For them ix_three_body_noalloc evaluates the three-body force with all its
+// working memory in one file-scope __device__ array of fixed size; the caller passes only its inputs and outputs.
+// Limits: kNoAllocMaxParticles particles, kNoAllocMaxSites sites, kNoAllocMaxNeighbors sites above any site within
+// the cutoff.  The array is allocated by the CUDA runtime when the library is loaded, on every GPU that loads it
+// (about 2.7 MB), and stays until the process exits.  Every call shares it: two calls that overlap on the GPU (on
+// different streams, or from different host threads on one device) race on it and must be serialized by the caller.
+// ---------------------------------------------------------------------------------------------------------------------
+
+namespace {
+
+constexpr int kNoAllocMaxParticles = 16384;
+constexpr int kNoAllocMaxSites = 4096;
+constexpr int kNoAllocMaxNeighbors = 128;
+constexpr int kNoAllocBlocks = 148 * 8;
+
+struct NoAllocScratch {
+    double sitePos[3 * kNoAllocMaxSites];
+    double siteRef[3 * kNoAllocMaxSites];
+    float4 siteParams[kNoAllocMaxSites];
+    int molecule[kNoAllocMaxSites];
+    int nbrCount[kNoAllocMaxSites];
+    int nbr[kNoAllocMaxSites * kNoAllocMaxNeighbors];
+    long long siteForce[3 * kNoAllocMaxSites];
+    long long particleForce[3 * kNoAllocMaxParticles];
+    double energyPartials[kNoAllocBlocks * kAtmWarps];
+    double energy[4];
+    int flag[2];
+    unsigned long long tripleCount;
+};
+
+// The scratch itself.  Host code must not use this name as a pointer: on the host it is only a stand-in for the
+// symbol, and its device address comes from cudaGetSymbolAddress (noAllocScratch() below).
+__device__ __align__(256) unsigned char g_noAllocScratch[sizeof(NoAllocScratch)];
+
+constexpr int kMaxDevices = 64;
+void* g_noAllocAddress[kMaxDevices] = {};
+std::mutex g_noAllocMutex;
+
+// Device address of the scratch on the current device, looked up once per device.
+int noAllocScratch(int device, NoAllocScratch** out) {
+    if (device < 0 || device >= kMaxDevices) return fail(nullptr, IX_ERR_NO_DEVICE, "device index %d out of range", device);
+    std::lock_guard<std::mutex> lock(g_noAllocMutex);
+    if (!g_noAllocAddress[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noAllocScratch);
+        if (e != cudaSuccess)
+            return fail(nullptr, IX_ERR_CUDA, "cudaGetSymbolAddress of the three-body scratch failed: %s",
+                        cudaGetErrorString(e));
+        g_noAllocAddress[device] = p;
+    }
+    *out = reinterpret_cast<NoAllocScratch*>(g_noAllocAddress[device]);
+    return IX_OK;
+}
+
+// Per call: site parameters in the kernels' layout, the effective molecules, and the accumulators cleared.
+__global__ void kNoAllocPrepare(NoAllocScratch* S, int numParticles, int numSites, const double* siteParams,
+                                const int* molecule, const uint8_t* alch) {
+    const int stride = gridDim.x * blockDim.x;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int s = t; s < numSites; s += stride) {
+        S->siteParams[s] = make_float4((float)siteParams[3 * s], (float)siteParams[3 * s + 1],
+                                       (float)siteParams[3 * s + 2], alch[s] ? 1.0f : 0.0f);
+        S->molecule[s] = molecule[s] < 0 ? -1 - s : molecule[s];
+        for (int d = 0; d < 3; d++) {
+            S->siteForce[d * numSites + s] = 0;
+            S->siteRef[3 * s + d] = 0.0;
+        }
+    }
+    for (int i = t; i < 3 * numParticles; i += stride) S->particleForce[i] = 0;
+    if (t == 0) {
+        S->flag[0] = 1;      // always build the neighbor list
+        S->flag[1] = 0;
+        S->tripleCount = 0;
+    }
+}
+
+// Site positions with the particle indices checked (an index outside [0, numParticles) is skipped).
+__global__ void kNoAllocCentroids(NoAllocScratch* S, int numParticles, int numSites, const int* offsets,
+                                  const int* particles, const double* pos) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= numSites) return;
+    double c[3] = {0.0, 0.0, 0.0};
+    int count = 0;
+    for (int k = offsets[s]; k < offsets[s + 1]; k++) {
+        const int p = particles[k];
+        if (p < 0 || p >= numParticles) continue;
+        for (int d = 0; d < 3; d++) c[d] += pos[3 * p + d];
+        count++;
+    }
+    for (int d = 0; d < 3; d++) S->sitePos[3 * s + d] = count ? c[d] / (double)count : 0.0;
+}
+
+__global__ void kNoAllocSpread(NoAllocScratch* S, int numParticles, int numSites, const int* offsets,
+                               const int* particles) {
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= numSites) return;
+    const int b = offsets[s], e = offsets[s + 1];
+    int count = 0;
+    for (int k = b; k < e; k++) count += (particles[k] >= 0 && particles[k] < numParticles);
+    if (!count) return;
+    const double inv = 1.0 / (double)count;
+    for (int d = 0; d < 3; d++) {
+        const long long v = S->siteForce[d * numSites + s];
+        if (v == 0) continue;
+        const long long share = __double2ll_rn((double)v * inv);
+        for (int k = b; k < e; k++) {
+            const int p = particles[k];
+            if (p >= 0 && p < numParticles) atomicAddFixed(S->particleForce + (size_t)d * numParticles + p, share);
+        }
+    }
+}
+
+__global__ void kNoAllocFinish(const NoAllocScratch* S, int numParticles, double* forces) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= numParticles) return;
+    for (int d = 0; d < 3; d++)
+        forces[3 * i + d] = (double)S->particleForce[(size_t)d * numParticles + i] / kFixedScale;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ix_three_body_noalloc(int num_particles, const double* d_positions, const double* box, int num_sites,
+                          const int32_t* d_site_offsets, const int32_t* d_site_particles,
+                          const double* d_site_params, const int32_t* d_molecule, const uint8_t* d_is_alchemical,
+                          double cutoff, double scale_factor, int damping_method, double damping_scale,
+                          double centroid_damping_radius, int periodic, double lambda, double* d_forces,
+                          double* d_energy, void* stream) {
+    if (num_particles <= 0 || num_particles > kNoAllocMaxParticles)
+        return fail(nullptr, IX_ERR_INVALID, "ix_three_body_noalloc: %d particles (the limit is %d)", num_particles,
+                    kNoAllocMaxParticles);
+    if (num_sites < 0 || num_sites > kNoAllocMaxSites)
+        return fail(nullptr, IX_ERR_INVALID, "ix_three_body_noalloc: %d sites (the limit is %d)", num_sites,
+                    kNoAllocMaxSites);
+    if (!d_positions || !d_forces || !d_energy || (num_sites > 0 && (!d_site_offsets || !d_site_particles ||
+                                                                     !d_site_params || !d_molecule ||
+                                                                     !d_is_alchemical)))
+        return fail(nullptr, IX_ERR_INVALID, "ix_three_body_noalloc: null argument");
+    if (periodic && !box) return fail(nullptr, IX_ERR_INVALID, "ix_three_body_noalloc: periodic without a box");
+    if (damping_method != IX_NO_DAMPING && damping_method != IX_TANG_TOENNIES)
+        return fail(nullptr, IX_ERR_INVALID, "InteraxThreeBodyForce: Illegal value for damping method");
+    if (cutoff <= 0) return fail(nullptr, IX_ERR_INVALID, "InteraxThreeBodyForce: The cutoff distance must be positive");
+    if (centroid_damping_radius < 0)
+        return fail(nullptr, IX_ERR_INVALID, "InteraxThreeBodyForce: The centroid damping radius cannot be negative");
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return fail(nullptr, IX_ERR_NO_DEVICE, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+    NoAllocScratch* S = nullptr;
+    IX_TRY(noAllocScratch(device, &S));
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const int tpb = 256;
+    kNoAllocPrepare<<<64, tpb, 0, st>>>(S, num_particles, num_sites, d_site_params, d_molecule, d_is_alchemical);
+    kNoAllocCentroids<<<(num_sites + tpb - 1) / tpb + 1, tpb, 0, st>>>(S, num_particles, num_sites, d_site_offsets,
+                                                                      d_site_particles, d_positions);
+    AtmConfig C{};
+    C.numSites = num_sites;
+    C.periodic = periodic != 0;
+    double unit[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    C.box = makeBox(box ? box : unit);
+    C.boxf = makeBoxF(C.box);
+    C.cutoff2 = (float)(cutoff * cutoff);
+    C.listCutoff2 = C.cutoff2;
+    C.scale = (float)scale_factor;
+    C.lambda = (float)lambda;
+    C.useTangToennies = damping_method == IX_TANG_TOENNIES;
+    C.twoBeta = (float)(2.0 * damping_scale);
+    C.invCentroidRadius = centroid_damping_radius > 0 ? (float)(1.0 / centroid_damping_radius) : 0.0f;
+    C.maxMove2 = 0.0f;
+    AtmBuffers A{};
+    A.siteParams = S->siteParams;
+    A.molecule = S->molecule;
+    A.sitePos = S->sitePos;
+    A.siteRef = S->siteRef;
+    A.flag = S->flag;
+    A.nbrCount = S->nbrCount;
+    A.nbr = S->nbr;
+    A.cap = kNoAllocMaxNeighbors;
+    A.siteForce = S->siteForce;
+    A.particleForce = S->particleForce;
+    A.numParticles = num_particles;
+    A.energyPartials = S->energyPartials;
+    A.tripleCount = &S->tripleCount;
+    if (num_sites > 0) {
+        kSiteNeighbors<<<(num_sites * 32 + tpb - 1) / tpb, tpb, 0, st>>>(A, C);
+        const int blocks = std::max(1, std::min((num_sites + kAtmWarps - 1) / kAtmWarps, kNoAllocBlocks));
+        kTriples<<<blocks, 32 * kAtmWarps, sizeof(AtmWarpStorage) * kAtmWarps, st>>>(A, C);
+        kNoAllocSpread<<<(num_sites + tpb - 1) / tpb, tpb, 0, st>>>(S, num_particles, num_sites, d_site_offsets,
+                                                                   d_site_particles);
+        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, 0, S->energyPartials, blocks * kAtmWarps, 0.0, S->energy);
+    }
+    else {
+        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, 0, nullptr, 0, 0.0, S->energy);
+    }
+    kNoAllocFinish<<<(num_particles + tpb - 1) / tpb, tpb, 0, st>>>(S, num_particles, d_forces);
+    e = cudaMemcpyAsync(d_energy, &S->energy[3], sizeof(double), cudaMemcpyDeviceToDevice, st);
+    if (e != cudaSuccess) return fail(nullptr, IX_ERR_CUDA, "ix_three_body_noalloc: %s", cudaGetErrorString(e));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(nullptr, IX_ERR_CUDA, "ix_three_body_noalloc: %s", cudaGetErrorString(e));
+    return IX_OK;
+}
+
+int ix_three_body_noalloc_overflow(int* overflow) {
+    if (!overflow) return fail(nullptr, IX_ERR_INVALID, "ix_three_body_noalloc_overflow: null argument");
+    int device = 0;
+    cudaError_t e = cudaGetDevice(&device);
+    if (e != cudaSuccess) return fail(nullptr, IX_ERR_NO_DEVICE, "cudaGetDevice failed: %s", cudaGetErrorString(e));
+    NoAllocScratch* S = nullptr;
+    IX_TRY(noAllocScratch(device, &S));
+    int flags[2] = {0, 0};
+    e = cudaMemcpy(flags, S->flag, sizeof(flags), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail(nullptr, IX_ERR_CUDA, "ix_three_body_noalloc_overflow: %s", cudaGetErrorString(e));
+    *overflow = flags[1] != 0;
+    return IX_OK;
 }
 
 }  // extern "C"
