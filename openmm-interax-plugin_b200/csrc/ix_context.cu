@@ -116,7 +116,8 @@ struct ix_ctx {
     float4 *dP0 = nullptr, *dP1 = nullptr, *dP2 = nullptr;
     int* dFlagsSorted = nullptr;
     int tileCap = 0;
-    int pairGridBlocks = 0;
+    int pairGridBlocks = 0;              // persistent grid of the general pair kernel
+    int pairGridBlocksLean = 0;          // and of its lean instantiation
     // three-body
     AtmBuffers A{};
     // MD
@@ -298,6 +299,94 @@ static void computeLrc(ix_ctx* ctx) {
 }
 
 // Per-particle float parameters in original order, with the term flags.
+// Coefficients of one ordered pair of overlap widths (w1, w2 > 0), double precision, rounded once to float.
+static void overlapCoefficients(double w1, double w2, float4& A, float4& B, float& k1, float& k2) {
+    const double a = std::min(w1, w2), b = std::max(w1, w2);
+    const double ia = 1.0 / a, ib = 1.0 / b, h = b - a, s = a + b;
+    const double is3 = 1.0 / (s * s * s);
+    auto split = [](double v, float& hi, float& lo) {
+        hi = (float)v;
+        lo = (float)(v - (double)hi);
+    };
+    split(ia, A.x, A.y);
+    split(ib, A.z, A.w);
+    B = make_float4((float)(ia - ib), (float)is3, (float)(ia * is3), (float)(0.5 * ia * ia * ib / (s * s)));
+    k1 = (float)(h * ia * ia * ia * ib * ib / (s * s));
+    k2 = (float)(4.0 * ia * ib * is3);
+}
+
+// Particles with identical parameters of all pair forces form a class; with at most kMaxClasses classes the kernel
+// reads the coefficients of a pair from a class-pair table instead of recomputing them (see PairCoef).  Sets the
+// class in bits 8..15 of each particle's flags.
+constexpr int kMaxClasses = 16;
+
+static int buildClassTable(ix_ctx* ctx, std::vector<int>& flags) {
+    const int n = ctx->n;
+    ctx->P.coef = nullptr;
+    ctx->P.numClasses = 0;
+    std::map<std::vector<double>, int> classes;
+    std::vector<int> cls(n);
+    std::vector<int> rep;
+    for (int i = 0; i < n; i++) {
+        std::vector<double> key;
+        const int strides[3] = {5, 2, 3};
+        for (int t = 0; t < 3; t++)
+            if (ctx->term[t].present)
+                key.insert(key.end(), ctx->term[t].params.begin() + (size_t)strides[t] * i,
+                           ctx->term[t].params.begin() + (size_t)strides[t] * (i + 1));
+        auto it = classes.find(key);
+        if (it == classes.end()) {
+            if ((int)classes.size() == kMaxClasses) return IX_OK;   // too many classes: per-particle path
+            it = classes.emplace(key, (int)classes.size()).first;
+            rep.push_back(i);
+        }
+        cls[i] = it->second;
+    }
+    const int T = (int)classes.size();
+    std::vector<PairCoef> table((size_t)T * T);
+    const double beta = ctx->term[0].dampingScale;
+    for (int ci = 0; ci < T; ci++)
+        for (int cj = 0; cj < T; cj++) {
+            PairCoef K;
+            std::memset(&K, 0, sizeof(K));
+            const int i = rep[ci], j = rep[cj];
+            if (ctx->term[0].present) {
+                const double* p = &ctx->term[0].params[5 * i];
+                const double* q = &ctx->term[0].params[5 * j];
+                // InteraxPairTerms.h:274-279
+                const double pref = p[3] * q[3] / std::max(p[3] * q[0] + q[3] * p[0], 1e-30);
+                const double c6 = pref * p[0] * q[0];
+                const double c8 = 1.5 * pref * (p[0] * q[1] + p[1] * q[0]);
+                const double c10 = pref * (2.0 * (p[0] * q[2] + p[2] * q[0]) + 4.2 * p[1] * q[1]);
+                const double ws = p[4] + q[4];
+                K.disp = make_float4((float)c6, (float)c8, (float)c10, ws != 0 ? (float)(2.0 * beta / ws) : 0.0f);
+            }
+            if (ctx->term[1].present) {
+                const double* p = &ctx->term[1].params[2 * i];
+                const double* q = &ctx->term[1].params[2 * j];
+                if (p[1] != 0 && q[1] != 0) overlapCoefficients(p[1], q[1], K.ovA, K.ovB, K.ovC.x, K.ovC.y);
+                K.ovC.z = (float)(p[0] * q[0] / (8.0 * M_PI));
+            }
+            if (ctx->term[2].present) {
+                const double* p = &ctx->term[2].params[3 * i];
+                const double* q = &ctx->term[2].params[3 * j];
+                if (p[2] != 0 && q[2] != 0) overlapCoefficients(p[2], q[2], K.srA, K.srB, K.srC.x, K.srC.y);
+                const double ws = p[2] + q[2];
+                K.srC.z = (float)(ws * ws * ws);
+                K.srK = make_float4((float)(0.5 * (p[0] + q[0])), (float)(0.5 * (p[1] + q[1])), 0.0f, 0.0f);
+            }
+            table[(size_t)ci * T + cj] = K;
+        }
+    PairCoef* dTable;
+    IX_TRY(deviceAlloc(ctx, "classTable", table.size(), &dTable));
+    IX_CUDA(ctx, cudaMemcpyAsync(dTable, table.data(), table.size() * sizeof(PairCoef), cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    for (int i = 0; i < n; i++) flags[i] |= cls[i] << kClassShift;
+    ctx->P.coef = dTable;
+    ctx->P.numClasses = T;
+    return IX_OK;
+}
+
 static int uploadPairParams(ix_ctx* ctx) {
     const int n = ctx->n;
     std::vector<float4> p0(n), p1(n), p2(n), p3(n);
@@ -348,6 +437,7 @@ static int uploadPairParams(ix_ctx* ctx) {
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP1o, p1.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP2o, p2.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP3o, p3.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+    IX_TRY(buildClassTable(ctx, flags));
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dFlagso, flags.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     computeLrc(ctx);
@@ -467,6 +557,8 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
     IX_TRY(deviceAlloc(ctx, "exclCounter", 1, &L.exclCounter));
     IX_TRY(deviceAlloc(ctx, "tasks", L.taskCap, &L.tasks));
     IX_TRY(deviceAlloc(ctx, "numTasks", 1, &L.numTasks));
+    IX_TRY(deviceAlloc(ctx, "taskCounter", 1, &L.taskCounter));
+    IX_TRY(deviceAlloc(ctx, "taskEnergy", 3 * (size_t)L.taskCap, &ctx->dPairPartials));
     IX_CUDA(ctx, cudaMemsetAsync(L.numTasks, 0, sizeof(int), ctx->stream));
     L.flag = ctx->dFlags;
     L.pos = ctx->dPos;
@@ -516,10 +608,12 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
     ctx->P.flags = ctx->dFlagsSorted;
     ctx->P.pairCount = ctx->dCounts;
     int perSM = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kPairTiles, 32 * kPairWarps, 0);
+    int perSMLean = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kPairTiles<false, false>, 32 * kPairWarps, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSMLean, kPairTiles<true, true>, 32 * kPairWarps, 0);
     ctx->pairGridBlocks = std::max(1, perSM) * ctx->numSMs;
-    IX_TRY(deviceAlloc(ctx, "pairPartials", 3 * (size_t)ctx->pairGridBlocks * kPairWarps, &ctx->dPairPartials));
-    ctx->P.energyPartials = ctx->dPairPartials;
+    ctx->pairGridBlocksLean = std::max(1, perSMLean) * ctx->numSMs;
+    ctx->P.taskEnergy = ctx->dPairPartials;
     ctx->pairAllocated = true;
     IX_TRY(uploadPairParams(ctx));
     return IX_OK;
@@ -633,13 +727,14 @@ __global__ void kFinalize(int n, int np, const int* slotOf, const long long* pai
 
 // Term energies from the per-warp partials: each thread sums a fixed strided subset, then a fixed reduction tree,
 // so the result is identical on every run.  lrcEnergy (the long range correction, from the host) joins term 0.
-__global__ void kReduceEnergies(const double* pairPartials, int numPairWarps, const double* atmPartials,
-                                int numAtmWarps, double lrcEnergy, double* outEnergy) {
+__global__ void kReduceEnergies(const double* pairPartials, const int* numPairPartials, int pairCap,
+                                const double* atmPartials, int numAtmWarps, double lrcEnergy, double* outEnergy) {
     __shared__ double red[4][256];
     const int t = threadIdx.x;
     double s[4] = {0.0, 0.0, 0.0, 0.0};
+    const int numPair = pairPartials ? min(*numPairPartials, pairCap) : 0;
     if (pairPartials)
-        for (int w = t; w < numPairWarps; w += 256)
+        for (int w = t; w < numPair; w += 256)
             for (int k = 0; k < 3; k++) s[k] += pairPartials[3 * w + k];
     if (atmPartials)
         for (int w = t; w < numAtmWarps; w += 256) s[3] += atmPartials[w];
@@ -693,7 +788,17 @@ static PairTermConfig pairConfig(const ix_ctx* ctx, unsigned terms) {
     double tc = ctx->cutoff * (1.0 + 1e-5) + 1e-5;
     C.testCutoff2 = (float)(tc * tc);
     C.box = ctx->G.box;
-    C.boxf = ctx->G.boxf;
+    for (int k = 0; k < 3; k++) {
+        const double v[3] = {C.box.a[k], C.box.b[k], C.box.c[k]};
+        float* hi[3] = {C.boxff.a, C.boxff.b, C.boxff.c};
+        float* lo[3] = {C.boxff.aLo, C.boxff.bLo, C.boxff.cLo};
+        for (int m = 0; m < 3; m++) {
+            hi[m][k] = (float)v[m];
+            lo[m][k] = (float)(v[m] - (double)hi[m][k]);
+        }
+        C.boxff.inv[k] = (float)C.box.inv[k];
+    }
+    C.boxff.triclinic = C.box.triclinic;
     return C;
 }
 
@@ -726,7 +831,7 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         kGatherParams<<<gNp, tpb, 0, st>>>(L, ctx->dP0o, ctx->dP1o, ctx->dP2o, ctx->dP3o, ctx->dFlagso, ctx->dP0,
                                            ctx->dP1, ctx->dP2, ctx->dP3, ctx->dFlagsSorted);
         kUpdateSortedPositions<<<gNp, tpb, 0, st>>>(L);
-        kBlockBounds<<<(L.nb * 32 + tpb - 1) / tpb, tpb, 0, st>>>(L);
+        kBlockBounds<<<(L.nb * 32 + tpb - 1) / tpb, tpb, 0, st>>>(L, ctx->G);
         const int warpsPerBlock = 8;
         const int gB = (L.nb + warpsPerBlock - 1) / warpsPerBlock;
         kBuildTiles<0><<<gB, 32 * warpsPerBlock, 0, st>>>(L, ctx->G);
@@ -735,8 +840,21 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         kClearFlag<<<1, 1, 0, st>>>(L.flag);
         IX_CUDA(ctx, cudaMemsetAsync(ctx->P.forceFixed, 0, 3 * (size_t)L.np * sizeof(long long), st));
         PairTermConfig C = pairConfig(ctx, terms);
+        // the lean instantiation when no selected term has a soft core, a switching function or the order-2 overlap
+        bool lean = true;
+        for (int t = 0; t < 3; t++)
+            if ((terms >> t) & 1u) lean = lean && C.softShift[t] == 0.0f && !C.useSwitch[t] && C.overlapMethod[t] == 0;
+        IX_CUDA(ctx, cudaMemsetAsync(L.taskCounter, 0, sizeof(int), st));
         if (ctx->profiling) cudaEventRecord(ctx->ev[0], st);
-        kPairTiles<<<ctx->pairGridBlocks, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        // the class-pair table serves the exact overlap method only
+        bool table = ctx->P.coef != nullptr;
+        for (int t = 1; t < 3; t++)
+            if ((terms >> t) & 1u) table = table && C.overlapMethod[t] == 0;
+        const int grid = lean ? ctx->pairGridBlocksLean : ctx->pairGridBlocks;
+        if (lean && table) kPairTiles<true, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        else if (lean) kPairTiles<true, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        else if (table) kPairTiles<false, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        else kPairTiles<false, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
         ctx->launches += ctx->G.periodic ? 15 : 16;
         if (ctx->profiling) cudaEventRecord(ctx->ev[1], st);
         ctx->evPair = ctx->profiling;
@@ -783,7 +901,7 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
     }
     kFinalize<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->L.np, ctx->L.slotOf, doPair ? ctx->P.forceFixed : nullptr,
                                               doAtm ? ctx->A.particleForce : nullptr, outForces, addFixed, stride);
-    kReduceEnergies<<<1, 256, 0, st>>>(doPair ? ctx->dPairPartials : nullptr, ctx->pairGridBlocks * kPairWarps,
+    kReduceEnergies<<<1, 256, 0, st>>>(doPair ? ctx->dPairPartials : nullptr, ctx->L.numTasks, ctx->L.taskCap,
                                        doAtm ? ctx->dAtmPartials : nullptr, ctx->atmGridBlocks * kAtmWarps,
                                        lrcEnergy, outEnergy);
     ctx->launches += 2;
@@ -1491,10 +1609,10 @@ int ix_three_body_noalloc(int num_particles, const double* d_positions, const do
         kTriples<<<blocks, 32 * kAtmWarps, sizeof(AtmWarpStorage) * kAtmWarps, st>>>(A, C);
         kNoAllocSpread<<<(num_sites + tpb - 1) / tpb, tpb, 0, st>>>(S, num_particles, num_sites, d_site_offsets,
                                                                    d_site_particles);
-        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, 0, S->energyPartials, blocks * kAtmWarps, 0.0, S->energy);
+        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, nullptr, 0, S->energyPartials, blocks * kAtmWarps, 0.0, S->energy);
     }
     else {
-        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, 0, nullptr, 0, 0.0, S->energy);
+        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, nullptr, 0, nullptr, 0, 0.0, S->energy);
     }
     kNoAllocFinish<<<(num_particles + tpb - 1) / tpb, tpb, 0, st>>>(S, num_particles, d_forces);
     e = cudaMemcpyAsync(d_energy, &S->energy[3], sizeof(double), cudaMemcpyDeviceToDevice, st);

@@ -13,7 +13,7 @@
 
 namespace ix {
 
-constexpr int kTaskTiles = 8;        // tiles of one i-block handled by one warp task
+constexpr int kTaskTiles = 1;        // tiles of one i-block handled by one warp task (small tasks: short tail)
 constexpr float kPairSkin = 0.1f;    // nm; rebuild when a particle has moved by more than half of it
 
 // Frame shared by the build and evaluation kernels.
@@ -60,6 +60,7 @@ struct ListBuffers {
     int* exclCounter;
     int2* tasks;                // taskCap: (first tile, number of tiles)
     int* numTasks;
+    int* taskCounter;           // next task of the pair kernel's dynamic schedule (zeroed before each launch)
     int tileCap, exclCap, taskCap;
     // exclusions (original indices), CSR with sorted partners and their range
     const int* exclStart;
@@ -265,7 +266,11 @@ __global__ void kUpdateSortedPositions(ListBuffers L) {
 }
 
 // Bounding box of each block (one warp per block), from the build-time positions.
-__global__ void kBlockBounds(ListBuffers L) {
+// The center's w is 1 when the block's tiles may place each j particle once, at its minimum image relative to the
+// block center, instead of taking the minimum image of every pair: that holds in a rectangular periodic box when
+// half of every box length exceeds the block's half extent plus the list cutoff plus the skin (room for the motion
+// between rebuilds), since then no interacting pair can need a different image.
+__global__ void kBlockBounds(ListBuffers L, ListGeometry G) {
     if (!rebuildRequested(L)) return;
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     int lane = threadIdx.x & 31;
@@ -274,8 +279,16 @@ __global__ void kBlockBounds(ListBuffers L) {
     float lo[3] = {warpMinF(p.x), warpMinF(p.y), warpMinF(p.z)};
     float hi[3] = {warpMaxF(p.x), warpMaxF(p.y), warpMaxF(p.z)};
     if (lane == 0) {
-        L.bbox[2 * warp] = make_float4(0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1]), 0.5f * (lo[2] + hi[2]), 0.0f);
-        L.bbox[2 * warp + 1] = make_float4(0.5f * (hi[0] - lo[0]), 0.5f * (hi[1] - lo[1]), 0.5f * (hi[2] - lo[2]), 0.0f);
+        const float half[3] = {0.5f * (hi[0] - lo[0]), 0.5f * (hi[1] - lo[1]), 0.5f * (hi[2] - lo[2])};
+        float shift = 0.0f;
+        if (G.periodic && !G.box.triclinic) {
+            const float len[3] = {(float)G.box.a[0], (float)G.box.b[1], (float)G.box.c[2]};
+            bool ok = true;
+            for (int d = 0; d < 3; d++) ok = ok && (half[d] + G.listCutoff + kPairSkin < 0.4999f * len[d]);
+            shift = ok ? 1.0f : 0.0f;
+        }
+        L.bbox[2 * warp] = make_float4(0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1]), 0.5f * (lo[2] + hi[2]), shift);
+        L.bbox[2 * warp + 1] = make_float4(half[0], half[1], half[2], 0.0f);
     }
 }
 

@@ -2,17 +2,22 @@
 // tile list (the reference runs them as snippets of OpenMM's nonbonded kernel in one pass,
 // platforms/common/src/CommonInteraxKernels.cpp:139-219, kernels interaxPairBegin.cc / interaxPairEnd.cc).
 //
-// One warp processes one task (up to kTaskTiles tiles of the same i-block).  Per tile:
-//   1. the 32 i and 32 j particles are staged in shared memory (double positions, float parameters);
-//   2. test phase: the 32 x 32 pairs are tested in rotation order (lane l, rotation k pairs i = l with slot
-//      j = (l + k) mod 32) with float positions and a small margin, and the candidates are compacted into a
-//      per-warp queue with ballots, so that the expensive phase runs with every lane busy;
-//   3. compute phase: each lane takes one queued pair, forms the displacement in double precision (minimum image in
-//      double), applies the exact cutoff test, evaluates the three terms in float and accumulates the pair force on
-//      i and j in shared memory;
-//   4. the j forces are added to the global 64-bit fixed-point force buffer (scale 2^32); the i forces once per task.
-// Energies accumulate per lane in double and are added in fixed point, so the result does not depend on the order in
-// which warps run.
+// Work is split into tasks of up to kTaskTiles tiles of one i-block; warps take tasks from a counter in global
+// memory until none is left (dynamic balance).  Per task and tile:
+//   1. staging: the 32 i particles (once per task) and the tile's 32 j particles are written to shared memory as
+//      float-float offsets from the i-block's center (the double-precision difference split into a float and its
+//      float remainder), with the float parameters.  In large rectangular boxes each j particle is placed at its
+//      minimum image relative to the block center here, once, instead of per pair;
+//   2. test phase: the 32 x 32 pairs are tested in rotation order (lane l, rotation k: i = l, j slot = (l + k) mod 32)
+//      in float with a small margin, and the candidates are compacted into a per-warp queue with ballots, so that
+//      the expensive phase runs with every lane busy;
+//   3. compute phase: each lane takes one queued pair, forms the displacement as (xj - xi) + (lo_j - lo_i) (the
+//      precision of the double difference, without double arithmetic), applies the exact cutoff test (borderline
+//      cases decided in double), evaluates the three terms in float and accumulates the pair force on i and j in
+//      shared memory;
+//   4. the j forces go to the global 64-bit fixed-point force buffer (scale 2^32) after each tile, the i forces after
+//      each task; each task's energies, summed per lane in double, are written to a per-task slot and summed in a
+//      fixed order afterwards.  Results do not depend on which warp ran which task.
 #pragma once
 
 #include "ix_nblist.cuh"
@@ -25,6 +30,14 @@ constexpr int kFlagReal = 1 << 3;
 constexpr int kFlagGateDisp = 1 << 4;    // alpha != 0
 constexpr int kFlagGateExch = 1 << 5;    // exchange width != 0
 constexpr int kFlagGateSr = 1 << 6;      // short-range width != 0
+
+// Periodic box as float-float vectors (for minimum images of float-float displacements).
+struct BoxFF {
+    float a[3], b[3], c[3];
+    float aLo[3], bLo[3], cLo[3];
+    float inv[3];
+    int triclinic;
+};
 
 struct PairTermConfig {
     int termMask;                // bit t: term t is evaluated in this call
@@ -39,7 +52,7 @@ struct PairTermConfig {
     float cutoff2, testCutoff2;
     double cutoff;
     Box box;
-    BoxF boxf;
+    BoxFF boxff;
 };
 
 struct PairBuffers {
@@ -49,15 +62,23 @@ struct PairBuffers {
     const float4* p3;            // sorted: the float remainders of p2's four values (float-float widths)
     const int* flags;            // sorted
     long long* forceFixed;       // 3 x np, sorted order, SoA
-    double* energyPartials;      // 3 per warp of the grid, summed in a fixed order afterwards
+    double* taskEnergy;          // 3 per task, summed in a fixed order afterwards
     unsigned long long* pairCount;
+    const PairCoef* coef;        // class-pair coefficients (numClasses^2), or null
+    int numClasses;
 };
 
+// Bits 8..15 of a particle's flags hold its parameter class when the class tables are in use.
+constexpr int kClassShift = 8;
+
 // Every pair term of one pair.  r, invR: distance; fi, fj: flags.  Adds each term's scaled energy to e[] and returns
-// the scaled dE/dr of all terms.
-__device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, float invR, float4 a0, float4 a1,
-                                           float4 a2, float4 a3, int fi, float4 b0, float4 b1, float4 b2,
-                                           float4 b3, int fj, bool iFirst, float e[3]) {
+// the scaled dE/dr of all terms.  LEAN: the configuration has no soft core, no switching function and no order-2
+// overlap, so those paths are compiled out.
+template <bool LEAN>
+__device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, float invR, const float4& a0,
+                                           const float4& a1, const float4& a2, const float4& a3, int fi,
+                                           const float4& b0, const float4& b1, const float4& b2, const float4& b3,
+                                           int fj, bool iFirst, float e[3]) {
     float dTotal = 0.0f;
     float shared8pi = 0.0f, sharedD8pi = 0.0f, sharedR = -1.0f;
 #pragma unroll
@@ -67,7 +88,7 @@ __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, flo
         if (!(fi & fj & gate)) continue;
         const bool alch = ((fi ^ fj) >> t) & 1;
         float rEff = r, invEff = invR, scR = 1.0f;
-        if (alch && C.softShift[t] > 0.0f) {
+        if (!LEAN && alch && C.softShift[t] > 0.0f) {
             // r_eff = (r^6 + (1 - lambda) R^6)^(1/6), dE/dr picks up (r/r_eff)^5 (interaxPairBegin.cc, interaxPairEnd.cc)
             const float r2 = r * r;
             const float u = fmaf(r2 * r2, r2, C.softShift[t]);
@@ -87,16 +108,15 @@ __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, flo
                 s8pi = shared8pi;
                 ds8pi = sharedD8pi;
             }
-            else if (t == 1) {
-                overlap8pi(rEff, Width{a2.x, a3.x, a2.y, a3.y}, Width{b2.x, b3.x, b2.y, b3.y}, C.overlapMethod[1],
-                           iFirst, s8pi, ds8pi);
-                shared8pi = s8pi;
-                sharedD8pi = ds8pi;
-                sharedR = rEff;
-            }
             else {
-                overlap8pi(rEff, Width{a2.z, a3.z, a2.w, a3.w}, Width{b2.z, b3.z, b2.w, b3.w}, C.overlapMethod[2],
-                           iFirst, s8pi, ds8pi);
+                const Width Wi = t == 1 ? Width{a2.x, a3.x, a2.y, a3.y} : Width{a2.z, a3.z, a2.w, a3.w};
+                const Width Wj = t == 1 ? Width{b2.x, b3.x, b2.y, b3.y} : Width{b2.z, b3.z, b2.w, b3.w};
+                overlap8pi(rEff, Wi, Wj, LEAN ? 0 : C.overlapMethod[t], iFirst, s8pi, ds8pi);
+                if (t == 1) {
+                    shared8pi = s8pi;
+                    sharedD8pi = ds8pi;
+                    sharedR = rEff;
+                }
             }
             if (t == 1) {
                 // exchange A_i A_j S (InteraxPairTerms.h:305-312)
@@ -115,13 +135,15 @@ __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, flo
                 D = fmaf(2.0f * l, st, k) * norm * ds8pi;
             }
         }
-        D *= scR;
-        if (C.useSwitch[t] && r > C.switchDist[t]) {
-            const float x = (r - C.switchDist[t]) * C.invSwitchWidth[t];
-            const float sv = fmaf(x * x * x, fmaf(x, fmaf(-6.0f, x, 15.0f), -10.0f), 1.0f);
-            const float sd = x * x * fmaf(x, fmaf(-30.0f, x, 60.0f), -30.0f) * C.invSwitchWidth[t];
-            D = fmaf(D, sv, E * sd);
-            E *= sv;
+        if (!LEAN) {
+            D *= scR;
+            if (C.useSwitch[t] && r > C.switchDist[t]) {
+                const float x = (r - C.switchDist[t]) * C.invSwitchWidth[t];
+                const float sv = fmaf(x * x * x, fmaf(x, fmaf(-6.0f, x, 15.0f), -10.0f), 1.0f);
+                const float sd = x * x * fmaf(x, fmaf(-30.0f, x, 60.0f), -30.0f) * C.invSwitchWidth[t];
+                D = fmaf(D, sv, E * sd);
+                E *= sv;
+            }
         }
         const float scale = alch ? C.lambda[t] : 1.0f;
         e[t] = fmaf(scale, E, e[t]);
@@ -130,45 +152,145 @@ __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, flo
     return dTotal;
 }
 
+// The same from the pair's class coefficients (see PairCoef).  Only the exact overlap method.
+template <bool LEAN>
+__device__ __forceinline__ float pairTermsTable(const PairTermConfig& C, float r, float invR, const PairCoef* K,
+                                                int fi, int fj, float e[3]) {
+    float dTotal = 0.0f;
+    float shared8pi = 0.0f, sharedD8pi = 0.0f, sharedR = -1.0f;
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+        if (!((C.termMask >> t) & 1)) continue;
+        const int gate = t == 0 ? kFlagGateDisp : (t == 1 ? kFlagGateExch : kFlagGateSr);
+        if (!(fi & fj & gate)) continue;
+        const bool alch = ((fi ^ fj) >> t) & 1;
+        float rEff = r, invEff = invR, scR = 1.0f;
+        if (!LEAN && alch && C.softShift[t] > 0.0f) {
+            const float r2 = r * r;
+            const float u = fmaf(r2 * r2, r2, C.softShift[t]);
+            rEff = ex2Approx(lg2Approx(u) * (1.0f / 6.0f));
+            invEff = rcpApprox(rEff);
+            const float q = r * invEff;
+            const float q2 = q * q;
+            scR = q2 * q2 * q;
+        }
+        float E, D;
+        if (t == 0) {
+            dispersionFromCoef(rEff, invEff, __ldg(&K->disp), E, D);
+        }
+        else if (t == 1) {
+            const float4 c = __ldg(&K->ovC);
+            float s8pi, ds8pi;
+            overlapFromCoef(rEff, __ldg(&K->ovA), __ldg(&K->ovB), c.x, c.y, s8pi, ds8pi);
+            shared8pi = s8pi;
+            sharedD8pi = ds8pi;
+            sharedR = rEff;
+            E = c.z * s8pi;
+            D = c.z * ds8pi;
+        }
+        else {
+            const float4 c = __ldg(&K->srC), kl = __ldg(&K->srK);
+            float s8pi, ds8pi;
+            if (C.shareOverlap && rEff == sharedR) {
+                s8pi = shared8pi;
+                ds8pi = sharedD8pi;
+            }
+            else overlapFromCoef(rEff, __ldg(&K->srA), __ldg(&K->srB), c.x, c.y, s8pi, ds8pi);
+            const float st = c.z * s8pi;
+            E = fmaf(kl.y, st, kl.x) * st;
+            D = fmaf(2.0f * kl.y, st, kl.x) * c.z * ds8pi;
+        }
+        if (!LEAN) {
+            D *= scR;
+            if (C.useSwitch[t] && r > C.switchDist[t]) {
+                const float x = (r - C.switchDist[t]) * C.invSwitchWidth[t];
+                const float sv = fmaf(x * x * x, fmaf(x, fmaf(-6.0f, x, 15.0f), -10.0f), 1.0f);
+                const float sd = x * x * fmaf(x, fmaf(-30.0f, x, 60.0f), -30.0f) * C.invSwitchWidth[t];
+                D = fmaf(D, sv, E * sd);
+                E *= sv;
+            }
+        }
+        const float scale = alch ? C.lambda[t] : 1.0f;
+        e[t] = fmaf(scale, E, e[t]);
+        dTotal = fmaf(scale, D, dTotal);
+    }
+    return dTotal;
+}
+
+// Minimum image of a float-float displacement (hi, lo), c then b then a as the reference's
+// ReferenceForce::getDeltaRPeriodic; the image is chosen from the float part.
+__device__ __forceinline__ void minimumImageFF(float& xh, float& xl, float& yh, float& yl, float& zh, float& zl,
+                                               const BoxFF& B) {
+    float s = floorf(fmaf(zh, B.inv[2], 0.5f));
+    xh -= s * B.c[0];
+    xl -= s * B.cLo[0];
+    yh -= s * B.c[1];
+    yl -= s * B.cLo[1];
+    zh -= s * B.c[2];
+    zl -= s * B.cLo[2];
+    s = floorf(fmaf(yh, B.inv[1], 0.5f));
+    xh -= s * B.b[0];
+    xl -= s * B.bLo[0];
+    yh -= s * B.b[1];
+    yl -= s * B.bLo[1];
+    s = floorf(fmaf(xh, B.inv[0], 0.5f));
+    xh -= s * B.a[0];
+    xl -= s * B.aLo[0];
+}
+
+__device__ __forceinline__ void minimumImageHi(float& x, float& y, float& z, const BoxFF& B) {
+    float s = floorf(fmaf(z, B.inv[2], 0.5f));
+    x -= s * B.c[0];
+    y -= s * B.c[1];
+    z -= s * B.c[2];
+    s = floorf(fmaf(y, B.inv[1], 0.5f));
+    x -= s * B.b[0];
+    y -= s * B.b[1];
+    s = floorf(fmaf(x, B.inv[0], 0.5f));
+    x -= s * B.a[0];
+}
+
+// Per-warp shared memory of the pair kernel (about 4.3 KB, so that eight 4-warp blocks fit on an SM).  Parameters
+// are not staged: the compute phase reads them through the read-only cache by sorted slot.
 struct PairWarpStorage {
-    double x[2][32], y[2][32], z[2][32];
-    float4 pf[2][32];
-    float4 a0[2][32], a1[2][32], a2[2][32], a3[2][32];
-    int flags[2][32], orig[2][32], slot[2][32];
+    float4 hi[2][32];            // position offsets from the i-block center (float part); side 0 = i, 1 = j
+    float4 lo[2][32];            // their float remainders
+    int flags[2][32];
+    int jslot[32];               // sorted slot of each j particle, -1 for padding
     float fx[2][32], fy[2][32], fz[2][32];
-    unsigned short queue[1024];
+    unsigned short queue[512];   // candidates of half a tile (16 rotations)
 };
 
 constexpr int kPairWarps = 4;
 
-__device__ __forceinline__ void stageParticle(PairWarpStorage& S, int side, int lane, int s, const ListBuffers& L,
-                                              const PairBuffers& P) {
+__device__ __forceinline__ void stageParticle(PairWarpStorage& S, int side, int lane, int s, double cx, double cy,
+                                              double cz, bool shiftImage, const PairTermConfig& C,
+                                              const ListBuffers& L, const PairBuffers& P) {
     if (s >= 0) {
-        S.x[side][lane] = L.spos[3 * s];
-        S.y[side][lane] = L.spos[3 * s + 1];
-        S.z[side][lane] = L.spos[3 * s + 2];
-        S.pf[side][lane] = L.sposf[s];
-        S.a0[side][lane] = P.p0[s];
-        S.a1[side][lane] = P.p1[s];
-        S.a2[side][lane] = P.p2[s];
-        S.a3[side][lane] = P.p3[s];
+        double x = L.spos[3 * s] - cx, y = L.spos[3 * s + 1] - cy, z = L.spos[3 * s + 2] - cz;
+        if (shiftImage) {
+            // rectangular box (the shift is only enabled there)
+            x -= C.box.a[0] * rint(x * C.box.inv[0]);
+            y -= C.box.b[1] * rint(y * C.box.inv[1]);
+            z -= C.box.c[2] * rint(z * C.box.inv[2]);
+        }
+        const float xh = (float)x, yh = (float)y, zh = (float)z;
+        S.hi[side][lane] = make_float4(xh, yh, zh, 0.0f);
+        S.lo[side][lane] = make_float4((float)(x - xh), (float)(y - yh), (float)(z - zh), 0.0f);
         S.flags[side][lane] = P.flags[s];
-        S.orig[side][lane] = L.sortedAtom[s];
-        S.slot[side][lane] = s;
     }
     else {
         S.flags[side][lane] = 0;
-        S.orig[side][lane] = -1;
-        S.slot[side][lane] = -1;
-        S.pf[side][lane] = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+        S.hi[side][lane] = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
+        S.lo[side][lane] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
+    if (side == 1) S.jslot[lane] = s;
     S.fx[side][lane] = 0.0f;
     S.fy[side][lane] = 0.0f;
     S.fz[side][lane] = 0.0f;
 }
 
-__device__ __forceinline__ void flushForce(const PairWarpStorage& S, int side, int lane, int np, long long* F) {
-    const int s = S.slot[side][lane];
+__device__ __forceinline__ void flushForce(const PairWarpStorage& S, int side, int lane, int s, int np, long long* F) {
     if (s < 0) return;
     const float fx = S.fx[side][lane], fy = S.fy[side][lane], fz = S.fz[side][lane];
     if (fx != 0.0f) atomicAddFixed(F + s, toFixed(fx));
@@ -176,102 +298,129 @@ __device__ __forceinline__ void flushForce(const PairWarpStorage& S, int side, i
     if (fz != 0.0f) atomicAddFixed(F + 2 * np + s, toFixed(fz));
 }
 
-__global__ void __launch_bounds__(32 * kPairWarps) kPairTiles(ListBuffers L, PairBuffers P, PairTermConfig C) {
+// One queued pair: displacement, exact cutoff test, the terms, and the force on i and j (shared memory).
+template <bool LEAN, bool TABLE>
+__device__ __forceinline__ void computeQueuedPair(PairWarpStorage& S, int entry, int iBase, bool perPairImage,
+                                                  const PairTermConfig& C, const ListBuffers& L,
+                                                  const PairBuffers& P, float e[3], unsigned long long& pairs) {
+    const int i = entry >> 5, j = entry & 31;
+    const float4 hi_i = S.hi[0][i], hi_j = S.hi[1][j], lo_i = S.lo[0][i], lo_j = S.lo[1][j];
+    float dxh = hi_j.x - hi_i.x, dyh = hi_j.y - hi_i.y, dzh = hi_j.z - hi_i.z;
+    float dxl = lo_j.x - lo_i.x, dyl = lo_j.y - lo_i.y, dzl = lo_j.z - lo_i.z;
+    if (perPairImage) minimumImageFF(dxh, dxl, dyh, dyl, dzh, dzl, C.boxff);
+    const float dx = dxh + dxl, dy = dyh + dyl, dz = dzh + dzl;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    bool inside = true;
+    if (C.useCutoff) {
+        inside = r2 < C.cutoff2;
+        if (fabsf(r2 - C.cutoff2) < 1e-5f * C.cutoff2) {
+            // decide as the reference does, on the double precision distance
+            double ddx = ((double)hi_j.x - (double)hi_i.x) + ((double)lo_j.x - (double)lo_i.x);
+            double ddy = ((double)hi_j.y - (double)hi_i.y) + ((double)lo_j.y - (double)lo_i.y);
+            double ddz = ((double)hi_j.z - (double)hi_i.z) + ((double)lo_j.z - (double)lo_i.z);
+            if (perPairImage) minimumImage(ddx, ddy, ddz, C.box);
+            const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz));
+            inside = sqrt(r2d) < C.cutoff;
+        }
+    }
+    const int fi = S.flags[0][i], fj = S.flags[1][j];
+    if (!inside || !(fi & fj & (kFlagGateDisp | kFlagGateExch | kFlagGateSr))) return;
+    float invR;
+    const float r = sqrtRefined(r2, invR);
+    float dEdR;
+    if (TABLE) {
+        const int ci = (fi >> kClassShift) & 0xff, cj = (fj >> kClassShift) & 0xff;
+        dEdR = pairTermsTable<LEAN>(C, r, invR, P.coef + ci * P.numClasses + cj, fi, fj, e);
+    }
+    else {
+        const int si = iBase + i, sj = S.jslot[j];
+        const float4 a0 = __ldg(P.p0 + si), a1 = __ldg(P.p1 + si), a2 = __ldg(P.p2 + si), a3 = __ldg(P.p3 + si);
+        const float4 b0 = __ldg(P.p0 + sj), b1 = __ldg(P.p1 + sj), b2 = __ldg(P.p2 + sj), b3 = __ldg(P.p3 + sj);
+        // InteraxOrder2 expands about the width of the particle with the lower original index
+        const bool iFirst = LEAN ? true : __ldg(L.sortedAtom + si) < __ldg(L.sortedAtom + sj);
+        dEdR = pairTerms<LEAN>(C, r, invR, a0, a1, a2, a3, fi, b0, b1, b2, b3, fj, iFirst, e);
+    }
+    const float fs = dEdR * invR;
+    const float fxv = dx * fs, fyv = dy * fs, fzv = dz * fs;
+    atomicAdd(&S.fx[0][i], fxv);
+    atomicAdd(&S.fy[0][i], fyv);
+    atomicAdd(&S.fz[0][i], fzv);
+    atomicAdd(&S.fx[1][j], -fxv);
+    atomicAdd(&S.fy[1][j], -fyv);
+    atomicAdd(&S.fz[1][j], -fzv);
+    pairs++;
+}
+
+template <bool LEAN, bool TABLE>
+__global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, PairBuffers P, PairTermConfig C) {
     __shared__ PairWarpStorage storage[kPairWarps];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     PairWarpStorage& S = storage[warp];
     const int numTasks = min(*L.numTasks, L.taskCap);
-    double eAcc[3] = {0.0, 0.0, 0.0};
     unsigned long long pairs = 0;
-    for (int task = blockIdx.x * kPairWarps + warp; task < numTasks; task += gridDim.x * kPairWarps) {
+    for (;;) {
+        int task = 0;
+        if (lane == 0) task = atomicAdd(L.taskCounter, 1);
+        task = __shfl_sync(0xffffffffu, task, 0);
+        if (task >= numTasks) break;
         const int2 tk = L.tasks[task];
         const int I = L.tileIBlock[tk.x];
+        const int iBase = I * 32;
+        const float4 center = L.bbox[2 * I];
+        const bool shiftImage = C.periodic && center.w != 0.0f;
+        const bool perPairImage = C.periodic && !shiftImage;
+        const double cx = center.x, cy = center.y, cz = center.z;
         __syncwarp();
-        stageParticle(S, 0, lane, I * 32 + lane, L, P);
+        stageParticle(S, 0, lane, iBase + lane, cx, cy, cz, false, C, L, P);
+        double eAcc[3] = {0.0, 0.0, 0.0};
         for (int t = tk.x; t < tk.x + tk.y; t++) {
             const int jslot = L.tileJ[32 * t + lane];
             const int ex = L.tileExcl[t];
             const unsigned excl = ex >= 0 ? L.exclMasks[32 * ex + lane] : 0u;
             __syncwarp();
-            stageParticle(S, 1, lane, jslot, L, P);
+            stageParticle(S, 1, lane, jslot, cx, cy, cz, shiftImage, C, L, P);
             __syncwarp();
-            // test phase
-            const float4 xi = S.pf[0][lane];
-            const int si = S.slot[0][lane];
+            const float4 xi = S.hi[0][lane];
+            const int si = iBase + lane;
             const int fiTest = S.flags[0][lane];
-            int qn = 0;
-#pragma unroll 4
-            for (int k = 0; k < 32; k++) {
-                const int jj = (lane + k) & 31;
-                const float4 xj = S.pf[1][jj];
-                bool valid = (fiTest & S.flags[1][jj] & kFlagReal) && S.slot[1][jj] > si && !((excl >> jj) & 1u);
-                if (C.useCutoff) {
-                    float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-                    if (C.periodic) minimumImageF(dx, dy, dz, C.boxf);
-                    valid = valid && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < C.testCutoff2;
-                }
-                const unsigned bal = __ballot_sync(0xffffffffu, valid);
-                if (valid) S.queue[qn + __popc(bal & laneMaskLt())] = (unsigned short)((lane << 5) | jj);
-                qn += __popc(bal);
-            }
-            __syncwarp();
-            // compute phase
             float e[3] = {0.0f, 0.0f, 0.0f};
-            for (int q = 0; q < qn; q += 32) {
-                if (q + lane < qn) {
-                    const int entry = S.queue[q + lane];
-                    const int i = entry >> 5, j = entry & 31;
-                    double dxd = S.x[1][j] - S.x[0][i];
-                    double dyd = S.y[1][j] - S.y[0][i];
-                    double dzd = S.z[1][j] - S.z[0][i];
-                    if (C.periodic) minimumImage(dxd, dyd, dzd, C.box);
-                    const float dx = (float)dxd, dy = (float)dyd, dz = (float)dzd;
-                    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                    bool inside = true;
+            for (int half = 0; half < 2; half++) {
+                // test phase over 16 rotations
+                int qn = 0;
+#pragma unroll 4
+                for (int k = 16 * half; k < 16 * half + 16; k++) {
+                    const int jj = (lane + k) & 31;
+                    const float4 xj = S.hi[1][jj];
+                    bool valid = (fiTest & S.flags[1][jj] & kFlagReal) && S.jslot[jj] > si && !((excl >> jj) & 1u);
                     if (C.useCutoff) {
-                        inside = r2 < C.cutoff2;
-                        if (fabsf(r2 - C.cutoff2) < 1e-5f * C.cutoff2) {
-                            // decide as the reference does, on the double precision distance
-                            const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(dxd, dxd), __dmul_rn(dyd, dyd)),
-                                                         __dmul_rn(dzd, dzd));
-                            inside = sqrt(r2d) < C.cutoff;
-                        }
+                        float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
+                        if (perPairImage) minimumImageHi(dx, dy, dz, C.boxff);
+                        valid = valid && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < C.testCutoff2;
                     }
-                    const int fi = S.flags[0][i], fj = S.flags[1][j];
-                    if (inside && (fi & fj & (kFlagGateDisp | kFlagGateExch | kFlagGateSr))) {
-                        float invR;
-                        const float r = sqrtRefined(r2, invR);
-                        const float dEdR = pairTerms(C, r, invR, S.a0[0][i], S.a1[0][i], S.a2[0][i], S.a3[0][i],
-                                                     fi, S.a0[1][j], S.a1[1][j], S.a2[1][j], S.a3[1][j], fj,
-                                                     S.orig[0][i] < S.orig[1][j], e);
-                        const float fs = dEdR * invR;
-                        const float fxv = dx * fs, fyv = dy * fs, fzv = dz * fs;
-                        atomicAdd(&S.fx[0][i], fxv);
-                        atomicAdd(&S.fy[0][i], fyv);
-                        atomicAdd(&S.fz[0][i], fzv);
-                        atomicAdd(&S.fx[1][j], -fxv);
-                        atomicAdd(&S.fy[1][j], -fyv);
-                        atomicAdd(&S.fz[1][j], -fzv);
-                        pairs++;
-                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, valid);
+                    if (valid) S.queue[qn + __popc(bal & laneMaskLt())] = (unsigned short)((lane << 5) | jj);
+                    qn += __popc(bal);
                 }
+                __syncwarp();
+                // compute phase
+                for (int q = 0; q < qn; q += 32)
+                    if (q + lane < qn)
+                        computeQueuedPair<LEAN, TABLE>(S, S.queue[q + lane], iBase, perPairImage, C, L, P, e, pairs);
+                __syncwarp();
             }
             eAcc[0] += e[0];
             eAcc[1] += e[1];
             eAcc[2] += e[2];
-            __syncwarp();
-            flushForce(S, 1, lane, L.np, P.forceFixed);
+            flushForce(S, 1, lane, jslot, L.np, P.forceFixed);
         }
         __syncwarp();
-        flushForce(S, 0, lane, L.np, P.forceFixed);
-    }
-    // each warp's energy, in a fixed order of its tasks and a fixed reduction tree; the partials of all warps are
-    // summed in a fixed order by kReduceEnergies, so the total is the same on every run
-    const int globalWarp = blockIdx.x * kPairWarps + warp;
-    for (int t = 0; t < 3; t++) {
-        const double sum = warpSumD(eAcc[t]);
-        if (lane == 0) P.energyPartials[3 * globalWarp + t] = sum;
+        flushForce(S, 0, lane, iBase + lane, L.np, P.forceFixed);
+        // the task's energies: a fixed reduction tree over the lanes, one slot per task
+        for (int t = 0; t < 3; t++) {
+            const double sum = warpSumD(eAcc[t]);
+            if (lane == 0) P.taskEnergy[3 * task + t] = sum;
+        }
     }
     for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
     if (lane == 0 && pairs) atomicAdd(P.pairCount, pairs);

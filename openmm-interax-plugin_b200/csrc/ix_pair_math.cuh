@@ -125,6 +125,110 @@ __device__ __forceinline__ void overlap8pi(float r, const Width& Wi, const Width
     else overlapExact(r, Wj, Wi, s8pi, ds8pi);
 }
 
+// ---------------------------------------------------------------------------------------------------------------------
+// Pair coefficients of two parameter classes.  When a system's particles fall into few distinct parameter tuples
+// (atom types), every coefficient that depends only on the two particles' parameters is computed once on the host in
+// double precision and rounded to float once: C6, C8, C10 and the damping rate of the dispersion, the overlap's
+// polynomial coefficients (with a <= b: 1/a, 1/b as float-float, 1/a - 1/b, 1/s^3, 1/(a s^3), 1/(2 a^2 b s^2),
+// h/(a^3 b^2 s^2), 4/(a b s^3)), A_i A_j/(8 pi), (s_i + s_j)^3, (K_i + K_j)/2 and (L_i + L_j)/2.  The kernel then
+// evaluates only the r-dependent part.
+// ---------------------------------------------------------------------------------------------------------------------
+struct PairCoef {
+    float4 disp;    // C6, C8, C10, dx/dr = 2 beta/(w_i + w_j)
+    float4 ovA;     // exchange overlap: 1/a, its float remainder, 1/b, its float remainder
+    float4 ovB;     // 1/a - 1/b, 1/s^3, 1/(a s^3), 1/(2 a^2 b s^2)
+    float4 ovC;     // h/(a^3 b^2 s^2), 4/(a b s^3), A_i A_j/(8 pi), unused
+    float4 srA;     // short-range overlap, as ovA (equal to it when the two forces share widths)
+    float4 srB;     // as ovB
+    float4 srC;     // as ovC .x .y; (s_i + s_j)^3 of the short-range widths; unused
+    float4 srK;     // (K_i + K_j)/2, (L_i + L_j)/2, unused, unused
+};
+
+// 8 pi S and its derivative from the coefficients (the cancellation-free form of overlapExact).
+__device__ __forceinline__ void overlapFromCoef(float r, const float4& A, const float4& B, float k1, float k2,
+                                                float& s8pi, float& ds8pi) {
+    const float ia = A.x, hab = B.x, is3 = B.y, c2 = B.z, c3 = B.w;
+    const float ea = expNegScaled(r, A.x, A.y);
+    const float d = r * hab;
+    float eP3, eP4;
+    if (d < 2.0f) {
+        float p4 = 1.0f / 1307674368000.0f;
+        p4 = fmaf(p4, d, 1.0f / 87178291200.0f);
+        p4 = fmaf(p4, d, 1.0f / 6227020800.0f);
+        p4 = fmaf(p4, d, 1.0f / 479001600.0f);
+        p4 = fmaf(p4, d, 1.0f / 39916800.0f);
+        p4 = fmaf(p4, d, 1.0f / 3628800.0f);
+        p4 = fmaf(p4, d, 1.0f / 362880.0f);
+        p4 = fmaf(p4, d, 1.0f / 40320.0f);
+        p4 = fmaf(p4, d, 1.0f / 5040.0f);
+        p4 = fmaf(p4, d, 1.0f / 720.0f);
+        p4 = fmaf(p4, d, 1.0f / 120.0f);
+        p4 = fmaf(p4, d, 1.0f / 24.0f);
+        eP3 = ea * fmaf(d, p4, 1.0f / 6.0f);
+        eP4 = ea * p4;
+    }
+    else {
+        const float eb = expNegScaled(r, A.z, A.w);
+        float id = rcpApprox(d);
+        id = fmaf(id, fmaf(-d, id, 1.0f), id);
+        eP3 = (eb - ea * fmaf(d, fmaf(0.5f, d, 1.0f), 1.0f)) * id * id * id;
+        eP4 = fmaf(ea, -1.0f / 6.0f, eP3) * id;
+    }
+    const float rk1 = r * k1;
+    const float br = r * r * (rk1 - k2);
+    const float dbr = r * fmaf(3.0f, rk1, -2.0f * k2);
+    const float poly = fmaf(r, fmaf(r, c3, c2), is3);
+    const float dpoly = fmaf(2.0f * r, c3, c2);
+    const float eg = fmaf(eP3, br, ea * poly);
+    const float egp = fmaf(eP3, dbr, fmaf(fmaf(-3.0f, eP4, eP3) * hab, br, ea * dpoly));
+    s8pi = eg;
+    ds8pi = fmaf(-eg, ia, egp);
+}
+
+// Damped C6/C8/C10 dispersion from the coefficients (InteraxPairTerms.h:223-293): the partial sums of the
+// exponential series by Horner's rule, the series form of f_n below x = (n+1)/2.
+__device__ __forceinline__ void dispersionFromCoef(float r, float invR, const float4& K, float& energy, float& dEdR) {
+    const float dxdr = K.w;
+    const float x = dxdr * r;
+    const float expX = expNeg(x);
+    const float x2 = x * x;
+    const float x3 = x2 * x;
+    const float t6 = x3 * x3 * (1.0f / 720.0f);
+    const float t7 = t6 * x * (1.0f / 7.0f);
+    const float t8 = t7 * x * (1.0f / 8.0f);
+    const float t9 = t8 * x * (1.0f / 9.0f);
+    const float t10 = t9 * x * (1.0f / 10.0f);
+    float s6 = fmaf(x, 1.0f / 720.0f, 1.0f / 120.0f);
+    s6 = fmaf(s6, x, 1.0f / 24.0f);
+    s6 = fmaf(s6, x, 1.0f / 6.0f);
+    s6 = fmaf(s6, x, 0.5f);
+    s6 = fmaf(s6, x, 1.0f);
+    s6 = fmaf(s6, x, 1.0f);
+    const float s8 = (s6 + t7) + t8;
+    const float s10 = (s8 + t9) + t10;
+    float f6 = fmaf(-expX, s6, 1.0f), f8 = fmaf(-expX, s8, 1.0f), f10 = fmaf(-expX, s10, 1.0f);
+    if (x < 5.5f) {
+        float term = t10, tail = 0.0f;
+#pragma unroll 1
+        for (int k = 11; k <= 28; k++) {
+            term = term * x * __fdividef(1.0f, (float)k);
+            tail += term;
+        }
+        const float tail8 = (tail + t10) + t9;
+        f10 = expX * tail;
+        if (x < 4.5f) f8 = expX * tail8;
+        if (x < 3.5f) f6 = expX * ((tail8 + t8) + t7);
+    }
+    const float invR2 = invR * invR;
+    const float e6 = K.x * invR2 * invR2 * invR2;
+    const float e8 = K.y * invR2 * invR2 * invR2 * invR2;
+    const float e10 = K.z * invR2 * invR2 * invR2 * invR2 * invR2;
+    energy = -fmaf(f6, e6, fmaf(f8, e8, f10 * e10));
+    const float g = expX * dxdr;
+    dEdR = -(e6 * fmaf(g, t6, -6.0f * f6 * invR) + e8 * fmaf(g, t8, -8.0f * f8 * invR) +
+             e10 * fmaf(g, t10, -10.0f * f10 * invR));
+}
+
 // Tang-Toennies damped C6/C8/C10 dispersion (InteraxPairTerms.h:267-293).  p = (m1, m2, m3, alpha), w the widths.
 __device__ __forceinline__ void dispersionEnergy(float r, float invR, float4 pi, float4 pj, float wi, float wj,
                                                  float twoBeta, float& energy, float& dEdR) {
