@@ -173,6 +173,11 @@ int ix_get_kernel_times(ix_ctx* ctx, double* pair_ms, double* three_body_ms);
  * reference). */
 int ix_get_launch_count(ix_ctx* ctx, long long* launches);
 
+/* Evaluations and MD steps are captured into CUDA graphs on first use and replayed with one launch until a parameter,
+ * the box, a setting or a buffer changes (default: enabled).  enable = 0 launches every kernel directly; the results
+ * are identical.  No counterpart in the reference (OpenMM launches kernels one by one). */
+int ix_set_graphs(ix_ctx* ctx, int enable);
+
 /* The CUDA stream the context launches on (as a void*), so callers can order their own work around it. */
 void* ix_get_stream(ix_ctx* ctx);
 

@@ -56,12 +56,35 @@ struct DeviceBuffer {
     size_t bytes = 0;
 };
 
+// What a captured graph was captured for: the selected terms, the output pointers and the MD time step.
+struct GraphKey {
+    unsigned terms = 0;
+    const void* out0 = nullptr;
+    const void* out1 = nullptr;
+    const void* out2 = nullptr;
+    int stride = 0;
+    double dt = 0.0;
+    bool operator==(const GraphKey& o) const {
+        return terms == o.terms && out0 == o.out0 && out1 == o.out1 && out2 == o.out2 && stride == o.stride &&
+               dt == o.dt;
+    }
+};
+
+struct LaunchGraph {
+    cudaGraphExec_t exec = nullptr;
+    GraphKey key;
+    unsigned long long version = 0;
+    long long launches = 0;              // kernels in the graph
+};
+
 }  // namespace
 
 struct ix_ctx {
     int n = 0;
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;      // the three-body chain, forked from and joined back into `stream`
+    cudaEvent_t evFork = nullptr, evJoin = nullptr;
     int numSMs = 148;
     std::string error;
     double defaultBox[9] = {2, 0, 0, 0, 2, 0, 0, 0, 2};
@@ -103,6 +126,8 @@ struct ix_ctx {
     int* dFlags = nullptr;               // pair list flags [4], atm flags [2]
     double* dOutForces = nullptr;        // n x 3
     double* dOutEnergy = nullptr;        // 4
+    double* dEnergyBlocks = nullptr;     // kReduceBlocks x 4 partial sums of the energy reduction
+    unsigned* dReduceTicket = nullptr;   // blocks of the energy reduction done (the last one finishes, then resets)
     // pair list
     ListBuffers L{};
     ListGeometry G{};
@@ -130,7 +155,16 @@ struct ix_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool evPair = false, evAtm = false;
     long long launches = 0;              // kernels of this library launched on the context
+    // CUDA graphs of the evaluation (host and device entry points) and of one MD step, replayed until a change of
+    // state that a captured launch depends on (parameters, box, buffers, settings) bumps the version
+    bool useGraphs = true;
+    unsigned long long version = 1;
+    LaunchGraph graphCompute, graphDevice, graphMd;
 };
+
+static void bumpVersion(ix_ctx* ctx) {
+    if (ctx) ctx->version++;
+}
 
 // ---------------------------------------------------------------------------------------------------------------------
 // helpers
@@ -161,6 +195,7 @@ static int deviceAlloc(ix_ctx* ctx, const std::string& name, size_t count, T** o
         *out = reinterpret_cast<T*>(b.p);
         return IX_OK;
     }
+    bumpVersion(ctx);
     if (b.p) cudaFree(b.p);
     b.p = nullptr;
     b.bytes = 0;
@@ -286,6 +321,7 @@ static int addPairForce(ix_ctx* ctx, int t, const ix_pair_settings* s, const dou
     T.alch.assign(alch, alch + ctx->n);
     T.anyAlch = std::any_of(T.alch.begin(), T.alch.end(), [](unsigned char a) { return a != 0; });
     ctx->pairDirty = true;
+    bumpVersion(ctx);
     ctx->pairAllocated = false;
     return IX_OK;
 }
@@ -442,6 +478,7 @@ static int uploadPairParams(ix_ctx* ctx) {
     IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     computeLrc(ctx);
     ctx->pairDirty = false;
+    bumpVersion(ctx);
     // a rebuild gathers the parameters into sorted order
     int one = 1;
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->L.flag, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
@@ -543,23 +580,19 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
     IX_TRY(deviceAlloc(ctx, "spos", 3 * (size_t)np, &L.spos));
     IX_TRY(deviceAlloc(ctx, "sposf", np, &L.sposf));
     IX_TRY(deviceAlloc(ctx, "bbox", 2 * (size_t)nb, &L.bbox));
+    IX_TRY(deviceAlloc(ctx, "partCount", (size_t)nb * kListParts, &L.partCount));
+    IX_TRY(deviceAlloc(ctx, "blockAtoms", nb, &L.blockAtoms));
     IX_TRY(deviceAlloc(ctx, "blockTiles", nb + 1, &L.blockTiles));
-    IX_TRY(deviceAlloc(ctx, "blockTasks", nb + 1, &L.blockTasks));
-    if (tileCap > (long long)1 << 28) return fail(ctx, IX_ERR_INVALID, "neighbor list too large (%lld tiles)", tileCap);
+    if (tileCap > (long long)1 << 26) return fail(ctx, IX_ERR_INVALID, "neighbor list too large (%lld tiles)", tileCap);
     ctx->tileCap = (int)tileCap;
     L.tileCap = (int)tileCap;
-    L.exclCap = (int)std::min<long long>(tileCap, 8LL * nb + 256);
-    L.taskCap = (int)(tileCap / kTaskTiles + nb + 1);
     IX_TRY(deviceAlloc(ctx, "tileJ", 32 * (size_t)L.tileCap, &L.tileJ));
     IX_TRY(deviceAlloc(ctx, "tileIBlock", L.tileCap, &L.tileIBlock));
-    IX_TRY(deviceAlloc(ctx, "tileExcl", L.tileCap, &L.tileExcl));
-    IX_TRY(deviceAlloc(ctx, "exclMasks", 32 * (size_t)L.exclCap, &L.exclMasks));
-    IX_TRY(deviceAlloc(ctx, "exclCounter", 1, &L.exclCounter));
-    IX_TRY(deviceAlloc(ctx, "tasks", L.taskCap, &L.tasks));
-    IX_TRY(deviceAlloc(ctx, "numTasks", 1, &L.numTasks));
+    IX_TRY(deviceAlloc(ctx, "tileMask", 64 * (size_t)L.tileCap, &L.tileMask));
+    IX_TRY(deviceAlloc(ctx, "numTiles", 1, &L.numTiles));
     IX_TRY(deviceAlloc(ctx, "taskCounter", 1, &L.taskCounter));
-    IX_TRY(deviceAlloc(ctx, "taskEnergy", 3 * (size_t)L.taskCap, &ctx->dPairPartials));
-    IX_CUDA(ctx, cudaMemsetAsync(L.numTasks, 0, sizeof(int), ctx->stream));
+    IX_TRY(deviceAlloc(ctx, "taskEnergy", 3 * (size_t)L.tileCap, &ctx->dPairPartials));
+    IX_CUDA(ctx, cudaMemsetAsync(L.numTiles, 0, sizeof(int), ctx->stream));
     L.flag = ctx->dFlags;
     L.pos = ctx->dPos;
     // exclusions CSR
@@ -606,6 +639,7 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
     ctx->P.p2 = ctx->dP2;
     ctx->P.p3 = ctx->dP3;
     ctx->P.flags = ctx->dFlagsSorted;
+    L.flags = ctx->dFlagsSorted;
     ctx->P.pairCount = ctx->dCounts;
     int perSM = 0;
     int perSMLean = 0;
@@ -615,6 +649,7 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
     ctx->pairGridBlocksLean = std::max(1, perSMLean) * ctx->numSMs;
     ctx->P.taskEnergy = ctx->dPairPartials;
     ctx->pairAllocated = true;
+    bumpVersion(ctx);
     IX_TRY(uploadPairParams(ctx));
     return IX_OK;
 }
@@ -673,6 +708,7 @@ static int allocateAtm(ix_ctx* ctx) {
     A.tripleCount = ctx->dCounts + 1;
     ctx->atmAllocated = true;
     ctx->atmDirty = true;
+    bumpVersion(ctx);
     return IX_OK;
 }
 
@@ -688,6 +724,7 @@ static int uploadAtmParams(ix_ctx* ctx) {
     int one = 1;
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->A.flag, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
     ctx->atmDirty = false;
+    bumpVersion(ctx);
     return IX_OK;
 }
 
@@ -727,17 +764,31 @@ __global__ void kFinalize(int n, int np, const int* slotOf, const long long* pai
 
 // Term energies from the per-warp partials: each thread sums a fixed strided subset, then a fixed reduction tree,
 // so the result is identical on every run.  lrcEnergy (the long range correction, from the host) joins term 0.
+constexpr int kReduceBlocks = 64;
+
 __global__ void kReduceEnergies(const double* pairPartials, const int* numPairPartials, int pairCap,
-                                const double* atmPartials, int numAtmWarps, double lrcEnergy, double* outEnergy) {
+                                const double* atmPartials, int numAtmWarps, double lrcEnergy, double* outEnergy,
+                                double* blockSums, unsigned* ticket) {
     __shared__ double red[4][256];
+    __shared__ bool last;
     const int t = threadIdx.x;
+    // each block sums a fixed contiguous share of each array; the last block to finish adds the block sums in order
+    auto share = [](int total, int& lo, int& hi) {
+        const int per = (total + gridDim.x - 1) / gridDim.x;
+        lo = min((int)blockIdx.x * per, total);
+        hi = min(lo + per, total);
+    };
     double s[4] = {0.0, 0.0, 0.0, 0.0};
-    const int numPair = pairPartials ? min(*numPairPartials, pairCap) : 0;
-    if (pairPartials)
-        for (int w = t; w < numPair; w += 256)
+    int lo, hi;
+    if (pairPartials) {
+        share(min(*numPairPartials, pairCap), lo, hi);
+        for (int w = lo + t; w < hi; w += 256)
             for (int k = 0; k < 3; k++) s[k] += pairPartials[3 * w + k];
-    if (atmPartials)
-        for (int w = t; w < numAtmWarps; w += 256) s[3] += atmPartials[w];
+    }
+    if (atmPartials) {
+        share(numAtmWarps, lo, hi);
+        for (int w = lo + t; w < hi; w += 256) s[3] += atmPartials[w];
+    }
     for (int k = 0; k < 4; k++) red[k][t] = s[k];
     __syncthreads();
     for (int half = 128; half > 0; half >>= 1) {
@@ -745,9 +796,19 @@ __global__ void kReduceEnergies(const double* pairPartials, const int* numPairPa
             for (int k = 0; k < 4; k++) red[k][t] += red[k][t + half];
         __syncthreads();
     }
-    if (t == 0 && outEnergy) {
-        for (int k = 0; k < 4; k++) outEnergy[k] = red[k][0];
-        outEnergy[0] += lrcEnergy;
+    if (t == 0) {
+        for (int k = 0; k < 4; k++) blockSums[4 * blockIdx.x + k] = red[k][0];
+        __threadfence();
+        // wraps to 0 on the last block, ready for the next launch
+        last = atomicInc(ticket, gridDim.x - 1) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (last && t < 4) {
+        __threadfence();
+        double v = 0.0;
+        for (int b = 0; b < (int)gridDim.x; b++) v += ((volatile double*)blockSums)[4 * b + t];
+        if (t == 0) v += lrcEnergy;
+        if (outEnergy) outEnergy[t] = v;
     }
 }
 
@@ -785,8 +846,6 @@ static PairTermConfig pairConfig(const ix_ctx* ctx, unsigned terms) {
     C.periodic = ctx->method == IX_CUTOFF_PERIODIC;
     C.cutoff = ctx->cutoff;
     C.cutoff2 = (float)(ctx->cutoff * ctx->cutoff);
-    double tc = ctx->cutoff * (1.0 + 1e-5) + 1e-5;
-    C.testCutoff2 = (float)(tc * tc);
     C.box = ctx->G.box;
     for (int k = 0; k < 3; k++) {
         const double v[3] = {C.box.a[k], C.box.b[k], C.box.c[k]};
@@ -802,6 +861,8 @@ static PairTermConfig pairConfig(const ix_ctx* ctx, unsigned terms) {
     return C;
 }
 
+static int stageUploads(ix_ctx* ctx, unsigned terms);
+
 // Launch the whole evaluation on the context's stream.  Forces go to outForces (device, n x 3 doubles) and/or are
 // added to addFixed; energies to outEnergy (device, 4 doubles).
 static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, double* outEnergy, long long* addFixed,
@@ -810,63 +871,17 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
     cudaStream_t st = ctx->stream;
     const bool doPair = (terms & 7u) != 0;
     const bool doAtm = (terms & 8u) != 0;
-    updateGeometry(ctx);
+    IX_TRY(stageUploads(ctx, terms));
     IX_CUDA(ctx, cudaMemsetAsync(ctx->dEnergyFixed, 0, 4 * sizeof(long long), st));
     IX_CUDA(ctx, cudaMemsetAsync(ctx->dCounts, 0, 2 * sizeof(unsigned long long), st));
-    double lrcEnergy = 0.0;
-    if (doPair) {
-        if (ctx->pairDirty) IX_TRY(uploadPairParams(ctx));
-        ListBuffers& L = ctx->L;
-        const int tpb = 256;
-        const int gN = (n + tpb - 1) / tpb, gNp = (L.np + tpb - 1) / tpb;
-        const int gCells = (L.numCells + tpb - 1) / tpb;
-        kCheckDisplacement<<<gN, tpb, 0, st>>>(L, 0.25f * kPairSkin * kPairSkin);
-        kResetCells<<<std::max(1, std::min(gCells, 1024)), tpb, 0, st>>>(L);
-        if (!ctx->G.periodic) kParticleBounds<<<gN, tpb, 0, st>>>(L);
-        kCellKeys<<<gN, tpb, 0, st>>>(L, ctx->G);
-        kScanCells<<<1, 1024, 0, st>>>(L);
-        kScatterCells<<<gN, tpb, 0, st>>>(L);
-        kSortWithinCells<<<gCells, tpb, 0, st>>>(L);
-        kSortedAtoms<<<gNp, tpb, 0, st>>>(L, ctx->G);
-        kGatherParams<<<gNp, tpb, 0, st>>>(L, ctx->dP0o, ctx->dP1o, ctx->dP2o, ctx->dP3o, ctx->dFlagso, ctx->dP0,
-                                           ctx->dP1, ctx->dP2, ctx->dP3, ctx->dFlagsSorted);
-        kUpdateSortedPositions<<<gNp, tpb, 0, st>>>(L);
-        kBlockBounds<<<(L.nb * 32 + tpb - 1) / tpb, tpb, 0, st>>>(L, ctx->G);
-        const int warpsPerBlock = 8;
-        const int gB = (L.nb + warpsPerBlock - 1) / warpsPerBlock;
-        kBuildTiles<0><<<gB, 32 * warpsPerBlock, 0, st>>>(L, ctx->G);
-        kScanBlocks<<<1, 1024, 0, st>>>(L);
-        kBuildTiles<1><<<gB, 32 * warpsPerBlock, 0, st>>>(L, ctx->G);
-        kClearFlag<<<1, 1, 0, st>>>(L.flag);
-        IX_CUDA(ctx, cudaMemsetAsync(ctx->P.forceFixed, 0, 3 * (size_t)L.np * sizeof(long long), st));
-        PairTermConfig C = pairConfig(ctx, terms);
-        // the lean instantiation when no selected term has a soft core, a switching function or the order-2 overlap
-        bool lean = true;
-        for (int t = 0; t < 3; t++)
-            if ((terms >> t) & 1u) lean = lean && C.softShift[t] == 0.0f && !C.useSwitch[t] && C.overlapMethod[t] == 0;
-        IX_CUDA(ctx, cudaMemsetAsync(L.taskCounter, 0, sizeof(int), st));
-        if (ctx->profiling) cudaEventRecord(ctx->ev[0], st);
-        // the class-pair table serves the exact overlap method only
-        bool table = ctx->P.coef != nullptr;
-        for (int t = 1; t < 3; t++)
-            if ((terms >> t) & 1u) table = table && C.overlapMethod[t] == 0;
-        const int grid = lean ? ctx->pairGridBlocksLean : ctx->pairGridBlocks;
-        if (lean && table) kPairTiles<true, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
-        else if (lean) kPairTiles<true, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
-        else if (table) kPairTiles<false, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
-        else kPairTiles<false, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
-        ctx->launches += ctx->G.periodic ? 15 : 16;
-        if (ctx->profiling) cudaEventRecord(ctx->ev[1], st);
-        ctx->evPair = ctx->profiling;
-        IX_CUDA(ctx, cudaGetLastError());
-        const PairTerm& D = ctx->term[0];
-        if ((terms & 1u) && (D.lrcCoef != 0 || D.lrcAlchCoef != 0)) {
-            double lam = lambdaOf(ctx, D.alchName, D.anyAlch);
-            lrcEnergy = (D.lrcCoef + lam * D.lrcAlchCoef) / (ctx->box[0] * ctx->box[4] * ctx->box[8]);
-        }
+    // the three-body chain runs on a second stream, concurrently with the pair list and pair kernel
+    const bool fork = doPair && doAtm;
+    cudaStream_t sa = fork ? ctx->stream2 : st;
+    if (fork) {
+        IX_CUDA(ctx, cudaEventRecord(ctx->evFork, st));
+        IX_CUDA(ctx, cudaStreamWaitEvent(sa, ctx->evFork, 0));
     }
     if (doAtm) {
-        if (ctx->atmDirty) IX_TRY(uploadAtmParams(ctx));
         AtmBuffers& A = ctx->A;
         AtmConfig C{};
         C.numSites = (int)ctx->siteParams.size() / 3;
@@ -884,26 +899,86 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         C.maxMove2 = 0.25f * kSiteSkin * kSiteSkin;
         const int tpb = 256;
         const int gS = (C.numSites + tpb - 1) / tpb;
-        IX_CUDA(ctx, cudaMemsetAsync(A.siteForce, 0, 3 * (size_t)C.numSites * sizeof(long long), st));
-        IX_CUDA(ctx, cudaMemsetAsync(A.particleForce, 0, 3 * (size_t)n * sizeof(long long), st));
-        kSiteCentroids<<<gS, tpb, 0, st>>>(A, C, ctx->dPos);
-        kSiteNeighbors<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, st>>>(A, C);
-        kClearFlag<<<1, 1, 0, st>>>(A.flag);
+        IX_CUDA(ctx, cudaMemsetAsync(A.siteForce, 0, 3 * (size_t)C.numSites * sizeof(long long), sa));
+        IX_CUDA(ctx, cudaMemsetAsync(A.particleForce, 0, 3 * (size_t)n * sizeof(long long), sa));
+        kSiteCentroids<<<gS, tpb, 0, sa>>>(A, C, ctx->dPos);
+        kSiteNeighbors<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, sa>>>(A, C);
+        kClearFlag<<<1, 1, 0, sa>>>(A.flag);
         const size_t smem = sizeof(AtmWarpStorage) * kAtmWarps;
         int blocks = ctx->atmGridBlocks;
-        if (ctx->profiling) cudaEventRecord(ctx->ev[2], st);
-        kTriples<<<std::max(1, blocks), 32 * kAtmWarps, smem, st>>>(A, C);
-        if (ctx->profiling) cudaEventRecord(ctx->ev[3], st);
+        if (ctx->profiling) cudaEventRecordWithFlags(ctx->ev[2], sa, cudaEventRecordExternal);
+        kTriples<<<std::max(1, blocks), 32 * kAtmWarps, smem, sa>>>(A, C);
+        if (ctx->profiling) cudaEventRecordWithFlags(ctx->ev[3], sa, cudaEventRecordExternal);
         ctx->evAtm = ctx->profiling;
-        kSpreadSiteForces<<<gS, tpb, 0, st>>>(A, C);
+        kSpreadSiteForces<<<gS, tpb, 0, sa>>>(A, C);
         ctx->launches += 5;
         IX_CUDA(ctx, cudaGetLastError());
     }
+    double lrcEnergy = 0.0;
+    if (doPair) {
+        ListBuffers& L = ctx->L;
+        const int tpb = 256;
+        const int gN = (n + tpb - 1) / tpb, gNp = (L.np + tpb - 1) / tpb;
+        const int gCells = (L.numCells + tpb - 1) / tpb;
+        kCheckDisplacement<<<gN, tpb, 0, st>>>(L, 0.25f * kPairSkin * kPairSkin);
+        kResetCells<<<std::max(1, std::min(gCells, 1024)), tpb, 0, st>>>(L);
+        if (!ctx->G.periodic) kParticleBounds<<<gN, tpb, 0, st>>>(L);
+        kCellKeys<<<gN, tpb, 0, st>>>(L, ctx->G);
+        kScanCells<<<1, 1024, 0, st>>>(L);
+        kScatterCells<<<gN, tpb, 0, st>>>(L);
+        kSortWithinCells<<<gCells, tpb, 0, st>>>(L);
+        kSortedAtoms<<<gNp, tpb, 0, st>>>(L, ctx->G);
+        kGatherParams<<<gNp, tpb, 0, st>>>(L, ctx->dP0o, ctx->dP1o, ctx->dP2o, ctx->dP3o, ctx->dFlagso, ctx->dP0,
+                                           ctx->dP1, ctx->dP2, ctx->dP3, ctx->dFlagsSorted);
+        kUpdateSortedPositions<<<gNp, tpb, 0, st>>>(L);
+        kBlockBounds<<<(L.nb * 32 + tpb - 1) / tpb, tpb, 0, st>>>(L, ctx->G);
+        const int warpsPerBlock = 8;
+        const int gParts = (L.nb * kListParts + warpsPerBlock - 1) / warpsPerBlock;
+        const int gB = (L.nb + warpsPerBlock - 1) / warpsPerBlock;
+        kListAtoms<0><<<gParts, 32 * warpsPerBlock, 0, st>>>(L, ctx->G);
+        kScanTiles<<<1, 1024, 0, st>>>(L);
+        kListAtoms<1><<<gParts, 32 * warpsPerBlock, 0, st>>>(L, ctx->G);
+        kTileHeaders<<<gB, 32 * warpsPerBlock, 0, st>>>(L);
+        kTileMasks<<<ctx->numSMs * 8, 32 * warpsPerBlock, 0, st>>>(L, ctx->G);
+        kClearFlag<<<1, 1, 0, st>>>(L.flag);
+        IX_CUDA(ctx, cudaMemsetAsync(ctx->P.forceFixed, 0, 3 * (size_t)L.np * sizeof(long long), st));
+        PairTermConfig C = pairConfig(ctx, terms);
+        // the lean instantiation when no selected term has a soft core, a switching function or the order-2 overlap
+        bool lean = true;
+        for (int t = 0; t < 3; t++)
+            if ((terms >> t) & 1u) lean = lean && C.softShift[t] == 0.0f && !C.useSwitch[t] && C.overlapMethod[t] == 0;
+        IX_CUDA(ctx, cudaMemsetAsync(L.taskCounter, 0, sizeof(int), st));
+        // the external flag makes the records event nodes when the evaluation is captured into a graph
+        if (ctx->profiling) cudaEventRecordWithFlags(ctx->ev[0], st, cudaEventRecordExternal);
+        // the class-pair table serves the exact overlap method only
+        bool table = ctx->P.coef != nullptr;
+        for (int t = 1; t < 3; t++)
+            if ((terms >> t) & 1u) table = table && C.overlapMethod[t] == 0;
+        const int grid = lean ? ctx->pairGridBlocksLean : ctx->pairGridBlocks;
+        if (lean && table) kPairTiles<true, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        else if (lean) kPairTiles<true, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        else if (table) kPairTiles<false, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        else kPairTiles<false, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        ctx->launches += ctx->G.periodic ? 17 : 18;
+        if (ctx->profiling) cudaEventRecordWithFlags(ctx->ev[1], st, cudaEventRecordExternal);
+        ctx->evPair = ctx->profiling;
+        IX_CUDA(ctx, cudaGetLastError());
+        const PairTerm& D = ctx->term[0];
+        if ((terms & 1u) && (D.lrcCoef != 0 || D.lrcAlchCoef != 0)) {
+            double lam = lambdaOf(ctx, D.alchName, D.anyAlch);
+            lrcEnergy = (D.lrcCoef + lam * D.lrcAlchCoef) / (ctx->box[0] * ctx->box[4] * ctx->box[8]);
+        }
+    }
+    if (fork) {
+        IX_CUDA(ctx, cudaEventRecord(ctx->evJoin, sa));
+        IX_CUDA(ctx, cudaStreamWaitEvent(st, ctx->evJoin, 0));
+    }
     kFinalize<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->L.np, ctx->L.slotOf, doPair ? ctx->P.forceFixed : nullptr,
                                               doAtm ? ctx->A.particleForce : nullptr, outForces, addFixed, stride);
-    kReduceEnergies<<<1, 256, 0, st>>>(doPair ? ctx->dPairPartials : nullptr, ctx->L.numTasks, ctx->L.taskCap,
-                                       doAtm ? ctx->dAtmPartials : nullptr, ctx->atmGridBlocks * kAtmWarps,
-                                       lrcEnergy, outEnergy);
+    kReduceEnergies<<<kReduceBlocks, 256, 0, st>>>(doPair ? ctx->dPairPartials : nullptr, ctx->L.numTiles,
+                                                   ctx->L.tileCap, doAtm ? ctx->dAtmPartials : nullptr,
+                                                   ctx->atmGridBlocks * kAtmWarps, lrcEnergy, outEnergy,
+                                                   ctx->dEnergyBlocks, ctx->dReduceTicket);
     ctx->launches += 2;
     IX_CUDA(ctx, cudaGetLastError());
     return IX_OK;
@@ -926,7 +1001,7 @@ static int checkOverflow(ix_ctx* ctx, unsigned terms, bool& redo) {
     redo = false;
     int flags[6];
     IX_CUDA(ctx, cudaMemcpy(flags, ctx->dFlags, sizeof(flags), cudaMemcpyDeviceToHost));
-    if ((terms & 7u) && (flags[1] || flags[2] || flags[3])) {
+    if ((terms & 7u) && flags[1]) {
         long long tiles = 0;
         int cnt = 0;
         IX_CUDA(ctx, cudaMemcpy(&cnt, ctx->L.blockTiles + ctx->L.nb, sizeof(int), cudaMemcpyDeviceToHost));
@@ -935,9 +1010,8 @@ static int checkOverflow(ix_ctx* ctx, unsigned terms, bool& redo) {
         IX_CUDA(ctx, cudaMemcpy(ctx->dFlags, zero, sizeof(zero), cudaMemcpyHostToDevice));
         ctx->pairAllocated = false;
         IX_TRY(allocatePair(ctx, tiles));
-        if (flags[2]) ctx->L.exclCap = std::min(ctx->L.tileCap, 4 * ctx->L.exclCap);
-        IX_TRY(deviceAlloc(ctx, "exclMasks", 32 * (size_t)ctx->L.exclCap, &ctx->L.exclMasks));
         redo = true;
+        bumpVersion(ctx);
     }
     if ((terms & 8u) && flags[5]) {
         ctx->atmCap = std::min(2 * ctx->atmCap, (((int)ctx->siteParams.size() / 3 + 31) / 32) * 32 + 32);
@@ -949,8 +1023,68 @@ static int checkOverflow(ix_ctx* ctx, unsigned terms, bool& redo) {
         if (flags[5] & 2) return fail(ctx, IX_ERR_INVALID,
                                       "InteraxThreeBodyForce: more than 256 sites within the cutoff of one site");
         redo = true;
+        bumpVersion(ctx);
     }
     return IX_OK;
+}
+
+// The uploads launchEvaluation would otherwise start itself.  They synchronize, so they run before a capture.
+static int stageUploads(ix_ctx* ctx, unsigned terms) {
+    updateGeometry(ctx);
+    if ((terms & 7u) && ctx->pairDirty) IX_TRY(uploadPairParams(ctx));
+    if ((terms & 8u) && ctx->atmDirty) IX_TRY(uploadAtmParams(ctx));
+    return IX_OK;
+}
+
+// Enqueue work on the context's stream through a cached CUDA graph: captured on first use and again after a change of
+// state (ctx->version) or of the key, otherwise replayed with one launch.  enqueue() must not synchronize.
+template <class F>
+static int launchGraph(ix_ctx* ctx, LaunchGraph& g, const GraphKey& key, F&& enqueue) {
+    if (!ctx->useGraphs) return enqueue();
+    if (!g.exec || g.version != ctx->version || !(g.key == key)) {
+        const long long before = ctx->launches;
+        IX_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue();
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        if (rc != IX_OK || e != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();
+            ctx->launches = before;
+            if (rc != IX_OK) return rc;
+            return fail(ctx, IX_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
+        }
+        if (g.exec) {
+            cudaGraphExecUpdateResultInfo info;
+            if (cudaGraphExecUpdate(g.exec, graph, &info) != cudaSuccess) {
+                cudaGetLastError();
+                cudaGraphExecDestroy(g.exec);
+                g.exec = nullptr;
+            }
+        }
+        if (!g.exec) {
+            const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
+            if (ie != cudaSuccess) {
+                cudaGraphDestroy(graph);
+                g.exec = nullptr;
+                ctx->launches = before;
+                return fail(ctx, IX_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(ie));
+            }
+        }
+        cudaGraphDestroy(graph);
+        g.launches = ctx->launches - before;
+        ctx->launches = before;
+        g.key = key;
+        g.version = ctx->version;
+    }
+    IX_CUDA(ctx, cudaGraphLaunch(g.exec, ctx->stream));
+    ctx->launches += g.launches;
+    return IX_OK;
+}
+
+static void releaseGraph(LaunchGraph& g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -1020,8 +1154,11 @@ int ix_ctx_create(int num_particles, int device, const double* default_box, ix_c
         std::memcpy(ctx->defaultBox, default_box, sizeof(ctx->defaultBox));
         std::memcpy(ctx->box, default_box, sizeof(ctx->box));
     }
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
-        delete ctx;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->evFork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->evJoin, cudaEventDisableTiming) != cudaSuccess) {
+        ix_ctx_destroy(ctx);
         return fail(nullptr, IX_ERR_CUDA, "cudaStreamCreate failed");
     }
     int rc = IX_OK;
@@ -1030,13 +1167,16 @@ int ix_ctx_create(int num_particles, int device, const double* default_box, ix_c
         (rc = deviceAlloc(ctx, "counts", 2, &ctx->dCounts)) != IX_OK ||
         (rc = deviceAlloc(ctx, "flags", 8, &ctx->dFlags)) != IX_OK ||
         (rc = deviceAlloc(ctx, "outForces", 3 * (size_t)num_particles, &ctx->dOutForces)) != IX_OK ||
-        (rc = deviceAlloc(ctx, "outEnergy", 4, &ctx->dOutEnergy)) != IX_OK) {
+        (rc = deviceAlloc(ctx, "outEnergy", 4, &ctx->dOutEnergy)) != IX_OK ||
+        (rc = deviceAlloc(ctx, "energyBlocks", 4 * kReduceBlocks, &ctx->dEnergyBlocks)) != IX_OK ||
+        (rc = deviceAlloc(ctx, "reduceTicket", 1, &ctx->dReduceTicket)) != IX_OK) {
         g_createError = ctx->error;
         ix_ctx_destroy(ctx);
         return rc;
     }
     int init[8] = {1, 0, 0, 0, 1, 0, 0, 0};
     cudaMemcpy(ctx->dFlags, init, sizeof(init), cudaMemcpyHostToDevice);
+    cudaMemset(ctx->dReduceTicket, 0, sizeof(unsigned));
     *out = ctx;
     return IX_OK;
 }
@@ -1045,10 +1185,16 @@ void ix_ctx_destroy(ix_ctx* ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    releaseGraph(ctx->graphCompute);
+    releaseGraph(ctx->graphDevice);
+    releaseGraph(ctx->graphMd);
     for (auto& kv : ctx->buffers)
         if (kv.second.p) cudaFree(kv.second.p);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
+    if (ctx->evFork) cudaEventDestroy(ctx->evFork);
+    if (ctx->evJoin) cudaEventDestroy(ctx->evJoin);
+    if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1124,6 +1270,7 @@ int ix_add_three_body(ix_ctx* ctx, int num_sites, const int32_t* site_offsets, c
     ctx->atmPeriodic = periodic != 0;
     ctx->atmAllocated = false;
     ctx->atmDirty = true;
+    bumpVersion(ctx);
     return IX_OK;
 }
 
@@ -1134,6 +1281,7 @@ static int updatePair(ix_ctx* ctx, int t, const double* params, int stride) {
     if (!params) return fail(ctx, IX_ERR_INVALID, "%s: null argument", kTermNames[t]);
     ctx->term[t].params.assign(params, params + (size_t)ctx->n * stride);
     ctx->pairDirty = true;
+    bumpVersion(ctx);
     return IX_OK;
 }
 
@@ -1177,6 +1325,7 @@ int ix_update_three_body(ix_ctx* ctx, const double* site_params, double scale_fa
     ctx->atmDampingScale = damping_scale;
     ctx->atmCentroidRadius = centroid_radius;
     ctx->atmDirty = true;
+    bumpVersion(ctx);
     return IX_OK;
 }
 
@@ -1184,6 +1333,7 @@ int ix_set_parameter(ix_ctx* ctx, const char* name, double value) {
     if (!ctx || !name) return IX_ERR_INVALID;
     ctx->mdForcesValid = false;
     ctx->parameters[name] = value;
+    bumpVersion(ctx);
     return IX_OK;
 }
 
@@ -1197,6 +1347,7 @@ int ix_set_positions(ix_ctx* ctx, const double* positions, const double* box) {
     if (box) {
         if (box[0] <= 0 || box[4] <= 0 || box[8] <= 0)
             return fail(ctx, IX_ERR_INVALID, "Illegal periodic box vectors");
+        if (std::memcmp(ctx->box, box, sizeof(ctx->box)) != 0) bumpVersion(ctx);
         std::memcpy(ctx->box, box, sizeof(ctx->box));
     }
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -1215,7 +1366,16 @@ int ix_compute(ix_ctx* ctx, int groups, int include_forces, int include_energy, 
     if (terms) IX_TRY(prepare(ctx, terms));
     double e[4] = {0, 0, 0, 0};
     for (int attempt = 0; attempt < 4; attempt++) {
-        if (terms) IX_TRY(launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0));
+        if (terms) {
+            IX_TRY(stageUploads(ctx, terms));
+            GraphKey key;
+            key.terms = terms;
+            key.out0 = ctx->dOutForces;
+            key.out1 = ctx->dOutEnergy;
+            IX_TRY(launchGraph(ctx, ctx->graphCompute, key, [&]() {
+                return launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0);
+            }));
+        }
         IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         bool redo = false;
         if (terms) IX_TRY(checkOverflow(ctx, terms, redo));
@@ -1248,7 +1408,15 @@ int ix_compute_device(ix_ctx* ctx, int groups, long long* d_force_fixed, int for
     unsigned terms = selectedTerms(ctx, groups);
     if (!terms) return IX_OK;
     IX_TRY(prepare(ctx, terms));
-    return launchEvaluation(ctx, terms, nullptr, d_term_energies, d_force_fixed, force_stride);
+    IX_TRY(stageUploads(ctx, terms));
+    GraphKey key;
+    key.terms = terms;
+    key.out1 = d_term_energies;
+    key.out2 = d_force_fixed;
+    key.stride = force_stride;
+    return launchGraph(ctx, ctx->graphDevice, key, [&]() {
+        return launchEvaluation(ctx, terms, nullptr, d_term_energies, d_force_fixed, force_stride);
+    });
 }
 
 int ix_compute_device_f64(ix_ctx* ctx, int groups, const double* d_positions, const double* box, double* d_forces,
@@ -1256,7 +1424,10 @@ int ix_compute_device_f64(ix_ctx* ctx, int groups, const double* d_positions, co
     if (!ctx) return IX_ERR_INVALID;
     ctx->mdForcesValid = false;
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
-    if (box) std::memcpy(ctx->box, box, sizeof(ctx->box));
+    if (box) {
+        if (std::memcmp(ctx->box, box, sizeof(ctx->box)) != 0) bumpVersion(ctx);
+        std::memcpy(ctx->box, box, sizeof(ctx->box));
+    }
     if (d_positions) {
         IX_CUDA(ctx, cudaMemcpyAsync(ctx->dPos, d_positions, 3 * (size_t)ctx->n * sizeof(double),
                                      cudaMemcpyDeviceToDevice, ctx->stream));
@@ -1269,12 +1440,19 @@ int ix_compute_device_f64(ix_ctx* ctx, int groups, const double* d_positions, co
         return IX_OK;
     }
     IX_TRY(prepare(ctx, terms));
-    return launchEvaluation(ctx, terms, d_forces, d_term_energies, nullptr, 0);
+    IX_TRY(stageUploads(ctx, terms));
+    GraphKey key;
+    key.terms = terms;
+    key.out0 = d_forces;
+    key.out1 = d_term_energies;
+    return launchGraph(ctx, ctx->graphDevice, key,
+                       [&]() { return launchEvaluation(ctx, terms, d_forces, d_term_energies, nullptr, 0); });
 }
 
 int ix_set_counting(ix_ctx* ctx, int enable) {
     if (!ctx) return IX_ERR_INVALID;
     ctx->counting = enable != 0;
+    bumpVersion(ctx);
     return IX_OK;
 }
 
@@ -1305,6 +1483,7 @@ int ix_md_set_masses(ix_ctx* ctx, const double* masses) {
     IX_TRY(deviceAlloc(ctx, "vel", 3 * (size_t)ctx->n, &ctx->dVel));
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dInvMass, inv.data(), ctx->n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
     ctx->haveMasses = true;
+    bumpVersion(ctx);
     return IX_OK;
 }
 
@@ -1314,6 +1493,7 @@ int ix_set_profiling(ix_ctx* ctx, int enable) {
     if (enable && !ctx->ev[0])
         for (auto& e : ctx->ev) IX_CUDA(ctx, cudaEventCreate(&e));
     ctx->profiling = enable != 0;
+    bumpVersion(ctx);
     ctx->evPair = ctx->evAtm = false;
     return IX_OK;
 }
@@ -1348,7 +1528,10 @@ int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt) {
     if (!ctx->havePositions) return fail(ctx, IX_ERR_STATE, "positions have not been set");
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
     unsigned terms = selectedTerms(ctx, -1);
-    if (terms) IX_TRY(prepare(ctx, terms));
+    if (terms) {
+        IX_TRY(prepare(ctx, terms));
+        IX_TRY(stageUploads(ctx, terms));
+    }
     const int n = ctx->n;
     const int g = (n + 255) / 256;
     if (!ctx->mdForcesValid) {
@@ -1356,13 +1539,29 @@ int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt) {
         else IX_CUDA(ctx, cudaMemsetAsync(ctx->dOutForces, 0, 3 * (size_t)n * sizeof(double), ctx->stream));
         ctx->mdForcesValid = true;
     }
-    for (int step = 0; step < num_steps; step++) {
+    // one step = half kick + drift, the evaluation at the new positions, half kick; replayed as one graph
+    GraphKey key;
+    key.terms = terms;
+    key.out0 = ctx->dOutForces;
+    key.out1 = ctx->dOutEnergy;
+    key.dt = dt;
+    auto step = [&]() -> int {
         kVerletFirstHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos);
         if (terms) IX_TRY(launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0));
         kVerletSecondHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel);
         ctx->launches += 2;
-    }
+        IX_CUDA(ctx, cudaGetLastError());
+        return IX_OK;
+    };
+    for (int s = 0; s < num_steps; s++) IX_TRY(launchGraph(ctx, ctx->graphMd, key, step));
     IX_CUDA(ctx, cudaGetLastError());
+    return IX_OK;
+}
+
+int ix_set_graphs(ix_ctx* ctx, int enable) {
+    if (!ctx) return IX_ERR_INVALID;
+    ctx->useGraphs = enable != 0;
+    bumpVersion(ctx);
     return IX_OK;
 }
 
@@ -1446,6 +1645,8 @@ struct NoAllocScratch {
     long long particleForce[3 * kNoAllocMaxParticles];
     double energyPartials[kNoAllocBlocks * kAtmWarps];
     double energy[4];
+    double energyBlocks[4];      // the energy reduction's block sum (one block)
+    unsigned reduceTicket;
     int flag[2];
     unsigned long long tripleCount;
 };
@@ -1609,10 +1810,12 @@ int ix_three_body_noalloc(int num_particles, const double* d_positions, const do
         kTriples<<<blocks, 32 * kAtmWarps, sizeof(AtmWarpStorage) * kAtmWarps, st>>>(A, C);
         kNoAllocSpread<<<(num_sites + tpb - 1) / tpb, tpb, 0, st>>>(S, num_particles, num_sites, d_site_offsets,
                                                                    d_site_particles);
-        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, nullptr, 0, S->energyPartials, blocks * kAtmWarps, 0.0, S->energy);
+        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, nullptr, 0, S->energyPartials, blocks * kAtmWarps, 0.0, S->energy,
+                                           S->energyBlocks, &S->reduceTicket);
     }
     else {
-        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, nullptr, 0, nullptr, 0, 0.0, S->energy);
+        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, nullptr, 0, nullptr, 0, 0.0, S->energy, S->energyBlocks,
+                                           &S->reduceTicket);
     }
     kNoAllocFinish<<<(num_particles + tpb - 1) / tpb, tpb, 0, st>>>(S, num_particles, d_forces);
     e = cudaMemcpyAsync(d_energy, &S->energy[3], sizeof(double), cudaMemcpyDeviceToDevice, st);

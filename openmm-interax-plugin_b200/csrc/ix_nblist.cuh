@@ -1,7 +1,10 @@
 // Device neighbor list of the fused pair pass: a deterministic cell sort of the particles into blocks of 32, block
 // bounding boxes, and per i-block lists of "tiles" (one i-block x 32 candidate j particles within cutoff + skin of the
-// i-block's box).  Every kernel of the build reads the rebuild flag and returns at once when it is clear, so the
-// whole pipeline can be launched every step (and captured in a CUDA graph) without a host round trip.
+// i-block's box).  Each tile carries its pair masks: bit j of row i is set when the pair (i, j) can interact before
+// the next rebuild (within cutoff + skin at build time, not excluded, j after i, some term gated on), and the
+// transposed column masks; the pair kernel visits only those pairs and needs no per-step candidate test.  Every
+// kernel of the build reads the rebuild flag and returns at once when it is clear, so the whole pipeline can be
+// launched every step (and captured in a CUDA graph) without a host round trip.
 //
 // The reference gets its list from OpenMM (NonbondedUtilities, called at platforms/common/src/
 // CommonInteraxKernels.cpp:209) and, on the Reference platform, a voxel hash (ReferenceInteraxPairIxn.h:86-87).
@@ -13,8 +16,15 @@
 
 namespace ix {
 
-constexpr int kTaskTiles = 1;        // tiles of one i-block handled by one warp task (small tasks: short tail)
 constexpr float kPairSkin = 0.1f;    // nm; rebuild when a particle has moved by more than half of it
+constexpr int kListParts = 8;        // warps sharing the candidate search of one i-block
+
+// Particle flags in the sorted parameter arrays.
+constexpr int kFlagReal = 1 << 3;
+constexpr int kFlagGateDisp = 1 << 4;    // alpha != 0
+constexpr int kFlagGateExch = 1 << 5;    // exchange width != 0
+constexpr int kFlagGateSr = 1 << 6;      // short-range width != 0
+constexpr int kFlagGates = kFlagGateDisp | kFlagGateExch | kFlagGateSr;
 
 // Frame shared by the build and evaluation kernels.
 struct ListGeometry {
@@ -29,7 +39,7 @@ struct ListGeometry {
 
 struct ListBuffers {
     int n, nb, np;
-    // rebuild control: flag[0] rebuild, flag[1] tile overflow, flag[2] exclusion-mask overflow, flag[3] task overflow
+    // rebuild control: flag[0] rebuild, flag[1] tile overflow, flag[2..3] unused
     int* flag;
     // original-order input positions and the positions at the last build
     const double* pos;
@@ -51,17 +61,16 @@ struct ListBuffers {
     float4* sposf;              // np
     float4* bbox;               // nb x 2: center (xyz), half extent (xyz)
     // tiles
-    int* blockTiles;            // nb + 1: tile count, then exclusive scan (offsets)
-    int* blockTasks;            // nb + 1
+    int* partCount;             // nb x kListParts: candidates found by each part of a block's search, then offsets
+    int* blockAtoms;            // nb: candidate j particles of each i-block
+    int* blockTiles;            // nb + 1: exclusive scan of the tile counts, then the total
     int* tileJ;                 // tileCap x 32
     int* tileIBlock;            // tileCap
-    int* tileExcl;              // tileCap: index of the exclusion masks or -1
-    unsigned* exclMasks;        // exclCap x 32
-    int* exclCounter;
-    int2* tasks;                // taskCap: (first tile, number of tiles)
-    int* numTasks;
-    int* taskCounter;           // next task of the pair kernel's dynamic schedule (zeroed before each launch)
-    int tileCap, exclCap, taskCap;
+    unsigned* tileMask;         // tileCap x 64: row masks (per i lane, bit = j slot), then column masks (per j lane)
+    int* numTiles;              // tiles to evaluate (0 after an overflow)
+    int* taskCounter;           // next tile of the pair kernel's dynamic schedule (zeroed before each launch)
+    int tileCap;
+    const int* flags;           // sorted particle flags (the term gates of each particle)
     // exclusions (original indices), CSR with sorted partners and their range
     const int* exclStart;
     const int* exclList;
@@ -100,7 +109,6 @@ __global__ void kResetCells(ListBuffers L) {
         int* mm = reinterpret_cast<int*>(L.bboxMinMax);
         mm[threadIdx.x] = threadIdx.x < 3 ? floatToOrdered(INFINITY) : floatToOrdered(-INFINITY);
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) *L.exclCounter = 0;
 }
 
 // Bounding box of all particles (non-periodic cell grids span it).
@@ -326,140 +334,153 @@ __device__ __forceinline__ bool isExcluded(const ListBuffers& L, int oi, int oj)
     return false;
 }
 
-// Tile construction for one i-block (one warp).  Pass 0 counts the tiles, pass 1 writes them at the block's offset.
-// Candidate j particles: those of blocks J >= I whose box is within the list cutoff of block I's box, and whose own
-// position is within it too; the diagonal block's pairs are halved in the pair kernel (j slot > i slot).
+// Candidate j particles of one i-block, searched by kListParts warps that split the blocks J >= I into contiguous
+// ranges: the particles of blocks whose box is within the list cutoff of block I's box, and whose own position is
+// within it too.  PASS 0 counts each part's candidates; PASS 1 writes their slots to the i-block's tile rows, part
+// after part and in slot order within a part, so the lists do not depend on scheduling.
 template <int PASS>
-__global__ void kBuildTiles(ListBuffers L, ListGeometry G) {
+__global__ void kListAtoms(ListBuffers L, ListGeometry G) {
     if (!rebuildRequested(L)) return;
-    __shared__ int buffer[8][64];
-    const int warpInBlock = threadIdx.x >> 5;
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    const int I = blockIdx.x * (blockDim.x >> 5) + warpInBlock;
+    const int I = w / kListParts, part = w % kListParts;
     if (I >= L.nb) return;
-    int* buf = buffer[warpInBlock];
+    const int span = L.nb - I;
+    const int J0 = I + (int)((long long)span * part / kListParts);
+    const int J1 = I + (int)((long long)span * (part + 1) / kListParts);
     const float4 ci = L.bbox[2 * I], ei = L.bbox[2 * I + 1];
     const float cut2 = G.useCutoff ? G.listCutoff * G.listCutoff : INFINITY;
-    int count = 0, tiles = 0;
-    int tileBase = PASS == 1 ? L.blockTiles[I] : 0;
-    const int oi = L.sortedAtom[I * 32 + lane];
-    auto emit = [&](int valid) {
-        // the first `valid` entries of buf form a tile
-        if (PASS == 1) {
-            int t = tileBase + tiles;
-            if (t < L.tileCap) {
-                int j = lane < valid ? buf[lane] : -1;
-                L.tileJ[32 * t + lane] = j;
-                if (lane == 0) L.tileIBlock[t] = I;
-                // exclusion mask of this lane's i particle against the tile's j slots
-                unsigned mask = 0;
-                if (oi >= 0) {
-                    for (int k = 0; k < valid; k++) {
-                        int oj = L.sortedAtom[buf[k]];
-                        if (oj >= 0 && isExcluded(L, oi, oj)) mask |= 1u << k;
-                    }
-                }
-                int excl = -1;
-                if (__any_sync(0xffffffffu, mask != 0)) {
-                    int e = 0;
-                    if (lane == 0) e = atomicAdd(L.exclCounter, 1);
-                    e = __shfl_sync(0xffffffffu, e, 0);
-                    if (e < L.exclCap) {
-                        L.exclMasks[32 * e + lane] = mask;
-                        excl = e;
-                    }
-                    else if (lane == 0) atomicOr(L.flag + 2, 1);
-                }
-                if (lane == 0) L.tileExcl[t] = excl;
-            }
-            else if (lane == 0) atomicOr(L.flag + 1, 1);
-        }
-        tiles++;
-    };
-    for (int J0 = I; J0 < L.nb; J0 += 32) {
-        const int Jl = J0 + lane;
-        bool cand = false;
-        if (Jl < L.nb) cand = boxBoxDist2(ci, ei, L.bbox[2 * Jl], L.bbox[2 * Jl + 1], G) < cut2;
+    long long base = 0;
+    if (PASS == 1) base = 32LL * L.blockTiles[I] + L.partCount[I * kListParts + part];
+    const long long end = 32LL * L.tileCap;
+    int count = 0;
+    for (int Jc = J0; Jc < J1; Jc += 32) {
+        const int Jl = Jc + lane;
+        const bool cand = Jl < J1 && boxBoxDist2(ci, ei, L.bbox[2 * Jl], L.bbox[2 * Jl + 1], G) < cut2;
         unsigned cmask = __ballot_sync(0xffffffffu, cand);
         while (cmask) {
-            const int J = J0 + __ffs(cmask) - 1;
+            const int J = Jc + __ffs(cmask) - 1;
             cmask &= cmask - 1;
             const int j = J * 32 + lane;
             bool keep = L.sortedAtom[j] >= 0;
             if (keep && G.useCutoff) keep = pointBoxDist2(L.sposf[j], ci, ei, G) < cut2;
-            unsigned kmask = __ballot_sync(0xffffffffu, keep);
-            if (keep) buf[count + __popc(kmask & laneMaskLt())] = j;
-            count += __popc(kmask);
-            __syncwarp();
-            if (count >= 32) {
-                emit(32);
-                __syncwarp();
-                int rest = count - 32;
-                int v = lane < rest ? buf[32 + lane] : 0;
-                __syncwarp();
-                if (lane < rest) buf[lane] = v;
-                __syncwarp();
-                count = rest;
+            const unsigned kmask = __ballot_sync(0xffffffffu, keep);
+            if (PASS == 1 && keep) {
+                const long long pos = base + count + __popc(kmask & laneMaskLt());
+                if (pos < end) L.tileJ[pos] = j;
             }
+            count += __popc(kmask);
         }
     }
-    if (count > 0) emit(count);
-    if (PASS == 0 && lane == 0) {
-        L.blockTiles[I] = tiles;
-        L.blockTasks[I] = (tiles + kTaskTiles - 1) / kTaskTiles;
-    }
-    if (PASS == 1 && lane == 0) {
-        int taskBase = L.blockTasks[I];
-        for (int k = 0; k * kTaskTiles < tiles; k++) {
-            int task = taskBase + k;
-            int first = tileBase + k * kTaskTiles;
-            int count = min(kTaskTiles, tiles - k * kTaskTiles);
-            if (task < L.taskCap && first + count <= L.tileCap) L.tasks[task] = make_int2(first, count);
-            else atomicOr(L.flag + 3, 1);
-        }
-    }
+    if (PASS == 0 && lane == 0) L.partCount[I * kListParts + part] = count;
 }
 
-// Exclusive scans of the per-block tile and task counts (one block of 1024 threads).
-__global__ void kScanBlocks(ListBuffers L) {
+// Per i-block: the offsets of its parts' candidates, its candidate and tile counts; then the exclusive scan of the
+// tile counts over the blocks (one block of 1024 threads).  On overflow no tile is scheduled (nothing is written
+// beyond the buffers); the host grows them and evaluates again.
+__global__ void kScanTiles(ListBuffers L) {
     if (!rebuildRequested(L)) return;
-    __shared__ int pa[1024], pb[1024];
+    __shared__ int partial[1024];
     const int t = threadIdx.x;
     const int per = (L.nb + 1023) / 1024;
     const int begin = min(t * per, L.nb), end = min(begin + per, L.nb);
-    int sa = 0, sb = 0;
+    int sum = 0;
     for (int c = begin; c < end; c++) {
-        sa += L.blockTiles[c];
-        sb += L.blockTasks[c];
+        int atoms = 0;
+        for (int p = 0; p < kListParts; p++) {
+            const int k = L.partCount[c * kListParts + p];
+            L.partCount[c * kListParts + p] = atoms;
+            atoms += k;
+        }
+        L.blockAtoms[c] = atoms;
+        const int tiles = (atoms + 31) / 32;
+        L.blockTiles[c] = tiles;
+        sum += tiles;
     }
-    pa[t] = sa;
-    pb[t] = sb;
+    partial[t] = sum;
     __syncthreads();
     for (int off = 1; off < 1024; off <<= 1) {
-        int va = t >= off ? pa[t - off] : 0;
-        int vb = t >= off ? pb[t - off] : 0;
+        const int v = t >= off ? partial[t - off] : 0;
         __syncthreads();
-        pa[t] += va;
-        pb[t] += vb;
+        partial[t] += v;
         __syncthreads();
     }
-    int ra = pa[t] - sa, rb = pb[t] - sb;
+    int run = partial[t] - sum;
     for (int c = begin; c < end; c++) {
-        int na = L.blockTiles[c], nbk = L.blockTasks[c];
-        L.blockTiles[c] = ra;
-        L.blockTasks[c] = rb;
-        ra += na;
-        rb += nbk;
+        const int k = L.blockTiles[c];
+        L.blockTiles[c] = run;
+        run += k;
     }
     if (t == 1023) {
-        L.blockTiles[L.nb] = pa[1023];
-        L.blockTasks[L.nb] = pb[1023];
-        const bool overflow = pa[1023] > L.tileCap || pb[1023] > L.taskCap;
-        // on overflow no task is scheduled (the pass writes no tile beyond the buffers); the host grows the
-        // buffers and evaluates again
-        *L.numTasks = overflow ? 0 : pb[1023];
-        if (pa[1023] > L.tileCap) atomicOr(L.flag + 1, 1);
-        if (pb[1023] > L.taskCap) atomicOr(L.flag + 3, 1);
+        const int total = partial[1023];
+        L.blockTiles[L.nb] = total;
+        *L.numTiles = total > L.tileCap ? 0 : total;
+        if (total > L.tileCap) atomicOr(L.flag + 1, 1);
+    }
+}
+
+// Tile headers of one i-block (one warp): the i-block of each of its tiles, and padding (-1) after the last candidate
+// of its last tile.
+__global__ void kTileHeaders(ListBuffers L) {
+    if (!rebuildRequested(L)) return;
+    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (I >= L.nb) return;
+    const int t0 = L.blockTiles[I], t1 = L.blockTiles[I + 1];
+    if (t1 > L.tileCap) return;
+    for (int t = t0 + lane; t < t1; t += 32) L.tileIBlock[t] = I;
+    const int rest = L.blockAtoms[I] & 31;
+    if (t1 > t0 && rest != 0 && lane >= rest) L.tileJ[32 * (t1 - 1) + lane] = -1;
+}
+
+// Pair masks of the tiles (one warp per tile).  A pair's bit is set when j's slot follows i's (each pair once), both
+// are real particles gated on for a common term, the pair is not excluded and its build-time distance (minimum image)
+// is within the list cutoff: then no pair outside the masks can come within the cutoff before the displacement check
+// requests the next build.  Row masks: lane = i slot, bit k = the tile's j lane k; column masks: the transpose.
+__global__ void kTileMasks(ListBuffers L, ListGeometry G) {
+    if (!rebuildRequested(L)) return;
+    const int lane = threadIdx.x & 31;
+    const int numTiles = *L.numTiles;
+    // the margin covers the float rounding of the build-time distance
+    const float cut2 = G.useCutoff ? G.listCutoff * G.listCutoff * (1.0f + 1e-5f) : INFINITY;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < numTiles; t += warps) {
+        const int si = L.tileIBlock[t] * 32 + lane;
+        const int oi = L.sortedAtom[si];
+        const float4 pi = L.sposf[si];
+        const int fi = L.flags[si];
+        const int2 range = oi >= 0 ? L.exclRange[oi] : make_int2(1, 0);
+        const int sj = L.tileJ[32 * t + lane];
+        int oj = -1, fj = 0;
+        float4 pj = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (sj >= 0) {
+            oj = L.sortedAtom[sj];
+            fj = L.flags[sj];
+            pj = L.sposf[sj];
+        }
+        unsigned mask = 0;
+        for (int k = 0; k < 32; k++) {
+            const int sk = __shfl_sync(0xffffffffu, sj, k);
+            const int ok = __shfl_sync(0xffffffffu, oj, k);
+            const int fk = __shfl_sync(0xffffffffu, fj, k);
+            float dx = __shfl_sync(0xffffffffu, pj.x, k) - pi.x;
+            float dy = __shfl_sync(0xffffffffu, pj.y, k) - pi.y;
+            float dz = __shfl_sync(0xffffffffu, pj.z, k) - pi.z;
+            bool in = oi >= 0 && ok >= 0 && sk > si && (fi & fk & kFlagGates) != 0;
+            if (in && G.useCutoff) {
+                if (G.periodic) minimumImageF(dx, dy, dz, G.boxf);
+                in = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < cut2;
+            }
+            if (in && ok >= range.x && ok <= range.y) in = !isExcluded(L, oi, ok);
+            if (in) mask |= 1u << k;
+        }
+        unsigned column = 0;
+        for (int k = 0; k < 32; k++) {
+            const unsigned b = __ballot_sync(0xffffffffu, (mask >> k) & 1u);
+            if (lane == k) column = b;
+        }
+        L.tileMask[64 * t + lane] = mask;
+        L.tileMask[64 * t + 32 + lane] = column;
     }
 }
 

@@ -2,34 +2,29 @@
 // tile list (the reference runs them as snippets of OpenMM's nonbonded kernel in one pass,
 // platforms/common/src/CommonInteraxKernels.cpp:139-219, kernels interaxPairBegin.cc / interaxPairEnd.cc).
 //
-// Work is split into tasks of up to kTaskTiles tiles of one i-block; warps take tasks from a counter in global
-// memory until none is left (dynamic balance).  Per task and tile:
-//   1. staging: the 32 i particles (once per task) and the tile's 32 j particles are written to shared memory as
+// Warps take tiles from a counter in global memory until none is left (dynamic balance).  Per tile:
+//   1. staging: the 32 i particles and the tile's 32 j particles are written to shared memory as
 //      float-float offsets from the i-block's center (the double-precision difference split into a float and its
-//      float remainder), with the float parameters.  In large rectangular boxes each j particle is placed at its
-//      minimum image relative to the block center here, once, instead of per pair;
-//   2. test phase: the 32 x 32 pairs are tested in rotation order (lane l, rotation k: i = l, j slot = (l + k) mod 32)
-//      in float with a small margin, and the candidates are compacted into a per-warp queue with ballots, so that
-//      the expensive phase runs with every lane busy;
-//   3. compute phase: each lane takes one queued pair, forms the displacement as (xj - xi) + (lo_j - lo_i) (the
-//      precision of the double difference, without double arithmetic), applies the exact cutoff test (borderline
-//      cases decided in double), evaluates the three terms in float and accumulates the pair force on i and j in
-//      shared memory;
-//   4. the j forces go to the global 64-bit fixed-point force buffer (scale 2^32) after each tile, the i forces after
-//      each task; each task's energies, summed per lane in double, are written to a per-task slot and summed in a
-//      fixed order afterwards.  Results do not depend on which warp ran which task.
+//      float remainder).  In large rectangular boxes each j particle is placed at its minimum image relative to the
+//      block center here, once, instead of per pair;
+//   2. queue: the tile's row masks (built with the list) give the candidate pairs; each lane writes its row's pairs
+//      to a per-warp queue at the row's offset (a warp prefix sum of the row counts), so that the expensive phase
+//      runs with every lane busy and no per-step candidate test;
+//   3. compute phase, in rounds of kPairRound queued pairs: each lane takes one pair, forms the displacement as
+//      (xj - xi) + (lo_j - lo_i) (the precision of the double difference, without double arithmetic), applies the
+//      exact cutoff test (borderline cases decided in double), evaluates the three terms in float and stores the
+//      pair force in shared memory;
+//   4. gather: lane i sums the forces of its row (contiguous in the queue), lane j those of its column (located from
+//      the column mask and the row offsets), in a fixed order and without atomics; both go to the global 64-bit
+//      fixed-point force buffer (scale 2^32) after the tile.  Each tile's energies, summed per lane and then over
+//      the lanes in double, are written to a per-tile slot and summed in a fixed order afterwards.  Results do not
+//      depend on which warp ran which tile.
 #pragma once
 
 #include "ix_nblist.cuh"
 #include "ix_pair_math.cuh"
 
 namespace ix {
-
-// Particle flags in the sorted parameter arrays.
-constexpr int kFlagReal = 1 << 3;
-constexpr int kFlagGateDisp = 1 << 4;    // alpha != 0
-constexpr int kFlagGateExch = 1 << 5;    // exchange width != 0
-constexpr int kFlagGateSr = 1 << 6;      // short-range width != 0
 
 // Periodic box as float-float vectors (for minimum images of float-float displacements).
 struct BoxFF {
@@ -49,7 +44,7 @@ struct PairTermConfig {
     int overlapMethod[3];
     int shareOverlap;            // exchange and short-range widths are identical for every particle
     int useCutoff, periodic;
-    float cutoff2, testCutoff2;
+    float cutoff2;
     double cutoff;
     Box box;
     BoxFF boxff;
@@ -238,30 +233,22 @@ __device__ __forceinline__ void minimumImageFF(float& xh, float& xl, float& yh, 
     xl -= s * B.aLo[0];
 }
 
-__device__ __forceinline__ void minimumImageHi(float& x, float& y, float& z, const BoxFF& B) {
-    float s = floorf(fmaf(z, B.inv[2], 0.5f));
-    x -= s * B.c[0];
-    y -= s * B.c[1];
-    z -= s * B.c[2];
-    s = floorf(fmaf(y, B.inv[1], 0.5f));
-    x -= s * B.b[0];
-    y -= s * B.b[1];
-    s = floorf(fmaf(x, B.inv[0], 0.5f));
-    x -= s * B.a[0];
-}
 
-// Per-warp shared memory of the pair kernel (about 4.3 KB, so that eight 4-warp blocks fit on an SM).  Parameters
+constexpr int kPairWarps = 4;
+constexpr int kPairRound = 128;  // queued pairs computed before their forces are gathered
+
+// Per-warp shared memory of the pair kernel (about 6.8 KB, so that eight 4-warp blocks fit on an SM).  Parameters
 // are not staged: the compute phase reads them through the read-only cache by sorted slot.
 struct PairWarpStorage {
     float4 hi[2][32];            // position offsets from the i-block center (float part); side 0 = i, 1 = j
     float4 lo[2][32];            // their float remainders
     int flags[2][32];
     int jslot[32];               // sorted slot of each j particle, -1 for padding
-    float fx[2][32], fy[2][32], fz[2][32];
-    unsigned short queue[512];   // candidates of half a tile (16 rotations)
+    int rowStart[32];            // queue offset of each row
+    unsigned rowMask[32];
+    unsigned short queue[1024];  // the tile's candidate pairs, row by row: (i << 5) | j
+    float4 force[kPairRound];    // force on i of each pair of the current round (j receives the opposite)
 };
-
-constexpr int kPairWarps = 4;
 
 __device__ __forceinline__ void stageParticle(PairWarpStorage& S, int side, int lane, int s, double cx, double cy,
                                               double cz, bool shiftImage, const PairTermConfig& C,
@@ -285,24 +272,20 @@ __device__ __forceinline__ void stageParticle(PairWarpStorage& S, int side, int 
         S.lo[side][lane] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
     if (side == 1) S.jslot[lane] = s;
-    S.fx[side][lane] = 0.0f;
-    S.fy[side][lane] = 0.0f;
-    S.fz[side][lane] = 0.0f;
 }
 
-__device__ __forceinline__ void flushForce(const PairWarpStorage& S, int side, int lane, int s, int np, long long* F) {
+__device__ __forceinline__ void flushForce(const float f[3], int s, int np, long long* F) {
     if (s < 0) return;
-    const float fx = S.fx[side][lane], fy = S.fy[side][lane], fz = S.fz[side][lane];
-    if (fx != 0.0f) atomicAddFixed(F + s, toFixed(fx));
-    if (fy != 0.0f) atomicAddFixed(F + np + s, toFixed(fy));
-    if (fz != 0.0f) atomicAddFixed(F + 2 * np + s, toFixed(fz));
+    if (f[0] != 0.0f) atomicAddFixed(F + s, toFixed(f[0]));
+    if (f[1] != 0.0f) atomicAddFixed(F + np + s, toFixed(f[1]));
+    if (f[2] != 0.0f) atomicAddFixed(F + 2 * np + s, toFixed(f[2]));
 }
 
-// One queued pair: displacement, exact cutoff test, the terms, and the force on i and j (shared memory).
+// One queued pair: displacement, exact cutoff test, the terms.  Returns the force on i (zero outside the cutoff).
 template <bool LEAN, bool TABLE>
-__device__ __forceinline__ void computeQueuedPair(PairWarpStorage& S, int entry, int iBase, bool perPairImage,
-                                                  const PairTermConfig& C, const ListBuffers& L,
-                                                  const PairBuffers& P, float e[3], unsigned long long& pairs) {
+__device__ __forceinline__ float4 computeQueuedPair(PairWarpStorage& S, int entry, int iBase, bool perPairImage,
+                                                    const PairTermConfig& C, const ListBuffers& L,
+                                                    const PairBuffers& P, float e[3], unsigned long long& pairs) {
     const int i = entry >> 5, j = entry & 31;
     const float4 hi_i = S.hi[0][i], hi_j = S.hi[1][j], lo_i = S.lo[0][i], lo_j = S.lo[1][j];
     float dxh = hi_j.x - hi_i.x, dyh = hi_j.y - hi_i.y, dzh = hi_j.z - hi_i.z;
@@ -324,7 +307,7 @@ __device__ __forceinline__ void computeQueuedPair(PairWarpStorage& S, int entry,
         }
     }
     const int fi = S.flags[0][i], fj = S.flags[1][j];
-    if (!inside || !(fi & fj & (kFlagGateDisp | kFlagGateExch | kFlagGateSr))) return;
+    if (!inside) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     float invR;
     const float r = sqrtRefined(r2, invR);
     float dEdR;
@@ -341,14 +324,8 @@ __device__ __forceinline__ void computeQueuedPair(PairWarpStorage& S, int entry,
         dEdR = pairTerms<LEAN>(C, r, invR, a0, a1, a2, a3, fi, b0, b1, b2, b3, fj, iFirst, e);
     }
     const float fs = dEdR * invR;
-    const float fxv = dx * fs, fyv = dy * fs, fzv = dz * fs;
-    atomicAdd(&S.fx[0][i], fxv);
-    atomicAdd(&S.fy[0][i], fyv);
-    atomicAdd(&S.fz[0][i], fzv);
-    atomicAdd(&S.fx[1][j], -fxv);
-    atomicAdd(&S.fy[1][j], -fyv);
-    atomicAdd(&S.fz[1][j], -fzv);
     pairs++;
+    return make_float4(dx * fs, dy * fs, dz * fs, 0.0f);
 }
 
 template <bool LEAN, bool TABLE>
@@ -357,70 +334,82 @@ __global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     PairWarpStorage& S = storage[warp];
-    const int numTasks = min(*L.numTasks, L.taskCap);
+    const int numTiles = min(*L.numTiles, L.tileCap);
+    const unsigned ltMask = laneMaskLt();
     unsigned long long pairs = 0;
     for (;;) {
-        int task = 0;
-        if (lane == 0) task = atomicAdd(L.taskCounter, 1);
-        task = __shfl_sync(0xffffffffu, task, 0);
-        if (task >= numTasks) break;
-        const int2 tk = L.tasks[task];
-        const int I = L.tileIBlock[tk.x];
+        int t = 0;
+        if (lane == 0) t = atomicAdd(L.taskCounter, 1);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= numTiles) break;
+        const int I = L.tileIBlock[t];
         const int iBase = I * 32;
         const float4 center = L.bbox[2 * I];
         const bool shiftImage = C.periodic && center.w != 0.0f;
         const bool perPairImage = C.periodic && !shiftImage;
         const double cx = center.x, cy = center.y, cz = center.z;
-        __syncwarp();
-        stageParticle(S, 0, lane, iBase + lane, cx, cy, cz, false, C, L, P);
-        double eAcc[3] = {0.0, 0.0, 0.0};
-        for (int t = tk.x; t < tk.x + tk.y; t++) {
+        float fi[3] = {0.0f, 0.0f, 0.0f};
+        {
             const int jslot = L.tileJ[32 * t + lane];
-            const int ex = L.tileExcl[t];
-            const unsigned excl = ex >= 0 ? L.exclMasks[32 * ex + lane] : 0u;
+            const unsigned row = L.tileMask[64 * t + lane];
+            const unsigned column = L.tileMask[64 * t + 32 + lane];
             __syncwarp();
+            stageParticle(S, 0, lane, iBase + lane, cx, cy, cz, false, C, L, P);
             stageParticle(S, 1, lane, jslot, cx, cy, cz, shiftImage, C, L, P);
+            // queue the tile's candidate pairs row by row
+            const int count = __popc(row);
+            int start = count;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, start, o);
+                if (lane >= o) start += v;
+            }
+            const int total = __shfl_sync(0xffffffffu, start, 31);
+            start -= count;
+            S.rowStart[lane] = start;
+            S.rowMask[lane] = row;
+            for (unsigned m = row, q = start; m; m &= m - 1, q++)
+                S.queue[q] = (unsigned short)((lane << 5) | (__ffs(m) - 1));
             __syncwarp();
-            const float4 xi = S.hi[0][lane];
-            const int si = iBase + lane;
-            const int fiTest = S.flags[0][lane];
             float e[3] = {0.0f, 0.0f, 0.0f};
-            for (int half = 0; half < 2; half++) {
-                // test phase over 16 rotations
-                int qn = 0;
-#pragma unroll 4
-                for (int k = 16 * half; k < 16 * half + 16; k++) {
-                    const int jj = (lane + k) & 31;
-                    const float4 xj = S.hi[1][jj];
-                    bool valid = (fiTest & S.flags[1][jj] & kFlagReal) && S.jslot[jj] > si && !((excl >> jj) & 1u);
-                    if (C.useCutoff) {
-                        float dx = xj.x - xi.x, dy = xj.y - xi.y, dz = xj.z - xi.z;
-                        if (perPairImage) minimumImageHi(dx, dy, dz, C.boxff);
-                        valid = valid && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < C.testCutoff2;
+            float fj[3] = {0.0f, 0.0f, 0.0f};
+            for (int base = 0; base < total; base += kPairRound) {
+                const int n = min(kPairRound, total - base);
+                for (int p = lane; p < n; p += 32)
+                    S.force[p] = computeQueuedPair<LEAN, TABLE>(S, S.queue[base + p], iBase, perPairImage, C, L, P,
+                                                                 e, pairs);
+                __syncwarp();
+                // i side: this lane's row, contiguous in the queue
+                const int a = max(start, base), b = min(start + count, base + n);
+                for (int q = a; q < b; q++) {
+                    const float4 f = S.force[q - base];
+                    fi[0] += f.x;
+                    fi[1] += f.y;
+                    fi[2] += f.z;
+                }
+                // j side: the pair (i, lane) of each row i of this round that holds it
+                unsigned rows = column & __ballot_sync(0xffffffffu, start < base + n && start + count > base);
+                while (rows) {
+                    const int i = __ffs(rows) - 1;
+                    rows &= rows - 1;
+                    const int q = S.rowStart[i] + __popc(S.rowMask[i] & ltMask) - base;
+                    if (q >= 0 && q < n) {
+                        const float4 f = S.force[q];
+                        fj[0] -= f.x;
+                        fj[1] -= f.y;
+                        fj[2] -= f.z;
                     }
-                    const unsigned bal = __ballot_sync(0xffffffffu, valid);
-                    if (valid) S.queue[qn + __popc(bal & laneMaskLt())] = (unsigned short)((lane << 5) | jj);
-                    qn += __popc(bal);
                 }
                 __syncwarp();
-                // compute phase
-                for (int q = 0; q < qn; q += 32)
-                    if (q + lane < qn)
-                        computeQueuedPair<LEAN, TABLE>(S, S.queue[q + lane], iBase, perPairImage, C, L, P, e, pairs);
-                __syncwarp();
             }
-            eAcc[0] += e[0];
-            eAcc[1] += e[1];
-            eAcc[2] += e[2];
-            flushForce(S, 1, lane, jslot, L.np, P.forceFixed);
+            flushForce(fj, jslot, L.np, P.forceFixed);
+            // the tile's energies: a fixed reduction tree over the lanes, one slot per tile
+            for (int k = 0; k < 3; k++) {
+                const double sum = warpSumD((double)e[k]);
+                if (lane == 0) P.taskEnergy[3 * t + k] = sum;
+            }
         }
-        __syncwarp();
-        flushForce(S, 0, lane, iBase + lane, L.np, P.forceFixed);
-        // the task's energies: a fixed reduction tree over the lanes, one slot per task
-        for (int t = 0; t < 3; t++) {
-            const double sum = warpSumD(eAcc[t]);
-            if (lane == 0) P.taskEnergy[3 * task + t] = sum;
-        }
+        flushForce(fi, iBase + lane, L.np, P.forceFixed);
     }
     for (int o = 16; o > 0; o >>= 1) pairs += __shfl_xor_sync(0xffffffffu, pairs, o);
     if (lane == 0 && pairs) atomicAdd(P.pairCount, pairs);

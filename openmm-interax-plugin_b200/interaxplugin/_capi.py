@@ -62,6 +62,7 @@ def lib():
             "ix_set_profiling": (ctypes.c_int, [P, ctypes.c_int]),
             "ix_get_kernel_times": (ctypes.c_int, [P, P, P]),
             "ix_get_launch_count": (ctypes.c_int, [P, P]),
+            "ix_set_graphs": (ctypes.c_int, [P, ctypes.c_int]),
             "ix_three_body_noalloc": (ctypes.c_int, [ctypes.c_int, P, P, ctypes.c_int, P, P, P, P, P, ctypes.c_double,
                                                      ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                      ctypes.c_int, ctypes.c_double, P, P, P]),

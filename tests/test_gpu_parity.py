@@ -679,6 +679,42 @@ def test_deterministic():
     assert np.array_equal(a.getForces(), b.getForces())
 
 
+def test_graphs_match_direct_launches():
+    """Evaluations and MD steps replayed from CUDA graphs equal direct launches bitwise, also after a parameter,
+    the box and the positions change between replays (each change must invalidate the captured graph)."""
+    cfg = W.CONFIGS["small"]
+    system, pos, box = W.water_box(cfg["num_waters"], cfg["box_length"], cfg["cutoff"], seed=5,
+                                   three_body_cutoff=cfg["three_body_cutoff"])
+    for f in range(3):
+        fc = system.getForce(f)
+        for i in range(0, system.getNumParticles(), 7):
+            fc.setParticleParameters(i, *tuple(fc.getParticleParameters(i))[:-1], True)
+    rng = np.random.default_rng(1)
+    ctxs = [Context(system), Context(system)]
+    ctxs[1]._check(ctxs[1]._lib.ix_set_graphs(ctxs[1]._ctx, 0))
+    box2 = np.asarray(box) * 1.01
+    steps = [(pos, box, 1.0), (pos + rng.normal(scale=0.01, size=pos.shape), box, 1.0),
+             (pos, box, 0.4), (pos, box2, 0.4), (pos + rng.normal(scale=0.05, size=pos.shape), box2, 0.7)]
+    for p, b, lam in steps:
+        states = []
+        for ctx in ctxs:
+            ctx.setPeriodicBoxVectors(*np.asarray(b))
+            ctx.setPositions(p)
+            ctx.setParameter("lambda_sterics", lam)
+            states.append(ctx.getState())
+        assert states[0].getPotentialEnergy() == states[1].getPotentialEnergy()
+        assert np.array_equal(states[0].getForces(), states[1].getForces())
+    vel = W.initial_velocities(system, 300.0, seed=2)
+    runs = []
+    for ctx in ctxs:
+        ctx.setPeriodicBoxVectors(*np.asarray(box))
+        ctx.setPositions(pos)
+        runs.append(ctx.runVelocityVerlet(25, 0.001, vel))
+    assert np.array_equal(runs[0][0], runs[1][0])
+    assert np.array_equal(runs[0][1], runs[1][1])
+    assert runs[0][2] == runs[1][2]
+
+
 def test_neighbor_list_follows_motion():
     """Moving the particles by more than the skin forces a rebuild; the result stays exact."""
     cfg = W.CONFIGS["small"]
