@@ -36,6 +36,9 @@ import numpy as np  # noqa: E402
 # driver, and the ATM triple with C9.
 F_PAIR = 612.4
 F_TRIPLE = 151.0
+# DRAM bytes (read + write) of one pair-kernel launch on this workload, from one ncu capture of an MD-step launch
+# (dram__bytes_read.sum + dram__bytes_write.sum); the kernel is FP32-issue bound, the traffic is reported beside it
+PAIR_TRAFFIC_BYTES = 12737280
 METRIC = "interactions/s"
 WORKLOAD = "water box 24,000 atoms (8,000 rigid-geometry waters, 6.208 nm periodic, cutoff 1.0 nm) + ATM on " \
            "8,000 molecular sites (cutoff 0.6 nm); velocity-Verlet 1 fs"
@@ -288,7 +291,7 @@ def run_ours(args, rank, world):
                    "ns_per_day": 86400 * dt_ps * 1e-3 / (ms_per_step * 1e-3),
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
-                     "frac": achieved / peak.value, "traffic": None,
+                     "frac": achieved / peak.value, "traffic": PAIR_TRAFFIC_BYTES,
                      "kernel": "kPairTiles", "kernel_ms": pair_ms, "ops_per_pair": F_PAIR,
                      "peak_source": "measured live: FMA-chain kernel on every SM (ix_measure_fp32_peak)",
                      "three_body_ms": float(np.mean(rows[:, 2])), "ops_per_triple": F_TRIPLE},
