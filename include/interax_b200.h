@@ -163,9 +163,10 @@ int ix_md_run(ix_ctx* ctx, int num_steps, double dt, double* positions, double* 
 int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt);
 int ix_md_finish(ix_ctx* ctx, double* positions, double* velocities, double* energy);
 
-/* Kernel timing for measurement: with profiling enabled, CUDA events bracket the pair and three-body kernels of each
- * evaluation; ix_get_kernel_times returns the durations (ms) of the last evaluation's kernels.  A measurement tool
- * with no counterpart in the reference. */
+/* Kernel timing for measurement: with profiling enabled (1), CUDA events bracket the pair and three-body kernels of
+ * each evaluation; ix_get_kernel_times returns the durations (ms) of the last evaluation's kernels.  Level 2 also runs
+ * the three-body chain after the pair chain instead of concurrently with it, so that each bracket times its kernels
+ * alone.  A measurement tool with no counterpart in the reference. */
 int ix_set_profiling(ix_ctx* ctx, int enable);
 int ix_get_kernel_times(ix_ctx* ctx, double* pair_ms, double* three_body_ms);
 

@@ -5,10 +5,14 @@
 //
 //   kSiteCentroids       site positions (unweighted centroids, double) and the site rebuild check
 //   kSiteNeighbors       (rebuild only) per site A the sites B > A of other molecules within cutoff + skin
-//   kTriples             one warp per site A: the neighbors within the cutoff are staged in shared memory with their
-//                        double-precision minimum-image displacements from A; the pairs (B, C) of them are
-//                        enumerated by a flat triangular index so that all lanes are busy; each triple is counted
-//                        once (A lowest), evaluated in float, and its forces on B and C accumulate in shared memory
+//   kTriplesFast         one warp per site A with at most kAtmFast listed neighbors: the neighbors within the cutoff
+//                        are staged in shared memory with their double-precision minimum-image displacements from A
+//                        (rounded to float); the pairs (B, C) of them are enumerated by a flat triangular index so
+//                        that all lanes are busy, in rounds of kAtmRound pairs; each triple is counted once (A
+//                        lowest) and evaluated in float; the forces on B and C of each pair are stored and gathered
+//                        per staged neighbor in a fixed order (no atomics)
+//   kTriplesWide         the same for the rare sites with longer lists (up to kAtmMaxStaged within the cutoff), with
+//                        the B and C forces accumulated by shared-memory atomics
 //   kSpreadSiteForces    the site forces, shared equally among each site's particles, into the particle forces
 #pragma once
 
@@ -40,16 +44,33 @@ struct AtmBuffers {
     const int* molecule;         // effective molecule (negative input already replaced by -1 - site)
     double* sitePos;             // numSites x 3
     double* siteRef;             // numSites x 3, at the last list build
-    int* flag;                   // [0] rebuild, [1] neighbor overflow
+    int* flag;                   // [0] rebuild, [1] neighbor overflow, [2] a list longer than kAtmFast
     int* nbrCount;               // numSites
     int* nbr;                    // numSites x cap
     int cap;
     long long* siteForce;        // 3 x numSites, SoA fixed point
     long long* particleForce;    // 3 x numParticles, SoA fixed point (original order)
     int numParticles;
-    double* energyPartials;      // one per warp of the triple kernel's grid
+    double* energyPartials;      // one per warp of the fast triple kernel's grid, then one per warp of the wide one
     unsigned long long* tripleCount;
 };
+
+constexpr int kAtmFast = 64;         // neighbor lists up to this length take the fast triple kernel
+constexpr int kAtmRound = 64;        // (B, C) pairs evaluated before their forces are gathered
+constexpr int kAtmFastWarps = 4;
+
+// The flat triangular index p = c (c - 1) / 2 + b of the pairs b < c < kAtmFast, decoded: b | c << 8.
+struct TrianglePairs {
+    unsigned short bc[kAtmFast * (kAtmFast - 1) / 2];
+};
+constexpr TrianglePairs makeTrianglePairs() {
+    TrianglePairs t{};
+    int p = 0;
+    for (int c = 1; c < kAtmFast; c++)
+        for (int b = 0; b < c; b++) t.bc[p++] = (unsigned short)(b | (c << 8));
+    return t;
+}
+__device__ const TrianglePairs kTrianglePairs = makeTrianglePairs();
 
 __global__ void kSiteCentroids(AtmBuffers A, AtmConfig C, const double* pos) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -108,6 +129,8 @@ __global__ void kSiteNeighbors(AtmBuffers A, AtmConfig C) {
     if (lane == 0) {
         A.nbrCount[a] = min(count, A.cap);
         if (count > A.cap) atomicOr(A.flag + 1, 1);
+        // flag[2]: some list is longer than the fast triple kernel takes (cleared before each build)
+        if (count > kAtmFast) atomicOr(A.flag + 2, 1);
     }
     for (int d = 0; d < 3; d++)
         if (lane == 0) A.siteRef[3 * a + d] = A.sitePos[3 * a + d];
@@ -141,6 +164,230 @@ __device__ __forceinline__ void centroidDampingF(float r, float invR0, float& g,
     dg = 6.0f * x6 * e * rcpApprox(r);
 }
 
+// One triple (A, B, C) from the displacements AB = (ax, ay, az) and AC = (bx, by, bz) (minimum images) and the three
+// sites' parameters: the C9 coefficient (InteraxThreeBodyForceImpl.h:69-72) with the scale and alchemical factor
+// (ReferenceInteraxThreeBodyIxn.cpp:116-120), the ATM energy and its gradients (InteraxThreeBodyTerms.h:97-146),
+// optionally Tang-Toennies and centroid damping.  Returns false when BC is outside the cutoff or C9 vanishes.
+// fA, fB, fC: the forces on the three sites.
+__device__ __forceinline__ bool atmTriple(const AtmConfig& C, const float4& pa, const float4& pb, const float4& pc,
+                                          float ax, float ay, float az, float bx, float by, float bz, float& energy,
+                                          float3& fA, float3& fB, float3& fC) {
+    // a = AB, b = AC, c = BC (minimum image of C - B)
+    float cx = bx - ax, cy = by - ay, cz = bz - az;
+    if (C.periodic) minimumImageF(cx, cy, cz, C.boxf);
+    const float w = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
+    if (!(w < C.cutoff2)) return false;
+    const float wa = pa.y, wb = pb.y, wc = pc.y;
+    float c9 = 1.5f * pa.x * pb.x * pc.x * wa * wb * wc * ((wa + wb) + wc) *
+               __fdividef(1.0f, (wa + wb) * (wb + wc) * (wc + wa)) * C.scale;
+    if (pa.w != 0.0f || pb.w != 0.0f || pc.w != 0.0f) c9 *= C.lambda;
+    if (c9 == 0.0f) return false;
+    const float u = fmaf(ax, ax, fmaf(ay, ay, az * az));
+    const float v = fmaf(bx, bx, fmaf(by, by, bz * bz));
+    const float pp = fmaf(ax, bx, fmaf(ay, by, az * bz));
+    const float qq = fmaf(ax, cx, fmaf(ay, cy, az * cz));
+    const float ss = fmaf(bx, cx, fmaf(by, cy, bz * cz));
+    const float P = u * v * w;
+    const float y = rsqrtApprox(P);
+    const float invP = y * y;
+    const float invP32 = invP * y;
+    const float invP52 = invP32 * invP;
+    const float pqs = pp * qq * ss;
+    energy = c9 * fmaf(-3.0f * pqs, invP52, invP32);
+    const float radial = c9 * fmaf(15.0f * pqs, invP52, -3.0f * invP32);
+    const float cross = -3.0f * c9 * invP52;
+    const float ru = radial * rcpApprox(u), rv = radial * rcpApprox(v), rw = radial * rcpApprox(w);
+    float gax = ax * ru + (bx * (qq * ss) + cx * (pp * ss)) * cross;
+    float gay = ay * ru + (by * (qq * ss) + cy * (pp * ss)) * cross;
+    float gaz = az * ru + (bz * (qq * ss) + cz * (pp * ss)) * cross;
+    float gbx = bx * rv + (ax * (qq * ss) + cx * (pp * qq)) * cross;
+    float gby = by * rv + (ay * (qq * ss) + cy * (pp * qq)) * cross;
+    float gbz = bz * rv + (az * (qq * ss) + cz * (pp * qq)) * cross;
+    float gcx = cx * rw + (ax * (pp * ss) + bx * (pp * qq)) * cross;
+    float gcy = cy * rw + (ay * (pp * ss) + by * (pp * qq)) * cross;
+    float gcz = cz * rw + (az * (pp * ss) + bz * (pp * qq)) * cross;
+    if (C.useTangToennies || C.invCentroidRadius > 0.0f) {
+        float len[3], invLen[3];
+        len[0] = sqrtRefined(u, invLen[0]);
+        len[1] = sqrtRefined(v, invLen[1]);
+        len[2] = sqrtRefined(w, invLen[2]);
+        const float widths[3] = {pa.z + pb.z, pa.z + pc.z, pb.z + pc.z};
+        float f[3], dfdr[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            if (C.useTangToennies) {
+                const float rate = C.twoBeta * __fdividef(1.0f, widths[k]);
+                tangToennies3f(rate * len[k], f[k], dfdr[k]);
+                dfdr[k] *= rate;
+            }
+            else {
+                f[k] = 1.0f;
+                dfdr[k] = 0.0f;
+            }
+            if (C.invCentroidRadius > 0.0f) {
+                float g, dg;
+                centroidDampingF(len[k], C.invCentroidRadius, g, dg);
+                dfdr[k] = fmaf(dfdr[k], g, f[k] * dg);
+                f[k] *= g;
+            }
+        }
+        const float damping = f[0] * f[1] * f[2];
+        const float sa = energy * dfdr[0] * f[1] * f[2] * invLen[0];
+        const float sb = energy * f[0] * dfdr[1] * f[2] * invLen[1];
+        const float sc = energy * f[0] * f[1] * dfdr[2] * invLen[2];
+        gax = fmaf(gax, damping, ax * sa);
+        gay = fmaf(gay, damping, ay * sa);
+        gaz = fmaf(gaz, damping, az * sa);
+        gbx = fmaf(gbx, damping, bx * sb);
+        gby = fmaf(gby, damping, by * sb);
+        gbz = fmaf(gbz, damping, bz * sb);
+        gcx = fmaf(gcx, damping, cx * sc);
+        gcy = fmaf(gcy, damping, cy * sc);
+        gcz = fmaf(gcz, damping, cz * sc);
+        energy *= damping;
+    }
+    // forceA += dEda + dEdb; forceB += dEdc - dEda; forceC -= dEdb + dEdc (InteraxThreeBodyTerms.h:142-144)
+    fA = make_float3(gax + gbx, gay + gby, gaz + gbz);
+    fB = make_float3(gcx - gax, gcy - gay, gcz - gaz);
+    fC = make_float3(-(gbx + gcx), -(gby + gcy), -(gbz + gcz));
+    return true;
+}
+
+// Stage the neighbors of site a that are within the cutoff (in list order) with their displacements from a and their
+// parameters; returns how many there are (at most `capacity` are stored).
+template <class Store>
+__device__ __forceinline__ int stageTripleNeighbors(const AtmBuffers& A, const AtmConfig& C, int a, int n, int lane,
+                                                    int capacity, Store store) {
+    int m = 0;
+    for (int k0 = 0; k0 < n; k0 += 32) {
+        const int k = k0 + lane;
+        bool in = false;
+        double d[3];
+        int b = -1;
+        if (k < n) {
+            b = A.nbr[(size_t)a * A.cap + k];
+            siteDelta(A, C, a, b, d);
+            in = (float)(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) < C.cutoff2;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, in);
+        if (in) {
+            const int slot = m + __popc(bal & laneMaskLt());
+            if (slot < capacity) store(slot, b, (float)d[0], (float)d[1], (float)d[2]);
+        }
+        m += __popc(bal);
+    }
+    return m;
+}
+
+struct AtmFastStorage {
+    float4 pos[kAtmFast];        // displacement from A; w holds the molecule (int bits)
+    float4 params[kAtmFast];
+    int site[kAtmFast];
+    float4 fb[kAtmRound];        // force on B of each pair of the current round
+    float4 fc[kAtmRound];        // force on C
+};
+
+// 72 registers (7 blocks of 4 warps per SM)
+__global__ void __launch_bounds__(32 * kAtmFastWarps, 7) kTriplesFast(AtmBuffers A, AtmConfig C) {
+    __shared__ AtmFastStorage storage[kAtmFastWarps];
+    AtmFastStorage& S = storage[threadIdx.x >> 5];
+    const int lane = threadIdx.x & 31;
+    const int warp = blockIdx.x * kAtmFastWarps + (threadIdx.x >> 5);
+    double eAcc = 0.0;
+    unsigned long long triples = 0;
+    for (int a = warp; a < C.numSites; a += gridDim.x * kAtmFastWarps) {
+        const int n = A.nbrCount[a];
+        if (n > kAtmFast) continue;      // the wide kernel takes this site
+        const float4 pa = A.siteParams[a];
+        __syncwarp();
+        const int m = stageTripleNeighbors(A, C, a, n, lane, kAtmFast,
+                                           [&](int slot, int b, float x, float y, float z) {
+                                               S.pos[slot] = make_float4(x, y, z, __int_as_float(A.molecule[b]));
+                                               S.params[slot] = A.siteParams[b];
+                                               S.site[slot] = b;
+                                           });
+        __syncwarp();
+        float fa[3] = {0.0f, 0.0f, 0.0f};
+        float f0[3] = {0.0f, 0.0f, 0.0f}, f1[3] = {0.0f, 0.0f, 0.0f};   // staged neighbors lane, lane + 32
+        float eSite = 0.0f;
+        int next0 = lane + 1, next1 = lane + 33;    // next C of the pairs (k, C) each lane gathers as B
+        const int numPairs = m * (m - 1) / 2;
+        for (int base = 0; base < numPairs; base += kAtmRound) {
+            const int count = min(kAtmRound, numPairs - base);
+            for (int q = lane; q < count; q += 32) {
+                const unsigned bc = __ldg(kTrianglePairs.bc + base + q);
+                const int b = bc & 0xff, c = bc >> 8;
+                const float4 xb = S.pos[b], xc = S.pos[c];
+                float3 fB = make_float3(0.0f, 0.0f, 0.0f), fC = fB;
+                if (__float_as_int(xb.w) != __float_as_int(xc.w)) {
+                    float e;
+                    float3 fA;
+                    if (atmTriple(C, pa, S.params[b], S.params[c], xb.x, xb.y, xb.z, xc.x, xc.y, xc.z, e, fA, fB, fC)) {
+                        fa[0] += fA.x;
+                        fa[1] += fA.y;
+                        fa[2] += fA.z;
+                        eSite += e;
+                        triples++;
+                    }
+                    else fB = fC = make_float3(0.0f, 0.0f, 0.0f);
+                }
+                S.fb[q] = make_float4(fB.x, fB.y, fB.z, 0.0f);
+                S.fc[q] = make_float4(fC.x, fC.y, fC.z, 0.0f);
+            }
+            __syncwarp();
+            // gather, for the staged neighbors k = lane and lane + 32: the pairs (b, k) with b < k (contiguous) and
+            // the pairs (k, c) with c > k (increasing p as c grows)
+            auto gather = [&](int k, float f[3], int& next) {
+                if (k >= m) return;
+                const int first = k * (k - 1) / 2;
+                const int lo = max(first, base), hi = min(first + k, base + count);
+                for (int p = lo; p < hi; p++) {
+                    const float4 v = S.fc[p - base];
+                    f[0] += v.x;
+                    f[1] += v.y;
+                    f[2] += v.z;
+                }
+                for (; next < m; next++) {
+                    const int p = next * (next - 1) / 2 + k;
+                    if (p >= base + count) break;
+                    const float4 v = S.fb[p - base];
+                    f[0] += v.x;
+                    f[1] += v.y;
+                    f[2] += v.z;
+                }
+            };
+            gather(lane, f0, next0);
+            gather(lane + 32, f1, next1);
+            __syncwarp();
+        }
+        // the staged neighbors' forces, then A's (a fixed reduction tree over the lanes)
+        auto flush = [&](int k, const float f[3]) {
+            if (k >= m) return;
+            const int b = S.site[k];
+            if (f[0] != 0.0f) atomicAddFixed(A.siteForce + b, toFixed(f[0]));
+            if (f[1] != 0.0f) atomicAddFixed(A.siteForce + C.numSites + b, toFixed(f[1]));
+            if (f[2] != 0.0f) atomicAddFixed(A.siteForce + 2 * C.numSites + b, toFixed(f[2]));
+        };
+        flush(lane, f0);
+        flush(lane + 32, f1);
+        for (int o = 16; o > 0; o >>= 1) {
+            fa[0] += __shfl_xor_sync(0xffffffffu, fa[0], o);
+            fa[1] += __shfl_xor_sync(0xffffffffu, fa[1], o);
+            fa[2] += __shfl_xor_sync(0xffffffffu, fa[2], o);
+        }
+        if (lane == 0) {
+            if (fa[0] != 0.0f) atomicAddFixed(A.siteForce + a, toFixed(fa[0]));
+            if (fa[1] != 0.0f) atomicAddFixed(A.siteForce + C.numSites + a, toFixed(fa[1]));
+            if (fa[2] != 0.0f) atomicAddFixed(A.siteForce + 2 * C.numSites + a, toFixed(fa[2]));
+        }
+        eAcc += (double)eSite;
+    }
+    const double sum = warpSumD(eAcc);
+    if (lane == 0) A.energyPartials[warp] = sum;
+    for (int o = 16; o > 0; o >>= 1) triples += __shfl_xor_sync(0xffffffffu, triples, o);
+    if (lane == 0 && triples) atomicAdd(A.tripleCount, triples);
+}
+
 struct AtmWarpStorage {
     float dx[256], dy[256], dz[256];
     float4 params[256];
@@ -152,7 +399,8 @@ struct AtmWarpStorage {
 constexpr int kAtmWarps = 4;
 constexpr int kAtmMaxStaged = 256;
 
-__global__ void __launch_bounds__(32 * kAtmWarps) kTriples(AtmBuffers A, AtmConfig C) {
+// Sites whose lists are longer than kAtmFast.  Energies go to energyPartials[partialsOffset + warp].
+__global__ void __launch_bounds__(32 * kAtmWarps) kTriplesWide(AtmBuffers A, AtmConfig C, int partialsOffset) {
     extern __shared__ unsigned char atmShared[];
     AtmWarpStorage& S = reinterpret_cast<AtmWarpStorage*>(atmShared)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
@@ -160,36 +408,21 @@ __global__ void __launch_bounds__(32 * kAtmWarps) kTriples(AtmBuffers A, AtmConf
     unsigned long long triples = 0;
     for (int a = blockIdx.x * kAtmWarps + (threadIdx.x >> 5); a < C.numSites; a += gridDim.x * kAtmWarps) {
         const int n = A.nbrCount[a];
+        if (n <= kAtmFast) continue;     // the fast kernel takes this site
         const float4 pa = A.siteParams[a];
-        // stage the neighbors within the cutoff
-        int m = 0;
-        for (int k0 = 0; k0 < n; k0 += 32) {
-            const int k = k0 + lane;
-            bool in = false;
-            double d[3];
-            int b = -1;
-            if (k < n) {
-                b = A.nbr[(size_t)a * A.cap + k];
-                siteDelta(A, C, a, b, d);
-                in = (float)(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) < C.cutoff2;
-            }
-            const unsigned bal = __ballot_sync(0xffffffffu, in);
-            if (in) {
-                const int slot = m + __popc(bal & laneMaskLt());
-                if (slot < kAtmMaxStaged) {
-                    S.dx[slot] = (float)d[0];
-                    S.dy[slot] = (float)d[1];
-                    S.dz[slot] = (float)d[2];
-                    S.params[slot] = A.siteParams[b];
-                    S.mol[slot] = A.molecule[b];
-                    S.site[slot] = b;
-                    S.fx[slot] = 0.0f;
-                    S.fy[slot] = 0.0f;
-                    S.fz[slot] = 0.0f;
-                }
-            }
-            m += __popc(bal);
-        }
+        __syncwarp();
+        int m = stageTripleNeighbors(A, C, a, n, lane, kAtmMaxStaged,
+                                     [&](int slot, int b, float x, float y, float z) {
+                                         S.dx[slot] = x;
+                                         S.dy[slot] = y;
+                                         S.dz[slot] = z;
+                                         S.params[slot] = A.siteParams[b];
+                                         S.mol[slot] = A.molecule[b];
+                                         S.site[slot] = b;
+                                         S.fx[slot] = 0.0f;
+                                         S.fy[slot] = 0.0f;
+                                         S.fz[slot] = 0.0f;
+                                     });
         if (m > kAtmMaxStaged) {
             if (lane == 0) atomicOr(A.flag + 1, 2);
             m = kAtmMaxStaged;
@@ -204,94 +437,20 @@ __global__ void __launch_bounds__(32 * kAtmWarps) kTriples(AtmBuffers A, AtmConf
             while ((c + 1) * c / 2 <= p) c++;
             const int b = p - c * (c - 1) / 2;
             if (S.mol[b] == S.mol[c]) continue;
-            // a = AB, b = AC, c = BC (minimum image of C - B)
-            const float ax = S.dx[b], ay = S.dy[b], az = S.dz[b];
-            const float bx = S.dx[c], by = S.dy[c], bz = S.dz[c];
-            float cx = bx - ax, cy = by - ay, cz = bz - az;
-            if (C.periodic) minimumImageF(cx, cy, cz, C.boxf);
-            const float w = fmaf(cx, cx, fmaf(cy, cy, cz * cz));
-            if (!(w < C.cutoff2)) continue;
-            const float4 pb = S.params[b], pc = S.params[c];
-            // C9 (InteraxThreeBodyForceImpl.h:69-72), scale and alchemical factor (ReferenceInteraxThreeBodyIxn.cpp:116-120)
-            const float wa = pa.y, wb = pb.y, wc = pc.y;
-            float c9 = 1.5f * pa.x * pb.x * pc.x * wa * wb * wc * ((wa + wb) + wc) *
-                       __fdividef(1.0f, (wa + wb) * (wb + wc) * (wc + wa)) * C.scale;
-            if (pa.w != 0.0f || pb.w != 0.0f || pc.w != 0.0f) c9 *= C.lambda;
-            if (c9 == 0.0f) continue;
-            const float u = fmaf(ax, ax, fmaf(ay, ay, az * az));
-            const float v = fmaf(bx, bx, fmaf(by, by, bz * bz));
-            const float pp = fmaf(ax, bx, fmaf(ay, by, az * bz));
-            const float qq = fmaf(ax, cx, fmaf(ay, cy, az * cz));
-            const float ss = fmaf(bx, cx, fmaf(by, cy, bz * cz));
-            const float P = u * v * w;
-            const float y = rsqrtApprox(P);
-            const float invP = y * y;
-            const float invP32 = invP * y;
-            const float invP52 = invP32 * invP;
-            const float pqs = pp * qq * ss;
-            float energy = c9 * fmaf(-3.0f * pqs, invP52, invP32);
-            const float radial = c9 * fmaf(15.0f * pqs, invP52, -3.0f * invP32);
-            const float cross = -3.0f * c9 * invP52;
-            const float ru = radial * rcpApprox(u), rv = radial * rcpApprox(v), rw = radial * rcpApprox(w);
-            float gax = ax * ru + (bx * (qq * ss) + cx * (pp * ss)) * cross;
-            float gay = ay * ru + (by * (qq * ss) + cy * (pp * ss)) * cross;
-            float gaz = az * ru + (bz * (qq * ss) + cz * (pp * ss)) * cross;
-            float gbx = bx * rv + (ax * (qq * ss) + cx * (pp * qq)) * cross;
-            float gby = by * rv + (ay * (qq * ss) + cy * (pp * qq)) * cross;
-            float gbz = bz * rv + (az * (qq * ss) + cz * (pp * qq)) * cross;
-            float gcx = cx * rw + (ax * (pp * ss) + bx * (pp * qq)) * cross;
-            float gcy = cy * rw + (ay * (pp * ss) + by * (pp * qq)) * cross;
-            float gcz = cz * rw + (az * (pp * ss) + bz * (pp * qq)) * cross;
-            if (C.useTangToennies || C.invCentroidRadius > 0.0f) {
-                float len[3], invLen[3];
-                len[0] = sqrtRefined(u, invLen[0]);
-                len[1] = sqrtRefined(v, invLen[1]);
-                len[2] = sqrtRefined(w, invLen[2]);
-                const float widths[3] = {pa.z + pb.z, pa.z + pc.z, pb.z + pc.z};
-                float f[3], dfdr[3];
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    if (C.useTangToennies) {
-                        const float rate = C.twoBeta * __fdividef(1.0f, widths[k]);
-                        tangToennies3f(rate * len[k], f[k], dfdr[k]);
-                        dfdr[k] *= rate;
-                    }
-                    else {
-                        f[k] = 1.0f;
-                        dfdr[k] = 0.0f;
-                    }
-                    if (C.invCentroidRadius > 0.0f) {
-                        float g, dg;
-                        centroidDampingF(len[k], C.invCentroidRadius, g, dg);
-                        dfdr[k] = fmaf(dfdr[k], g, f[k] * dg);
-                        f[k] *= g;
-                    }
-                }
-                const float damping = f[0] * f[1] * f[2];
-                const float sa = energy * dfdr[0] * f[1] * f[2] * invLen[0];
-                const float sb = energy * f[0] * dfdr[1] * f[2] * invLen[1];
-                const float sc = energy * f[0] * f[1] * dfdr[2] * invLen[2];
-                gax = fmaf(gax, damping, ax * sa);
-                gay = fmaf(gay, damping, ay * sa);
-                gaz = fmaf(gaz, damping, az * sa);
-                gbx = fmaf(gbx, damping, bx * sb);
-                gby = fmaf(gby, damping, by * sb);
-                gbz = fmaf(gbz, damping, bz * sb);
-                gcx = fmaf(gcx, damping, cx * sc);
-                gcy = fmaf(gcy, damping, cy * sc);
-                gcz = fmaf(gcz, damping, cz * sc);
-                energy *= damping;
-            }
-            // forceA += dEda + dEdb; forceB += dEdc - dEda; forceC -= dEdb + dEdc (InteraxThreeBodyTerms.h:142-144)
-            fax += gax + gbx;
-            fay += gay + gby;
-            faz += gaz + gbz;
-            atomicAdd(&S.fx[b], gcx - gax);
-            atomicAdd(&S.fy[b], gcy - gay);
-            atomicAdd(&S.fz[b], gcz - gaz);
-            atomicAdd(&S.fx[c], -(gbx + gcx));
-            atomicAdd(&S.fy[c], -(gby + gcy));
-            atomicAdd(&S.fz[c], -(gbz + gcz));
+            float energy;
+            float3 fA, fB, fC;
+            if (!atmTriple(C, pa, S.params[b], S.params[c], S.dx[b], S.dy[b], S.dz[b], S.dx[c], S.dy[c], S.dz[c],
+                           energy, fA, fB, fC))
+                continue;
+            fax += fA.x;
+            fay += fA.y;
+            faz += fA.z;
+            atomicAdd(&S.fx[b], fB.x);
+            atomicAdd(&S.fy[b], fB.y);
+            atomicAdd(&S.fz[b], fB.z);
+            atomicAdd(&S.fx[c], fC.x);
+            atomicAdd(&S.fy[c], fC.y);
+            atomicAdd(&S.fz[c], fC.z);
             eAcc += energy;
             triples++;
         }
@@ -315,13 +474,13 @@ __global__ void __launch_bounds__(32 * kAtmWarps) kTriples(AtmBuffers A, AtmConf
         __syncwarp();
     }
     const double sum = warpSumD(eAcc);
-    if (lane == 0) A.energyPartials[blockIdx.x * kAtmWarps + (threadIdx.x >> 5)] = sum;
+    if (lane == 0) A.energyPartials[partialsOffset + blockIdx.x * kAtmWarps + (threadIdx.x >> 5)] = sum;
     for (int o = 16; o > 0; o >>= 1) triples += __shfl_xor_sync(0xffffffffu, triples, o);
     if (lane == 0 && triples) atomicAdd(A.tripleCount, triples);
 }
 
 // Each particle of a site receives the site force divided by the number of particles
-// (ReferenceInteraxThreeBodyIxn.cpp:127-133).
+// (ReferenceInteraxThreeBodyIxn.cpp:127-133).  The site forces are cleared as they are read.
 __global__ void kSpreadSiteForces(AtmBuffers A, AtmConfig C) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= C.numSites) return;
@@ -330,6 +489,7 @@ __global__ void kSpreadSiteForces(AtmBuffers A, AtmConfig C) {
     for (int d = 0; d < 3; d++) {
         const long long v = A.siteForce[d * C.numSites + s];
         if (v == 0) continue;
+        A.siteForce[d * C.numSites + s] = 0;
         const long long share = __double2ll_rn((double)v * inv);
         for (int k = b; k < e; k++) atomicAddFixed(A.particleForce + (size_t)d * A.numParticles + A.siteParticles[k], share);
     }

@@ -84,7 +84,9 @@ struct ix_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;      // the three-body chain, forked from and joined back into `stream`
+    cudaStream_t streamBody = nullptr;   // captures the branches of conditional graph nodes
     cudaEvent_t evFork = nullptr, evJoin = nullptr;
+    bool capturing = false;              // launches are being captured into a graph
     int numSMs = 148;
     std::string error;
     double defaultBox[9] = {2, 0, 0, 0, 2, 0, 0, 0, 2};
@@ -121,8 +123,7 @@ struct ix_ctx {
     // device memory
     std::map<std::string, DeviceBuffer> buffers;
     double* dPos = nullptr;              // n x 3
-    long long* dEnergyFixed = nullptr;   // 4
-    unsigned long long* dCounts = nullptr;   // pairs, triples
+    unsigned long long* dCounts = nullptr;   // pairs, triples being counted; then those of the last evaluation
     int* dFlags = nullptr;               // pair list flags [4], atm flags [2]
     double* dOutForces = nullptr;        // n x 3
     double* dOutEnergy = nullptr;        // 4
@@ -136,7 +137,8 @@ struct ix_ctx {
     float4* dP3 = nullptr;
     double* dPairPartials = nullptr;     // per-warp energies of the pair kernel (3 per warp)
     double* dAtmPartials = nullptr;      // per-warp energies of the triple kernel
-    int atmGridBlocks = 0;
+    int atmFastBlocks = 0;               // grid of the fast triple kernel
+    int atmGridBlocks = 0;               // grid of the wide triple kernel
     int* dFlagso = nullptr;
     float4 *dP0 = nullptr, *dP1 = nullptr, *dP2 = nullptr;
     int* dFlagsSorted = nullptr;
@@ -152,6 +154,7 @@ struct ix_ctx {
     bool mdForcesValid = false;          // dOutForces holds all-group forces of the current positions
     // optional CUDA-event timing of the pair and triple kernels (ix_set_profiling)
     bool profiling = false;
+    bool serialize = false;              // profiling level 2: the three-body chain runs after the pair chain
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     bool evPair = false, evAtm = false;
     long long launches = 0;              // kernels of this library launched on the context
@@ -164,6 +167,11 @@ struct ix_ctx {
 
 static void bumpVersion(ix_ctx* ctx) {
     if (ctx) ctx->version++;
+}
+
+// Energy slots of the triple kernels: one per warp of the fast grid, then one per warp of the wide grid.
+static size_t atmPartialCount(const ix_ctx* ctx) {
+    return (size_t)ctx->atmFastBlocks * kAtmFastWarps + (size_t)ctx->atmGridBlocks * kAtmWarps;
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -634,6 +642,9 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
     IX_TRY(deviceAlloc(ctx, "p2", np, &ctx->dP2));
     IX_TRY(deviceAlloc(ctx, "flagsSorted", np, &ctx->dFlagsSorted));
     IX_TRY(deviceAlloc(ctx, "forceFixed", 3 * (size_t)np, &ctx->P.forceFixed));
+    // accumulators start at zero here; afterwards the kernels that read them clear them
+    IX_CUDA(ctx, cudaMemsetAsync(ctx->P.forceFixed, 0, 3 * (size_t)np * sizeof(long long), ctx->stream));
+    IX_CUDA(ctx, cudaMemsetAsync(L.taskCounter, 0, sizeof(int), ctx->stream));
     ctx->P.p0 = ctx->dP0;
     ctx->P.p1 = ctx->dP1;
     ctx->P.p2 = ctx->dP2;
@@ -688,6 +699,9 @@ static int allocateAtm(ix_ctx* ctx) {
     IX_TRY(deviceAlloc(ctx, "nbrCount", ns, &A.nbrCount));
     IX_TRY(deviceAlloc(ctx, "siteForce", 3 * (size_t)ns, &A.siteForce));
     IX_TRY(deviceAlloc(ctx, "atmParticleForce", 3 * (size_t)ctx->n, &A.particleForce));
+    // accumulators start at zero here; afterwards the kernels that read them clear them
+    IX_CUDA(ctx, cudaMemsetAsync(A.siteForce, 0, 3 * (size_t)ns * sizeof(long long), ctx->stream));
+    IX_CUDA(ctx, cudaMemsetAsync(A.particleForce, 0, 3 * (size_t)ctx->n * sizeof(long long), ctx->stream));
     // neighbor capacity: twice the expected half list at the site density, at least 64, at most all sites
     if (ctx->atmCap == 0) {
         double volume = ctx->atmPeriodic ? ctx->box[0] * ctx->box[4] * ctx->box[8] : std::max(1.0, ns / 30.0);
@@ -702,8 +716,10 @@ static int allocateAtm(ix_ctx* ctx) {
     IX_TRY(deviceAlloc(ctx, "nbr", (size_t)ns * A.cap, &A.nbr));
     A.flag = ctx->dFlags + 4;
     A.numParticles = ctx->n;
-    ctx->atmGridBlocks = std::max(1, std::min((ns + kAtmWarps - 1) / kAtmWarps, ctx->numSMs * 8));
-    IX_TRY(deviceAlloc(ctx, "atmPartials", (size_t)ctx->atmGridBlocks * kAtmWarps, &ctx->dAtmPartials));
+    // fast kernel: one warp per site; wide kernel (long lists): a grid that scans every site
+    ctx->atmFastBlocks = std::max(1, (ns + kAtmFastWarps - 1) / kAtmFastWarps);
+    ctx->atmGridBlocks = std::max(1, std::min((ns + kAtmWarps - 1) / kAtmWarps, ctx->numSMs * 2));
+    IX_TRY(deviceAlloc(ctx, "atmPartials", atmPartialCount(ctx), &ctx->dAtmPartials));
     A.energyPartials = ctx->dAtmPartials;
     A.tripleCount = ctx->dCounts + 1;
     ctx->atmAllocated = true;
@@ -732,21 +748,25 @@ static int uploadAtmParams(ix_ctx* ctx) {
 // evaluation
 // ---------------------------------------------------------------------------------------------------------------------
 
-__global__ void kFinalize(int n, int np, const int* slotOf, const long long* pairForce, const long long* atmForce,
+// The accumulators are read and cleared here, so the next evaluation starts from zero without memsets (they are
+// zeroed once when allocated).
+__global__ void kFinalize(int n, int np, const int* slotOf, long long* pairForce, long long* atmForce,
                           double* outForces, long long* addFixed, int stride) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         long long f[3] = {0, 0, 0};
         if (pairForce) {
             int s = slotOf[i];
-            f[0] = pairForce[s];
-            f[1] = pairForce[np + s];
-            f[2] = pairForce[2 * np + s];
+            for (int d = 0; d < 3; d++) {
+                f[d] = pairForce[d * np + s];
+                pairForce[d * np + s] = 0;
+            }
         }
         if (atmForce) {
-            f[0] += atmForce[i];
-            f[1] += atmForce[n + i];
-            f[2] += atmForce[2 * n + i];
+            for (int d = 0; d < 3; d++) {
+                f[d] += atmForce[d * n + i];
+                atmForce[d * n + i] = 0;
+            }
         }
         if (outForces) {
             const double inv = 1.0 / kFixedScale;
@@ -762,13 +782,15 @@ __global__ void kFinalize(int n, int np, const int* slotOf, const long long* pai
     }
 }
 
-// Term energies from the per-warp partials: each thread sums a fixed strided subset, then a fixed reduction tree,
-// so the result is identical on every run.  lrcEnergy (the long range correction, from the host) joins term 0.
+// Term energies from the per-tile / per-warp partials: each block sums a fixed share, then the last block adds the
+// block sums in order, so the result is identical on every run.  lrcEnergy (the long range correction, from the host)
+// joins term 0.  The last block also publishes the interaction counts (counts[0..1] -> counts[2..3], clearing the
+// accumulators) and resets the pair kernel's tile counter for the next evaluation.
 constexpr int kReduceBlocks = 64;
 
 __global__ void kReduceEnergies(const double* pairPartials, const int* numPairPartials, int pairCap,
                                 const double* atmPartials, int numAtmWarps, double lrcEnergy, double* outEnergy,
-                                double* blockSums, unsigned* ticket) {
+                                double* blockSums, unsigned* ticket, unsigned long long* counts, int* taskCounter) {
     __shared__ double red[4][256];
     __shared__ bool last;
     const int t = threadIdx.x;
@@ -809,6 +831,15 @@ __global__ void kReduceEnergies(const double* pairPartials, const int* numPairPa
         for (int b = 0; b < (int)gridDim.x; b++) v += ((volatile double*)blockSums)[4 * b + t];
         if (t == 0) v += lrcEnergy;
         if (outEnergy) outEnergy[t] = v;
+        if (t == 0) {
+            if (counts) {
+                counts[2] = counts[0];
+                counts[3] = counts[1];
+                counts[0] = 0;
+                counts[1] = 0;
+            }
+            if (taskCounter) *taskCounter = 0;
+        }
     }
 }
 
@@ -863,6 +894,72 @@ static PairTermConfig pairConfig(const ix_ctx* ctx, unsigned terms) {
 
 static int stageUploads(ix_ctx* ctx, unsigned terms);
 
+__global__ void kSetCondition(cudaGraphConditionalHandle handle, const int* flag) {
+    cudaGraphSetConditional(handle, *(volatile const int*)flag != 0 ? 1u : 0u);
+}
+
+// Profiling events: while capturing, external event-record nodes of the graph; launched directly, ordinary records.
+static void recordTiming(ix_ctx* ctx, int i, cudaStream_t s) {
+    if (!ctx->profiling) return;
+    if (ctx->capturing) cudaEventRecordWithFlags(ctx->ev[i], s, cudaEventRecordExternal);
+    else cudaEventRecord(ctx->ev[i], s);
+}
+
+__global__ void kClearFlagIf(int* target, const int* gate) {
+    if (*(volatile const int*)gate != 0) *target = 0;
+}
+
+// Launch `body` (a callable taking the stream to launch on) when *flag is set, else `orElse` (size 2) or nothing.
+// While the evaluation is being captured into a graph this is a conditional node whose branches are captured on the
+// context's third stream; the flag is read on the device each time the graph runs, so a step without a list rebuild
+// launches none of the rebuild kernels.  Launched directly, `body` runs, its kernels reading the flag themselves
+// (and `body` containing `orElse`'s work).  The launch counter keeps the kernels of the branch taken when the flag
+// is clear.
+template <class Body, class Else>
+static int launchConditional(ix_ctx* ctx, cudaStream_t st, const int* flag, Body body, Else orElse, int size) {
+    if (!ctx->capturing) return body(st);
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t numDeps = 0;
+    IX_CUDA(ctx, cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &numDeps));
+    cudaGraphConditionalHandle handle;
+    IX_CUDA(ctx, cudaGraphConditionalHandleCreate(&handle, graph, 0, cudaGraphCondAssignDefault));
+    kSetCondition<<<1, 1, 0, st>>>(handle, flag);
+    ctx->launches += 1;
+    IX_CUDA(ctx, cudaStreamGetCaptureInfo(st, &status, nullptr, &graph, &deps, &numDeps));
+    cudaGraphNodeParams params = {};
+    params.type = cudaGraphNodeTypeConditional;
+    params.conditional.handle = handle;
+    params.conditional.type = cudaGraphCondTypeIf;
+    params.conditional.size = (unsigned)size;
+    cudaGraphNode_t node;
+    IX_CUDA(ctx, cudaGraphAddNode(&node, graph, deps, numDeps, &params));
+    for (int k = 0; k < size; k++) {
+        IX_CUDA(ctx, cudaStreamBeginCaptureToGraph(ctx->streamBody, params.conditional.phGraph_out[k], nullptr,
+                                                   nullptr, 0, cudaStreamCaptureModeThreadLocal));
+        const long long before = ctx->launches;
+        const int rc = k == 0 ? body(ctx->streamBody) : orElse(ctx->streamBody);
+        cudaGraph_t captured = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(ctx->streamBody, &captured);
+        if (k == 0) ctx->launches = before;
+        if (rc != IX_OK) return rc;
+        IX_CUDA(ctx, e);
+    }
+    IX_CUDA(ctx, cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies));
+    return IX_OK;
+}
+
+template <class Body>
+static int launchIf(ix_ctx* ctx, cudaStream_t st, const int* flag, Body body) {
+    return launchConditional(ctx, st, flag, body, body, 1);
+}
+
+template <class Body, class Else>
+static int launchIfElse(ix_ctx* ctx, cudaStream_t st, const int* flag, Body body, Else orElse) {
+    return launchConditional(ctx, st, flag, body, orElse, 2);
+}
+
 // Launch the whole evaluation on the context's stream.  Forces go to outForces (device, n x 3 doubles) and/or are
 // added to addFixed; energies to outEnergy (device, 4 doubles).
 static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, double* outEnergy, long long* addFixed,
@@ -872,10 +969,8 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
     const bool doPair = (terms & 7u) != 0;
     const bool doAtm = (terms & 8u) != 0;
     IX_TRY(stageUploads(ctx, terms));
-    IX_CUDA(ctx, cudaMemsetAsync(ctx->dEnergyFixed, 0, 4 * sizeof(long long), st));
-    IX_CUDA(ctx, cudaMemsetAsync(ctx->dCounts, 0, 2 * sizeof(unsigned long long), st));
     // the three-body chain runs on a second stream, concurrently with the pair list and pair kernel
-    const bool fork = doPair && doAtm;
+    const bool fork = doPair && doAtm && !ctx->serialize;
     cudaStream_t sa = fork ? ctx->stream2 : st;
     if (fork) {
         IX_CUDA(ctx, cudaEventRecord(ctx->evFork, st));
@@ -899,19 +994,30 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         C.maxMove2 = 0.25f * kSiteSkin * kSiteSkin;
         const int tpb = 256;
         const int gS = (C.numSites + tpb - 1) / tpb;
-        IX_CUDA(ctx, cudaMemsetAsync(A.siteForce, 0, 3 * (size_t)C.numSites * sizeof(long long), sa));
-        IX_CUDA(ctx, cudaMemsetAsync(A.particleForce, 0, 3 * (size_t)n * sizeof(long long), sa));
         kSiteCentroids<<<gS, tpb, 0, sa>>>(A, C, ctx->dPos);
-        kSiteNeighbors<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, sa>>>(A, C);
-        kClearFlag<<<1, 1, 0, sa>>>(A.flag);
-        const size_t smem = sizeof(AtmWarpStorage) * kAtmWarps;
-        int blocks = ctx->atmGridBlocks;
-        if (ctx->profiling) cudaEventRecordWithFlags(ctx->ev[2], sa, cudaEventRecordExternal);
-        kTriples<<<std::max(1, blocks), 32 * kAtmWarps, smem, sa>>>(A, C);
-        if (ctx->profiling) cudaEventRecordWithFlags(ctx->ev[3], sa, cudaEventRecordExternal);
+        ctx->launches += 1;
+        // site list rebuild (the centroid kernel set the flag); the long-list flag is recomputed with the lists
+        IX_TRY(launchIf(ctx, sa, A.flag, [&](cudaStream_t s) {
+            kClearFlagIf<<<1, 1, 0, s>>>(A.flag + 2, A.flag);
+            kSiteNeighbors<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, s>>>(A, C);
+            kClearFlag<<<1, 1, 0, s>>>(A.flag);
+            ctx->launches += 3;
+            return IX_OK;
+        }));
+        recordTiming(ctx, 2, sa);
+        kTriplesFast<<<ctx->atmFastBlocks, 32 * kAtmFastWarps, 0, sa>>>(A, C);
+        ctx->launches += 1;
+        // the sites whose lists are too long for the fast kernel, if there are any
+        IX_TRY(launchIf(ctx, sa, A.flag + 2, [&](cudaStream_t s) {
+            const size_t smem = sizeof(AtmWarpStorage) * kAtmWarps;
+            kTriplesWide<<<ctx->atmGridBlocks, 32 * kAtmWarps, smem, s>>>(A, C, ctx->atmFastBlocks * kAtmFastWarps);
+            ctx->launches += 1;
+            return IX_OK;
+        }));
+        recordTiming(ctx, 3, sa);
         ctx->evAtm = ctx->profiling;
         kSpreadSiteForces<<<gS, tpb, 0, sa>>>(A, C);
-        ctx->launches += 5;
+        ctx->launches += 1;
         IX_CUDA(ctx, cudaGetLastError());
     }
     double lrcEnergy = 0.0;
@@ -921,35 +1027,46 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         const int gN = (n + tpb - 1) / tpb, gNp = (L.np + tpb - 1) / tpb;
         const int gCells = (L.numCells + tpb - 1) / tpb;
         kCheckDisplacement<<<gN, tpb, 0, st>>>(L, 0.25f * kPairSkin * kPairSkin);
-        kResetCells<<<std::max(1, std::min(gCells, 1024)), tpb, 0, st>>>(L);
-        if (!ctx->G.periodic) kParticleBounds<<<gN, tpb, 0, st>>>(L);
-        kCellKeys<<<gN, tpb, 0, st>>>(L, ctx->G);
-        kScanCells<<<1, 1024, 0, st>>>(L);
-        kScatterCells<<<gN, tpb, 0, st>>>(L);
-        kSortWithinCells<<<gCells, tpb, 0, st>>>(L);
-        kSortedAtoms<<<gNp, tpb, 0, st>>>(L, ctx->G);
-        kGatherParams<<<gNp, tpb, 0, st>>>(L, ctx->dP0o, ctx->dP1o, ctx->dP2o, ctx->dP3o, ctx->dFlagso, ctx->dP0,
-                                           ctx->dP1, ctx->dP2, ctx->dP3, ctx->dFlagsSorted);
-        kUpdateSortedPositions<<<gNp, tpb, 0, st>>>(L);
-        kBlockBounds<<<(L.nb * 32 + tpb - 1) / tpb, tpb, 0, st>>>(L, ctx->G);
-        const int warpsPerBlock = 8;
-        const int gParts = (L.nb * kListParts + warpsPerBlock - 1) / warpsPerBlock;
-        const int gB = (L.nb + warpsPerBlock - 1) / warpsPerBlock;
-        kListAtoms<0><<<gParts, 32 * warpsPerBlock, 0, st>>>(L, ctx->G);
-        kScanTiles<<<1, 1024, 0, st>>>(L);
-        kListAtoms<1><<<gParts, 32 * warpsPerBlock, 0, st>>>(L, ctx->G);
-        kTileHeaders<<<gB, 32 * warpsPerBlock, 0, st>>>(L);
-        kTileMasks<<<ctx->numSMs * 8, 32 * warpsPerBlock, 0, st>>>(L, ctx->G);
-        kClearFlag<<<1, 1, 0, st>>>(L.flag);
-        IX_CUDA(ctx, cudaMemsetAsync(ctx->P.forceFixed, 0, 3 * (size_t)L.np * sizeof(long long), st));
+        ctx->launches += 1;
+        // the current positions in the build frame, every step
+        auto refresh = [&](cudaStream_t s) {
+            kUpdateSortedPositions<<<gNp, tpb, 0, s>>>(L);
+            ctx->launches += 1;
+            return IX_OK;
+        };
+        // list rebuild (the displacement check set the flag): cell sort, then the tiles and their masks from the
+        // refreshed positions
+        auto rebuild = [&](cudaStream_t s) {
+            kResetCells<<<std::max(1, std::min(gCells, 1024)), tpb, 0, s>>>(L);
+            if (!ctx->G.periodic) kParticleBounds<<<gN, tpb, 0, s>>>(L);
+            kCellKeys<<<gN, tpb, 0, s>>>(L, ctx->G);
+            kScanCells<<<1, 1024, 0, s>>>(L);
+            kScatterCells<<<gN, tpb, 0, s>>>(L);
+            kSortWithinCells<<<gCells, tpb, 0, s>>>(L);
+            kSortedAtoms<<<gNp, tpb, 0, s>>>(L, ctx->G);
+            kGatherParams<<<gNp, tpb, 0, s>>>(L, ctx->dP0o, ctx->dP1o, ctx->dP2o, ctx->dP3o, ctx->dFlagso, ctx->dP0,
+                                              ctx->dP1, ctx->dP2, ctx->dP3, ctx->dFlagsSorted);
+            refresh(s);
+            kBlockBounds<<<(L.nb * 32 + tpb - 1) / tpb, tpb, 0, s>>>(L, ctx->G);
+            const int warpsPerBlock = 8;
+            const int gParts = (L.nb * kListParts + warpsPerBlock - 1) / warpsPerBlock;
+            const int gB = (L.nb + warpsPerBlock - 1) / warpsPerBlock;
+            kListAtoms<0><<<gParts, 32 * warpsPerBlock, 0, s>>>(L, ctx->G);
+            kScanTiles<<<1, 1024, 0, s>>>(L);
+            kListAtoms<1><<<gParts, 32 * warpsPerBlock, 0, s>>>(L, ctx->G);
+            kTileHeaders<<<gB, 32 * warpsPerBlock, 0, s>>>(L);
+            kTileMasks<<<ctx->numSMs * 8, 32 * warpsPerBlock, 0, s>>>(L, ctx->G);
+            kClearFlag<<<1, 1, 0, s>>>(L.flag);
+            ctx->launches += ctx->G.periodic ? 14 : 15;
+            return IX_OK;
+        };
+        IX_TRY(launchIfElse(ctx, st, L.flag, rebuild, refresh));
         PairTermConfig C = pairConfig(ctx, terms);
         // the lean instantiation when no selected term has a soft core, a switching function or the order-2 overlap
         bool lean = true;
         for (int t = 0; t < 3; t++)
             if ((terms >> t) & 1u) lean = lean && C.softShift[t] == 0.0f && !C.useSwitch[t] && C.overlapMethod[t] == 0;
-        IX_CUDA(ctx, cudaMemsetAsync(L.taskCounter, 0, sizeof(int), st));
-        // the external flag makes the records event nodes when the evaluation is captured into a graph
-        if (ctx->profiling) cudaEventRecordWithFlags(ctx->ev[0], st, cudaEventRecordExternal);
+        recordTiming(ctx, 0, st);
         // the class-pair table serves the exact overlap method only
         bool table = ctx->P.coef != nullptr;
         for (int t = 1; t < 3; t++)
@@ -959,8 +1076,8 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         else if (lean) kPairTiles<true, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
         else if (table) kPairTiles<false, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
         else kPairTiles<false, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
-        ctx->launches += ctx->G.periodic ? 17 : 18;
-        if (ctx->profiling) cudaEventRecordWithFlags(ctx->ev[1], st, cudaEventRecordExternal);
+        ctx->launches += 1;
+        recordTiming(ctx, 1, st);
         ctx->evPair = ctx->profiling;
         IX_CUDA(ctx, cudaGetLastError());
         const PairTerm& D = ctx->term[0];
@@ -977,8 +1094,9 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
                                               doAtm ? ctx->A.particleForce : nullptr, outForces, addFixed, stride);
     kReduceEnergies<<<kReduceBlocks, 256, 0, st>>>(doPair ? ctx->dPairPartials : nullptr, ctx->L.numTiles,
                                                    ctx->L.tileCap, doAtm ? ctx->dAtmPartials : nullptr,
-                                                   ctx->atmGridBlocks * kAtmWarps, lrcEnergy, outEnergy,
-                                                   ctx->dEnergyBlocks, ctx->dReduceTicket);
+                                                   (int)atmPartialCount(ctx), lrcEnergy, outEnergy,
+                                                   ctx->dEnergyBlocks, ctx->dReduceTicket, ctx->dCounts,
+                                                   doPair ? ctx->L.taskCounter : nullptr);
     ctx->launches += 2;
     IX_CUDA(ctx, cudaGetLastError());
     return IX_OK;
@@ -1044,7 +1162,9 @@ static int launchGraph(ix_ctx* ctx, LaunchGraph& g, const GraphKey& key, F&& enq
     if (!g.exec || g.version != ctx->version || !(g.key == key)) {
         const long long before = ctx->launches;
         IX_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        ctx->capturing = true;
         const int rc = enqueue();
+        ctx->capturing = false;
         cudaGraph_t graph = nullptr;
         const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
         if (rc != IX_OK || e != cudaSuccess) {
@@ -1054,15 +1174,12 @@ static int launchGraph(ix_ctx* ctx, LaunchGraph& g, const GraphKey& key, F&& enq
             if (rc != IX_OK) return rc;
             return fail(ctx, IX_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
         }
+        // a new instantiation (the conditional nodes' handles belong to the captured graph)
         if (g.exec) {
-            cudaGraphExecUpdateResultInfo info;
-            if (cudaGraphExecUpdate(g.exec, graph, &info) != cudaSuccess) {
-                cudaGetLastError();
-                cudaGraphExecDestroy(g.exec);
-                g.exec = nullptr;
-            }
+            cudaGraphExecDestroy(g.exec);
+            g.exec = nullptr;
         }
-        if (!g.exec) {
+        {
             const cudaError_t ie = cudaGraphInstantiate(&g.exec, graph, 0);
             if (ie != cudaSuccess) {
                 cudaGraphDestroy(graph);
@@ -1156,6 +1273,7 @@ int ix_ctx_create(int num_particles, int device, const double* default_box, ix_c
     }
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->streamBody, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->evFork, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->evJoin, cudaEventDisableTiming) != cudaSuccess) {
         ix_ctx_destroy(ctx);
@@ -1163,8 +1281,7 @@ int ix_ctx_create(int num_particles, int device, const double* default_box, ix_c
     }
     int rc = IX_OK;
     if ((rc = deviceAlloc(ctx, "pos", 3 * (size_t)num_particles, &ctx->dPos)) != IX_OK ||
-        (rc = deviceAlloc(ctx, "energyFixed", 4, &ctx->dEnergyFixed)) != IX_OK ||
-        (rc = deviceAlloc(ctx, "counts", 2, &ctx->dCounts)) != IX_OK ||
+        (rc = deviceAlloc(ctx, "counts", 4, &ctx->dCounts)) != IX_OK ||
         (rc = deviceAlloc(ctx, "flags", 8, &ctx->dFlags)) != IX_OK ||
         (rc = deviceAlloc(ctx, "outForces", 3 * (size_t)num_particles, &ctx->dOutForces)) != IX_OK ||
         (rc = deviceAlloc(ctx, "outEnergy", 4, &ctx->dOutEnergy)) != IX_OK ||
@@ -1177,6 +1294,7 @@ int ix_ctx_create(int num_particles, int device, const double* default_box, ix_c
     int init[8] = {1, 0, 0, 0, 1, 0, 0, 0};
     cudaMemcpy(ctx->dFlags, init, sizeof(init), cudaMemcpyHostToDevice);
     cudaMemset(ctx->dReduceTicket, 0, sizeof(unsigned));
+    cudaMemset(ctx->dCounts, 0, 4 * sizeof(unsigned long long));
     *out = ctx;
     return IX_OK;
 }
@@ -1195,6 +1313,7 @@ void ix_ctx_destroy(ix_ctx* ctx) {
     if (ctx->evFork) cudaEventDestroy(ctx->evFork);
     if (ctx->evJoin) cudaEventDestroy(ctx->evJoin);
     if (ctx->stream2) cudaStreamDestroy(ctx->stream2);
+    if (ctx->streamBody) cudaStreamDestroy(ctx->streamBody);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }
@@ -1384,7 +1503,7 @@ int ix_compute(ix_ctx* ctx, int groups, int include_forces, int include_energy, 
     if (terms) {
         IX_CUDA(ctx, cudaMemcpy(e, ctx->dOutEnergy, sizeof(e), cudaMemcpyDeviceToHost));
         unsigned long long c[2];
-        IX_CUDA(ctx, cudaMemcpy(c, ctx->dCounts, sizeof(c), cudaMemcpyDeviceToHost));
+        IX_CUDA(ctx, cudaMemcpy(c, ctx->dCounts + 2, sizeof(c), cudaMemcpyDeviceToHost));
         ctx->lastPairs = (terms & 7u) ? (long long)c[0] : 0;
         ctx->lastTriples = (terms & 8u) ? (long long)c[1] : 0;
     }
@@ -1493,6 +1612,7 @@ int ix_set_profiling(ix_ctx* ctx, int enable) {
     if (enable && !ctx->ev[0])
         for (auto& e : ctx->ev) IX_CUDA(ctx, cudaEventCreate(&e));
     ctx->profiling = enable != 0;
+    ctx->serialize = enable == 2;
     bumpVersion(ctx);
     ctx->evPair = ctx->evAtm = false;
     return IX_OK;
@@ -1585,7 +1705,7 @@ int ix_md_finish(ix_ctx* ctx, double* positions, double* velocities, double* ene
         return fail(ctx, IX_ERR_STATE, "neighbor list overflow during MD; the lists were grown, rerun the steps");
     }
     unsigned long long c[2] = {0, 0};
-    IX_CUDA(ctx, cudaMemcpy(c, ctx->dCounts, sizeof(c), cudaMemcpyDeviceToHost));
+    IX_CUDA(ctx, cudaMemcpy(c, ctx->dCounts + 2, sizeof(c), cudaMemcpyDeviceToHost));
     ctx->lastPairs = (terms & 7u) ? (long long)c[0] : 0;
     ctx->lastTriples = (terms & 8u) ? (long long)c[1] : 0;
     const int n = ctx->n;
@@ -1632,7 +1752,8 @@ namespace {
 constexpr int kNoAllocMaxParticles = 16384;
 constexpr int kNoAllocMaxSites = 4096;
 constexpr int kNoAllocMaxNeighbors = 128;
-constexpr int kNoAllocBlocks = 148 * 8;
+constexpr int kNoAllocFastBlocks = kNoAllocMaxSites / kAtmFastWarps;   // one warp per site
+constexpr int kNoAllocBlocks = 148 * 2;                                 // grid of the wide triple kernel
 
 struct NoAllocScratch {
     double sitePos[3 * kNoAllocMaxSites];
@@ -1643,11 +1764,11 @@ struct NoAllocScratch {
     int nbr[kNoAllocMaxSites * kNoAllocMaxNeighbors];
     long long siteForce[3 * kNoAllocMaxSites];
     long long particleForce[3 * kNoAllocMaxParticles];
-    double energyPartials[kNoAllocBlocks * kAtmWarps];
+    double energyPartials[kNoAllocFastBlocks * kAtmFastWarps + kNoAllocBlocks * kAtmWarps];
     double energy[4];
     double energyBlocks[4];      // the energy reduction's block sum (one block)
     unsigned reduceTicket;
-    int flag[2];
+    int flag[3];
     unsigned long long tripleCount;
 };
 
@@ -1693,6 +1814,7 @@ __global__ void kNoAllocPrepare(NoAllocScratch* S, int numParticles, int numSite
     if (t == 0) {
         S->flag[0] = 1;      // always build the neighbor list
         S->flag[1] = 0;
+        S->flag[2] = 0;
         S->tripleCount = 0;
     }
 }
@@ -1806,16 +1928,20 @@ int ix_three_body_noalloc(int num_particles, const double* d_positions, const do
     A.tripleCount = &S->tripleCount;
     if (num_sites > 0) {
         kSiteNeighbors<<<(num_sites * 32 + tpb - 1) / tpb, tpb, 0, st>>>(A, C);
+        const int fastBlocks = (num_sites + kAtmFastWarps - 1) / kAtmFastWarps;
         const int blocks = std::max(1, std::min((num_sites + kAtmWarps - 1) / kAtmWarps, kNoAllocBlocks));
-        kTriples<<<blocks, 32 * kAtmWarps, sizeof(AtmWarpStorage) * kAtmWarps, st>>>(A, C);
+        kTriplesFast<<<fastBlocks, 32 * kAtmFastWarps, 0, st>>>(A, C);
+        kTriplesWide<<<blocks, 32 * kAtmWarps, sizeof(AtmWarpStorage) * kAtmWarps, st>>>(A, C,
+                                                                                        fastBlocks * kAtmFastWarps);
         kNoAllocSpread<<<(num_sites + tpb - 1) / tpb, tpb, 0, st>>>(S, num_particles, num_sites, d_site_offsets,
                                                                    d_site_particles);
-        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, nullptr, 0, S->energyPartials, blocks * kAtmWarps, 0.0, S->energy,
-                                           S->energyBlocks, &S->reduceTicket);
+        kReduceEnergies<<<1, 256, 0, st>>>(nullptr, nullptr, 0, S->energyPartials,
+                                           fastBlocks * kAtmFastWarps + blocks * kAtmWarps, 0.0, S->energy,
+                                           S->energyBlocks, &S->reduceTicket, nullptr, nullptr);
     }
     else {
         kReduceEnergies<<<1, 256, 0, st>>>(nullptr, nullptr, 0, nullptr, 0, 0.0, S->energy, S->energyBlocks,
-                                           &S->reduceTicket);
+                                           &S->reduceTicket, nullptr, nullptr);
     }
     kNoAllocFinish<<<(num_particles + tpb - 1) / tpb, tpb, 0, st>>>(S, num_particles, d_forces);
     e = cudaMemcpyAsync(d_energy, &S->energy[3], sizeof(double), cudaMemcpyDeviceToDevice, st);

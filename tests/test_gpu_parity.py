@@ -10,6 +10,7 @@ oracle.  Single pairs and triples are checked against the reference's single-pre
 (energy 2e-5 of sum |E_pair|, force 2e-4 of the largest force; three-body 1e-5 / 1e-4), since a lone pair's energy
 may be a near-cancellation of terms.
 """
+import ctypes
 import math
 
 import numpy as np
@@ -704,6 +705,17 @@ def test_graphs_match_direct_launches():
             states.append(ctx.getState())
         assert states[0].getPotentialEnergy() == states[1].getPotentialEnergy()
         assert np.array_equal(states[0].getForces(), states[1].getForces())
+    # kernel timing (events in the graph or on the streams; level 2 serialises the three-body chain): same results
+    reference = states[0]
+    for ctx in ctxs:
+        ctx._check(ctx._lib.ix_set_profiling(ctx._ctx, 2))
+        st = ctx.getState()
+        assert st.getPotentialEnergy() == reference.getPotentialEnergy()
+        assert np.array_equal(st.getForces(), reference.getForces())
+        pair_ms, atm_ms = ctypes.c_double(), ctypes.c_double()
+        ctx._check(ctx._lib.ix_get_kernel_times(ctx._ctx, ctypes.byref(pair_ms), ctypes.byref(atm_ms)))
+        assert pair_ms.value > 0 and atm_ms.value > 0
+        ctx._check(ctx._lib.ix_set_profiling(ctx._ctx, 0))
     vel = W.initial_velocities(system, 300.0, seed=2)
     runs = []
     for ctx in ctxs:
