@@ -319,11 +319,113 @@ def run_ours(args, rank, world):
     print(json.dumps(line))
 
 
+def run_clusters(args, rank, world, num_clusters=4096, plain_sample=128):
+    """Batched configuration: 4,096 water clusters of 2..32 waters (NoCutoff pair forces, ATM without cutoff), one
+    energy+force evaluation of all of them per step through one CUDA graph, against the plain per-system path (one
+    Context per cluster, evaluated one after the other) on a sample of the same clusters.  Each rank evaluates its own
+    set of clusters (no collective)."""
+    import torch
+    from interaxplugin import BatchContext, Context
+    from interaxplugin import workloads as W
+
+    device = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(device)
+    rng = np.random.default_rng(args.seed + 7919 * rank)
+    systems, positions = [], []
+    for k in range(num_clusters):
+        s, p, _ = W.water_cluster(int(rng.integers(2, 33)), seed=args.seed * 100003 + 7919 * rank + k)
+        systems.append(s)
+        positions.append(p)
+    batch = BatchContext(systems, device=device)
+    L = batch._lib
+    pos = np.ascontiguousarray(np.concatenate(positions))
+    hpos = torch.from_numpy(pos).pin_memory()
+    hfor = torch.empty(pos.shape, dtype=torch.float64).pin_memory()
+    hen = torch.empty((num_clusters, 4), dtype=torch.float64).pin_memory()
+    batch.compute(positions)
+    pairs, triples = batch.getCounts()
+    dpos = torch.from_numpy(pos).cuda()
+    dfor = torch.empty(pos.shape, dtype=torch.float64, device="cuda")
+    den = torch.empty((num_clusters, 4), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.ExternalStream(L.ix_batch_get_stream(batch._batch))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def device_step():
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        batch._check(L.ix_batch_compute_device(batch._batch, ctypes.c_void_p(dpos.data_ptr()),
+                                               ctypes.c_void_p(dfor.data_ptr()), ctypes.c_void_p(den.data_ptr())))
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    for _ in range(args.warmup):
+        device_step()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(device) as clocks:
+        ms = [device_step() for _ in range(args.steps)]
+    step_ms = float(np.sum(ms))
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([step_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+    value = world * num_clusters * args.steps / (step_ms * 1e-3)
+    # e2e: host positions in, host forces and energies out, per step
+    e2e_t = 0.0
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        batch._check(L.ix_batch_compute(batch._batch, ctypes.c_void_p(hpos.data_ptr()),
+                                        ctypes.c_void_p(hfor.data_ptr()), ctypes.c_void_p(hen.data_ptr())))
+        if k >= args.warmup:
+            e2e_t += time.perf_counter() - t0
+    e2e = world * num_clusters * args.steps / e2e_t
+    # the plain per-system drop-in: one Context per cluster, host API, on a sample of the clusters
+    ctxs = [Context(systems[k], properties={"DeviceIndex": device}) for k in range(plain_sample)]
+    for k, c in enumerate(ctxs):
+        c.setPositions(positions[k])
+        c.getState()
+    t0 = time.perf_counter()
+    for rep in range(3):
+        for k, c in enumerate(ctxs):
+            c.setPositions(positions[k])
+            c.getState()
+    plain = 3 * plain_sample / (time.perf_counter() - t0)
+    if rank != 0:
+        return
+    line = {
+        "metric": "evaluations/s", "value": value, "unit": "evaluations/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{num_clusters} non-periodic water clusters of 2..32 waters per GPU, all four forces "
+                               "(NoCutoff pairs, ATM without cutoff), one batched evaluation per step",
+                   "atoms": int(pos.shape[0]), "pairs_per_step": pairs, "triples_per_step": triples,
+                   "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+        "plain_per_system": {"value": plain, "unit": "evaluations/s",
+                             "sample": f"{plain_sample} of the clusters, one Context each, positions in and "
+                                       "forces out per evaluation"},
+        "batched_over_plain": e2e / plain,
+        "e2e": {"value": e2e, "unit": "evaluations/s", "h2d_bytes_per_step": int(pos.nbytes),
+                "d2h_bytes_per_step": int(pos.nbytes + num_clusters * 4 * 8)},
+        "interactions_per_s": world * (pairs + triples) / (step_ms / args.steps * 1e-3),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     rank, world = dist_init(args)
     try:
-        if args.impl == "reference":
+        if args.config == "clusters":
+            run_clusters(args, rank, world)
+        elif args.impl == "reference":
             run_reference(args, rank, world)
         else:
             run_ours(args, rank, world)

@@ -217,6 +217,41 @@ int ix_three_body_noalloc_overflow(int* overflow);
 /* Library version string. */
 const char* ix_version(void);
 
+/* ---- Batches of independent small systems -------------------------------------------------------------------------
+ * Many non-periodic systems (clusters, dimer scans, copies at several lambda values) evaluated together: one static
+ * launch sequence over all of them, captured once into a CUDA graph.  The systems are described like contexts (the
+ * ix_batch_add_* functions take the arguments of the ix_add_* functions plus the system index and validate them the
+ * same way); every system must carry the same forces with the same settings, and only particle parameters,
+ * exclusions and three-body sites may differ.  Positions and forces are the systems' particles concatenated in system
+ * order (3 doubles each); energies are 4 per system (dispersion, exchange, short range, three-body, kJ/mol).  Each
+ * system's results are the same alone or in any batch.  The reference evaluates one System per Context; this is the
+ * batched form of that evaluation, with no counterpart there. */
+typedef struct ix_batch ix_batch;
+
+int ix_batch_create(int device, ix_batch** out);
+void ix_batch_destroy(ix_batch* batch);
+const char* ix_batch_last_error(const ix_batch* batch);
+int ix_batch_add_system(ix_batch* batch, int num_particles, int* system);
+int ix_batch_add_dispersion(ix_batch* batch, int system, const ix_pair_settings* settings, const double* params,
+                            const uint8_t* is_alchemical, double damping_scale, int use_long_range_correction);
+int ix_batch_add_exchange(ix_batch* batch, int system, const ix_pair_settings* settings, const double* params,
+                          const uint8_t* is_alchemical, int overlap_method);
+int ix_batch_add_short_range(ix_batch* batch, int system, const ix_pair_settings* settings, const double* params,
+                             const uint8_t* is_alchemical, int overlap_method);
+int ix_batch_add_three_body(ix_batch* batch, int system, int num_sites, const int32_t* site_offsets,
+                            const int32_t* site_particles, const double* site_params, const int32_t* molecule,
+                            const uint8_t* is_alchemical, double cutoff, double scale_factor, int damping_method,
+                            double damping_scale, double centroid_damping_radius, int periodic,
+                            const char* alchemical_parameter, int force_group);
+int ix_batch_set_parameter(ix_batch* batch, const char* name, double value);
+int ix_batch_num_particles(const ix_batch* batch, int* num_particles, int* num_systems);
+/* Host buffers; synchronous.  The first call (and the first after a change) builds the device arrays and the graph. */
+int ix_batch_compute(ix_batch* batch, const double* positions, double* forces, double* energies);
+/* Device buffers (any may be NULL), asynchronous on the batch's stream. */
+int ix_batch_compute_device(ix_batch* batch, const double* d_positions, double* d_forces, double* d_energies);
+int ix_batch_get_counts(ix_batch* batch, long long* num_pairs, long long* num_triples);
+void* ix_batch_get_stream(ix_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

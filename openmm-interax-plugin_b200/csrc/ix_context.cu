@@ -364,39 +364,47 @@ static void overlapCoefficients(double w1, double w2, float4& A, float4& B, floa
 // class in bits 8..15 of each particle's flags.
 constexpr int kMaxClasses = 16;
 
-static int buildClassTable(ix_ctx* ctx, std::vector<int>& flags) {
-    const int n = ctx->n;
-    ctx->P.coef = nullptr;
-    ctx->P.numClasses = 0;
+// The class-pair table of one or more systems that share their pair forces' layout (a context, or the systems of a
+// batch): flags[s][i] |= class << kClassShift.  Returns the number of classes, 0 when there are more than kMaxClasses
+// (then nothing is changed and the kernel takes the per-particle path).
+static int classTableHost(const std::vector<const ix_ctx*>& sys, std::vector<std::vector<int>*>& flags,
+                          std::vector<PairCoef>& table) {
     std::map<std::vector<double>, int> classes;
-    std::vector<int> cls(n);
-    std::vector<int> rep;
-    for (int i = 0; i < n; i++) {
-        std::vector<double> key;
-        const int strides[3] = {5, 2, 3};
-        for (int t = 0; t < 3; t++)
-            if (ctx->term[t].present)
-                key.insert(key.end(), ctx->term[t].params.begin() + (size_t)strides[t] * i,
-                           ctx->term[t].params.begin() + (size_t)strides[t] * (i + 1));
-        auto it = classes.find(key);
-        if (it == classes.end()) {
-            if ((int)classes.size() == kMaxClasses) return IX_OK;   // too many classes: per-particle path
-            it = classes.emplace(key, (int)classes.size()).first;
-            rep.push_back(i);
+    std::vector<std::vector<int>> cls(sys.size());
+    std::vector<std::pair<const ix_ctx*, int>> rep;
+    for (size_t s = 0; s < sys.size(); s++) {
+        const ix_ctx* c = sys[s];
+        cls[s].resize(c->n);
+        for (int i = 0; i < c->n; i++) {
+            std::vector<double> key;
+            const int strides[3] = {5, 2, 3};
+            for (int t = 0; t < 3; t++)
+                if (c->term[t].present)
+                    key.insert(key.end(), c->term[t].params.begin() + (size_t)strides[t] * i,
+                               c->term[t].params.begin() + (size_t)strides[t] * (i + 1));
+            auto it = classes.find(key);
+            if (it == classes.end()) {
+                if ((int)classes.size() == kMaxClasses) return 0;   // too many classes: per-particle path
+                it = classes.emplace(key, (int)classes.size()).first;
+                rep.push_back({c, i});
+            }
+            cls[s][i] = it->second;
         }
-        cls[i] = it->second;
     }
     const int T = (int)classes.size();
-    std::vector<PairCoef> table((size_t)T * T);
-    const double beta = ctx->term[0].dampingScale;
+    table.assign((size_t)T * T, PairCoef{});
+    const double beta = sys[0]->term[0].dampingScale;
     for (int ci = 0; ci < T; ci++)
         for (int cj = 0; cj < T; cj++) {
             PairCoef K;
             std::memset(&K, 0, sizeof(K));
-            const int i = rep[ci], j = rep[cj];
+            const ix_ctx* ctx = rep[ci].first;   // the classes' parameter layouts are the same in every system
+            const int i = rep[ci].second;
+            const ix_ctx* ctxJ = rep[cj].first;
+            const int j = rep[cj].second;
             if (ctx->term[0].present) {
                 const double* p = &ctx->term[0].params[5 * i];
-                const double* q = &ctx->term[0].params[5 * j];
+                const double* q = &ctxJ->term[0].params[5 * j];
                 // InteraxPairTerms.h:274-279
                 const double pref = p[3] * q[3] / std::max(p[3] * q[0] + q[3] * p[0], 1e-30);
                 const double c6 = pref * p[0] * q[0];
@@ -407,13 +415,13 @@ static int buildClassTable(ix_ctx* ctx, std::vector<int>& flags) {
             }
             if (ctx->term[1].present) {
                 const double* p = &ctx->term[1].params[2 * i];
-                const double* q = &ctx->term[1].params[2 * j];
+                const double* q = &ctxJ->term[1].params[2 * j];
                 if (p[1] != 0 && q[1] != 0) overlapCoefficients(p[1], q[1], K.ovA, K.ovB, K.ovC.x, K.ovC.y);
                 K.ovC.z = (float)(p[0] * q[0] / (8.0 * M_PI));
             }
             if (ctx->term[2].present) {
                 const double* p = &ctx->term[2].params[3 * i];
-                const double* q = &ctx->term[2].params[3 * j];
+                const double* q = &ctxJ->term[2].params[3 * j];
                 if (p[2] != 0 && q[2] != 0) overlapCoefficients(p[2], q[2], K.srA, K.srB, K.srC.x, K.srC.y);
                 const double ws = p[2] + q[2];
                 K.srC.z = (float)(ws * ws * ws);
@@ -421,21 +429,38 @@ static int buildClassTable(ix_ctx* ctx, std::vector<int>& flags) {
             }
             table[(size_t)ci * T + cj] = K;
         }
+    for (size_t s = 0; s < sys.size(); s++)
+        for (int i = 0; i < sys[s]->n; i++) (*flags[s])[i] |= cls[s][i] << kClassShift;
+    return T;
+}
+
+static int buildClassTable(ix_ctx* ctx, std::vector<int>& flags) {
+    ctx->P.coef = nullptr;
+    ctx->P.numClasses = 0;
+    std::vector<const ix_ctx*> sys{ctx};
+    std::vector<std::vector<int>*> fl{&flags};
+    std::vector<PairCoef> table;
+    const int T = classTableHost(sys, fl, table);
+    if (T == 0) return IX_OK;
     PairCoef* dTable;
     IX_TRY(deviceAlloc(ctx, "classTable", table.size(), &dTable));
     IX_CUDA(ctx, cudaMemcpyAsync(dTable, table.data(), table.size() * sizeof(PairCoef), cudaMemcpyHostToDevice,
                                  ctx->stream));
-    for (int i = 0; i < n; i++) flags[i] |= cls[i] << kClassShift;
     ctx->P.coef = dTable;
     ctx->P.numClasses = T;
     return IX_OK;
 }
 
-static int uploadPairParams(ix_ctx* ctx) {
+// The float parameter arrays of a context's pair forces, in its particle order (see PairBuffers) and the flags:
+// alchemical bits per term, gate bits, real bit.
+static void packPairParams(const ix_ctx* ctx, std::vector<float4>& p0, std::vector<float4>& p1,
+                           std::vector<float4>& p2, std::vector<float4>& p3, std::vector<int>& flags) {
     const int n = ctx->n;
-    std::vector<float4> p0(n), p1(n), p2(n), p3(n);
-    std::vector<int> flags(n);
-    std::vector<bool> equalWidths(n, true);
+    p0.resize(n);
+    p1.resize(n);
+    p2.resize(n);
+    p3.resize(n);
+    flags.resize(n);
     for (int i = 0; i < n; i++) {
         float4 a = make_float4(0, 0, 0, 0), b = make_float4(0, 0, 0, 0), c = make_float4(0, 0, 0, 0);
         int f = kFlagReal;
@@ -470,13 +495,19 @@ static int uploadPairParams(ix_ctx* ctx) {
         p1[i] = b;
         p2[i] = c;
         flags[i] = f;
-        equalWidths[i] = (wx == ws);
         // float remainders of the widths and their reciprocals (float-float values for the kernel)
         const double wide[4] = {wx, wx != 0 ? 1.0 / wx : 0.0, ws, ws != 0 ? 1.0 / ws : 0.0};
         float lo[4];
         for (int k = 0; k < 4; k++) lo[k] = (float)(wide[k] - (double)(float)wide[k]);
         p3[i] = make_float4(lo[0], lo[1], lo[2], lo[3]);
     }
+}
+
+static int uploadPairParams(ix_ctx* ctx) {
+    const int n = ctx->n;
+    std::vector<float4> p0, p1, p2, p3;
+    std::vector<int> flags;
+    packPairParams(ctx, p0, p1, p2, p3, flags);
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP0o, p0.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP1o, p1.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
     IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP2o, p2.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
@@ -1966,3 +1997,6 @@ int ix_three_body_noalloc_overflow(int* overflow) {
 }
 
 }  // extern "C"
+
+// batched evaluation of many small systems (its own translation-unit part; reuses the helpers above)
+#include "ix_batch.cuh"

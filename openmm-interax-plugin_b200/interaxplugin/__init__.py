@@ -17,6 +17,9 @@ def __getattr__(name):
     if name in ("Context", "State", "Platform"):
         from . import context
         return getattr(context, name)
+    if name == "BatchContext":
+        from . import batch
+        return batch.BatchContext
     if name in ("XmlSerializer",):
         from . import serialization
         return getattr(serialization, name)

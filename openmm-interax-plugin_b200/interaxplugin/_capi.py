@@ -67,6 +67,25 @@ def lib():
                                                      ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                      ctypes.c_int, ctypes.c_double, P, P, P]),
             "ix_three_body_noalloc_overflow": (ctypes.c_int, [P]),
+            "ix_batch_create": (ctypes.c_int, [ctypes.c_int, ctypes.POINTER(P)]),
+            "ix_batch_destroy": (None, [P]),
+            "ix_batch_last_error": (ctypes.c_char_p, [P]),
+            "ix_batch_add_system": (ctypes.c_int, [P, ctypes.c_int, P]),
+            "ix_batch_add_dispersion": (ctypes.c_int, [P, ctypes.c_int, ctypes.POINTER(PairSettings), P, P,
+                                                       ctypes.c_double, ctypes.c_int]),
+            "ix_batch_add_exchange": (ctypes.c_int, [P, ctypes.c_int, ctypes.POINTER(PairSettings), P, P,
+                                                     ctypes.c_int]),
+            "ix_batch_add_short_range": (ctypes.c_int, [P, ctypes.c_int, ctypes.POINTER(PairSettings), P, P,
+                                                        ctypes.c_int]),
+            "ix_batch_add_three_body": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, P, P, P, P, P, ctypes.c_double,
+                                                       ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                                       ctypes.c_double, ctypes.c_int, ctypes.c_char_p, ctypes.c_int]),
+            "ix_batch_set_parameter": (ctypes.c_int, [P, ctypes.c_char_p, ctypes.c_double]),
+            "ix_batch_num_particles": (ctypes.c_int, [P, P, P]),
+            "ix_batch_compute": (ctypes.c_int, [P, P, P, P]),
+            "ix_batch_compute_device": (ctypes.c_int, [P, P, P, P]),
+            "ix_batch_get_counts": (ctypes.c_int, [P, P, P]),
+            "ix_batch_get_stream": (P, [P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
