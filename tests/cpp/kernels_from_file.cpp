@@ -1,6 +1,6 @@
 // Drives the C++ kernel classes of include/interax_b200_kernels.hpp the way a platform would: Force objects with the
 // reference's accessors, a ContextAccess over plain arrays, the factory by kernel name.  Reads a system written by
-// tests/test_gpu_cpp_kernels.py, writes the per-kernel energies and the summed forces.
+// tests/test_cpp_kernels.py, writes the per-kernel energies and the summed forces.
 //
 //   kernels_from_file <input> <output>
 #include <cstdio>
