@@ -419,12 +419,123 @@ def run_clusters(args, rank, world, num_clusters=4096, plain_sample=128):
     print(json.dumps(line))
 
 
+def run_lambda(args, rank, world, num_windows=16, num_alchemical=30):
+    """Alchemical windows: a 96,000-atom water box (32,000 waters, 9.855 nm, pair cutoff 1.0 nm, ATM on 32,000 sites
+    with cutoff 0.8 nm) with 30 waters decoupled by lambda_sterics, evaluated at 16 windows linspace(0, 1, 16) per step
+    (energies and forces of every window).  --config lambda has no soft core, so every window is E0 + lambda E1 and
+    the 16 windows cost two evaluations plus an interpolation kernel; --config lambda-softcore (R = 0.1 nm) evaluates
+    the pair terms at every window and the three-body term (linear in lambda) at 0 and 1.  Each counts 16 full
+    energy+force evaluations per step.  Compared with the plain path: setParameter + getState
+    per window."""
+    import torch
+    from interaxplugin import Context, _capi
+    from interaxplugin import workloads as W
+
+    softcore = 0.1 if args.config == "lambda-softcore" else 0.0
+    device = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(device)
+    cfg = W.CONFIGS["96k"]
+    system, pos, box = W.water_box(cfg["num_waters"], cfg["box_length"], cfg["cutoff"], seed=args.seed + rank,
+                                   three_body_cutoff=cfg["three_body_cutoff"],
+                                   alchemical_waters=range(num_alchemical), softcore_radius=softcore)
+    ctx = Context(system, properties={"DeviceIndex": device})
+    L = _capi.lib()
+    n = system.getNumParticles()
+    ctx.setPositions(pos)
+    values = np.linspace(0.0, 1.0, num_windows)
+    energies = np.zeros((num_windows, 4))
+    dfor = torch.empty((num_windows, n, 3), dtype=torch.float64, device="cuda")
+    stream = torch.cuda.ExternalStream(L.ix_get_stream(ctx._ctx))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    name = b"lambda_sterics"
+
+    def device_step():
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx._check(L.ix_compute_windows_device(ctx._ctx, name, num_windows, _capi.ptr(values), _capi.ptr(energies),
+                                               ctypes.c_void_p(dfor.data_ptr())))
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b)
+
+    for _ in range(args.warmup):
+        device_step()
+    pairs, triples = ctx.getCounts()
+    launches0 = ctypes.c_longlong()
+    ctx._check(L.ix_get_launch_count(ctx._ctx, ctypes.byref(launches0)))
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(device) as clocks:
+        ms = [device_step() for _ in range(args.steps)]
+    launches1 = ctypes.c_longlong()
+    ctx._check(L.ix_get_launch_count(ctx._ctx, ctypes.byref(launches1)))
+    step_ms = float(np.sum(ms))
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([step_ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        step_ms = float(t.item())
+    value = world * num_windows * args.steps / (step_ms * 1e-3)
+    # e2e: host positions in (pinned), every window's energies and forces out to host memory, per step
+    hpos = torch.from_numpy(np.ascontiguousarray(pos)).pin_memory()
+    hfor = np.zeros((num_windows, n, 3))
+    e2e_t = 0.0
+    for k in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx._check(L.ix_set_positions(ctx._ctx, ctypes.c_void_p(hpos.data_ptr()), None))
+        ctx._check(L.ix_compute_windows(ctx._ctx, name, num_windows, _capi.ptr(values), _capi.ptr(energies),
+                                        _capi.ptr(hfor)))
+        if k >= args.warmup:
+            e2e_t += time.perf_counter() - t0
+    e2e = world * num_windows * args.steps / e2e_t
+    # the plain path: one setParameter + getState per window
+    reps = 2
+    ctx.setParameter("lambda_sterics", 0.5)
+    ctx.getState()
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        for lam in values:
+            ctx.setParameter("lambda_sterics", lam)
+            ctx.getState()
+    plain = reps * num_windows / (time.perf_counter() - t0)
+    if rank != 0:
+        return
+    line = {
+        "metric": "evaluations/s", "value": value, "unit": "evaluations/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"96,000-atom water box (32,000 waters, 9.855 nm, cutoff 1.0 nm, ATM on 32,000 sites "
+                               f"cutoff 0.8 nm), {num_alchemical} waters alchemical, {num_windows} lambda_sterics "
+                               f"windows per step, soft-core radius {softcore} nm",
+                   "windows_method": "two evaluations + linear interpolation (exact: no soft core)" if softcore == 0
+                   else "pair terms evaluated at every window (soft core); ATM and LRC from 0 and 1, interpolated",
+                   "pairs_per_window": pairs, "triples_per_window": triples,
+                   "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+        "plain_per_window": {"value": plain, "unit": "evaluations/s",
+                             "sample": "setParameter + getState (forces to host) per window"},
+        "windows_over_plain": e2e / plain,
+        "interactions_per_s": world * num_windows * (pairs + triples) / (step_ms / args.steps * 1e-3),
+        "e2e": {"value": e2e, "unit": "evaluations/s", "h2d_bytes_per_step": int(n * 3 * 8),
+                "d2h_bytes_per_step": int(num_windows * (n * 3 + 4) * 8)},
+        "gpu_launches": int(launches1.value - launches0.value),
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     rank, world = dist_init(args)
     try:
         if args.config == "clusters":
             run_clusters(args, rank, world)
+        elif args.config in ("lambda", "lambda-softcore"):
+            run_lambda(args, rank, world)
         elif args.impl == "reference":
             run_reference(args, rank, world)
         else:

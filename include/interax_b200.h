@@ -179,6 +179,19 @@ int ix_get_launch_count(ix_ctx* ctx, long long* launches);
  * are identical.  No counterpart in the reference (OpenMM launches kernels one by one). */
 int ix_set_graphs(ix_ctx* ctx, int enable);
 
+/* The context evaluated at several values of one alchemical parameter (lambda windows; the other parameters keep
+ * their values, and the parameter's own value is restored).  energies: num_windows x 4 term energies; forces:
+ * num_windows x num_particles x 3 (may be NULL).  Host buffers, synchronous.  Every term is linear in the parameter
+ * when no force that uses it has a soft core: then two evaluations (at 0 and 1) give all windows; with a soft core
+ * every window is evaluated in full.  The reference evaluates one value per Context::setParameter and getState. */
+int ix_compute_windows(ix_ctx* ctx, const char* parameter, int num_windows, const double* values, double* energies,
+                       double* forces);
+
+/* ix_compute_windows with the forces written to device memory: d_forces (FP64, num_windows x num_particles x 3, on
+ * the context's device, or NULL).  energies stay a host buffer; returns after the forces are written. */
+int ix_compute_windows_device(ix_ctx* ctx, const char* parameter, int num_windows, const double* values,
+                              double* energies, double* d_forces);
+
 /* The CUDA stream the context launches on (as a void*), so callers can order their own work around it. */
 void* ix_get_stream(ix_ctx* ctx);
 

@@ -64,9 +64,10 @@ struct GraphKey {
     const void* out2 = nullptr;
     int stride = 0;
     double dt = 0.0;
+    double param = 0.0;                  // value of the window parameter a window graph was captured with
     bool operator==(const GraphKey& o) const {
         return terms == o.terms && out0 == o.out0 && out1 == o.out1 && out2 == o.out2 && stride == o.stride &&
-               dt == o.dt;
+               dt == o.dt && std::memcmp(&param, &o.param, sizeof(param)) == 0;
     }
 };
 
@@ -163,6 +164,8 @@ struct ix_ctx {
     bool useGraphs = true;
     unsigned long long version = 1;
     LaunchGraph graphCompute, graphDevice, graphMd;
+    std::vector<LaunchGraph> graphWindows;  // evaluations at window values of one parameter, one graph per value
+    size_t windowNext = 0;                  // slot replaced next when graphWindows is full
 };
 
 static void bumpVersion(ix_ctx* ctx) {
@@ -1337,6 +1340,7 @@ void ix_ctx_destroy(ix_ctx* ctx) {
     releaseGraph(ctx->graphCompute);
     releaseGraph(ctx->graphDevice);
     releaseGraph(ctx->graphMd);
+    for (auto& g : ctx->graphWindows) releaseGraph(g);
     for (auto& kv : ctx->buffers)
         if (kv.second.p) cudaFree(kv.second.p);
     for (auto& e : ctx->ev)
@@ -1507,39 +1511,58 @@ int ix_set_positions(ix_ctx* ctx, const double* positions, const double* box) {
     return IX_OK;
 }
 
+// Enqueue one evaluation of the selected terms into dOutForces / dOutEnergy through the graph g, captured with the
+// given key parameter.
+static int enqueueResident(ix_ctx* ctx, unsigned terms, LaunchGraph& g, double param) {
+    IX_TRY(stageUploads(ctx, terms));
+    GraphKey key;
+    key.terms = terms;
+    key.out0 = ctx->dOutForces;
+    key.out1 = ctx->dOutEnergy;
+    key.param = param;
+    return launchGraph(ctx, g, key, [&]() {
+        return launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0);
+    });
+}
+
+// Record the interacting pair and triple counts of the last evaluation (synchronous).
+static int readCounts(ix_ctx* ctx, unsigned terms) {
+    unsigned long long c[2];
+    IX_CUDA(ctx, cudaMemcpy(c, ctx->dCounts + 2, sizeof(c), cudaMemcpyDeviceToHost));
+    ctx->lastPairs = (terms & 7u) ? (long long)c[0] : 0;
+    ctx->lastTriples = (terms & 8u) ? (long long)c[1] : 0;
+    return IX_OK;
+}
+
+// One evaluation of the selected terms at the current positions and parameters, left on the device: forces in
+// dOutForces, term energies copied to e.  Grows the neighbor lists and repeats on an overflow.
+static int evaluateResident(ix_ctx* ctx, unsigned terms, double e[4], LaunchGraph* graph = nullptr,
+                            double param = 0.0) {
+    for (int t = 0; t < 4; t++) e[t] = 0.0;
+    if (!terms) return IX_OK;
+    IX_TRY(prepare(ctx, terms));
+    for (int attempt = 0; attempt < 4; attempt++) {
+        IX_TRY(enqueueResident(ctx, terms, graph ? *graph : ctx->graphCompute, param));
+        IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        bool redo = false;
+        IX_TRY(checkOverflow(ctx, terms, redo));
+        if (!redo) break;
+    }
+    IX_CUDA(ctx, cudaMemcpy(e, ctx->dOutEnergy, 4 * sizeof(double), cudaMemcpyDeviceToHost));
+    IX_TRY(readCounts(ctx, terms));
+    for (int t = 0; t < 4; t++)
+        if (!((terms >> t) & 1u)) e[t] = 0.0;
+    return IX_OK;
+}
+
 int ix_compute(ix_ctx* ctx, int groups, int include_forces, int include_energy, double* term_energies,
                double* energy, double* forces) {
     if (!ctx) return IX_ERR_INVALID;
     ctx->mdForcesValid = false;
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
     unsigned terms = selectedTerms(ctx, groups);
-    if (terms) IX_TRY(prepare(ctx, terms));
-    double e[4] = {0, 0, 0, 0};
-    for (int attempt = 0; attempt < 4; attempt++) {
-        if (terms) {
-            IX_TRY(stageUploads(ctx, terms));
-            GraphKey key;
-            key.terms = terms;
-            key.out0 = ctx->dOutForces;
-            key.out1 = ctx->dOutEnergy;
-            IX_TRY(launchGraph(ctx, ctx->graphCompute, key, [&]() {
-                return launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0);
-            }));
-        }
-        IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        bool redo = false;
-        if (terms) IX_TRY(checkOverflow(ctx, terms, redo));
-        if (!redo) break;
-    }
-    if (terms) {
-        IX_CUDA(ctx, cudaMemcpy(e, ctx->dOutEnergy, sizeof(e), cudaMemcpyDeviceToHost));
-        unsigned long long c[2];
-        IX_CUDA(ctx, cudaMemcpy(c, ctx->dCounts + 2, sizeof(c), cudaMemcpyDeviceToHost));
-        ctx->lastPairs = (terms & 7u) ? (long long)c[0] : 0;
-        ctx->lastTriples = (terms & 8u) ? (long long)c[1] : 0;
-    }
-    for (int t = 0; t < 4; t++)
-        if (!((terms >> t) & 1u)) e[t] = 0.0;
+    double e[4];
+    IX_TRY(evaluateResident(ctx, terms, e));
     if (term_energies) std::memcpy(term_energies, e, sizeof(e));
     if (energy) *energy = e[0] + e[1] + e[2] + e[3];
     if (forces) {
@@ -1713,6 +1736,169 @@ int ix_set_graphs(ix_ctx* ctx, int enable) {
     if (!ctx) return IX_ERR_INVALID;
     ctx->useGraphs = enable != 0;
     bumpVersion(ctx);
+    return IX_OK;
+}
+
+// out[w] = (accumulate ? out[w] : 0) + f0 + lambda_w (f1 - f0): the forces of terms linear in the window parameter at
+// each window, FP64, n x 3 per window.
+__global__ void kWindowForces(size_t n3, int num_windows, const double* __restrict__ lambdas,
+                              const double* __restrict__ f0, const double* __restrict__ f1, double* __restrict__ out,
+                              int accumulate) {
+    for (int w = blockIdx.y; w < num_windows; w += gridDim.y) {
+        const double lam = lambdas[w];
+        double* o = out + (size_t)w * n3;
+        for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += (size_t)gridDim.x * blockDim.x) {
+            const double v = fma(lam, f1[k] - f0[k], f0[k]);
+            o[k] = accumulate ? o[k] + v : v;
+        }
+    }
+}
+
+static const size_t kMaxWindowGraphs = 40;
+
+// The graph of an evaluation of the given terms at one value of the window parameter: the cached one, a new slot, or
+// (when the cache is full) the slot replaced longest ago.  The reference is used at once, before the cache grows.
+static LaunchGraph& windowGraph(ix_ctx* ctx, unsigned terms, double value) {
+    for (auto& g : ctx->graphWindows)
+        if (g.exec && g.key.terms == terms && std::memcmp(&g.key.param, &value, sizeof(value)) == 0) return g;
+    if (ctx->graphWindows.size() < kMaxWindowGraphs) {
+        ctx->graphWindows.emplace_back();
+        return ctx->graphWindows.back();
+    }
+    return ctx->graphWindows[ctx->windowNext++ % ctx->graphWindows.size()];
+}
+
+// One pass over the windows (see computeWindows).  redo: a neighbor list overflowed after the first window and was
+// grown; the pass must be repeated.
+static int windowsPass(ix_ctx* ctx, const std::string& name, int num_windows, const double* values, double* energies,
+                       double* d_forces, bool& redo) {
+    redo = false;
+    const size_t n3 = 3 * (size_t)ctx->n;
+    const unsigned terms = selectedTerms(ctx, -1);
+    bool pairNonlinear = false;
+    for (int t = 0; t < 3; t++) {
+        const PairTerm& T = ctx->term[t];
+        pairNonlinear = pairNonlinear || (T.present && T.anyAlch && T.alchName == name && T.softcoreRadius > 0);
+    }
+    const unsigned pairTerms = terms & 7u;
+    const unsigned linearTerms = pairNonlinear ? (terms & 8u) : terms;
+    double *dLin0 = nullptr, *dLin1 = nullptr, *dLambda = nullptr, *dWinEnergy = nullptr;
+    IX_TRY(deviceAlloc(ctx, "windowLambda", (size_t)num_windows, &dLambda));
+    if (linearTerms && d_forces) IX_TRY(deviceAlloc(ctx, "windowBase", n3, &dLin0));
+    if (linearTerms && d_forces && pairNonlinear) IX_TRY(deviceAlloc(ctx, "windowSlope", n3, &dLin1));
+    if (pairNonlinear) IX_TRY(deviceAlloc(ctx, "windowEnergy", 4 * (size_t)num_windows, &dWinEnergy));
+    // the terms linear in the parameter: evaluated at 0 and 1
+    double e0[4] = {0, 0, 0, 0}, e1[4] = {0, 0, 0, 0};
+    long long pairs = 0, triples = 0;
+    if (linearTerms) {
+        ctx->parameters[name] = 0.0;
+        IX_TRY(evaluateResident(ctx, linearTerms, e0, &windowGraph(ctx, linearTerms, 0.0), 0.0));
+        if (d_forces)
+            IX_CUDA(ctx, cudaMemcpyAsync(dLin0, ctx->dOutForces, n3 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+        ctx->parameters[name] = 1.0;
+        IX_TRY(evaluateResident(ctx, linearTerms, e1, &windowGraph(ctx, linearTerms, 1.0), 1.0));
+        if (d_forces && pairNonlinear)
+            IX_CUDA(ctx, cudaMemcpyAsync(dLin1, ctx->dOutForces, n3 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                         ctx->stream));
+        else dLin1 = ctx->dOutForces;
+        pairs = ctx->lastPairs;
+        triples = ctx->lastTriples;
+    }
+    // pair terms with a soft core: every window evaluated, back to back after the first
+    std::vector<double> pairEnergy(4 * (size_t)num_windows, 0.0);
+    if (pairNonlinear) {
+        IX_TRY(prepare(ctx, pairTerms));
+        for (int w = 0; w < num_windows; w++) {
+            ctx->parameters[name] = values[w];
+            if (w == 0) {
+                double e[4];
+                IX_TRY(evaluateResident(ctx, pairTerms, e, &windowGraph(ctx, pairTerms, values[w]), values[w]));
+            }
+            else IX_TRY(enqueueResident(ctx, pairTerms, windowGraph(ctx, pairTerms, values[w]), values[w]));
+            IX_CUDA(ctx, cudaMemcpyAsync(dWinEnergy + 4 * (size_t)w, ctx->dOutEnergy, 4 * sizeof(double),
+                                         cudaMemcpyDeviceToDevice, ctx->stream));
+            if (d_forces)
+                IX_CUDA(ctx, cudaMemcpyAsync(d_forces + w * n3, ctx->dOutForces, n3 * sizeof(double),
+                                             cudaMemcpyDeviceToDevice, ctx->stream));
+        }
+        IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        IX_TRY(checkOverflow(ctx, pairTerms, redo));
+        if (redo) return IX_OK;
+        IX_CUDA(ctx, cudaMemcpy(pairEnergy.data(), dWinEnergy, pairEnergy.size() * sizeof(double),
+                                cudaMemcpyDeviceToHost));
+        IX_TRY(readCounts(ctx, pairTerms));
+        pairs = ctx->lastPairs;
+    }
+    ctx->lastPairs = pairs;
+    ctx->lastTriples = triples;
+    for (int w = 0; w < num_windows; w++)
+        for (int k = 0; k < 4; k++)
+            energies[4 * w + k] = pairEnergy[4 * (size_t)w + k] + e0[k] + values[w] * (e1[k] - e0[k]);
+    if (d_forces) {
+        if (linearTerms) {
+            IX_CUDA(ctx, cudaMemcpyAsync(dLambda, values, num_windows * sizeof(double), cudaMemcpyHostToDevice,
+                                         ctx->stream));
+            const unsigned bx = (unsigned)std::max<size_t>(std::min<size_t>((n3 + 255) / 256, 1184), 1);
+            const dim3 grid(bx, (unsigned)std::min(num_windows, 65535));
+            kWindowForces<<<grid, 256, 0, ctx->stream>>>(n3, num_windows, dLambda, dLin0, dLin1, d_forces,
+                                                         pairNonlinear ? 1 : 0);
+            ctx->launches += 1;
+            IX_CUDA(ctx, cudaGetLastError());
+        }
+        else if (!pairNonlinear)
+            IX_CUDA(ctx, cudaMemsetAsync(d_forces, 0, num_windows * n3 * sizeof(double), ctx->stream));
+        IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    }
+    return IX_OK;
+}
+
+// The context evaluated at several values of one alchemical parameter, forces left on the device (d_forces, n x 3
+// per window, or null).  Terms whose alchemical scaling is linear in the parameter (pairs with exactly one
+// alchemical particle and no soft core, triples with an alchemical site, the long-range correction coef + lambda
+// alchCoef) are evaluated at 0 and 1 and interpolated for every window by kWindowForces; pair terms with a soft core
+// (the alchemical pairs' distances depend on the parameter) are evaluated at every window, back to back.  Each value
+// has its own cached graph, so repeated window sets replay without capturing.  The parameter keeps its value.
+static int computeWindows(ix_ctx* ctx, const char* parameter, int num_windows, const double* values, double* energies,
+                          double* d_forces) {
+    if (!parameter || num_windows < 0 || (num_windows > 0 && (!values || !energies)))
+        return fail(ctx, IX_ERR_INVALID, "ix_compute_windows: null argument");
+    for (int w = 0; w < num_windows; w++)
+        if (!std::isfinite(values[w])) return fail(ctx, IX_ERR_INVALID, "ix_compute_windows: window %d is not finite", w);
+    if (num_windows == 0) return IX_OK;
+    ctx->mdForcesValid = false;
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    const std::string name = parameter;
+    const auto saved = ctx->parameters.find(name);
+    const bool hadValue = saved != ctx->parameters.end();
+    const double oldValue = hadValue ? saved->second : 0.0;
+    int rc = IX_OK;
+    for (int attempt = 0; attempt < 3; attempt++) {
+        bool redo = false;
+        rc = windowsPass(ctx, name, num_windows, values, energies, d_forces, redo);
+        if (rc != IX_OK || !redo) break;
+    }
+    // the graphs of plain evaluations were captured with the old value: restoring it keeps them valid
+    if (hadValue) ctx->parameters[name] = oldValue;
+    else ctx->parameters.erase(name);
+    return rc;
+}
+
+int ix_compute_windows_device(ix_ctx* ctx, const char* parameter, int num_windows, const double* values,
+                              double* energies, double* d_forces) {
+    if (!ctx) return IX_ERR_INVALID;
+    return computeWindows(ctx, parameter, num_windows, values, energies, d_forces);
+}
+
+int ix_compute_windows(ix_ctx* ctx, const char* parameter, int num_windows, const double* values, double* energies,
+                       double* forces) {
+    if (!ctx) return IX_ERR_INVALID;
+    double* dForces = nullptr;
+    const size_t n3 = 3 * (size_t)ctx->n;
+    if (forces && num_windows > 0) IX_TRY(deviceAlloc(ctx, "windowForces", (size_t)num_windows * n3, &dForces));
+    IX_TRY(computeWindows(ctx, parameter, num_windows, values, energies, dForces));
+    if (dForces)
+        IX_CUDA(ctx, cudaMemcpy(forces, dForces, (size_t)num_windows * n3 * sizeof(double), cudaMemcpyDeviceToHost));
     return IX_OK;
 }
 

@@ -63,6 +63,8 @@ def lib():
             "ix_get_kernel_times": (ctypes.c_int, [P, P, P]),
             "ix_get_launch_count": (ctypes.c_int, [P, P]),
             "ix_set_graphs": (ctypes.c_int, [P, ctypes.c_int]),
+            "ix_compute_windows": (ctypes.c_int, [P, ctypes.c_char_p, ctypes.c_int, P, P, P]),
+            "ix_compute_windows_device": (ctypes.c_int, [P, ctypes.c_char_p, ctypes.c_int, P, P, P]),
             "ix_three_body_noalloc": (ctypes.c_int, [ctypes.c_int, P, P, ctypes.c_int, P, P, P, P, P, ctypes.c_double,
                                                      ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_double,
                                                      ctypes.c_int, ctypes.c_double, P, P, P]),

@@ -242,6 +242,18 @@ class Context:
                                                force.getScaleFactor(), force.getDampingScale(),
                                                force.getCentroidDampingRadius()))
 
+    def computeWindows(self, name, values, getForces=True):
+        """Term energies (num_windows x 4) and, optionally, forces (num_windows x n x 3) of the current positions at
+        each value of the alchemical parameter `name` (the C ABI's ix_compute_windows).  The parameter keeps its
+        value."""
+        values = _capi.arr(np.asarray(values, dtype=np.float64).reshape(-1), np.float64)
+        n = self._system.getNumParticles()
+        energies = np.zeros((len(values), 4))
+        forces = np.zeros((len(values), n, 3)) if getForces else None
+        self._check(self._lib.ix_compute_windows(self._ctx, name.encode(), len(values), _capi.ptr(values),
+                                                 _capi.ptr(energies), _capi.ptr(forces) if getForces else None))
+        return (energies, forces) if getForces else energies
+
     # -- MD -----------------------------------------------------------------------------------------------------
     def runVelocityVerlet(self, steps, dt, velocities):
         """Run `steps` velocity-Verlet steps of `dt` ps on the device; returns (positions, velocities, energy)."""
