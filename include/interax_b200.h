@@ -33,6 +33,7 @@ extern "C" {
 #define IX_ERR_CUDA 2        /* a CUDA runtime error; the message names the call */
 #define IX_ERR_STATE 3       /* call made in the wrong order (e.g. compute before positions) */
 #define IX_ERR_NO_DEVICE 4   /* no CUDA device, or the requested device is missing */
+#define IX_ERR_MEMORY 5      /* a server's device memory budget cannot hold the allocation */
 
 /* Nonbonded methods (InteraxPairForce.h:79-96) */
 #define IX_NO_CUTOFF 0
@@ -264,6 +265,57 @@ int ix_batch_compute(ix_batch* batch, const double* positions, double* forces, d
 int ix_batch_compute_device(ix_batch* batch, const double* d_positions, double* d_forces, double* d_energies);
 int ix_batch_get_counts(ix_batch* batch, long long* num_pairs, long long* num_triples);
 void* ix_batch_get_stream(ix_batch* batch);
+/* Velocity-Verlet MD of every system at once (host buffers, synchronous): system s takes steps[s] steps of dt ps and
+ * then stays put.  masses: one per particle (amu); positions and velocities (NULL = at rest) are updated in place;
+ * forces and energies (may be NULL) are those of the final positions.  Each system's trajectory is the same alone or
+ * in any batch. */
+int ix_batch_md_run(ix_batch* batch, const int* steps, double dt, const double* masses, double* positions,
+                    double* velocities, double* forces, double* energies);
+
+/* ---- Served requests -----------------------------------------------------------------------------------------------
+ * A request server for a stream of independent energy+force / MD requests of mixed sizes on one GPU.  A native worker
+ * thread admits requests while their estimated device memory fits the budget (an arena of that size holds every
+ * admitted request's state, so a request that does not fit waits until others finish), keeps each admitted request's
+ * positions, parameters and neighbor lists resident on the device until its last step, and overlaps the work of all
+ * admitted requests: periodic systems run as contexts on their own streams, small non-periodic systems with the same
+ * force settings are gathered into batched cohorts (one CUDA graph per MD step for the whole cohort).  Requests
+ * admitted while others run join as soon as memory and a slot are free (continuous batching).  A request's result is
+ * the same as that of the request run alone.  No counterpart in the reference, which evaluates one Context at a time.
+ *
+ * A request is described like a context, on the host only: ix_request_create, the ix_add_* functions on it,
+ * ix_request_set_state, then ix_server_submit (which takes ownership). */
+typedef struct ix_server ix_server;
+
+typedef struct {
+    long long submitted, admitted, completed, failed;
+    long long contexts, cohorts;              /* units launched: single-request contexts and batched cohorts */
+    long long pending, running;               /* requests waiting for admission, requests admitted and not done */
+    double budget_bytes, reserved_bytes, peak_reserved_bytes, arena_bytes, peak_arena_bytes;
+} ix_server_stats;
+
+/* A host-only request description of num_particles particles (box: 9 doubles, NULL for non-periodic). */
+int ix_request_create(int num_particles, const double* box, ix_ctx** out);
+/* Starting state: positions (n x 3, required), velocities (n x 3, NULL = at rest), masses (n, required for MD). */
+int ix_request_set_state(ix_ctx* request, const double* positions, const double* velocities, const double* masses);
+int ix_server_create(int device, double budget_bytes, int max_running, ix_server** out);
+/* Cohorts: non-periodic requests of at most small_atoms particles are batched, up to max_cohort per cohort; a cohort
+ * starts when it is full, when its oldest request has waited window_seconds, or when the GPU is idle. */
+int ix_server_set_batching(ix_server* server, int small_atoms, int max_cohort, double window_seconds);
+void ix_server_destroy(ix_server* server);
+const char* ix_server_last_error(const ix_server* server);
+/* Queue a request for `steps` velocity-Verlet steps of dt ps (0 steps: one energy+force evaluation).  On success the
+ * server owns `request` and *id identifies it. */
+int ix_server_submit(ix_server* server, ix_ctx* request, int steps, double dt, long long* id);
+/* Ids of requests completed since the last poll or wait (up to max_ids); wait blocks until one completes or the
+ * timeout passes. */
+int ix_server_poll(ix_server* server, int max_ids, long long* ids, int* count);
+int ix_server_wait(ix_server* server, double timeout_seconds, int max_ids, long long* ids, int* count);
+/* Result of a completed request, then released: final positions, velocities, forces (n x 3 each, may be NULL),
+ * term energies (4, may be NULL) and the seconds from submission to completion.  Returns the request's own status
+ * (its error message in ix_server_last_error). */
+int ix_server_result(ix_server* server, long long id, double* positions, double* velocities, double* forces,
+                     double* term_energies, double* latency_seconds);
+int ix_server_stats_get(ix_server* server, ix_server_stats* stats);
 
 #ifdef __cplusplus
 }

@@ -53,10 +53,35 @@ __global__ void kBatchEnergies(int numSystems, const int* tileStart, const doubl
     for (int k = 0; k < 4; k++) out[4 * s + k] = e[k];
 }
 
+// Velocity-Verlet halves for a batch: particles whose system has taken its steps (step >= stopStep) stay put.
+__global__ void kBatchVerletFirst(int n, double dt, const double* invMass, const double* force, double* vel,
+                                  double* pos, const int* stopStep, const int* step) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || *step >= stopStep[i]) return;
+    const double h = 0.5 * dt * invMass[i];
+    for (int d = 0; d < 3; d++) {
+        const double v = vel[3 * i + d] + h * force[3 * i + d];
+        vel[3 * i + d] = v;
+        pos[3 * i + d] += dt * v;
+    }
+}
+
+__global__ void kBatchVerletSecond(int n, double dt, const double* invMass, const double* force, double* vel,
+                                   const int* stopStep, int* step) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && *step < stopStep[i]) {
+        const double h = 0.5 * dt * invMass[i];
+        for (int d = 0; d < 3; d++) vel[3 * i + d] += h * force[3 * i + d];
+    }
+}
+
+__global__ void kBatchStepDone(int* step) { *step += 1; }
+
 }  // namespace
 
 struct ix_batch {
     int device = 0;
+    DeviceArena* arena = nullptr;        // the owning server's device memory (null: cudaMalloc)
     int numSMs = 148;
     cudaStream_t stream = nullptr;
     std::string error;
@@ -89,6 +114,14 @@ struct ix_batch {
     const double* graphPositions = nullptr;
     double* graphForces = nullptr;
     double* graphEnergies = nullptr;
+    // velocity-Verlet MD of the whole batch: each system runs its own number of steps, after which its particles stay
+    // where they are (their forces and energies are still evaluated, unchanged)
+    double* dVel = nullptr;              // numParticles x 3
+    double* dInvMass = nullptr;          // numParticles
+    int* dStopStep = nullptr;            // numParticles: steps of the particle's system
+    int* dStep = nullptr;                // steps taken so far (device counter)
+    cudaGraphExec_t stepGraph = nullptr;
+    double stepDt = 0.0;
 };
 
 namespace {
@@ -114,10 +147,15 @@ int batchAlloc(ix_batch* b, const std::string& name, size_t count, T** out) {
     DeviceBuffer& d = b->buffers[name];
     const size_t bytes = std::max<size_t>(count * sizeof(T), 16);
     if (!d.p || d.bytes < bytes) {
-        if (d.p) cudaFree(d.p);
+        arenaFree(b->arena, d.p);
         d.p = nullptr;
         d.bytes = 0;
-        cudaError_t e = cudaMalloc(&d.p, bytes);
+        cudaError_t e = arenaMalloc(b->arena, &d.p, bytes);
+        if (e != cudaSuccess && b->arena) {
+            d.p = nullptr;
+            return batchFail(b, IX_ERR_MEMORY, "device memory budget exhausted: %zu bytes (%s) do not fit", bytes,
+                             name.c_str());
+        }
         if (e != cudaSuccess)
             return batchFail(b, IX_ERR_CUDA, "cudaMalloc of %zu bytes (%s) failed: %s", bytes, name.c_str(),
                              cudaGetErrorString(e));
@@ -145,6 +183,30 @@ int batchForward(ix_batch* b, int system, int rc) {
 
 namespace {
 
+// Whether a system can join a batch: non-periodic pair and three-body forces.
+bool batchable(const ix_ctx* c) {
+    return !(c->pairShared && c->method == IX_CUTOFF_PERIODIC) && !(c->atmPresent && c->atmPeriodic);
+}
+
+// Whether two systems have the same forces with the same settings (what systems of one batch must share).
+bool sameBatchSettings(const ix_ctx* c, const ix_ctx* c0) {
+    bool same = c->pairShared == c0->pairShared && c->atmPresent == c0->atmPresent;
+    if (same && c0->pairShared) same = c->method == c0->method && c->cutoff == c0->cutoff;
+    for (int t = 0; t < 3 && same; t++) {
+        const PairTerm &T = c->term[t], &T0 = c0->term[t];
+        same = T.present == T0.present;
+        if (same && T.present)
+            same = T.alchName == T0.alchName && T.useSwitch == T0.useSwitch &&
+                   T.switchDistance == T0.switchDistance && T.softcoreRadius == T0.softcoreRadius &&
+                   T.overlapMethod == T0.overlapMethod && T.dampingScale == T0.dampingScale;
+    }
+    if (same && c0->atmPresent)
+        same = c->atmCutoff == c0->atmCutoff && c->atmScale == c0->atmScale && c->atmDamping == c0->atmDamping &&
+               c->atmDampingScale == c0->atmDampingScale && c->atmCentroidRadius == c0->atmCentroidRadius &&
+               c->atmAlchName == c0->atmAlchName;
+    return same;
+}
+
 // Every system must carry the same forces with the same settings: one launch configuration serves them all.
 int checkBatchSystems(ix_batch* b) {
     const ix_ctx* c0 = b->systems[0];
@@ -152,29 +214,13 @@ int checkBatchSystems(ix_batch* b) {
         return batchFail(b, IX_ERR_INVALID, "batched systems must be non-periodic (NoCutoff or CutoffNonPeriodic)");
     if (c0->atmPresent && c0->atmPeriodic)
         return batchFail(b, IX_ERR_INVALID, "batched systems must be non-periodic (three-body force)");
-    for (size_t s = 1; s < b->systems.size(); s++) {
-        const ix_ctx* c = b->systems[s];
-        bool same = c->pairShared == c0->pairShared && c->atmPresent == c0->atmPresent;
-        if (same && c0->pairShared) same = c->method == c0->method && c->cutoff == c0->cutoff;
-        for (int t = 0; t < 3 && same; t++) {
-            const PairTerm &T = c->term[t], &T0 = c0->term[t];
-            same = T.present == T0.present;
-            if (same && T.present)
-                same = T.alchName == T0.alchName && T.useSwitch == T0.useSwitch &&
-                       T.switchDistance == T0.switchDistance && T.softcoreRadius == T0.softcoreRadius &&
-                       T.overlapMethod == T0.overlapMethod && T.dampingScale == T0.dampingScale;
-        }
-        if (same && c0->atmPresent)
-            same = c->atmCutoff == c0->atmCutoff && c->atmScale == c0->atmScale && c->atmDamping == c0->atmDamping &&
-                   c->atmDampingScale == c0->atmDampingScale && c->atmCentroidRadius == c0->atmCentroidRadius &&
-                   c->atmAlchName == c0->atmAlchName;
-        if (!same)
+    for (size_t s = 1; s < b->systems.size(); s++)
+        if (!sameBatchSettings(b->systems[s], c0))
             return batchFail(b, IX_ERR_INVALID,
                              "system %zu: every system of a batch must have the same forces with the same settings "
                              "(nonbonded method, cutoffs, switching, soft core, overlap method, damping, alchemical "
                              "parameter); only particle parameters, exclusions and sites may differ",
                              s);
-    }
     return IX_OK;
 }
 
@@ -428,6 +474,10 @@ int buildBatch(ix_batch* b) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
     }
+    if (b->stepGraph) {
+        cudaGraphExecDestroy(b->stepGraph);
+        b->stepGraph = nullptr;
+    }
     for (ix_ctx* c : b->systems)
         for (auto& kv : b->parameters) c->parameters[kv.first] = kv.second;
     const ix_ctx* c0 = b->systems[0];
@@ -496,6 +546,72 @@ int buildBatch(ix_batch* b) {
     return IX_OK;
 }
 
+// MD state of the whole batch: masses (numParticles), velocities (numParticles x 3; null = at rest) and the number of
+// steps of each system.  Resets the step counter.
+int batchMdSetup(ix_batch* b, const double* masses, const double* velocities, const int* steps) {
+    if (!b->built || b->dirty) IX_TRY(buildBatch(b));
+    const int n = b->numParticles, S = (int)b->systems.size();
+    std::vector<double> inv(n);
+    for (int i = 0; i < n; i++) {
+        if (!(masses[i] >= 0)) return batchFail(b, IX_ERR_INVALID, "Illegal mass for particle %d", i);
+        inv[i] = masses[i] > 0 ? 1.0 / masses[i] : 0.0;
+    }
+    std::vector<int> stop(n);
+    for (int s = 0; s < S; s++) {
+        if (steps[s] < 0) return batchFail(b, IX_ERR_INVALID, "system %d: negative number of steps", s);
+        for (int i = b->particleStart[s]; i < b->particleStart[s + 1]; i++) stop[i] = steps[s];
+    }
+    const double* oldVel = b->dVel;
+    const double* oldInv = b->dInvMass;
+    const int* oldStop = b->dStopStep;
+    const int* oldStep = b->dStep;
+    IX_TRY(batchUpload(b, "invMass", inv, &b->dInvMass));
+    IX_TRY(batchUpload(b, "stopStep", stop, &b->dStopStep));
+    IX_TRY(batchUpload(b, "step", std::vector<int>{0}, &b->dStep));
+    IX_TRY(batchAlloc(b, "velocities", 3 * (size_t)n, &b->dVel));
+    if (velocities)
+        IX_BCUDA(b, cudaMemcpy(b->dVel, velocities, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    else IX_BCUDA(b, cudaMemset(b->dVel, 0, 3 * (size_t)n * sizeof(double)));
+    if (b->stepGraph && (oldVel != b->dVel || oldInv != b->dInvMass || oldStop != b->dStopStep || oldStep != b->dStep)) {
+        cudaGraphExecDestroy(b->stepGraph);
+        b->stepGraph = nullptr;
+    }
+    return IX_OK;
+}
+
+// Enqueue one MD step of the batch on its stream: a captured graph of the first half-kick and drift, the evaluation
+// at the new positions and the second half-kick (systems past their steps stay put), then the step counter.
+int batchMdStep(ix_batch* b, double dt) {
+    if (b->stepGraph && b->stepDt != dt) {
+        cudaGraphExecDestroy(b->stepGraph);
+        b->stepGraph = nullptr;
+    }
+    if (!b->stepGraph) {
+        const int n = b->numParticles, g = (n + 255) / 256;
+        IX_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        kBatchVerletFirst<<<g, 256, 0, b->stream>>>(n, dt, b->dInvMass, b->dForces, b->dVel, b->dPos, b->dStopStep,
+                                                    b->dStep);
+        int rc = enqueueBatch(b);
+        kBatchVerletSecond<<<g, 256, 0, b->stream>>>(n, dt, b->dInvMass, b->dForces, b->dVel, b->dStopStep, b->dStep);
+        kBatchStepDone<<<1, 1, 0, b->stream>>>(b->dStep);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(b->stream, &graph);
+        if (rc == IX_OK && e != cudaSuccess) rc = batchFail(b, IX_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
+        if (rc == IX_OK) {
+            const cudaError_t ie = cudaGraphInstantiate(&b->stepGraph, graph, 0);
+            if (ie != cudaSuccess) {
+                b->stepGraph = nullptr;
+                rc = batchFail(b, IX_ERR_CUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(ie));
+            }
+        }
+        if (graph) cudaGraphDestroy(graph);
+        if (rc != IX_OK) return rc;
+        b->stepDt = dt;
+    }
+    IX_BCUDA(b, cudaGraphLaunch(b->stepGraph, b->stream));
+    return IX_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -532,8 +648,8 @@ void ix_batch_destroy(ix_batch* b) {
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    for (auto& kv : b->buffers)
-        if (kv.second.p) cudaFree(kv.second.p);
+    if (b->stepGraph) cudaGraphExecDestroy(b->stepGraph);
+    for (auto& kv : b->buffers) arenaFree(b->arena, kv.second.p);
     for (ix_ctx* c : b->systems) delete c;   // host-side descriptions only
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -636,6 +752,38 @@ int ix_batch_compute(ix_batch* b, const double* positions, double* forces, doubl
     if (!b->built || b->dirty) IX_TRY(buildBatch(b));
     IX_BCUDA(b, cudaMemcpyAsync(b->dPos, positions, n3 * sizeof(double), cudaMemcpyHostToDevice, b->stream));
     IX_TRY(ix_batch_compute_device(b, nullptr, nullptr, nullptr));
+    if (forces) IX_BCUDA(b, cudaMemcpyAsync(forces, b->dForces, n3 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    if (energies)
+        IX_BCUDA(b, cudaMemcpyAsync(energies, b->dEnergies, 4 * b->systems.size() * sizeof(double),
+                                    cudaMemcpyDeviceToHost, b->stream));
+    unsigned long long c[4];
+    IX_BCUDA(b, cudaMemcpyAsync(c, b->dCounts, sizeof(c), cudaMemcpyDeviceToHost, b->stream));
+    IX_BCUDA(b, cudaStreamSynchronize(b->stream));
+    b->lastPairs = (long long)c[2];
+    b->lastTriples = (long long)c[3];
+    return IX_OK;
+}
+
+int ix_batch_md_run(ix_batch* b, const int* steps, double dt, const double* masses, double* positions,
+                    double* velocities, double* forces, double* energies) {
+    if (!b) return IX_ERR_INVALID;
+    if (!steps || !masses || !positions) return batchFail(b, IX_ERR_INVALID, "ix_batch_md_run: null argument");
+    if (!(dt > 0)) return batchFail(b, IX_ERR_INVALID, "ix_batch_md_run: the step size must be positive");
+    const size_t n3 = 3 * (size_t)b->particleStart.back();
+    for (size_t i = 0; i < n3; i++)
+        if (!std::isfinite(positions[i]))
+            return batchFail(b, IX_ERR_INVALID, "Particle coordinate is NaN or infinite (particle %zu)", i / 3);
+    IX_BCUDA(b, cudaSetDevice(b->device));
+    if (!b->built || b->dirty) IX_TRY(buildBatch(b));
+    IX_TRY(batchMdSetup(b, masses, velocities, steps));
+    IX_BCUDA(b, cudaMemcpyAsync(b->dPos, positions, n3 * sizeof(double), cudaMemcpyHostToDevice, b->stream));
+    IX_BCUDA(b, cudaGraphLaunch(b->graph, b->stream));   // forces at the starting positions
+    int maxSteps = 0;
+    for (size_t s = 0; s < b->systems.size(); s++) maxSteps = std::max(maxSteps, steps[s]);
+    for (int k = 0; k < maxSteps; k++) IX_TRY(batchMdStep(b, dt));
+    IX_BCUDA(b, cudaMemcpyAsync(positions, b->dPos, n3 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+    if (velocities)
+        IX_BCUDA(b, cudaMemcpyAsync(velocities, b->dVel, n3 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
     if (forces) IX_BCUDA(b, cudaMemcpyAsync(forces, b->dForces, n3 * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
     if (energies)
         IX_BCUDA(b, cudaMemcpyAsync(energies, b->dEnergies, 4 * b->systems.size() * sizeof(double),

@@ -56,6 +56,95 @@ struct DeviceBuffer {
     size_t bytes = 0;
 };
 
+// Device memory of the contexts and batches a server runs.  Chunks come from cudaMalloc and are sub-allocated
+// first-fit on the host; they go back to the driver only when the arena is destroyed, because cudaFree waits for the
+// whole device and would stall every request in flight.  Live bytes are bounded by the budget (`limit`).
+struct DeviceArena {
+    struct Chunk {
+        char* base = nullptr;
+        size_t bytes = 0;
+        std::map<size_t, size_t> free;   // offset -> size of each free range, coalesced
+    };
+    static constexpr size_t kAlign = 512;
+    std::mutex m;
+    std::vector<Chunk> chunks;
+    std::map<char*, std::pair<size_t, size_t>> live;   // allocation -> (chunk, bytes)
+    size_t limit = 0, chunkBytes = size_t(256) << 20, inUse = 0, peak = 0, capacity = 0;
+
+    void* alloc(size_t bytes) {
+        bytes = (std::max<size_t>(bytes, 1) + kAlign - 1) / kAlign * kAlign;
+        std::lock_guard<std::mutex> lock(m);
+        if (inUse + bytes > limit) return nullptr;
+        for (size_t c = 0;; c++) {
+            if (c == chunks.size()) {
+                const size_t want = std::max(chunkBytes, bytes);
+                if (capacity + want > limit + chunkBytes) return nullptr;
+                Chunk k;
+                if (cudaMalloc(reinterpret_cast<void**>(&k.base), want) != cudaSuccess) {
+                    cudaGetLastError();
+                    return nullptr;
+                }
+                k.bytes = want;
+                k.free[0] = want;
+                chunks.push_back(std::move(k));
+                capacity += want;
+            }
+            auto& fr = chunks[c].free;
+            for (auto it = fr.begin(); it != fr.end(); ++it) {
+                if (it->second < bytes) continue;
+                const size_t off = it->first, rest = it->second - bytes;
+                fr.erase(it);
+                if (rest) fr[off + bytes] = rest;
+                char* p = chunks[c].base + off;
+                live[p] = {c, bytes};
+                inUse += bytes;
+                peak = std::max(peak, inUse);
+                return p;
+            }
+        }
+    }
+
+    void release(void* ptr) {
+        std::lock_guard<std::mutex> lock(m);
+        auto it = live.find(static_cast<char*>(ptr));
+        if (it == live.end()) return;
+        Chunk& k = chunks[it->second.first];
+        size_t off = static_cast<size_t>(it->first - k.base), bytes = it->second.second;
+        inUse -= bytes;
+        live.erase(it);
+        auto next = k.free.lower_bound(off);
+        if (next != k.free.end() && next->first == off + bytes) {
+            bytes += next->second;
+            next = k.free.erase(next);
+        }
+        if (next != k.free.begin()) {
+            auto prev = std::prev(next);
+            if (prev->first + prev->second == off) {
+                prev->second += bytes;
+                return;
+            }
+        }
+        k.free[off] = bytes;
+    }
+
+    ~DeviceArena() {
+        for (auto& k : chunks) cudaFree(k.base);
+    }
+};
+
+// Device allocation through an arena when one is given, else straight from the driver.
+inline cudaError_t arenaMalloc(DeviceArena* arena, void** p, size_t bytes) {
+    if (!arena) return cudaMalloc(p, bytes);
+    *p = arena->alloc(bytes);
+    return *p ? cudaSuccess : cudaErrorMemoryAllocation;
+}
+
+inline void arenaFree(DeviceArena* arena, void* p) {
+    if (!p) return;
+    if (arena) arena->release(p);
+    else cudaFree(p);
+}
+
 // What a captured graph was captured for: the selected terms, the output pointers and the MD time step.
 struct GraphKey {
     unsigned terms = 0;
@@ -83,6 +172,8 @@ struct LaunchGraph {
 struct ix_ctx {
     int n = 0;
     int device = 0;
+    DeviceArena* arena = nullptr;        // the owning server's device memory (null: cudaMalloc)
+    std::vector<double> requestPos, requestVel, requestMass;   // starting state of a server request description
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;      // the three-body chain, forked from and joined back into `stream`
     cudaStream_t streamBody = nullptr;   // captures the branches of conditional graph nodes
@@ -207,12 +298,18 @@ static int deviceAlloc(ix_ctx* ctx, const std::string& name, size_t count, T** o
         return IX_OK;
     }
     bumpVersion(ctx);
-    if (b.p) cudaFree(b.p);
+    arenaFree(ctx->arena, b.p);
     b.p = nullptr;
     b.bytes = 0;
-    cudaError_t e = cudaMalloc(&b.p, bytes);
-    if (e != cudaSuccess) return fail(ctx, IX_ERR_CUDA, "cudaMalloc of %zu bytes (%s) failed: %s", bytes, name.c_str(),
-                                      cudaGetErrorString(e));
+    cudaError_t e = arenaMalloc(ctx->arena, &b.p, bytes);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        if (ctx->arena)
+            return fail(ctx, IX_ERR_MEMORY, "device memory budget exhausted: %zu bytes (%s) do not fit", bytes,
+                        name.c_str());
+        return fail(ctx, IX_ERR_CUDA, "cudaMalloc of %zu bytes (%s) failed: %s", bytes, name.c_str(),
+                    cudaGetErrorString(e));
+    }
     b.bytes = bytes;
     *out = reinterpret_cast<T*>(b.p);
     return IX_OK;
@@ -1242,6 +1339,35 @@ static void releaseGraph(LaunchGraph& g) {
 // C ABI
 // ---------------------------------------------------------------------------------------------------------------------
 
+// The device side of a context: streams, events and the buffers every evaluation uses (through ctx->arena when a
+// server owns the context).  A context described on the host only (a server request) gets it on admission.
+static int ctxInitDevice(ix_ctx* ctx) {
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaDeviceProp prop;
+    IX_CUDA(ctx, cudaGetDeviceProperties(&prop, ctx->device));
+    ctx->numSMs = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&ctx->streamBody, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->evFork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->evJoin, cudaEventDisableTiming) != cudaSuccess)
+        return fail(ctx, IX_ERR_CUDA, "cudaStreamCreate failed");
+    const int n = ctx->n;
+    IX_TRY(deviceAlloc(ctx, "pos", 3 * (size_t)n, &ctx->dPos));
+    IX_TRY(deviceAlloc(ctx, "counts", 4, &ctx->dCounts));
+    IX_TRY(deviceAlloc(ctx, "flags", 8, &ctx->dFlags));
+    IX_TRY(deviceAlloc(ctx, "outForces", 3 * (size_t)n, &ctx->dOutForces));
+    IX_TRY(deviceAlloc(ctx, "outEnergy", 4, &ctx->dOutEnergy));
+    IX_TRY(deviceAlloc(ctx, "energyBlocks", 4 * kReduceBlocks, &ctx->dEnergyBlocks));
+    IX_TRY(deviceAlloc(ctx, "reduceTicket", 1, &ctx->dReduceTicket));
+    int init[8] = {1, 0, 0, 0, 1, 0, 0, 0};
+    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dFlags, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    IX_CUDA(ctx, cudaMemsetAsync(ctx->dReduceTicket, 0, sizeof(unsigned), ctx->stream));
+    IX_CUDA(ctx, cudaMemsetAsync(ctx->dCounts, 0, 4 * sizeof(unsigned long long), ctx->stream));
+    IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return IX_OK;
+}
+
 extern "C" {
 
 const char* ix_version(void) { return "interax-b200 0.1 (sm_100a)"; }
@@ -1300,35 +1426,16 @@ int ix_ctx_create(int num_particles, int device, const double* default_box, ix_c
     ix_ctx* ctx = new ix_ctx();
     ctx->n = num_particles;
     ctx->device = device;
-    ctx->numSMs = prop.multiProcessorCount;
     if (default_box) {
         std::memcpy(ctx->defaultBox, default_box, sizeof(ctx->defaultBox));
         std::memcpy(ctx->box, default_box, sizeof(ctx->box));
     }
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->streamBody, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->evFork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->evJoin, cudaEventDisableTiming) != cudaSuccess) {
-        ix_ctx_destroy(ctx);
-        return fail(nullptr, IX_ERR_CUDA, "cudaStreamCreate failed");
-    }
-    int rc = IX_OK;
-    if ((rc = deviceAlloc(ctx, "pos", 3 * (size_t)num_particles, &ctx->dPos)) != IX_OK ||
-        (rc = deviceAlloc(ctx, "counts", 4, &ctx->dCounts)) != IX_OK ||
-        (rc = deviceAlloc(ctx, "flags", 8, &ctx->dFlags)) != IX_OK ||
-        (rc = deviceAlloc(ctx, "outForces", 3 * (size_t)num_particles, &ctx->dOutForces)) != IX_OK ||
-        (rc = deviceAlloc(ctx, "outEnergy", 4, &ctx->dOutEnergy)) != IX_OK ||
-        (rc = deviceAlloc(ctx, "energyBlocks", 4 * kReduceBlocks, &ctx->dEnergyBlocks)) != IX_OK ||
-        (rc = deviceAlloc(ctx, "reduceTicket", 1, &ctx->dReduceTicket)) != IX_OK) {
+    const int rc = ctxInitDevice(ctx);
+    if (rc != IX_OK) {
         g_createError = ctx->error;
         ix_ctx_destroy(ctx);
         return rc;
     }
-    int init[8] = {1, 0, 0, 0, 1, 0, 0, 0};
-    cudaMemcpy(ctx->dFlags, init, sizeof(init), cudaMemcpyHostToDevice);
-    cudaMemset(ctx->dReduceTicket, 0, sizeof(unsigned));
-    cudaMemset(ctx->dCounts, 0, 4 * sizeof(unsigned long long));
     *out = ctx;
     return IX_OK;
 }
@@ -1341,8 +1448,7 @@ void ix_ctx_destroy(ix_ctx* ctx) {
     releaseGraph(ctx->graphDevice);
     releaseGraph(ctx->graphMd);
     for (auto& g : ctx->graphWindows) releaseGraph(g);
-    for (auto& kv : ctx->buffers)
-        if (kv.second.p) cudaFree(kv.second.p);
+    for (auto& kv : ctx->buffers) arenaFree(ctx->arena, kv.second.p);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->evFork) cudaEventDestroy(ctx->evFork);
@@ -2186,3 +2292,4 @@ int ix_three_body_noalloc_overflow(int* overflow) {
 
 // batched evaluation of many small systems (its own translation-unit part; reuses the helpers above)
 #include "ix_batch.cuh"
+#include "ix_server.cuh"

@@ -20,6 +20,9 @@ def __getattr__(name):
     if name == "BatchContext":
         from . import batch
         return batch.BatchContext
+    if name == "Server":
+        from . import server
+        return server.Server
     if name in ("XmlSerializer",):
         from . import serialization
         return getattr(serialization, name)

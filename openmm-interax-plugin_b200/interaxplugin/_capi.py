@@ -19,6 +19,13 @@ class PairSettings(ctypes.Structure):
                 ("exclusions", P)]
 
 
+class ServerStats(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_longlong) for k in ("submitted", "admitted", "completed", "failed", "contexts", "cohorts",
+                                                  "pending", "running")] + \
+               [(k, ctypes.c_double) for k in ("budget_bytes", "reserved_bytes", "peak_reserved_bytes", "arena_bytes",
+                                               "peak_arena_bytes")]
+
+
 _lib = None
 
 
@@ -88,6 +95,18 @@ def lib():
             "ix_batch_compute_device": (ctypes.c_int, [P, P, P, P]),
             "ix_batch_get_counts": (ctypes.c_int, [P, P, P]),
             "ix_batch_get_stream": (P, [P]),
+            "ix_batch_md_run": (ctypes.c_int, [P, P, ctypes.c_double, P, P, P, P, P]),
+            "ix_request_create": (ctypes.c_int, [ctypes.c_int, P, ctypes.POINTER(P)]),
+            "ix_request_set_state": (ctypes.c_int, [P, P, P, P]),
+            "ix_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(P)]),
+            "ix_server_set_batching": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
+            "ix_server_destroy": (None, [P]),
+            "ix_server_last_error": (ctypes.c_char_p, [P]),
+            "ix_server_submit": (ctypes.c_int, [P, P, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_longlong)]),
+            "ix_server_poll": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.POINTER(ctypes.c_int)]),
+            "ix_server_wait": (ctypes.c_int, [P, ctypes.c_double, ctypes.c_int, P, ctypes.POINTER(ctypes.c_int)]),
+            "ix_server_result": (ctypes.c_int, [P, ctypes.c_longlong, P, P, P, P, ctypes.POINTER(ctypes.c_double)]),
+            "ix_server_stats_get": (ctypes.c_int, [P, ctypes.POINTER(ServerStats)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)

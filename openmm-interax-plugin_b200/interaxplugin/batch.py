@@ -94,6 +94,26 @@ class BatchContext:
         forces = [self._forces[self._offsets[s]:self._offsets[s + 1]].copy() for s in range(len(self._systems))]
         return self._energies.copy(), forces
 
+    def runVelocityVerlet(self, steps, dt, positions, velocities=None):
+        """steps[s] velocity-Verlet steps of dt ps for System s, all Systems at once on the device (masses from the
+        Systems).  Returns (positions, velocities, forces, energies), positions, velocities and forces as lists of
+        (n_s, 3) arrays, energies (num_systems, 4) at the final positions."""
+        def flat(a):
+            if isinstance(a, (list, tuple)):
+                a = np.concatenate([np.asarray(p, dtype=np.float64).reshape(-1, 3) for p in a])
+            return _capi.arr(np.asarray(a, dtype=np.float64).reshape(-1, 3), np.float64).copy()
+        pos = flat(positions)
+        vel = np.zeros_like(pos) if velocities is None else flat(velocities)
+        if pos.shape[0] != self._offsets[-1] or vel.shape != pos.shape:
+            raise OpenMMException("positions and velocities must hold every particle of every System of the batch")
+        st = _capi.arr(np.broadcast_to(np.asarray(steps, dtype=np.int32), (len(self._systems),)), np.int32)
+        mass = _capi.arr([s.getParticleMass(i) for s in self._systems for i in range(s.getNumParticles())],
+                         np.float64)
+        self._check(self._lib.ix_batch_md_run(self._batch, _capi.ptr(st), float(dt), _capi.ptr(mass), _capi.ptr(pos),
+                                              _capi.ptr(vel), _capi.ptr(self._forces), _capi.ptr(self._energies)))
+        split = lambda a: [a[self._offsets[s]:self._offsets[s + 1]].copy() for s in range(len(self._systems))]
+        return split(pos), split(vel), split(self._forces), self._energies.copy()
+
     def getCounts(self):
         p, t = ctypes.c_longlong(), ctypes.c_longlong()
         self._check(self._lib.ix_batch_get_counts(self._batch, ctypes.byref(p), ctypes.byref(t)))

@@ -58,6 +58,57 @@ def _term_index(force):
     return 3 if isinstance(force, InteraxThreeBodyForce) else None
 
 
+def _pair_settings(force, n):
+    if force.getNumParticles() != n:
+        raise OpenMMException(f"{type(force).__name__} must have exactly as many particles as the System it "
+                              "belongs to.")
+    ex = _capi.arr(force._exclusion_array(), np.int32)
+    s = _capi.PairSettings(force.getNonbondedMethod(), force.getCutoffDistance(),
+                           int(force.getUseSwitchingFunction()), force.getSwitchingDistance(),
+                           force.getSoftcoreRadius(), force.getForceGroup(),
+                           force.getAlchemicalParameterName().encode(), len(ex), _capi.ptr(ex))
+    return s, ex
+
+
+def describe_forces(lib, handle, system, check):
+    """Describe a System's InteraxFF forces to a context or request handle with the ix_add_* functions (what the
+    reference's kernels' initialize() receive, InteraxKernels.h:64-67, 99-102, 134-137, 169-172).  Returns
+    {term index: force} and the alchemical parameter names that have alchemical particles or sites."""
+    n = system.getNumParticles()
+    forces, names = {}, []
+    for force in system._forces:
+        t = _term_index(force)
+        if t is None:
+            continue
+        if t < 3:
+            s, ex = _pair_settings(force, n)
+            params = _capi.arr(force._params_array(), np.float64)
+            alch = _capi.arr(force._alch_array(), np.uint8)
+            if t == 0:
+                rc = lib.ix_add_dispersion(handle, ctypes.byref(s), _capi.ptr(params), _capi.ptr(alch),
+                                           force.getDampingScale(), int(force.getUseLongRangeCorrection()))
+            elif t == 1:
+                rc = lib.ix_add_exchange(handle, ctypes.byref(s), _capi.ptr(params), _capi.ptr(alch),
+                                         force.getOverlapMethod())
+            else:
+                rc = lib.ix_add_short_range(handle, ctypes.byref(s), _capi.ptr(params), _capi.ptr(alch),
+                                            force.getOverlapMethod())
+        else:
+            off, part, params, mol, alch = force._site_arrays()
+            rc = lib.ix_add_three_body(
+                handle, force.getNumSites(), _capi.ptr(_capi.arr(off, np.int32)), _capi.ptr(_capi.arr(part, np.int32)),
+                _capi.ptr(_capi.arr(params, np.float64)), _capi.ptr(_capi.arr(mol, np.int32)),
+                _capi.ptr(_capi.arr(alch, np.uint8)), force.getCutoffDistance(), force.getScaleFactor(),
+                force.getDampingMethod(), force.getDampingScale(), force.getCentroidDampingRadius(),
+                int(force.usesPeriodicBoundaryConditions()), force.getAlchemicalParameterName().encode(),
+                force.getForceGroup())
+        check(rc)
+        if alch.any():
+            names.append(force.getAlchemicalParameterName())
+        forces[t] = force
+    return forces, names
+
+
 class Context:
     def __init__(self, system, integrator=None, platform=None, properties=None):
         self._system = system
@@ -86,60 +137,9 @@ class Context:
             msg = self._lib.ix_last_error(None).decode()
             self._ctx = ctypes.c_void_p()
             raise OpenMMException(msg)
-        for force in system._forces:
-            t = _term_index(force)
-            if t is None:
-                continue
-            if t < 3:
-                self._add_pair(t, force, n)
-            else:
-                self._add_three_body(force)
-            self._forces[t] = force
-
-    def _settings(self, force, n):
-        if force.getNumParticles() != n:
-            raise OpenMMException(f"{type(force).__name__} must have exactly as many particles as the System it "
-                                  "belongs to.")
-        ex = _capi.arr(force._exclusion_array(), np.int32)
-        s = _capi.PairSettings(force.getNonbondedMethod(), force.getCutoffDistance(),
-                               int(force.getUseSwitchingFunction()), force.getSwitchingDistance(),
-                               force.getSoftcoreRadius(), force.getForceGroup(),
-                               force.getAlchemicalParameterName().encode(), len(ex), _capi.ptr(ex))
-        return s, ex
-
-    def _add_pair(self, t, force, n):
-        s, ex = self._settings(force, n)
-        params = _capi.arr(force._params_array(), np.float64)
-        alch = _capi.arr(force._alch_array(), np.uint8)
-        if alch.any():
-            self._parameters.setdefault(force.getAlchemicalParameterName(), 1.0)
-        L = self._lib
-        if t == 0:
-            rc = L.ix_add_dispersion(self._ctx, ctypes.byref(s), _capi.ptr(params), _capi.ptr(alch),
-                                     force.getDampingScale(), int(force.getUseLongRangeCorrection()))
-        elif t == 1:
-            rc = L.ix_add_exchange(self._ctx, ctypes.byref(s), _capi.ptr(params), _capi.ptr(alch),
-                                   force.getOverlapMethod())
-        else:
-            rc = L.ix_add_short_range(self._ctx, ctypes.byref(s), _capi.ptr(params), _capi.ptr(alch),
-                                      force.getOverlapMethod())
-        self._check(rc)
-        self._overlap = getattr(self, "_overlap", {})
-        if t > 0:
-            self._overlap[t] = force.getOverlapMethod()
-
-    def _add_three_body(self, force):
-        off, part, params, mol, alch = force._site_arrays()
-        if alch.any():
-            self._parameters.setdefault(force.getAlchemicalParameterName(), 1.0)
-        rc = self._lib.ix_add_three_body(
-            self._ctx, force.getNumSites(), _capi.ptr(_capi.arr(off, np.int32)), _capi.ptr(_capi.arr(part, np.int32)),
-            _capi.ptr(_capi.arr(params, np.float64)), _capi.ptr(_capi.arr(mol, np.int32)),
-            _capi.ptr(_capi.arr(alch, np.uint8)), force.getCutoffDistance(), force.getScaleFactor(),
-            force.getDampingMethod(), force.getDampingScale(), force.getCentroidDampingRadius(),
-            int(force.usesPeriodicBoundaryConditions()), force.getAlchemicalParameterName().encode(),
-            force.getForceGroup())
-        self._check(rc)
+        self._forces, names = describe_forces(self._lib, self._ctx, system, self._check)
+        for name in names:
+            self._parameters.setdefault(name, 1.0)
 
     def __del__(self):
         if getattr(self, "_ctx", None) and self._ctx.value:
