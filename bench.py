@@ -55,6 +55,11 @@ def parse():
     # graph: each step replays one CUDA graph (conditional nodes skip the list rebuild); direct: kernel by kernel,
     # the same kernels and results (profilers cannot see into graphs with conditional nodes)
     p.add_argument("--launch", default="graph", choices=["graph", "direct"])
+    # served stream: Poisson arrival rate (requests/s; 0 = all at once) and the server's running-request limit
+    p.add_argument("--rate", type=float, default=0.0)
+    p.add_argument("--max-running", type=int, default=256)
+    p.add_argument("--requests", type=int, default=20000)
+    p.add_argument("--server-threads", type=int, default=1)
     return p.parse_args()
 
 
@@ -528,6 +533,131 @@ def run_lambda(args, rank, world, num_windows=16, num_alchemical=30):
     print(json.dumps(line))
 
 
+def served_pool(seed, levels=24):
+    """Request templates of the served stream: relaxed periodic water boxes of 1,000..20,000 atoms (cutoff 1.0 nm,
+    ATM cutoff 0.6 nm, box edge >= 2.15 nm) and water clusters of 50..999 atoms (NoCutoff, ATM without cutoff),
+    log-spaced sizes, with 300 K velocities."""
+    from interaxplugin import Context
+    from interaxplugin import workloads as W
+    boxes, clusters = [], []
+    for k, w in enumerate(np.unique(np.round(np.geomspace(1000, 20000, levels) / 3).astype(int))):
+        system, pos, _ = W.water_box(int(w), W.box_length_for(int(w)), 1.0, seed=seed + k, three_body_cutoff=0.6)
+        pos = relax(Context(system), system, pos, iterations=30)
+        boxes.append((system, pos, W.initial_velocities(system, 300.0, seed=seed + k)))
+    for k, w in enumerate(np.unique(np.round(np.geomspace(50, 999, levels) / 3).astype(int))):
+        system, pos, _ = W.water_cluster(int(w), seed=seed + 1000 + k)
+        pos = relax(Context(system), system, pos, iterations=30)
+        clusters.append((system, pos, W.initial_velocities(system, 300.0, seed=seed + 1000 + k)))
+    return boxes, clusters
+
+
+def run_served(args, rank, world, num_requests=20000, budget=120e9, plain_sample=150):
+    """Served stream: 20,000 energy+force requests with Poisson arrivals, sizes log-uniform in 50..20,000 atoms (water
+    boxes from 1,000 atoms, clusters below), each 1..50 velocity-Verlet steps of 1 fs, through the request server
+    with a 120 GB device budget.  Evaluations = initial evaluation + one per step.  Latency is from the scheduled
+    arrival to the completion seen by the server."""
+    import torch
+    from interaxplugin import Context, Server
+
+    device = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(device)
+    rng = np.random.default_rng(args.seed + 7919 * rank)
+    boxes, clusters = served_pool(args.seed + 100 * rank)
+    sizes_b = np.log([s.getNumParticles() for s, _, _ in boxes])
+    sizes_c = np.log([s.getNumParticles() for s, _, _ in clusters])
+    reqs = []
+    for _ in range(num_requests):
+        a = math.log(50) + rng.random() * (math.log(20000) - math.log(50))
+        if a >= math.log(1000):
+            tpl = boxes[int(np.abs(sizes_b - a).argmin())]
+        else:
+            tpl = clusters[int(np.abs(sizes_c - a).argmin())]
+        reqs.append((tpl, int(rng.integers(1, 51))))
+    rate = args.rate
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, num_requests)) if rate > 0 else np.zeros(num_requests)
+    evals = sum(n + 1 for _, n in reqs)
+    atoms = sum(t[0].getNumParticles() for t, _ in reqs)
+    srv = Server(device=device, budget_bytes=budget, max_running=args.max_running, threads=args.server_threads)
+    # warm-up: a few requests of each kind (graph captures, pinned staging)
+    for tpl in boxes[:2] + clusters[:2]:
+        srv.submit(tpl[0], tpl[1], tpl[2], steps=2, dt=0.001)
+    srv.run_all()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+    lag, done, ids = {}, {}, {}
+    with ClockSampler(device) as clocks:
+        t0 = time.perf_counter()
+        for i, ((system, pos, vel), n) in enumerate(reqs):
+            due = t0 + arrivals[i]
+            while True:
+                now = time.perf_counter()
+                if now >= due:
+                    break
+                for rid in srv.poll():
+                    done[rid] = srv.result(rid)
+                if due - time.perf_counter() > 2e-3:
+                    time.sleep(1e-3)
+            rid = srv.submit(system, pos, vel, steps=n, dt=0.001)
+            lag[rid] = time.perf_counter() - due
+            ids[rid] = i
+        while len(done) < num_requests:
+            got = srv.wait(60.0)
+            if not got:
+                raise RuntimeError("served stream timed out")
+            for rid in got:
+                done[rid] = srv.result(rid)
+        t1 = time.perf_counter()
+    stats = srv.stats()
+    srv.close()
+    failed = [r for r in done.values() if r.status != 0]
+    if failed:
+        raise RuntimeError(f"{len(failed)} requests failed: {failed[0].error}")
+    lat = np.array([done[rid].latency + max(lag[rid], 0.0) for rid in done])
+    wall = t1 - t0
+    value = world * evals / wall
+    # the plain per-system path on a sample of the same requests: one Context per request, positions and
+    # velocities in, steps, state out
+    t_plain, e_plain = 0.0, 0
+    for (system, pos, vel), n in reqs[:plain_sample]:
+        ta = time.perf_counter()
+        ctx = Context(system, properties={"DeviceIndex": device})
+        ctx.setPositions(pos)
+        ctx.runVelocityVerlet(n, 0.001, vel)
+        ctx.getState()
+        del ctx
+        t_plain += time.perf_counter() - ta
+        e_plain += n + 1
+    plain = e_plain / t_plain
+    if rank != 0:
+        return
+    line = {
+        "metric": "evaluations/s", "value": value, "unit": "evaluations/s", "n_gpus": world, "steps": num_requests,
+        "warmup": 4, "ms_per_step": 1000 * wall / num_requests, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"served stream of {num_requests} energy+force requests, Poisson arrivals at "
+                               f"{rate:g}/s (0 = all at once), sizes log-uniform 50..20,000 atoms (periodic water "
+                               "boxes from 1,000 atoms, cutoff 1.0 nm, ATM 0.6 nm; clusters below, NoCutoff), 1..50 "
+                               "velocity-Verlet steps of 1 fs each, 120 GB device budget; a step = one request",
+                   "evaluations": evals, "atoms_total": atoms, "wall_s": wall,
+                   "templates": f"{len(boxes)} box and {len(clusters)} cluster sizes, relaxed",
+                   "max_running": args.max_running, "server_threads": args.server_threads,
+                   "parallelism": f"replicas x{world}"},
+        "latency_ms": {"p50": 1000 * float(np.percentile(lat, 50)), "p99": 1000 * float(np.percentile(lat, 99)),
+                       "mean": 1000 * float(lat.mean()), "max": 1000 * float(lat.max())},
+        "requests_per_s": world * num_requests / wall,
+        "server": {k: stats[k] for k in ("contexts", "cohorts", "peak_reserved_bytes", "peak_arena_bytes",
+                                         "worker_seconds")},
+        "plain_per_system": {"value": plain, "unit": "evaluations/s",
+                             "sample": f"the first {plain_sample} requests, one Context each, sequentially"},
+        "served_over_plain": value / world / plain,
+        "e2e": {"value": value, "unit": "evaluations/s", "h2d_bytes_per_step": int(48 * atoms / num_requests),
+                "d2h_bytes_per_step": int(72 * atoms / num_requests + 32)},
+        "clocks": clocks.summary(),
+    }
+    print(json.dumps(line))
+
+
 def main():
     args = parse()
     rank, world = dist_init(args)
@@ -536,6 +666,8 @@ def main():
             run_clusters(args, rank, world)
         elif args.config in ("lambda", "lambda-softcore"):
             run_lambda(args, rank, world)
+        elif args.config == "served":
+            run_served(args, rank, world, num_requests=args.requests)
         elif args.impl == "reference":
             run_reference(args, rank, world)
         else:

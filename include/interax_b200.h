@@ -291,13 +291,19 @@ typedef struct {
     long long contexts, cohorts;              /* units launched: single-request contexts and batched cohorts */
     long long pending, running;               /* requests waiting for admission, requests admitted and not done */
     double budget_bytes, reserved_bytes, peak_reserved_bytes, arena_bytes, peak_arena_bytes;
+    /* worker thread seconds: context set-up, context enqueue, cohort build, cohort enqueue, unit teardown, event
+     * checks, admission scans, idle waits; within set-up and enqueue: pinned staging, device set-up, state uploads,
+     * the steps' launches */
+    double worker_seconds[12];
 } ix_server_stats;
 
 /* A host-only request description of num_particles particles (box: 9 doubles, NULL for non-periodic). */
 int ix_request_create(int num_particles, const double* box, ix_ctx** out);
 /* Starting state: positions (n x 3, required), velocities (n x 3, NULL = at rest), masses (n, required for MD). */
 int ix_request_set_state(ix_ctx* request, const double* positions, const double* velocities, const double* masses);
-int ix_server_create(int device, double budget_bytes, int max_running, ix_server** out);
+/* threads: native worker threads (1..64) that launch and collect requests in parallel; max_running: requests
+ * admitted at once, over all threads. */
+int ix_server_create(int device, double budget_bytes, int max_running, int threads, ix_server** out);
 /* Cohorts: non-periodic requests of at most small_atoms particles are batched, up to max_cohort per cohort; a cohort
  * starts when it is full, when its oldest request has waited window_seconds, or when the GPU is idle. */
 int ix_server_set_batching(ix_server* server, int small_atoms, int max_cohort, double window_seconds);

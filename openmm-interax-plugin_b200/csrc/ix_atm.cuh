@@ -11,8 +11,8 @@
 //                        that all lanes are busy, in rounds of kAtmRound pairs; each triple is counted once (A
 //                        lowest) and evaluated in float; the forces on B and C of each pair are stored and gathered
 //                        per staged neighbor in a fixed order (no atomics)
-//   kTriplesWide         the same for the rare sites with longer lists (up to kAtmMaxStaged within the cutoff), with
-//                        the B and C forces accumulated by shared-memory atomics
+//   kTriplesWide         the same for the rare sites with longer lists (chunked beyond kAtmMaxStaged within the
+//                        cutoff, so any length), with the B and C forces accumulated by shared-memory atomics
 //   kSpreadSiteForces    the site forces, shared equally among each site's particles, into the particle forces
 #pragma once
 
@@ -257,7 +257,7 @@ __device__ __forceinline__ bool atmTriple(const AtmConfig& C, const float4& pa, 
 // parameters; returns how many there are (at most `capacity` are stored).
 template <class Store>
 __device__ __forceinline__ int stageTripleNeighbors(const AtmBuffers& A, const AtmConfig& C, int a, int n, int lane,
-                                                    int capacity, Store store) {
+                                                    int first, int capacity, Store store) {
     int m = 0;
     for (int k0 = 0; k0 < n; k0 += 32) {
         const int k = k0 + lane;
@@ -271,8 +271,8 @@ __device__ __forceinline__ int stageTripleNeighbors(const AtmBuffers& A, const A
         }
         const unsigned bal = __ballot_sync(0xffffffffu, in);
         if (in) {
-            const int slot = m + __popc(bal & laneMaskLt());
-            if (slot < capacity) store(slot, b, (float)d[0], (float)d[1], (float)d[2]);
+            const int slot = m + __popc(bal & laneMaskLt()) - first;
+            if (slot >= 0 && slot < capacity) store(slot, b, (float)d[0], (float)d[1], (float)d[2]);
         }
         m += __popc(bal);
     }
@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(32 * kAtmFastWarps, 7) kTriplesFast(AtmBuffers
         if (n > kAtmFast) continue;      // the wide kernel takes this site
         const float4 pa = A.siteParams[a];
         __syncwarp();
-        const int m = stageTripleNeighbors(A, C, a, n, lane, kAtmFast,
+        const int m = stageTripleNeighbors(A, C, a, n, lane, 0, kAtmFast,
                                            [&](int slot, int b, float x, float y, float z) {
                                                S.pos[slot] = make_float4(x, y, z, __int_as_float(A.molecule[b]));
                                                S.params[slot] = A.siteParams[b];
@@ -398,8 +398,13 @@ struct AtmWarpStorage {
 
 constexpr int kAtmWarps = 4;
 constexpr int kAtmMaxStaged = 256;
+constexpr int kAtmChunk = kAtmMaxStaged / 2;
 
-// Sites whose lists are longer than kAtmFast.  Energies go to energyPartials[partialsOffset + warp].
+// Sites whose lists are longer than kAtmFast.  Up to kAtmMaxStaged neighbors within the cutoff are staged at once and
+// their pairs enumerated by a flat triangular index; a longer list is taken in chunks of kAtmChunk, each pair of
+// chunks (I <= J) staged side by side, so any length is handled.  The forces on B and C accumulate in shared memory
+// and are flushed to the fixed-point site forces after each staging.  Energies go to energyPartials[partialsOffset +
+// warp].
 __global__ void __launch_bounds__(32 * kAtmWarps) kTriplesWide(AtmBuffers A, AtmConfig C, int partialsOffset) {
     extern __shared__ unsigned char atmShared[];
     AtmWarpStorage& S = reinterpret_cast<AtmWarpStorage*>(atmShared)[threadIdx.x >> 5];
@@ -410,38 +415,29 @@ __global__ void __launch_bounds__(32 * kAtmWarps) kTriplesWide(AtmBuffers A, Atm
         const int n = A.nbrCount[a];
         if (n <= kAtmFast) continue;     // the fast kernel takes this site
         const float4 pa = A.siteParams[a];
-        __syncwarp();
-        int m = stageTripleNeighbors(A, C, a, n, lane, kAtmMaxStaged,
-                                     [&](int slot, int b, float x, float y, float z) {
-                                         S.dx[slot] = x;
-                                         S.dy[slot] = y;
-                                         S.dz[slot] = z;
-                                         S.params[slot] = A.siteParams[b];
-                                         S.mol[slot] = A.molecule[b];
-                                         S.site[slot] = b;
-                                         S.fx[slot] = 0.0f;
-                                         S.fy[slot] = 0.0f;
-                                         S.fz[slot] = 0.0f;
-                                     });
-        if (m > kAtmMaxStaged) {
-            if (lane == 0) atomicOr(A.flag + 1, 2);
-            m = kAtmMaxStaged;
-        }
-        __syncwarp();
+        auto stage = [&](int first, int base, int capacity) {
+            return stageTripleNeighbors(A, C, a, n, lane, first, capacity,
+                                        [&](int slot, int b, float x, float y, float z) {
+                                            const int k = base + slot;
+                                            S.dx[k] = x;
+                                            S.dy[k] = y;
+                                            S.dz[k] = z;
+                                            S.params[k] = A.siteParams[b];
+                                            S.mol[k] = A.molecule[b];
+                                            S.site[k] = b;
+                                            S.fx[k] = 0.0f;
+                                            S.fy[k] = 0.0f;
+                                            S.fz[k] = 0.0f;
+                                        });
+        };
         float fax = 0.0f, fay = 0.0f, faz = 0.0f;
-        const int numPairs = m * (m - 1) / 2;
-        for (int p = lane; p < numPairs; p += 32) {
-            // p = c (c - 1)/2 + b with b < c
-            int c = (int)((1.0f + sqrtf(1.0f + 8.0f * (float)p)) * 0.5f);
-            while (c * (c - 1) / 2 > p) c--;
-            while ((c + 1) * c / 2 <= p) c++;
-            const int b = p - c * (c - 1) / 2;
-            if (S.mol[b] == S.mol[c]) continue;
+        auto pair = [&](int b, int c) {
+            if (S.mol[b] == S.mol[c]) return;
             float energy;
             float3 fA, fB, fC;
             if (!atmTriple(C, pa, S.params[b], S.params[c], S.dx[b], S.dy[b], S.dz[b], S.dx[c], S.dy[c], S.dz[c],
                            energy, fA, fB, fC))
-                continue;
+                return;
             fax += fA.x;
             fay += fA.y;
             faz += fA.z;
@@ -453,13 +449,51 @@ __global__ void __launch_bounds__(32 * kAtmWarps) kTriplesWide(AtmBuffers A, Atm
             atomicAdd(&S.fz[c], fC.z);
             eAcc += energy;
             triples++;
-        }
+        };
+        auto triangle = [&](int m) {
+            const int numPairs = m * (m - 1) / 2;
+            for (int p = lane; p < numPairs; p += 32) {
+                // p = c (c - 1)/2 + b with b < c
+                int c = (int)((1.0f + sqrtf(1.0f + 8.0f * (float)p)) * 0.5f);
+                while (c * (c - 1) / 2 > p) c--;
+                while ((c + 1) * c / 2 <= p) c++;
+                pair(p - c * (c - 1) / 2, c);
+            }
+        };
+        auto flush = [&](int lo, int hi) {
+            for (int k = lo + lane; k < hi; k += 32) {
+                const int b = S.site[k];
+                if (S.fx[k] != 0.0f) atomicAddFixed(A.siteForce + b, toFixed(S.fx[k]));
+                if (S.fy[k] != 0.0f) atomicAddFixed(A.siteForce + C.numSites + b, toFixed(S.fy[k]));
+                if (S.fz[k] != 0.0f) atomicAddFixed(A.siteForce + 2 * C.numSites + b, toFixed(S.fz[k]));
+            }
+        };
         __syncwarp();
-        for (int k = lane; k < m; k += 32) {
-            const int b = S.site[k];
-            if (S.fx[k] != 0.0f) atomicAddFixed(A.siteForce + b, toFixed(S.fx[k]));
-            if (S.fy[k] != 0.0f) atomicAddFixed(A.siteForce + C.numSites + b, toFixed(S.fy[k]));
-            if (S.fz[k] != 0.0f) atomicAddFixed(A.siteForce + 2 * C.numSites + b, toFixed(S.fz[k]));
+        const int m = stage(0, 0, kAtmMaxStaged);
+        __syncwarp();
+        if (m <= kAtmMaxStaged) {
+            triangle(m);
+            __syncwarp();
+            flush(0, m);
+        }
+        else {
+            const int chunks = (m + kAtmChunk - 1) / kAtmChunk;
+            for (int I = 0; I < chunks; I++) {
+                const int cI = min(kAtmChunk, m - I * kAtmChunk);
+                for (int J = I; J < chunks; J++) {
+                    const int cJ = min(kAtmChunk, m - J * kAtmChunk);
+                    __syncwarp();
+                    stage(I * kAtmChunk, 0, kAtmChunk);
+                    if (J != I) stage(J * kAtmChunk, kAtmChunk, kAtmChunk);
+                    __syncwarp();
+                    if (J == I) triangle(cI);
+                    else
+                        for (int p = lane; p < cI * cJ; p += 32) pair(p / cJ, kAtmChunk + p % cJ);
+                    __syncwarp();
+                    flush(0, cI);
+                    if (J != I) flush(kAtmChunk, kAtmChunk + cJ);
+                }
+            }
         }
         for (int o = 16; o > 0; o >>= 1) {
             fax += __shfl_xor_sync(0xffffffffu, fax, o);

@@ -56,79 +56,114 @@ struct DeviceBuffer {
     size_t bytes = 0;
 };
 
-// Device memory of the contexts and batches a server runs.  Chunks come from cudaMalloc and are sub-allocated
-// first-fit on the host; they go back to the driver only when the arena is destroyed, because cudaFree waits for the
-// whole device and would stall every request in flight.  Live bytes are bounded by the budget (`limit`).
-struct DeviceArena {
-    struct Chunk {
-        char* base = nullptr;
-        size_t bytes = 0;
-        std::map<size_t, size_t> free;   // offset -> size of each free range, coalesced
+// Free ranges of memory chunks, best fit by size (O(log n) per allocation and release, however fragmented), with
+// neighbouring free ranges of the same chunk merged on release.
+struct RangeHeap {
+    struct Range {
+        size_t bytes;
+        int chunk;
     };
+    std::map<char*, Range> byAddr;                 // free ranges
+    std::multimap<size_t, char*> bySize;           // the same, by size
+    std::map<char*, Range> live;                   // allocations
+
+    void addFree(char* p, size_t bytes, int chunk) {
+        byAddr[p] = {bytes, chunk};
+        bySize.emplace(bytes, p);
+    }
+    void eraseFree(std::map<char*, Range>::iterator it) {
+        auto range = bySize.equal_range(it->second.bytes);
+        for (auto s = range.first; s != range.second; ++s)
+            if (s->second == it->first) {
+                bySize.erase(s);
+                break;
+            }
+        byAddr.erase(it);
+    }
+    char* take(size_t bytes) {
+        auto s = bySize.lower_bound(bytes);
+        if (s == bySize.end()) return nullptr;
+        char* p = s->second;
+        auto it = byAddr.find(p);
+        const Range r = it->second;
+        eraseFree(it);
+        if (r.bytes > bytes) addFree(p + bytes, r.bytes - bytes, r.chunk);
+        live[p] = {bytes, r.chunk};
+        return p;
+    }
+    size_t give(char* p) {   // returns the bytes released (0: not an allocation of this heap)
+        auto it = live.find(p);
+        if (it == live.end()) return 0;
+        Range r = it->second;
+        const size_t released = r.bytes;
+        live.erase(it);
+        auto next = byAddr.find(p + r.bytes);
+        if (next != byAddr.end() && next->second.chunk == r.chunk) {
+            r.bytes += next->second.bytes;
+            eraseFree(next);
+        }
+        auto after = byAddr.lower_bound(p);
+        if (after != byAddr.begin()) {
+            auto prev = std::prev(after);
+            if (prev->second.chunk == r.chunk && prev->first + prev->second.bytes == p) {
+                char* q = prev->first;
+                const size_t merged = prev->second.bytes + r.bytes;
+                eraseFree(prev);
+                addFree(q, merged, r.chunk);
+                return released;
+            }
+        }
+        addFree(p, r.bytes, r.chunk);
+        return released;
+    }
+};
+
+// Device memory of the contexts and batches a server runs.  Chunks come from cudaMalloc and are sub-allocated on
+// the host; they go back to the driver only when the arena is destroyed, because cudaFree waits for the whole device
+// and would stall every request in flight.  Live bytes are bounded by the budget (`limit`).
+struct DeviceArena {
     static constexpr size_t kAlign = 512;
     std::mutex m;
-    std::vector<Chunk> chunks;
-    std::map<char*, std::pair<size_t, size_t>> live;   // allocation -> (chunk, bytes)
+    std::vector<char*> chunks;
+    RangeHeap heap;
     size_t limit = 0, chunkBytes = size_t(256) << 20, inUse = 0, peak = 0, capacity = 0;
+
+    // Add a chunk of `bytes` (cudaMalloc of a large chunk waits for the device, so a server adds its first chunk
+    // before it runs anything).
+    bool grow(size_t bytes) {
+        char* base = nullptr;
+        if (cudaMalloc(reinterpret_cast<void**>(&base), bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        chunks.push_back(base);
+        capacity += bytes;
+        heap.addFree(base, bytes, (int)chunks.size() - 1);
+        return true;
+    }
 
     void* alloc(size_t bytes) {
         bytes = (std::max<size_t>(bytes, 1) + kAlign - 1) / kAlign * kAlign;
         std::lock_guard<std::mutex> lock(m);
         if (inUse + bytes > limit) return nullptr;
-        for (size_t c = 0;; c++) {
-            if (c == chunks.size()) {
-                const size_t want = std::max(chunkBytes, bytes);
-                if (capacity + want > limit + chunkBytes) return nullptr;
-                Chunk k;
-                if (cudaMalloc(reinterpret_cast<void**>(&k.base), want) != cudaSuccess) {
-                    cudaGetLastError();
-                    return nullptr;
-                }
-                k.bytes = want;
-                k.free[0] = want;
-                chunks.push_back(std::move(k));
-                capacity += want;
-            }
-            auto& fr = chunks[c].free;
-            for (auto it = fr.begin(); it != fr.end(); ++it) {
-                if (it->second < bytes) continue;
-                const size_t off = it->first, rest = it->second - bytes;
-                fr.erase(it);
-                if (rest) fr[off + bytes] = rest;
-                char* p = chunks[c].base + off;
-                live[p] = {c, bytes};
-                inUse += bytes;
-                peak = std::max(peak, inUse);
-                return p;
-            }
+        char* p = heap.take(bytes);
+        if (!p) {
+            const size_t want = std::max(chunkBytes, bytes);
+            if (capacity + want > limit + chunkBytes || !grow(want)) return nullptr;
+            p = heap.take(bytes);
         }
+        inUse += bytes;
+        peak = std::max(peak, inUse);
+        return p;
     }
 
     void release(void* ptr) {
         std::lock_guard<std::mutex> lock(m);
-        auto it = live.find(static_cast<char*>(ptr));
-        if (it == live.end()) return;
-        Chunk& k = chunks[it->second.first];
-        size_t off = static_cast<size_t>(it->first - k.base), bytes = it->second.second;
-        inUse -= bytes;
-        live.erase(it);
-        auto next = k.free.lower_bound(off);
-        if (next != k.free.end() && next->first == off + bytes) {
-            bytes += next->second;
-            next = k.free.erase(next);
-        }
-        if (next != k.free.begin()) {
-            auto prev = std::prev(next);
-            if (prev->first + prev->second == off) {
-                prev->second += bytes;
-                return;
-            }
-        }
-        k.free[off] = bytes;
+        inUse -= heap.give(static_cast<char*>(ptr));
     }
 
     ~DeviceArena() {
-        for (auto& k : chunks) cudaFree(k.base);
+        for (char* c : chunks) cudaFree(c);
     }
 };
 
@@ -174,6 +209,8 @@ struct ix_ctx {
     int device = 0;
     DeviceArena* arena = nullptr;        // the owning server's device memory (null: cudaMalloc)
     std::vector<double> requestPos, requestVel, requestMass;   // starting state of a server request description
+    char* uploadBuf = nullptr;           // pinned host staging of a server's context (null: pageable copies)
+    size_t uploadCap = 0, uploadUsed = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;      // the three-body chain, forked from and joined back into `stream`
     cudaStream_t streamBody = nullptr;   // captures the branches of conditional graph nodes
@@ -320,6 +357,31 @@ static int deviceAlloc(ix_ctx* ctx, const std::string& name, size_t count, T** o
         int _rc = (expr);           \
         if (_rc != IX_OK) return _rc; \
     } while (0)
+
+// Copy host data to the device in the context's stream order.  A server's context has pinned staging: the data is
+// copied there first and the transfer is asynchronous, with no wait for the stream (a pageable copy waits for the
+// stream's earlier work, which on a busy GPU means waiting for other requests' kernels).
+static int stageCopy(ix_ctx* ctx, void* dst, const void* src, size_t bytes) {
+    if (!bytes) return IX_OK;
+    if (ctx->uploadBuf && ctx->uploadUsed + bytes <= ctx->uploadCap) {
+        char* p = ctx->uploadBuf + ctx->uploadUsed;
+        ctx->uploadUsed += (bytes + 63) / 64 * 64;
+        std::memcpy(p, src, bytes);
+        src = p;
+    }
+    const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, IX_ERR_CUDA, "cudaMemcpyAsync failed: %s", cudaGetErrorString(e));
+    return IX_OK;
+}
+
+// Wait for the uploads just issued (pageable ones only; staged ones stay valid until the stream has run them).
+static int uploadsDone(ix_ctx* ctx) {
+    if (ctx->uploadBuf) return IX_OK;
+    const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return fail(ctx, IX_ERR_CUDA, "cudaStreamSynchronize failed: %s", cudaGetErrorString(e));
+    return IX_OK;
+}
+
 
 static Box makeBox(const double* b) {
     Box box;
@@ -544,8 +606,7 @@ static int buildClassTable(ix_ctx* ctx, std::vector<int>& flags) {
     if (T == 0) return IX_OK;
     PairCoef* dTable;
     IX_TRY(deviceAlloc(ctx, "classTable", table.size(), &dTable));
-    IX_CUDA(ctx, cudaMemcpyAsync(dTable, table.data(), table.size() * sizeof(PairCoef), cudaMemcpyHostToDevice,
-                                 ctx->stream));
+    IX_TRY(stageCopy(ctx, dTable, table.data(), table.size() * sizeof(PairCoef)));
     ctx->P.coef = dTable;
     ctx->P.numClasses = T;
     return IX_OK;
@@ -608,19 +669,19 @@ static int uploadPairParams(ix_ctx* ctx) {
     std::vector<float4> p0, p1, p2, p3;
     std::vector<int> flags;
     packPairParams(ctx, p0, p1, p2, p3, flags);
-    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP0o, p0.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
-    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP1o, p1.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
-    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP2o, p2.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
-    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dP3o, p3.data(), n * sizeof(float4), cudaMemcpyHostToDevice, ctx->stream));
+    IX_TRY(stageCopy(ctx, ctx->dP0o, p0.data(), n * sizeof(float4)));
+    IX_TRY(stageCopy(ctx, ctx->dP1o, p1.data(), n * sizeof(float4)));
+    IX_TRY(stageCopy(ctx, ctx->dP2o, p2.data(), n * sizeof(float4)));
+    IX_TRY(stageCopy(ctx, ctx->dP3o, p3.data(), n * sizeof(float4)));
     IX_TRY(buildClassTable(ctx, flags));
-    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dFlagso, flags.data(), n * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    IX_TRY(stageCopy(ctx, ctx->dFlagso, flags.data(), n * sizeof(int)));
+    IX_TRY(uploadsDone(ctx));
     computeLrc(ctx);
     ctx->pairDirty = false;
     bumpVersion(ctx);
     // a rebuild gathers the parameters into sorted order
     int one = 1;
-    IX_CUDA(ctx, cudaMemcpyAsync(ctx->L.flag, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    IX_TRY(stageCopy(ctx, ctx->L.flag, &one, sizeof(int)));
     return IX_OK;
 }
 
@@ -704,7 +765,7 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
 
     int* cellRank;
     IX_TRY(deviceAlloc(ctx, "cellRank", numCells, &cellRank));
-    IX_CUDA(ctx, cudaMemcpyAsync(cellRank, rank.data(), numCells * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    IX_TRY(stageCopy(ctx, cellRank, rank.data(), numCells * sizeof(int)));
     L.cellRank = cellRank;
     IX_TRY(deviceAlloc(ctx, "cellKey", n, &L.cellKey));
     IX_TRY(deviceAlloc(ctx, "cellCount", numCells, &L.cellCount));
@@ -754,10 +815,10 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
     IX_TRY(deviceAlloc(ctx, "exclStart", n + 1, &dStart));
     IX_TRY(deviceAlloc(ctx, "exclList", std::max<size_t>(list.size(), 1), &dList));
     IX_TRY(deviceAlloc(ctx, "exclRange", n, &dRange));
-    IX_CUDA(ctx, cudaMemcpyAsync(dStart, start.data(), (n + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    IX_TRY(stageCopy(ctx, dStart, start.data(), (n + 1) * sizeof(int)));
     if (!list.empty())
-        IX_CUDA(ctx, cudaMemcpyAsync(dList, list.data(), list.size() * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    IX_CUDA(ctx, cudaMemcpyAsync(dRange, range.data(), n * sizeof(int2), cudaMemcpyHostToDevice, ctx->stream));
+        IX_TRY(stageCopy(ctx, dList, list.data(), list.size() * sizeof(int)));
+    IX_TRY(stageCopy(ctx, dRange, range.data(), n * sizeof(int2)));
     L.exclStart = dStart;
     L.exclList = dList;
     L.exclRange = dRange;
@@ -815,12 +876,11 @@ static int allocateAtm(ix_ctx* ctx) {
     IX_TRY(deviceAlloc(ctx, "siteParticles", std::max<size_t>(ctx->siteParticles.size(), 1), &dPart));
     IX_TRY(deviceAlloc(ctx, "siteMolecule", ns, &dMol));
     IX_TRY(deviceAlloc(ctx, "siteParams", ns, &dParams));
-    IX_CUDA(ctx, cudaMemcpyAsync(dOff, ctx->siteOffsets.data(), (ns + 1) * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
-    IX_CUDA(ctx, cudaMemcpyAsync(dPart, ctx->siteParticles.data(), ctx->siteParticles.size() * sizeof(int),
-                                 cudaMemcpyHostToDevice, ctx->stream));
+    IX_TRY(stageCopy(ctx, dOff, ctx->siteOffsets.data(), (ns + 1) * sizeof(int)));
+    IX_TRY(stageCopy(ctx, dPart, ctx->siteParticles.data(), ctx->siteParticles.size() * sizeof(int)));
     std::vector<int> mol(ns);
     for (int i = 0; i < ns; i++) mol[i] = ctx->molecule[i] < 0 ? -1 - i : ctx->molecule[i];
-    IX_CUDA(ctx, cudaMemcpyAsync(dMol, mol.data(), ns * sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    IX_TRY(stageCopy(ctx, dMol, mol.data(), ns * sizeof(int)));
     A.siteOffsets = dOff;
     A.siteParticles = dPart;
     A.molecule = dMol;
@@ -865,11 +925,10 @@ static int uploadAtmParams(ix_ctx* ctx) {
     for (int i = 0; i < ns; i++)
         p[i] = make_float4((float)ctx->siteParams[3 * i], (float)ctx->siteParams[3 * i + 1],
                            (float)ctx->siteParams[3 * i + 2], ctx->siteAlch[i] ? 1.0f : 0.0f);
-    IX_CUDA(ctx, cudaMemcpyAsync((void*)ctx->A.siteParams, p.data(), ns * sizeof(float4), cudaMemcpyHostToDevice,
-                                 ctx->stream));
-    IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    IX_TRY(stageCopy(ctx, (void*)ctx->A.siteParams, p.data(), ns * sizeof(float4)));
+    IX_TRY(uploadsDone(ctx));
     int one = 1;
-    IX_CUDA(ctx, cudaMemcpyAsync(ctx->A.flag, &one, sizeof(int), cudaMemcpyHostToDevice, ctx->stream));
+    IX_TRY(stageCopy(ctx, ctx->A.flag, &one, sizeof(int)));
     ctx->atmDirty = false;
     bumpVersion(ctx);
     return IX_OK;
@@ -1264,13 +1323,10 @@ static int checkOverflow(ix_ctx* ctx, unsigned terms, bool& redo) {
     }
     if ((terms & 8u) && flags[5]) {
         ctx->atmCap = std::min(2 * ctx->atmCap, (((int)ctx->siteParams.size() / 3 + 31) / 32) * 32 + 32);
-        if (flags[5] & 2) ctx->atmCap = std::max(ctx->atmCap, 256);
         int f[2] = {1, 0};
         IX_CUDA(ctx, cudaMemcpy(ctx->dFlags + 4, f, sizeof(f), cudaMemcpyHostToDevice));
         IX_TRY(allocateAtm(ctx));
         IX_TRY(uploadAtmParams(ctx));
-        if (flags[5] & 2) return fail(ctx, IX_ERR_INVALID,
-                                      "InteraxThreeBodyForce: more than 256 sites within the cutoff of one site");
         redo = true;
         bumpVersion(ctx);
     }
@@ -1343,14 +1399,13 @@ static void releaseGraph(LaunchGraph& g) {
 // server owns the context).  A context described on the host only (a server request) gets it on admission.
 static int ctxInitDevice(ix_ctx* ctx) {
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
-    cudaDeviceProp prop;
-    IX_CUDA(ctx, cudaGetDeviceProperties(&prop, ctx->device));
-    ctx->numSMs = prop.multiProcessorCount;
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&ctx->streamBody, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->evFork, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&ctx->evJoin, cudaEventDisableTiming) != cudaSuccess)
+    IX_CUDA(ctx, cudaDeviceGetAttribute(&ctx->numSMs, cudaDevAttrMultiProcessorCount, ctx->device));
+    // streams and events a server hands over from its pool are kept
+    if ((!ctx->stream && cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) ||
+        (!ctx->stream2 && cudaStreamCreateWithFlags(&ctx->stream2, cudaStreamNonBlocking) != cudaSuccess) ||
+        (!ctx->streamBody && cudaStreamCreateWithFlags(&ctx->streamBody, cudaStreamNonBlocking) != cudaSuccess) ||
+        (!ctx->evFork && cudaEventCreateWithFlags(&ctx->evFork, cudaEventDisableTiming) != cudaSuccess) ||
+        (!ctx->evJoin && cudaEventCreateWithFlags(&ctx->evJoin, cudaEventDisableTiming) != cudaSuccess))
         return fail(ctx, IX_ERR_CUDA, "cudaStreamCreate failed");
     const int n = ctx->n;
     IX_TRY(deviceAlloc(ctx, "pos", 3 * (size_t)n, &ctx->dPos));
@@ -1361,10 +1416,10 @@ static int ctxInitDevice(ix_ctx* ctx) {
     IX_TRY(deviceAlloc(ctx, "energyBlocks", 4 * kReduceBlocks, &ctx->dEnergyBlocks));
     IX_TRY(deviceAlloc(ctx, "reduceTicket", 1, &ctx->dReduceTicket));
     int init[8] = {1, 0, 0, 0, 1, 0, 0, 0};
-    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dFlags, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    IX_TRY(stageCopy(ctx, ctx->dFlags, init, sizeof(init)));
     IX_CUDA(ctx, cudaMemsetAsync(ctx->dReduceTicket, 0, sizeof(unsigned), ctx->stream));
     IX_CUDA(ctx, cudaMemsetAsync(ctx->dCounts, 0, 4 * sizeof(unsigned long long), ctx->stream));
-    IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    IX_TRY(uploadsDone(ctx));
     return IX_OK;
 }
 
@@ -1611,8 +1666,7 @@ int ix_set_positions(ix_ctx* ctx, const double* positions, const double* box) {
         std::memcpy(ctx->box, box, sizeof(ctx->box));
     }
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
-    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dPos, positions, 3 * (size_t)ctx->n * sizeof(double), cudaMemcpyHostToDevice,
-                                 ctx->stream));
+    IX_TRY(stageCopy(ctx, ctx->dPos, positions, 3 * (size_t)ctx->n * sizeof(double)));
     ctx->havePositions = true;
     return IX_OK;
 }
@@ -1760,7 +1814,7 @@ int ix_md_set_masses(ix_ctx* ctx, const double* masses) {
     }
     IX_TRY(deviceAlloc(ctx, "invMass", ctx->n, &ctx->dInvMass));
     IX_TRY(deviceAlloc(ctx, "vel", 3 * (size_t)ctx->n, &ctx->dVel));
-    IX_CUDA(ctx, cudaMemcpyAsync(ctx->dInvMass, inv.data(), ctx->n * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+    IX_TRY(stageCopy(ctx, ctx->dInvMass, inv.data(), ctx->n * sizeof(double)));
     ctx->haveMasses = true;
     bumpVersion(ctx);
     return IX_OK;
@@ -1943,8 +1997,7 @@ static int windowsPass(ix_ctx* ctx, const std::string& name, int num_windows, co
             energies[4 * w + k] = pairEnergy[4 * (size_t)w + k] + e0[k] + values[w] * (e1[k] - e0[k]);
     if (d_forces) {
         if (linearTerms) {
-            IX_CUDA(ctx, cudaMemcpyAsync(dLambda, values, num_windows * sizeof(double), cudaMemcpyHostToDevice,
-                                         ctx->stream));
+            IX_TRY(stageCopy(ctx, dLambda, values, num_windows * sizeof(double)));
             const unsigned bx = (unsigned)std::max<size_t>(std::min<size_t>((n3 + 255) / 256, 1184), 1);
             const dim3 grid(bx, (unsigned)std::min(num_windows, 65535));
             kWindowForces<<<grid, 256, 0, ctx->stream>>>(n3, num_windows, dLambda, dLin0, dLin1, d_forces,
@@ -2049,8 +2102,7 @@ int ix_md_run(ix_ctx* ctx, int num_steps, double dt, double* positions, double* 
     if (!ctx->haveMasses) return fail(ctx, IX_ERR_STATE, "ix_md_run: masses have not been set");
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
     if (velocities)
-        IX_CUDA(ctx, cudaMemcpyAsync(ctx->dVel, velocities, 3 * (size_t)ctx->n * sizeof(double), cudaMemcpyHostToDevice,
-                                     ctx->stream));
+        IX_TRY(stageCopy(ctx, ctx->dVel, velocities, 3 * (size_t)ctx->n * sizeof(double)));
     IX_TRY(ix_md_steps_async(ctx, num_steps, dt));
     return ix_md_finish(ctx, positions, velocities, energy);
 }

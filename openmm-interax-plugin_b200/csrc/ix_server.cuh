@@ -1,23 +1,30 @@
 // A request server: continuous batching of independent energy+force / MD requests of mixed sizes on one GPU.
 // Included at the end of ix_context.cu (after ix_batch.cuh), whose contexts and batches it runs.
 //
-// One native worker thread owns the device side.  Each pass of its loop
-//   1. moves newly submitted requests into the pending queue (FIFO),
+// Native worker threads (shards) own the device side; each runs its own requests (small requests all go to shard 0,
+// so that they gather into large cohorts; periodic requests are spread over all shards, whose host work of launching
+// them then proceeds in parallel).  Each pass of a shard's loop
+//   1. moves newly submitted requests into the shard's pending queue (FIFO),
 //   2. admits pending requests while the running count and the device memory budget allow (a request whose estimate
 //      does not fit waits; later, smaller requests may pass it), launching each admitted periodic request as a
 //      context on its own streams and gathering admitted small non-periodic requests into a cohort (an ix_batch run
 //      with per-system step counts, one CUDA graph per MD step of the whole cohort),
 //   3. checks the events that mark finished requests: their results were copied by their own stream into pinned
 //      staging, so the worker only unpacks them, and frees the unit's memory when its last request is done.
-// All launches are asynchronous, so every admitted request's work overlaps on the device.  A request's state
+// All launches are asynchronous, so every admitted request's work overlaps on the device.  Device memory comes from one
+// arena bounded by the budget; the estimate of each request is reserved atomically at admission, so shards never
+// over-commit it.  A context's streams and events go back to its shard's pool and its CUDA graphs to a reaper thread
+// when it finishes, so that no teardown call of the worker waits for the device.  A request's state
 // (positions, velocities, parameters, neighbor lists) stays resident on the device from admission to its last step.
 // Its results are those of the same request run alone: a context runs the same kernels either way, and a batched
 // system's evaluation is independent of the other systems of its batch.
 #pragma once
 
+#include <atomic>
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <memory>
 #include <thread>
 
 namespace {
@@ -26,66 +33,44 @@ double serverNow() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
 
-// Host memory that the device can copy into asynchronously: chunks from cudaHostAlloc, sub-allocated first-fit.
+// Adds the seconds of its scope to one of the worker's time counters.
+struct PhaseTimer {
+    double& total;
+    double t0;
+    explicit PhaseTimer(double& t) : total(t), t0(serverNow()) {}
+    ~PhaseTimer() { total += serverNow() - t0; }
+};
+
+// Host memory that the device can copy into asynchronously: chunks from cudaHostAlloc, sub-allocated best fit.
 struct PinnedPool {
-    struct Chunk {
-        char* base = nullptr;
-        size_t bytes = 0;
-        std::map<size_t, size_t> free;
-    };
-    std::vector<Chunk> chunks;
-    std::map<char*, std::pair<size_t, size_t>> live;
-    size_t chunkBytes = size_t(64) << 20;
+    std::mutex m;
+    std::vector<char*> chunks;
+    RangeHeap heap;
+    size_t chunkBytes = size_t(256) << 20;
 
     char* alloc(size_t bytes) {
         bytes = (std::max<size_t>(bytes, 1) + 255) / 256 * 256;
-        for (size_t c = 0;; c++) {
-            if (c == chunks.size()) {
-                Chunk k;
-                k.bytes = std::max(chunkBytes, bytes);
-                if (cudaHostAlloc(reinterpret_cast<void**>(&k.base), k.bytes, cudaHostAllocDefault) != cudaSuccess) {
-                    cudaGetLastError();
-                    return nullptr;
-                }
-                k.free[0] = k.bytes;
-                chunks.push_back(std::move(k));
-            }
-            auto& fr = chunks[c].free;
-            for (auto it = fr.begin(); it != fr.end(); ++it) {
-                if (it->second < bytes) continue;
-                const size_t off = it->first, rest = it->second - bytes;
-                fr.erase(it);
-                if (rest) fr[off + bytes] = rest;
-                char* p = chunks[c].base + off;
-                live[p] = {c, bytes};
-                return p;
-            }
+        std::lock_guard<std::mutex> lock(m);
+        char* p = heap.take(bytes);
+        if (p) return p;
+        char* base = nullptr;
+        const size_t want = std::max(chunkBytes, bytes);
+        if (cudaHostAlloc(reinterpret_cast<void**>(&base), want, cudaHostAllocDefault) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
         }
+        chunks.push_back(base);
+        heap.addFree(base, want, (int)chunks.size() - 1);
+        return heap.take(bytes);
     }
 
     void release(char* p) {
-        auto it = live.find(p);
-        if (it == live.end()) return;
-        Chunk& k = chunks[it->second.first];
-        size_t off = static_cast<size_t>(p - k.base), bytes = it->second.second;
-        live.erase(it);
-        auto next = k.free.lower_bound(off);
-        if (next != k.free.end() && next->first == off + bytes) {
-            bytes += next->second;
-            next = k.free.erase(next);
-        }
-        if (next != k.free.begin()) {
-            auto prev = std::prev(next);
-            if (prev->first + prev->second == off) {
-                prev->second += bytes;
-                return;
-            }
-        }
-        k.free[off] = bytes;
+        std::lock_guard<std::mutex> lock(m);
+        heap.give(p);
     }
 
     ~PinnedPool() {
-        for (auto& k : chunks) cudaFreeHost(k.base);
+        for (char* c : chunks) cudaFreeHost(c);
     }
 };
 
@@ -116,37 +101,59 @@ struct ServerUnit {
     std::vector<Mark> marks;
     size_t next = 0;
     char* staging = nullptr;             // pinned copies of the results, written by the unit's stream
-    size_t reserved = 0;                 // device bytes the unit holds
+    size_t reserved = 0;                 // device bytes reserved for the unit (its actual bytes once launched)
     int restarts = 0;
+};
+
+// A context's streams and events, kept for the next context of the shard.
+struct StreamSet {
+    cudaStream_t stream = nullptr, stream2 = nullptr, body = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+struct ServerShard {
+    int index = 0;
+    std::thread worker;
+    std::deque<ServerRequest*> incoming;     // guarded by the server's mutex
+    std::deque<ServerRequest*> pending;
+    std::vector<ServerUnit*> units;
+    std::vector<cudaEvent_t> freeEvents;
+    std::vector<StreamSet> streams;
+    std::vector<cudaStream_t> cohortStreams;
+    long long running = 0;
+    double workerSec[12] = {};           // see ix_server_stats::worker_seconds
 };
 
 }  // namespace
 
 struct ix_server {
     int device = 0;
+    int numSMs = 148;
     DeviceArena arena;
     PinnedPool pinned;
     double budget = 0.0;
-    int maxRunning = 256;
+    std::atomic<long long> reserved{0};      // device bytes reserved by admitted units, all shards
+    std::atomic<long long> peakReserved{0};
+    int maxRunning = 256;                    // per shard
     int smallAtoms = 1024;
     int maxCohort = 512;
     double window = 200e-6;
-    std::thread worker;
-    std::mutex m;                        // guards incoming, done, doneIds, results, error, stats, stop
+    std::vector<std::unique_ptr<ServerShard>> shards;
+    std::mutex m;                        // guards the shards' incoming queues, done, doneIds, error, stats, stop
     std::condition_variable cvSubmit, cvDone;
     bool stop = false;
-    std::deque<ServerRequest*> incoming;
     std::map<long long, ServerRequest*> done;
     std::deque<long long> doneIds;
     long long nextId = 1;
+    size_t nextShard = 0;
     std::string error;
     ix_server_stats stats{};
-    // worker-owned
-    std::deque<ServerRequest*> pending;
-    std::vector<ServerUnit*> units;
-    std::vector<cudaEvent_t> freeEvents;
-    size_t reserved = 0;
-    long long running = 0;
+    // CUDA graphs of finished contexts, destroyed by the reaper thread
+    std::thread reaper;
+    std::mutex graveM;
+    std::condition_variable graveCv;
+    std::deque<cudaGraphExec_t> grave;
+    bool graveStop = false;
 };
 
 namespace {
@@ -161,10 +168,32 @@ size_t estimateRequestBytes(const ix_ctx* c, bool small) {
     return (size_t(8) << 20) + 6144 * n + 4096 * sites;
 }
 
-cudaEvent_t serverEvent(ix_server* S) {
-    if (!S->freeEvents.empty()) {
-        cudaEvent_t e = S->freeEvents.back();
-        S->freeEvents.pop_back();
+// Reserve device bytes against the budget; false if they do not fit.
+bool reserveBytes(ix_server* S, size_t bytes) {
+    const long long b = (long long)bytes;
+    long long cur = S->reserved.load();
+    while ((double)(cur + b) <= S->budget)
+        if (S->reserved.compare_exchange_weak(cur, cur + b)) {
+            long long peak = S->peakReserved.load();
+            while (cur + b > peak && !S->peakReserved.compare_exchange_weak(peak, cur + b)) {
+            }
+            return true;
+        }
+    return false;
+}
+
+void unreserveBytes(ix_server* S, size_t bytes) { S->reserved -= (long long)bytes; }
+
+size_t bufferBytes(const std::map<std::string, DeviceBuffer>& buffers) {
+    size_t total = 0;
+    for (const auto& kv : buffers) total += kv.second.bytes;
+    return total;
+}
+
+cudaEvent_t shardEvent(ServerShard* H) {
+    if (!H->freeEvents.empty()) {
+        cudaEvent_t e = H->freeEvents.back();
+        H->freeEvents.pop_back();
         return e;
     }
     cudaEvent_t e = nullptr;
@@ -172,7 +201,7 @@ cudaEvent_t serverEvent(ix_server* S) {
     return e;
 }
 
-void serverFinish(ix_server* S, ServerRequest* r, int status, const std::string& error) {
+void serverFinish(ix_server* S, ServerShard* H, ServerRequest* r, int status, const std::string& error) {
     r->tDone = serverNow();
     r->status = status;
     r->error = error;
@@ -187,23 +216,82 @@ void serverFinish(ix_server* S, ServerRequest* r, int status, const std::string&
         if (status == IX_OK) S->stats.completed++;
         else S->stats.failed++;
     }
-    S->running--;
+    if (H) H->running--;
     S->cvDone.notify_all();
 }
 
+// Destroy a finished context without waiting for the device: its streams and events go back to the shard's pool,
+// its graphs to the reaper, its memory to the arena.
+void retireContext(ix_server* S, ServerShard* H, ix_ctx* c) {
+    if (c->stream) cudaStreamSynchronize(c->stream);   // idle already: its last event has completed
+    StreamSet set;
+    set.stream = c->stream;
+    set.stream2 = c->stream2;
+    set.body = c->streamBody;
+    set.fork = c->evFork;
+    set.join = c->evJoin;
+    if (set.stream && set.stream2 && set.body && set.fork && set.join) {
+        H->streams.push_back(set);
+        c->stream = c->stream2 = c->streamBody = nullptr;
+        c->evFork = c->evJoin = nullptr;
+    }
+    {
+        std::lock_guard<std::mutex> lock(S->graveM);
+        for (LaunchGraph* g : {&c->graphCompute, &c->graphDevice, &c->graphMd})
+            if (g->exec) {
+                S->grave.push_back(g->exec);
+                g->exec = nullptr;
+            }
+        for (auto& g : c->graphWindows)
+            if (g.exec) {
+                S->grave.push_back(g.exec);
+                g.exec = nullptr;
+            }
+    }
+    S->graveCv.notify_one();
+    ix_ctx_destroy(c);
+}
+
+void reaperLoop(ix_server* S) {
+    cudaSetDevice(S->device);
+    std::unique_lock<std::mutex> lock(S->graveM);
+    for (;;) {
+        S->graveCv.wait(lock, [&] { return S->graveStop || !S->grave.empty(); });
+        if (S->grave.empty() && S->graveStop) break;
+        cudaGraphExec_t g = S->grave.front();
+        S->grave.pop_front();
+        lock.unlock();
+        cudaGraphExecDestroy(g);
+        lock.lock();
+    }
+}
+
+// Requests with at least this many steps run each step as one CUDA graph (the capture costs about a millisecond);
+// shorter ones launch their kernels directly.
+#ifndef IX_SERVER_GRAPH_STEPS
+#define IX_SERVER_GRAPH_STEPS 16
+#endif
+constexpr int kServerGraphSteps = IX_SERVER_GRAPH_STEPS;
+
 // Enqueue a periodic request's whole run on its context's stream: positions, masses and velocities in, the first
 // evaluation and every step, then the final state copied into the pinned staging, and the event that marks it done.
-int enqueueContextRun(ix_server* S, ServerUnit* u) {
+int enqueueContextRun(ServerShard* H, ServerUnit* u) {
     ServerRequest* r = u->members[0];
     ix_ctx* c = u->ctx;
     const size_t n3 = 3 * (size_t)c->n;
-    IX_TRY(ix_set_positions(c, r->pos.data(), nullptr));
-    if (r->mass.empty()) r->mass.assign(c->n, 1.0);
-    IX_TRY(ix_md_set_masses(c, r->mass.data()));
-    if (r->vel.empty()) IX_CUDA(c, cudaMemsetAsync(c->dVel, 0, n3 * sizeof(double), c->stream));
-    else IX_CUDA(c, cudaMemcpyAsync(c->dVel, r->vel.data(), n3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    {
+        PhaseTimer t(H->workerSec[10]);
+        IX_TRY(ix_set_positions(c, r->pos.data(), nullptr));
+        if (r->mass.empty()) r->mass.assign(c->n, 1.0);
+        IX_TRY(ix_md_set_masses(c, r->mass.data()));
+        if (r->vel.empty()) IX_CUDA(c, cudaMemsetAsync(c->dVel, 0, n3 * sizeof(double), c->stream));
+        else IX_TRY(stageCopy(c, c->dVel, r->vel.data(), n3 * sizeof(double)));
+    }
     c->mdForcesValid = false;
-    IX_TRY(ix_md_steps_async(c, r->steps, r->dt));
+    {
+        PhaseTimer t(H->workerSec[11]);
+        IX_TRY(ix_md_steps_async(c, r->steps, r->dt));
+    }
     double* st = reinterpret_cast<double*>(u->staging);
     IX_CUDA(c, cudaMemcpyAsync(st, c->dPos, n3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     IX_CUDA(c, cudaMemcpyAsync(st + n3, c->dVel, n3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -211,7 +299,7 @@ int enqueueContextRun(ix_server* S, ServerUnit* u) {
     IX_CUDA(c, cudaMemcpyAsync(st + 3 * n3, c->dOutEnergy, 4 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     IX_CUDA(c, cudaMemcpyAsync(st + 3 * n3 + 4, c->dFlags, 8 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     ServerUnit::Mark mk;
-    mk.event = serverEvent(S);
+    mk.event = shardEvent(H);
     mk.first = 0;
     mk.last = 1;
     IX_CUDA(c, cudaEventRecord(mk.event, c->stream));
@@ -220,47 +308,75 @@ int enqueueContextRun(ix_server* S, ServerUnit* u) {
     return IX_OK;
 }
 
-// Admit a periodic request: its description becomes a device context in the server's arena.
-void launchContext(ix_server* S, ServerRequest* r) {
+// Launch an admitted periodic request (its estimate already reserved): its description becomes a device context in
+// the server's arena, with streams from the shard's pool.
+void launchContext(ix_server* S, ServerShard* H, ServerRequest* r) {
     ServerUnit* u = new ServerUnit();
     u->members.push_back(r);
+    u->reserved = r->estimate;
     ix_ctx* c = r->sys;
     c->arena = &S->arena;
     c->device = S->device;
+    c->useGraphs = r->steps >= kServerGraphSteps;
+    if (!H->streams.empty()) {
+        const StreamSet set = H->streams.back();
+        H->streams.pop_back();
+        c->stream = set.stream;
+        c->stream2 = set.stream2;
+        c->streamBody = set.body;
+        c->evFork = set.fork;
+        c->evJoin = set.join;
+    }
     u->ctx = c;
-    size_t before;
+    int rc;
     {
-        std::lock_guard<std::mutex> lock(S->arena.m);
-        before = S->arena.inUse;
-    }
-    int rc = ctxInitDevice(c);
-    if (rc == IX_OK) {
-        u->staging = S->pinned.alloc((9 * (size_t)c->n + 8) * sizeof(double));
+        PhaseTimer t(H->workerSec[0]);
+        // pinned staging: the results, then every upload of the request (parameters, lists, state)
+        const size_t results = (9 * (size_t)c->n + 8) * sizeof(double);
+        const size_t uploads = 320 * (size_t)c->n + 64 * (c->siteParams.size() / 3) + 8 * c->exclusions.size() +
+                               (size_t(64) << 10);
+        {
+            PhaseTimer tp(H->workerSec[8]);
+            u->staging = S->pinned.alloc(results + uploads);
+        }
+        rc = IX_OK;
         if (!u->staging) rc = fail(c, IX_ERR_MEMORY, "pinned host staging could not be allocated");
+        else {
+            c->uploadBuf = u->staging + results;
+            c->uploadCap = uploads;
+            c->uploadUsed = 0;
+            PhaseTimer td(H->workerSec[9]);
+            rc = ctxInitDevice(c);
+        }
     }
-    if (rc == IX_OK) rc = enqueueContextRun(S, u);
-    {
-        std::lock_guard<std::mutex> lock(S->arena.m);
-        u->reserved = S->arena.inUse - before;
+    if (rc == IX_OK) {
+        PhaseTimer t(H->workerSec[1]);
+        rc = enqueueContextRun(H, u);
     }
     if (rc != IX_OK) {
         const std::string msg = c->error;
-        if (c->stream) cudaStreamSynchronize(c->stream);
-        for (auto& mk : u->marks) S->freeEvents.push_back(mk.event);
+        for (auto& mk : u->marks) H->freeEvents.push_back(mk.event);
         if (u->staging) S->pinned.release(u->staging);
-        u->ctx = nullptr;
+        r->sys = nullptr;
+        retireContext(S, H, c);
+        unreserveBytes(S, u->reserved);
         delete u;
-        serverFinish(S, r, rc, msg);   // destroys the context and frees its memory
+        serverFinish(S, H, r, rc, msg);
         return;
     }
-    S->reserved += u->reserved;
-    S->units.push_back(u);
+    // a context that holds more than its estimate reserves the difference too
+    const size_t actual = bufferBytes(c->buffers);
+    if (actual > u->reserved) {
+        S->reserved += (long long)(actual - u->reserved);
+        u->reserved = actual;
+    }
+    H->units.push_back(u);
     std::lock_guard<std::mutex> lock(S->m);
     S->stats.contexts++;
     S->stats.admitted++;
 }
 
-// Whether a small request can join a cohort started by c0: the same force settings, parameters and step size.
+// Whether a small request can join a cohort started by r0: the same force settings, parameters and step size.
 bool cohortCompatible(const ServerRequest* r, const ServerRequest* r0) {
     return r->dt == r0->dt && r->sys->parameters == r0->sys->parameters && sameBatchSettings(r->sys, r0->sys);
 }
@@ -268,7 +384,7 @@ bool cohortCompatible(const ServerRequest* r, const ServerRequest* r0) {
 // Enqueue a cohort's whole run on its batch's stream: the first evaluation, then every step up to the longest
 // request; after the last step of each group of requests (members are ordered by steps) their final state is copied
 // into the pinned staging and an event marks them done.
-int enqueueCohortRun(ix_server* S, ServerUnit* u) {
+int enqueueCohortRun(ServerShard* H, ServerUnit* u) {
     ix_batch* b = u->batch;
     const int nm = (int)u->members.size(), np = b->numParticles;
     std::vector<double> pos(3 * (size_t)np), vel(3 * (size_t)np, 0.0), mass((size_t)np, 1.0);
@@ -302,7 +418,7 @@ int enqueueCohortRun(ix_server* S, ServerUnit* u) {
         IX_BCUDA(b, cudaMemcpyAsync(st + 3 * n3 + 4 * (size_t)first, b->dEnergies + 4 * (size_t)first,
                                     4 * (size_t)(last - first) * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
         ServerUnit::Mark mk;
-        mk.event = serverEvent(S);
+        mk.event = shardEvent(H);
         mk.first = first;
         mk.last = last;
         IX_BCUDA(b, cudaEventRecord(mk.event, b->stream));
@@ -312,72 +428,69 @@ int enqueueCohortRun(ix_server* S, ServerUnit* u) {
     return IX_OK;
 }
 
-// Admit a cohort of small requests as one batch in the server's arena.
-void launchCohort(ix_server* S, std::vector<ServerRequest*>& members) {
+// Launch an admitted cohort of small requests (their estimates already reserved) as one batch in the server's arena.
+void launchCohort(ix_server* S, ServerShard* H, std::vector<ServerRequest*>& members, size_t reserved) {
     std::stable_sort(members.begin(), members.end(),
                      [](const ServerRequest* a, const ServerRequest* b) { return a->steps < b->steps; });
     ServerUnit* u = new ServerUnit();
     u->members = members;
+    u->reserved = reserved;
     ix_batch* b = new ix_batch();
     b->device = S->device;
+    b->numSMs = S->numSMs;
     b->arena = &S->arena;
     b->particleStart.push_back(0);
     u->batch = b;
-    size_t before;
-    {
-        std::lock_guard<std::mutex> lock(S->arena.m);
-        before = S->arena.inUse;
-    }
     int rc = IX_OK;
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, S->device) == cudaSuccess) b->numSMs = prop.multiProcessorCount;
-    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+    if (!H->cohortStreams.empty()) {
+        b->stream = H->cohortStreams.back();
+        H->cohortStreams.pop_back();
+    }
+    else if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
         rc = batchFail(b, IX_ERR_CUDA, "cudaStreamCreate failed");
     for (ServerRequest* r : members) {
         b->systems.push_back(r->sys);   // the batch owns the descriptions from here on
         b->particleStart.push_back(b->particleStart.back() + r->sys->n);
         r->sys = nullptr;
     }
-    if (rc == IX_OK) rc = buildBatch(b);
-    if (rc == IX_OK) {
-        const size_t np = (size_t)b->numParticles;
-        u->staging = S->pinned.alloc((9 * np + 4 * members.size()) * sizeof(double));
-        if (!u->staging) rc = batchFail(b, IX_ERR_MEMORY, "pinned host staging could not be allocated");
-    }
-    if (rc == IX_OK) rc = enqueueCohortRun(S, u);
     {
-        std::lock_guard<std::mutex> lock(S->arena.m);
-        u->reserved = S->arena.inUse - before;
+        PhaseTimer t(H->workerSec[2]);
+        if (rc == IX_OK) rc = buildBatch(b);
+        if (rc == IX_OK) {
+            const size_t np = (size_t)b->numParticles;
+            u->staging = S->pinned.alloc((9 * np + 4 * members.size()) * sizeof(double));
+            if (!u->staging) rc = batchFail(b, IX_ERR_MEMORY, "pinned host staging could not be allocated");
+        }
+    }
+    if (rc == IX_OK) {
+        PhaseTimer t(H->workerSec[3]);
+        rc = enqueueCohortRun(H, u);
     }
     if (rc != IX_OK) {
         const std::string msg = b->error;
         if (b->stream) cudaStreamSynchronize(b->stream);
-        for (auto& mk : u->marks) S->freeEvents.push_back(mk.event);
+        for (auto& mk : u->marks) H->freeEvents.push_back(mk.event);
         if (u->staging) S->pinned.release(u->staging);
         ix_batch_destroy(b);
-        for (ServerRequest* r : members) serverFinish(S, r, rc, msg);
+        unreserveBytes(S, u->reserved);
+        for (ServerRequest* r : members) serverFinish(S, H, r, rc, msg);
         delete u;
         return;
     }
-    S->reserved += u->reserved;
-    S->units.push_back(u);
+    const size_t actual = bufferBytes(b->buffers);
+    if (actual > u->reserved) {
+        S->reserved += (long long)(actual - u->reserved);
+        u->reserved = actual;
+    }
+    H->units.push_back(u);
     std::lock_guard<std::mutex> lock(S->m);
     S->stats.cohorts++;
     S->stats.admitted += (long long)members.size();
 }
 
-// Unpack the members of a finished mark from the unit's pinned staging.
-void unpackMark(ix_server* S, ServerUnit* u, const ServerUnit::Mark& mk) {
+// Unpack the members of a finished mark of a cohort from the unit's pinned staging.
+void unpackCohortMark(ix_server* S, ServerShard* H, ServerUnit* u, const ServerUnit::Mark& mk) {
     const double* st = reinterpret_cast<const double*>(u->staging);
-    if (u->ctx) {
-        ServerRequest* r = u->members[0];
-        const size_t n3 = 3 * (size_t)u->ctx->n;
-        r->pos.assign(st, st + n3);
-        r->vel.assign(st + n3, st + 2 * n3);
-        r->forces.assign(st + 2 * n3, st + 3 * n3);
-        std::memcpy(r->energies, st + 3 * n3, sizeof(r->energies));
-        return;
-    }
     const ix_batch* b = u->batch;
     const size_t n3 = 3 * (size_t)b->numParticles;
     for (int k = mk.first; k < mk.last; k++) {
@@ -387,26 +500,37 @@ void unpackMark(ix_server* S, ServerUnit* u, const ServerUnit::Mark& mk) {
         r->vel.assign(st + n3 + a, st + n3 + e);
         r->forces.assign(st + 2 * n3 + a, st + 2 * n3 + e);
         std::memcpy(r->energies, st + 3 * n3 + 4 * (size_t)k, sizeof(r->energies));
-        serverFinish(S, r, IX_OK, "");
+        serverFinish(S, H, r, IX_OK, "");
     }
 }
 
-void releaseUnit(ix_server* S, ServerUnit* u) {
-    for (auto& mk : u->marks) S->freeEvents.push_back(mk.event);
+// Release a unit whose requests are all finished (or failed).
+void releaseUnit(ix_server* S, ServerShard* H, ServerUnit* u) {
+    for (auto& mk : u->marks) H->freeEvents.push_back(mk.event);
     u->marks.clear();
     if (u->staging) S->pinned.release(u->staging);
     u->staging = nullptr;
-    if (u->batch) ix_batch_destroy(u->batch);   // frees the cohort's memory and descriptions
-    u->batch = nullptr;
-    S->reserved -= u->reserved;
+    if (u->ctx) {
+        u->members[0]->sys = nullptr;
+        retireContext(S, H, u->ctx);
+        u->ctx = nullptr;
+    }
+    if (u->batch) {
+        cudaStreamSynchronize(u->batch->stream);
+        H->cohortStreams.push_back(u->batch->stream);   // the stream goes back to the pool
+        u->batch->stream = nullptr;
+        ix_batch_destroy(u->batch);   // frees the cohort's memory and descriptions
+        u->batch = nullptr;
+    }
+    unreserveBytes(S, u->reserved);
 }
 
-// Check the units' events; finish the requests whose results have arrived.  Returns whether anything finished.
-bool collect(ix_server* S) {
+// Check the shard's events; finish the requests whose results have arrived.  Returns whether anything finished.
+bool collect(ix_server* S, ServerShard* H) {
     bool progress = false;
-    for (size_t i = 0; i < S->units.size();) {
-        ServerUnit* u = S->units[i];
-        bool failed = false;
+    for (size_t i = 0; i < H->units.size();) {
+        ServerUnit* u = H->units[i];
+        int failCode = IX_OK;
         std::string msg;
         while (u->next < u->marks.size()) {
             const ServerUnit::Mark& mk = u->marks[u->next];
@@ -414,180 +538,189 @@ bool collect(ix_server* S) {
             if (q == cudaErrorNotReady) break;
             progress = true;
             if (q != cudaSuccess) {
-                failed = true;
+                failCode = IX_ERR_CUDA;
                 msg = std::string("CUDA error while running the request: ") + cudaGetErrorString(q);
                 break;
             }
             if (u->ctx) {
                 // an overflow of a neighbor list during the steps: grow the lists and run the request again
+                const double* st = reinterpret_cast<const double*>(u->staging);
+                const size_t n3 = 3 * (size_t)u->ctx->n;
                 int flags[8];
-                std::memcpy(flags, reinterpret_cast<const double*>(u->staging) + 9 * (size_t)u->ctx->n + 4,
-                            sizeof(flags));
+                std::memcpy(flags, st + 3 * n3 + 4, sizeof(flags));
                 if (flags[1] || flags[5]) {
                     bool redo = false;
                     int rc = checkOverflow(u->ctx, selectedTerms(u->ctx, -1), redo);
                     if (rc == IX_OK && ++u->restarts <= 3) {
-                        S->freeEvents.push_back(mk.event);
+                        H->freeEvents.push_back(mk.event);
                         u->marks.clear();
-                        rc = enqueueContextRun(S, u);
+                        u->ctx->uploadUsed = 0;   // the stream has run every earlier upload
+                        rc = enqueueContextRun(H, u);
                         if (rc == IX_OK) continue;
                     }
-                    failed = true;
+                    failCode = rc != IX_OK ? rc : IX_ERR_STATE;
                     msg = rc != IX_OK ? u->ctx->error : "neighbor lists kept overflowing";
                     break;
                 }
+                ServerRequest* r = u->members[0];
+                r->pos.assign(st, st + n3);
+                r->vel.assign(st + n3, st + 2 * n3);
+                r->forces.assign(st + 2 * n3, st + 3 * n3);
+                std::memcpy(r->energies, st + 3 * n3, sizeof(r->energies));
             }
-            unpackMark(S, u, mk);
+            else unpackCohortMark(S, H, u, u->marks[u->next]);
             u->next++;
         }
-        if (failed) {
-            if (u->ctx) {
-                ServerRequest* r = u->members[0];
-                cudaStreamSynchronize(u->ctx->stream);
-                r->sys = nullptr;
-                releaseUnit(S, u);
-                ix_ctx_destroy(u->ctx);
-                u->ctx = nullptr;
-                serverFinish(S, r, IX_ERR_CUDA, msg);
-            }
-            else {
-                cudaStreamSynchronize(u->batch->stream);
+        const bool finished = failCode != IX_OK || u->next >= u->marks.size();
+        if (!finished) {
+            i++;
+            continue;
+        }
+        {
+            PhaseTimer t(H->workerSec[4]);
+            // the requests not yet finished: a context's one request, or the cohort members from the current mark
+            std::vector<ServerRequest*> rest;
+            if (u->ctx) rest.push_back(u->members[0]);
+            else if (failCode != IX_OK)
                 for (size_t m = (size_t)u->marks[u->next].first; m < u->members.size(); m++)
-                    serverFinish(S, u->members[m], IX_ERR_CUDA, msg);
-                releaseUnit(S, u);
-            }
-            delete u;
-            S->units[i] = S->units.back();
-            S->units.pop_back();
-            continue;
+                    rest.push_back(u->members[m]);
+            releaseUnit(S, H, u);
+            for (ServerRequest* r : rest) serverFinish(S, H, r, failCode, msg);
         }
-        if (u->next >= u->marks.size()) {
-            if (u->ctx) {
-                ServerRequest* r = u->members[0];
-                r->sys = nullptr;
-                releaseUnit(S, u);
-                ix_ctx_destroy(u->ctx);   // frees the context's memory in the arena
-                u->ctx = nullptr;
-                serverFinish(S, r, IX_OK, "");
-            }
-            else releaseUnit(S, u);
-            delete u;
-            S->units[i] = S->units.back();
-            S->units.pop_back();
-            continue;
-        }
-        i++;
+        delete u;
+        H->units[i] = H->units.back();
+        H->units.pop_back();
     }
     return progress;
 }
 
-// Admit pending requests while the running count and the budget allow.  Small requests gather into one cohort per
-// pass, which starts when it is full, when its oldest request has waited the batching window, or when the GPU has
-// nothing else to do; otherwise its requests go back to the queue to wait for more.  A request older than a quarter
-// second that does not fit stops the requests behind it from passing it.  Returns whether anything was launched.
-bool admit(ix_server* S) {
+// Admit the shard's pending requests while its running count and the budget allow.  Small requests gather into one
+// cohort per pass, which starts when it is full, when its oldest request has waited the batching window, or when the
+// shard has nothing else on the GPU; otherwise its requests go back to the queue to wait for more.  A request older
+// than a quarter second that does not fit stops the requests behind it from passing it.  Returns whether anything
+// was launched.
+bool admit(ix_server* S, ServerShard* H) {
     const double now = serverNow();
-    const double budget = S->budget;
     std::vector<ServerRequest*> cohort;
     size_t cohortBytes = 0;
     bool launched = false;
     int scanned = 0;
-    for (auto it = S->pending.begin(); it != S->pending.end() && scanned < 4096; scanned++) {
+    for (auto it = H->pending.begin(); it != H->pending.end() && scanned < 4096; scanned++) {
         ServerRequest* r = *it;
-        if (S->running >= S->maxRunning) break;
-        if ((double)r->estimate > budget) {
-            it = S->pending.erase(it);
-            S->running++;
+        if (H->running >= S->maxRunning) break;
+        if ((double)r->estimate > S->budget) {
+            it = H->pending.erase(it);
+            H->running++;
             char buf[160];
             snprintf(buf, sizeof(buf), "the request needs about %zu bytes of device memory; the budget is %.0f",
-                     r->estimate, budget);
-            serverFinish(S, r, IX_ERR_MEMORY, buf);
+                     r->estimate, S->budget);
+            serverFinish(S, H, r, IX_ERR_MEMORY, buf);
             continue;
         }
-        const bool fits = (double)(S->reserved + cohortBytes + r->estimate) <= budget;
+        bool taken = false;
         if (r->small) {
             const bool joins = cohort.empty() || ((int)cohort.size() < S->maxCohort && cohortCompatible(r, cohort[0]));
-            if (joins && fits) {
+            if (joins && reserveBytes(S, r->estimate)) {
                 cohort.push_back(r);
                 cohortBytes += r->estimate;
-                S->running++;
-                it = S->pending.erase(it);
+                taken = true;
+            }
+            else if (!joins) {
+                ++it;
                 continue;
             }
         }
-        else if (fits) {
-            it = S->pending.erase(it);
-            S->running++;
-            launchContext(S, r);
+        else if (reserveBytes(S, r->estimate)) {
+            it = H->pending.erase(it);
+            H->running++;
+            launchContext(S, H, r);
             launched = true;
             continue;
         }
-        if (!fits && now - r->tSubmit > 0.25) break;   // no passing a request that has waited long
+        if (taken) {
+            H->running++;
+            it = H->pending.erase(it);
+            continue;
+        }
+        if (now - r->tSubmit > 0.25) break;   // it does not fit: no passing a request that has waited long
         ++it;
     }
     if (!cohort.empty()) {
         const bool full = (int)cohort.size() >= S->maxCohort;
         const bool waited = now - cohort[0]->tSubmit >= S->window;
-        if (full || waited || S->units.empty()) {
-            launchCohort(S, cohort);
+        if (full || waited || H->units.empty()) {
+            launchCohort(S, H, cohort, cohortBytes);
             launched = true;
         }
         else {
-            for (auto r = cohort.rbegin(); r != cohort.rend(); ++r) S->pending.push_front(*r);
-            S->running -= (long long)cohort.size();
+            unreserveBytes(S, cohortBytes);
+            for (auto r = cohort.rbegin(); r != cohort.rend(); ++r) H->pending.push_front(*r);
+            H->running -= (long long)cohort.size();
         }
     }
     return launched;
 }
 
-void serverLoop(ix_server* S) {
+void shardLoop(ix_server* S, ServerShard* H) {
     cudaSetDevice(S->device);
     for (;;) {
         {
             std::unique_lock<std::mutex> lock(S->m);
-            if (S->units.empty() && S->pending.empty())
-                S->cvSubmit.wait(lock, [&] { return S->stop || !S->incoming.empty(); });
+            if (H->units.empty() && H->pending.empty())
+                S->cvSubmit.wait(lock, [&] { return S->stop || !H->incoming.empty(); });
             if (S->stop) break;
-            while (!S->incoming.empty()) {
-                S->pending.push_back(S->incoming.front());
-                S->incoming.pop_front();
+            while (!H->incoming.empty()) {
+                H->pending.push_back(H->incoming.front());
+                H->incoming.pop_front();
             }
         }
-        const bool progress = admit(S) | collect(S);
-        {
-            std::lock_guard<std::mutex> lock(S->m);
-            S->stats.pending = (long long)S->pending.size() + (long long)S->incoming.size();
-            S->stats.running = S->running;
-            S->stats.reserved_bytes = (double)S->reserved;
-            S->stats.peak_reserved_bytes = std::max(S->stats.peak_reserved_bytes, (double)S->reserved);
-        }
-        if (!progress) {
+        const double l0 = H->workerSec[0] + H->workerSec[1] + H->workerSec[2] + H->workerSec[3];
+        const double c0 = H->workerSec[4];
+        const double t0 = serverNow();
+        const bool admitted = admit(S, H);
+        const double t1 = serverNow();
+        const bool collected = collect(S, H);
+        const double t2 = serverNow();
+        H->workerSec[6] += (t1 - t0) - (H->workerSec[0] + H->workerSec[1] + H->workerSec[2] + H->workerSec[3] - l0);
+        H->workerSec[5] += (t2 - t1) - (H->workerSec[4] - c0);
+        if (!admitted && !collected) {
+            PhaseTimer t(H->workerSec[7]);
             std::unique_lock<std::mutex> lock(S->m);
-            S->cvSubmit.wait_for(lock, std::chrono::microseconds(20), [&] { return S->stop || !S->incoming.empty(); });
+            S->cvSubmit.wait_for(lock, std::chrono::microseconds(20), [&] { return S->stop || !H->incoming.empty(); });
         }
     }
     // shutdown: wait for the units in flight, release them, fail what never ran
-    for (ServerUnit* u : S->units) {
+    for (ServerUnit* u : H->units) {
+        std::vector<ServerRequest*> rest;
         if (u->ctx) {
             cudaStreamSynchronize(u->ctx->stream);
-            u->members[0]->sys = nullptr;
-            releaseUnit(S, u);
-            ix_ctx_destroy(u->ctx);
-            u->ctx = nullptr;
-            serverFinish(S, u->members[0], IX_ERR_STATE, "the server was destroyed");
+            rest.push_back(u->members[0]);
         }
         else {
             cudaStreamSynchronize(u->batch->stream);
             for (size_t m = u->next < u->marks.size() ? (size_t)u->marks[u->next].first : u->members.size();
                  m < u->members.size(); m++)
-                serverFinish(S, u->members[m], IX_ERR_STATE, "the server was destroyed");
-            releaseUnit(S, u);
+                rest.push_back(u->members[m]);
         }
+        releaseUnit(S, H, u);
+        for (ServerRequest* r : rest) serverFinish(S, H, r, IX_ERR_STATE, "the server was destroyed");
         delete u;
     }
-    S->units.clear();
-    for (ServerRequest* r : S->pending) serverFinish(S, r, IX_ERR_STATE, "the server was destroyed");
-    S->pending.clear();
+    H->units.clear();
+    for (ServerRequest* r : H->pending) serverFinish(S, nullptr, r, IX_ERR_STATE, "the server was destroyed");
+    H->pending.clear();
+    for (const StreamSet& set : H->streams) {
+        cudaStreamDestroy(set.stream);
+        cudaStreamDestroy(set.stream2);
+        cudaStreamDestroy(set.body);
+        cudaEventDestroy(set.fork);
+        cudaEventDestroy(set.join);
+    }
+    H->streams.clear();
+    for (cudaStream_t st : H->cohortStreams) cudaStreamDestroy(st);
+    H->cohortStreams.clear();
+    for (cudaEvent_t e : H->freeEvents) cudaEventDestroy(e);
+    H->freeEvents.clear();
 }
 
 int serverFail(ix_server* S, int code, const char* fmt, ...) {
@@ -642,30 +775,67 @@ int ix_request_set_state(ix_ctx* request, const double* positions, const double*
     return IX_OK;
 }
 
-int ix_server_create(int device, double budget_bytes, int max_running, ix_server** out) {
+int ix_server_create(int device, double budget_bytes, int max_running, int threads, ix_server** out) {
     if (!out) return serverFail(nullptr, IX_ERR_INVALID, "ix_server_create: out is NULL");
     *out = nullptr;
     if (!(budget_bytes > 0)) return serverFail(nullptr, IX_ERR_INVALID, "ix_server_create: the budget must be positive");
     if (max_running <= 0) return serverFail(nullptr, IX_ERR_INVALID, "ix_server_create: max_running must be positive");
+    if (threads <= 0 || threads > 64)
+        return serverFail(nullptr, IX_ERR_INVALID, "ix_server_create: threads must be in 1..64");
     int count = 0;
     cudaError_t e = cudaGetDeviceCount(&count);
     if (e != cudaSuccess || count == 0)
         return serverFail(nullptr, IX_ERR_NO_DEVICE, "no CUDA device available (%s)", cudaGetErrorString(e));
     if (device < 0 || device >= count)
         return serverFail(nullptr, IX_ERR_NO_DEVICE, "CUDA device %d does not exist (%d devices)", device, count);
-    cudaDeviceProp prop;
-    cudaGetDeviceProperties(&prop, device);
-    if (prop.major < 10)
-        return serverFail(nullptr, IX_ERR_NO_DEVICE, "device %d (%s, sm_%d%d) is not a Blackwell (sm_100) GPU", device,
-                          prop.name, prop.major, prop.minor);
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device);
+    if (major < 10)
+        return serverFail(nullptr, IX_ERR_NO_DEVICE, "device %d (sm_%d) is not a Blackwell (sm_100) GPU", device, major);
     ix_server* S = new ix_server();
     S->device = device;
+    cudaDeviceGetAttribute(&S->numSMs, cudaDevAttrMultiProcessorCount, device);
     S->budget = budget_bytes;
-    S->maxRunning = max_running;
+    S->maxRunning = std::max(1, max_running / threads);
+    // the arena's first chunk (up to 4 GB) and the pinned staging are allocated now, before anything runs: growing
+    // either while the GPU is busy waits for the device
     S->arena.limit = (size_t)budget_bytes;
-    S->arena.chunkBytes = std::min<size_t>(S->arena.chunkBytes, std::max<size_t>((size_t)budget_bytes / 4, 1 << 20));
+    S->arena.chunkBytes = std::min<size_t>(size_t(1) << 30, std::max<size_t>((size_t)budget_bytes / 4, 1 << 20));
+    cudaSetDevice(device);
+    S->arena.grow(std::min<size_t>((size_t)budget_bytes, size_t(4) << 30));
     S->stats.budget_bytes = budget_bytes;
-    S->worker = std::thread(serverLoop, S);
+    S->pinned.chunkBytes = size_t(1) << 30;
+    S->pinned.release(S->pinned.alloc(1));
+    S->reaper = std::thread(reaperLoop, S);
+    // streams and events for every request a shard can run at once, created now: creating them while the GPU is
+    // busy waits for it
+    for (int k = 0; k < threads; k++) {
+        S->shards.emplace_back(new ServerShard());
+        ServerShard* H = S->shards.back().get();
+        H->index = k;
+        cudaSetDevice(device);
+        for (int i = 0; i < S->maxRunning; i++) {
+            StreamSet set;
+            if (cudaStreamCreateWithFlags(&set.stream, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaStreamCreateWithFlags(&set.stream2, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaStreamCreateWithFlags(&set.body, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&set.fork, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&set.join, cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                break;
+            }
+            H->streams.push_back(set);
+        }
+        for (int i = 0; i < 2 * S->maxRunning; i++) {
+            cudaEvent_t e = nullptr;
+            if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) {
+                cudaGetLastError();
+                break;
+            }
+            H->freeEvents.push_back(e);
+        }
+    }
+    for (auto& H : S->shards) H->worker = std::thread(shardLoop, S, H.get());
     *out = S;
     return IX_OK;
 }
@@ -688,14 +858,21 @@ void ix_server_destroy(ix_server* S) {
         S->stop = true;
     }
     S->cvSubmit.notify_all();
-    if (S->worker.joinable()) S->worker.join();
-    cudaSetDevice(S->device);
-    for (ServerRequest* r : S->incoming) {
-        if (r->sys) ix_ctx_destroy(r->sys);
-        delete r;
+    for (auto& H : S->shards)
+        if (H->worker.joinable()) H->worker.join();
+    {
+        std::lock_guard<std::mutex> lock(S->graveM);
+        S->graveStop = true;
     }
+    S->graveCv.notify_all();
+    if (S->reaper.joinable()) S->reaper.join();
+    cudaSetDevice(S->device);
+    for (auto& H : S->shards)
+        for (ServerRequest* r : H->incoming) {
+            if (r->sys) ix_ctx_destroy(r->sys);
+            delete r;
+        }
     for (auto& kv : S->done) delete kv.second;
-    for (cudaEvent_t e : S->freeEvents) cudaEventDestroy(e);
     delete S;
 }
 
@@ -726,11 +903,13 @@ int ix_server_submit(ix_server* S, ix_ctx* request, int steps, double dt, long l
         r->small = batchable(request) && request->n <= S->smallAtoms;
         r->estimate = estimateRequestBytes(request, r->small);
         r->id = S->nextId++;
-        S->incoming.push_back(r);
+        // small requests gather on shard 0 (larger cohorts); the others go round the shards
+        ServerShard* H = r->small ? S->shards[0].get() : S->shards[S->nextShard++ % S->shards.size()].get();
+        H->incoming.push_back(r);
         S->stats.submitted++;
         if (id) *id = r->id;
     }
-    S->cvSubmit.notify_one();
+    S->cvSubmit.notify_all();
     return IX_OK;
 }
 
@@ -789,6 +968,16 @@ int ix_server_stats_get(ix_server* S, ix_server_stats* stats) {
     if (!S || !stats) return IX_ERR_INVALID;
     std::lock_guard<std::mutex> lock(S->m);
     *stats = S->stats;
+    stats->pending = 0;
+    stats->running = 0;
+    for (int k = 0; k < 12; k++) stats->worker_seconds[k] = 0;
+    for (auto& H : S->shards) {
+        stats->pending += (long long)(H->incoming.size() + H->pending.size());
+        stats->running += H->running;
+        for (int k = 0; k < 12; k++) stats->worker_seconds[k] += H->workerSec[k];
+    }
+    stats->reserved_bytes = (double)S->reserved.load();
+    stats->peak_reserved_bytes = (double)S->peakReserved.load();
     {
         std::lock_guard<std::mutex> alock(S->arena.m);
         stats->arena_bytes = (double)S->arena.inUse;

@@ -23,7 +23,7 @@ class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_longlong) for k in ("submitted", "admitted", "completed", "failed", "contexts", "cohorts",
                                                   "pending", "running")] + \
                [(k, ctypes.c_double) for k in ("budget_bytes", "reserved_bytes", "peak_reserved_bytes", "arena_bytes",
-                                               "peak_arena_bytes")]
+                                               "peak_arena_bytes")] + [("worker_seconds", ctypes.c_double * 12)]
 
 
 _lib = None
@@ -98,7 +98,8 @@ def lib():
             "ix_batch_md_run": (ctypes.c_int, [P, P, ctypes.c_double, P, P, P, P, P]),
             "ix_request_create": (ctypes.c_int, [ctypes.c_int, P, ctypes.POINTER(P)]),
             "ix_request_set_state": (ctypes.c_int, [P, P, P, P]),
-            "ix_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(P)]),
+            "ix_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                                ctypes.POINTER(P)]),
             "ix_server_set_batching": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_double]),
             "ix_server_destroy": (None, [P]),
             "ix_server_last_error": (ctypes.c_char_p, [P]),

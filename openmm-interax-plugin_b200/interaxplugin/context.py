@@ -70,11 +70,13 @@ def _pair_settings(force, n):
     return s, ex
 
 
-def describe_forces(lib, handle, system, check):
+def describe_forces(lib, handle, system, check, keep=None):
     """Describe a System's InteraxFF forces to a context or request handle with the ix_add_* functions (what the
     reference's kernels' initialize() receive, InteraxKernels.h:64-67, 99-102, 134-137, 169-172).  Returns
-    {term index: force} and the alchemical parameter names that have alchemical particles or sites."""
+    {term index: force} and the alchemical parameter names that have alchemical particles or sites.  `keep`, if
+    given, receives every array the calls point into (for callers that replay the calls later)."""
     n = system.getNumParticles()
+    keep = [] if keep is None else keep
     forces, names = {}, []
     for force in system._forces:
         t = _term_index(force)
@@ -84,6 +86,7 @@ def describe_forces(lib, handle, system, check):
             s, ex = _pair_settings(force, n)
             params = _capi.arr(force._params_array(), np.float64)
             alch = _capi.arr(force._alch_array(), np.uint8)
+            keep += [s, ex, params, alch]
             if t == 0:
                 rc = lib.ix_add_dispersion(handle, ctypes.byref(s), _capi.ptr(params), _capi.ptr(alch),
                                            force.getDampingScale(), int(force.getUseLongRangeCorrection()))
@@ -95,11 +98,13 @@ def describe_forces(lib, handle, system, check):
                                             force.getOverlapMethod())
         else:
             off, part, params, mol, alch = force._site_arrays()
+            arrays = [_capi.arr(off, np.int32), _capi.arr(part, np.int32), _capi.arr(params, np.float64),
+                      _capi.arr(mol, np.int32), _capi.arr(alch, np.uint8)]
+            keep += arrays
             rc = lib.ix_add_three_body(
-                handle, force.getNumSites(), _capi.ptr(_capi.arr(off, np.int32)), _capi.ptr(_capi.arr(part, np.int32)),
-                _capi.ptr(_capi.arr(params, np.float64)), _capi.ptr(_capi.arr(mol, np.int32)),
-                _capi.ptr(_capi.arr(alch, np.uint8)), force.getCutoffDistance(), force.getScaleFactor(),
-                force.getDampingMethod(), force.getDampingScale(), force.getCentroidDampingRadius(),
+                handle, force.getNumSites(), *[_capi.ptr(a) for a in arrays], force.getCutoffDistance(),
+                force.getScaleFactor(), force.getDampingMethod(), force.getDampingScale(),
+                force.getCentroidDampingRadius(),
                 int(force.usesPeriodicBoundaryConditions()), force.getAlchemicalParameterName().encode(),
                 force.getForceGroup())
         check(rc)

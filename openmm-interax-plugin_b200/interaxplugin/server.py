@@ -28,28 +28,54 @@ class Result:
 
 class Server:
     def __init__(self, device=0, budget_bytes=120e9, max_running=256, small_atoms=1024, max_cohort=512,
-                 window_seconds=200e-6):
+                 window_seconds=200e-6, threads=1):
         self._lib = _capi.lib()
         self._srv = ctypes.c_void_p()
-        rc = self._lib.ix_server_create(int(device), float(budget_bytes), int(max_running), ctypes.byref(self._srv))
+        rc = self._lib.ix_server_create(int(device), float(budget_bytes), int(max_running), int(threads),
+                                        ctypes.byref(self._srv))
         if rc != _capi.IX_OK:
             self._srv = ctypes.c_void_p()
             raise OpenMMException(self._lib.ix_server_last_error(None).decode())
         self._check(self._lib.ix_server_set_batching(self._srv, int(small_atoms), int(max_cohort),
                                                      float(window_seconds)))
         self._sizes = {}
+        self._templates = {}
 
     def _check(self, rc):
         if rc != _capi.IX_OK:
             raise OpenMMException(self._lib.ix_server_last_error(self._srv).decode())
 
+    class _Recorder:
+        """Stands in for the library while describe_forces runs once per System: records the ix_add_* calls so that
+        each request replays them without converting the System again."""
+
+        def __init__(self):
+            self.calls = []
+
+        def __getattr__(self, name):
+            def record(handle, *args):
+                self.calls.append((name, args))
+                return _capi.IX_OK
+            return record
+
+    def _template(self, system):
+        t = self._templates.get(id(system))
+        if t is None or t[0] is not system:
+            rec, keep = self._Recorder(), []
+            describe_forces(rec, None, system, lambda rc: None, keep)
+            n = system.getNumParticles()
+            box = _capi.arr(np.asarray(system.getDefaultPeriodicBoxVectors()).reshape(9), np.float64)
+            mass = _capi.arr([system.getParticleMass(i) for i in range(n)], np.float64)
+            t = (system, n, box, mass, rec.calls, keep)
+            self._templates[id(system)] = t
+        return t
+
     def submit(self, system, positions, velocities=None, steps=0, dt=0.001, parameters=None):
         """Queue `steps` velocity-Verlet steps of `dt` ps of `system` from the given state (0 steps: one energy+force
         evaluation).  Masses come from the System.  Returns the request id."""
         L = self._lib
-        n = system.getNumParticles()
+        _, n, box, mass, calls, _ = self._template(system)
         req = ctypes.c_void_p()
-        box = _capi.arr(np.asarray(system.getDefaultPeriodicBoxVectors()).reshape(9), np.float64)
         if L.ix_request_create(n, _capi.ptr(box), ctypes.byref(req)) != _capi.IX_OK:
             raise OpenMMException(L.ix_last_error(None).decode())
         owned = True
@@ -57,12 +83,12 @@ class Server:
             def check(rc):
                 if rc != _capi.IX_OK:
                     raise OpenMMException(L.ix_last_error(req).decode())
-            describe_forces(L, req, system, check)
+            for name, args in calls:
+                check(getattr(L, name)(req, *args))
             for k, v in (parameters or {}).items():
                 check(L.ix_set_parameter(req, k.encode(), float(v)))
             pos = _capi.arr(np.asarray(positions, dtype=np.float64).reshape(n, 3), np.float64)
             vel = None if velocities is None else _capi.arr(np.asarray(velocities).reshape(n, 3), np.float64)
-            mass = _capi.arr([system.getParticleMass(i) for i in range(n)], np.float64)
             check(L.ix_request_set_state(req, _capi.ptr(pos), _capi.ptr(vel), _capi.ptr(mass)))
             rid = ctypes.c_longlong()
             self._check(L.ix_server_submit(self._srv, req, int(steps), float(dt), ctypes.byref(rid)))
@@ -110,7 +136,12 @@ class Server:
     def stats(self):
         s = _capi.ServerStats()
         self._check(self._lib.ix_server_stats_get(self._srv, ctypes.byref(s)))
-        return {k: getattr(s, k) for k, _ in s._fields_}
+        out = {k: getattr(s, k) for k, _ in s._fields_}
+        out["worker_seconds"] = dict(zip(("context_setup", "context_enqueue", "cohort_build", "cohort_enqueue",
+                                          "teardown", "event_checks", "admission", "idle", "pinned_staging",
+                                          "device_setup", "state_uploads", "step_launches"),
+                                         list(s.worker_seconds)))
+        return out
 
     def close(self):
         if getattr(self, "_srv", None) and self._srv.value:

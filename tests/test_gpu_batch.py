@@ -34,6 +34,21 @@ def test_batch_matches_oracle_per_system():
     assert pairs > 0 and triples > 0
 
 
+def test_batch_long_site_lists():
+    """A 300-water cluster (site lists longer than one staging of the wide triple kernel) in a mix with small ones."""
+    systems = clusters(3, seed=4) + [W.water_cluster(300, seed=5)[:2]]
+    batch = BatchContext([s for s, _ in systems])
+    energies, forces = batch.compute([p for _, p in systems])
+    system, pos = systems[-1]
+    absE = []
+    e_ref, f_ref = pyoracle.evaluate(system, pos, abs_energy=absE)
+    e_err, f_err = errors(energies[-1].sum(), forces[-1], e_ref, f_ref, max(absE[0], abs(e_ref)))
+    assert e_err <= ENERGY_TOL and f_err <= FORCE_RMS_TOL, (e_err, f_err)
+    alone = BatchContext([system])
+    e1, f1 = alone.compute([pos])
+    assert np.array_equal(e1[0], energies[-1]) and np.array_equal(f1[0], forces[-1])
+
+
 def test_batch_alone_and_in_mix_identical():
     systems = clusters(16, seed=2)
     mix = BatchContext([s for s, _ in systems])

@@ -665,6 +665,16 @@ def test_water_24k_box():
     assert pairs == cnt[0] and triples == c3[0]
 
 
+def test_atm_lists_longer_than_staging():
+    """A 300-water cluster without cutoffs: every site has up to 299 later sites, more than one staging of the wide
+    triple kernel holds, so the (B, C) pairs are taken chunk by chunk."""
+    system, pos, _ = W.water_cluster(300, seed=3)
+    e, f, e_ref, f_ref, ctx = compare(system, pos, scale="abs")
+    cnt = []
+    pyoracle.three_body(system.getForce(3), pos, np.eye(3) * 10.0, counts=cnt)   # non-periodic: box unused
+    assert ctx.getCounts()[1] == cnt[0]
+
+
 def test_deterministic():
     """Fixed-point accumulation: two evaluations of the same input are bitwise identical."""
     cfg = W.CONFIGS["small"]
