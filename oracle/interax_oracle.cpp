@@ -365,6 +365,15 @@ static double computeC9(double a1, double w1, double a2, double w2, double a3, d
     return 1.5 * a1 * a2 * a3 * w1 * w2 * w3 * (w1 + w2 + w3) / ((w1 + w2) * (w2 + w3) * (w3 + w1));
 }
 
+double atmTriple(const Vec3& ab, const Vec3& ac, const Vec3& bc, double c9, const double* rates, Vec3& fA, Vec3& fB,
+                 Vec3& fC, double centroidRadius) {
+    return computeTripleT<double>(ab, ac, bc, c9, rates, fA, fB, fC, centroidRadius);
+}
+
+double atmC9(double a1, double w1, double a2, double w2, double a3, double w3) {
+    return computeC9(a1, w1, a2, w2, a3, w3);
+}
+
 // ReferenceInteraxThreeBodyIxn::calculateIxn (ReferenceInteraxThreeBodyIxn.cpp:84-135).  The reference builds an
 // N x N neighbor matrix and loops over i < j < k; here each site keeps the sorted list of its neighbors above it and
 // the triples are enumerated in the same i, j, k order, so the energies and forces are summed in the same order.
@@ -460,16 +469,6 @@ double computeThreeBody(const std::vector<Vec3>& pos, const Vec3* box, const Thr
 using namespace ixo;
 
 extern "C" {
-
-struct ox_pair_settings {
-    int method;
-    double cutoff;
-    int use_switch;
-    double switch_distance;
-    double softcore_radius;
-    int num_exclusions;
-    const int* exclusions;   // 2 x num_exclusions
-};
 
 static void toVectors(int n, const double* xyz, const double* box9, std::vector<Vec3>& pos, Vec3 box[3]) {
     pos.resize(n);

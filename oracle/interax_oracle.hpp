@@ -30,6 +30,12 @@ inline double vsqrt(double v) { return std::sqrt(v); }
 inline double vabs(double v) { return std::fabs(v); }
 inline double vpow(double a, double b) { return std::pow(a, b); }
 inline double vval(double v) { return v; }
+// single precision, for the restatement of the CPU platform (cpu_platform.cpp), which evaluates the pair terms in float
+inline float vexp(float v) { return std::exp(v); }
+inline float vsqrt(float v) { return std::sqrt(v); }
+inline float vabs(float v) { return std::fabs(v); }
+inline float vpow(float a, float b) { return std::pow(a, b); }
+inline double vval(float v) { return v; }
 
 // A double that counts the operations performed on it: +, -, *, / and negation as arithmetic, exp, sqrt and pow as
 // transcendental.  Used to fix the algorithmic work per pair and per triple.
@@ -376,4 +382,20 @@ struct ThreeBodySettings {
 double computeThreeBody(const std::vector<Vec3>& pos, const Vec3* box, const ThreeBodySettings& s, double lambda,
                         std::vector<Vec3>& forces, int64_t* numTriples = nullptr, OpCounter* ops = nullptr);
 
+// One triple in double precision (InteraxThreeBodyTerms.h:97-146): energy returned, forces added to fA, fB, fC.
+double atmTriple(const Vec3& ab, const Vec3& ac, const Vec3& bc, double c9, const double* rates, Vec3& fA, Vec3& fB,
+                 Vec3& fC, double centroidRadius);
+double atmC9(double a1, double w1, double a2, double w2, double a3, double w3);
+
 }  // namespace ixo
+
+// Settings of a pair force as the C interface takes them (ctypes).
+extern "C" struct ox_pair_settings {
+    int method;
+    double cutoff;
+    int use_switch;
+    double switch_distance;
+    double softcore_radius;
+    int num_exclusions;
+    const int* exclusions;   // 2 x num_exclusions
+};

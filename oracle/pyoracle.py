@@ -162,3 +162,88 @@ def taylor_table():
     d = np.zeros(63)
     lib().ox_overlap_taylor_table(_ptr(v), _ptr(d))
     return v.reshape(7, 9), d.reshape(7, 9)
+
+
+class CpuPlatform:
+    """The restatement of the reference's CPU platform (oracle/cpu_platform.cpp) for one System: the forces are set up
+    once, as the CPU kernels' initialize() does, and evaluate() runs them on `threads` host threads (all cores by
+    default): the pair forces in single precision, one pass each with its own neighbor list, the three-body force in
+    double precision.  Used as the timed CPU baseline; its results agree with the FP64 oracle to single precision."""
+
+    def __init__(self, system, threads=None):
+        L = lib()
+        if not getattr(L, "_cpu_ready", False):
+            P = ctypes.c_void_p
+            L.ox_cpu_threads.restype = ctypes.c_int
+            L.ox_cpu_pair_create.restype = P
+            L.ox_cpu_pair_create.argtypes = [ctypes.c_int, ctypes.c_int, P, P, P, ctypes.c_double, ctypes.c_int,
+                                             ctypes.c_int]
+            L.ox_cpu_pair_evaluate.restype = ctypes.c_double
+            L.ox_cpu_pair_evaluate.argtypes = [P, P, P, ctypes.c_double, ctypes.c_int, P, P]
+            L.ox_cpu_pair_destroy.argtypes = [P]
+            L.ox_cpu_three_body_create.restype = P
+            L.ox_cpu_three_body_create.argtypes = [ctypes.c_int, P, P, P, P, P, ctypes.c_double, ctypes.c_double,
+                                                   ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int]
+            L.ox_cpu_three_body_evaluate.restype = ctypes.c_double
+            L.ox_cpu_three_body_evaluate.argtypes = [P, P, P, ctypes.c_double, ctypes.c_int, P, P]
+            L.ox_cpu_three_body_destroy.argtypes = [P]
+            L._cpu_ready = True
+        self._lib = L
+        self.threads = int(threads) if threads else L.ox_cpu_threads()
+        self._system = system
+        self._handles = []
+        for force in system._forces:
+            term = term_of(force)
+            if term is None:
+                continue
+            if term < 3:
+                ex = _c(force._exclusion_array(), np.int32)
+                s = _PairSettings(force.getNonbondedMethod(), force.getCutoffDistance(),
+                                  int(force.getUseSwitchingFunction()), force.getSwitchingDistance(),
+                                  force.getSoftcoreRadius(), len(ex), _ptr(ex))
+                params = _c(force._params_array(), np.float64)
+                alch = _c(force._alch_array(), np.uint8)
+                h = L.ox_cpu_pair_create(term, system.getNumParticles(), ctypes.byref(s), _ptr(params), _ptr(alch),
+                                         force.getDampingScale() if term == 0 else 1.0,
+                                         int(force.getUseLongRangeCorrection()) if term == 0 else 0,
+                                         force.getOverlapMethod() if term != 0 else 0)
+            else:
+                off, part, params, mol, alch = force._site_arrays()
+                h = L.ox_cpu_three_body_create(
+                    force.getNumSites(), _ptr(_c(off, np.int32)), _ptr(_c(part, np.int32)),
+                    _ptr(_c(params, np.float64)), _ptr(_c(mol, np.int32)), _ptr(_c(alch, np.uint8)),
+                    force.getCutoffDistance(), force.getScaleFactor(), force.getDampingMethod(),
+                    force.getDampingScale(), force.getCentroidDampingRadius(),
+                    int(force.usesPeriodicBoundaryConditions()))
+            self._handles.append((force, term, h))
+
+    def evaluate(self, positions, box=None, parameters=None, counts=None):
+        """Total energy and forces (N x 3); `counts`, if a list, receives the interacting pairs of the dispersion
+        force and the interacting triples."""
+        L = self._lib
+        parameters = parameters or {}
+        if box is None:
+            box = self._system.getDefaultPeriodicBoxVectors()
+        pos = _c(positions, np.float64)
+        boxa = _c(np.asarray(box, dtype=np.float64).reshape(9), np.float64)
+        forces = np.zeros((len(pos), 3))
+        energy = 0.0
+        for force, term, h in self._handles:
+            lam = parameters.get(force.getAlchemicalParameterName(), 1.0)
+            cnt = ctypes.c_longlong()
+            if term < 3:
+                energy += L.ox_cpu_pair_evaluate(h, _ptr(pos), _ptr(boxa), lam, self.threads, _ptr(forces),
+                                                 ctypes.byref(cnt))
+            else:
+                energy += L.ox_cpu_three_body_evaluate(h, _ptr(pos), _ptr(boxa), lam, self.threads, _ptr(forces),
+                                                       ctypes.byref(cnt))
+            if counts is not None and term in (0, 3):
+                counts.append(cnt.value)
+        return energy, forces
+
+    def __del__(self):
+        for _, term, h in getattr(self, "_handles", []):
+            if term < 3:
+                self._lib.ox_cpu_pair_destroy(h)
+            else:
+                self._lib.ox_cpu_three_body_destroy(h)
