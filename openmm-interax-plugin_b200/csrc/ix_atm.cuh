@@ -35,6 +35,7 @@ struct AtmConfig {
     float twoBeta;               // 2 x damping scale
     float invCentroidRadius;     // 0 = no centroid damping
     float maxMove2;
+    int zeroSlots, zeroOffset;   // energy slots the fast kernel clears (those of a wide kernel that may not run)
 };
 
 struct AtmBuffers {
@@ -88,6 +89,7 @@ __global__ void kSiteCentroids(AtmBuffers A, AtmConfig C, const double* pos) {
         for (int d = 0; d < 3; d++) {
             c[d] /= n;
             A.sitePos[3 * s + d] = c[d];
+            A.siteForce[d * C.numSites + s] = 0;   // the triple kernels of this evaluation accumulate from zero
         }
         const double dx = c[0] - A.siteRef[3 * s], dy = c[1] - A.siteRef[3 * s + 1], dz = c[2] - A.siteRef[3 * s + 2];
         moved = (float)(dx * dx + dy * dy + dz * dz) > C.maxMove2;
@@ -290,6 +292,8 @@ struct AtmFastStorage {
 // 72 registers (7 blocks of 4 warps per SM)
 __global__ void __launch_bounds__(32 * kAtmFastWarps, 7) kTriplesFast(AtmBuffers A, AtmConfig C) {
     __shared__ AtmFastStorage storage[kAtmFastWarps];
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C.zeroSlots; k += gridDim.x * blockDim.x)
+        A.energyPartials[C.zeroOffset + k] = 0.0;
     AtmFastStorage& S = storage[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const int warp = blockIdx.x * kAtmFastWarps + (threadIdx.x >> 5);
@@ -405,7 +409,10 @@ constexpr int kAtmChunk = kAtmMaxStaged / 2;
 // chunks (I <= J) staged side by side, so any length is handled.  The forces on B and C accumulate in shared memory
 // and are flushed to the fixed-point site forces after each staging.  Energies go to energyPartials[partialsOffset +
 // warp].
-__global__ void __launch_bounds__(32 * kAtmWarps) kTriplesWide(AtmBuffers A, AtmConfig C, int partialsOffset) {
+// `gate` (may be null): the kernel returns at once unless *gate is set (a list longer than kAtmFast exists).
+__global__ void __launch_bounds__(32 * kAtmWarps) kTriplesWide(AtmBuffers A, AtmConfig C, int partialsOffset,
+                                                               const int* gate) {
+    if (gate && *(volatile const int*)gate == 0) return;
     extern __shared__ unsigned char atmShared[];
     AtmWarpStorage& S = reinterpret_cast<AtmWarpStorage*>(atmShared)[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;

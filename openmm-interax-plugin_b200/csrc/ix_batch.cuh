@@ -443,7 +443,7 @@ int enqueueBatch(ix_batch* b) {
         kTriplesFast<<<b->atmFastBlocks, 32 * kAtmFastWarps, 0, st>>>(A, C);
         if (b->atmWideBlocks > 0)
             kTriplesWide<<<b->atmWideBlocks, 32 * kAtmWarps, sizeof(AtmWarpStorage) * kAtmWarps, st>>>(
-                A, C, b->atmFastBlocks * kAtmFastWarps);
+                A, C, b->atmFastBlocks * kAtmFastWarps, nullptr);
         kSpreadSiteForces<<<gS, tpb, 0, st>>>(A, C);
     }
     kFinalize<<<(b->numParticles + tpb - 1) / tpb, tpb, 0, st>>>(b->numParticles, L.np, L.slotOf, b->P.forceFixed,

@@ -266,6 +266,8 @@ struct ix_ctx {
     float4* dP3 = nullptr;
     double* dPairPartials = nullptr;     // per-warp energies of the pair kernel (3 per warp)
     double* dAtmPartials = nullptr;      // per-warp energies of the triple kernel
+    int* dParticleSiteStart = nullptr;   // n + 1: the sites of each particle (CSR)
+    int* dParticleSites = nullptr;
     int atmFastBlocks = 0;               // grid of the fast triple kernel
     int atmGridBlocks = 0;               // grid of the wide triple kernel
     int* dFlagso = nullptr;
@@ -889,6 +891,20 @@ static int allocateAtm(ix_ctx* ctx) {
     IX_TRY(deviceAlloc(ctx, "siteRef", 3 * (size_t)ns, &A.siteRef));
     IX_TRY(deviceAlloc(ctx, "nbrCount", ns, &A.nbrCount));
     IX_TRY(deviceAlloc(ctx, "siteForce", 3 * (size_t)ns, &A.siteForce));
+    {
+        // the sites of each particle, so that the finishing kernel gives each particle its share of its sites' forces
+        std::vector<int> start(ctx->n + 1, 0), list(ctx->siteParticles.size());
+        for (int p : ctx->siteParticles) start[p + 1]++;
+        for (int i = 0; i < ctx->n; i++) start[i + 1] += start[i];
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (int sidx = 0; sidx < ns; sidx++)
+            for (int k = ctx->siteOffsets[sidx]; k < ctx->siteOffsets[sidx + 1]; k++)
+                list[fill[ctx->siteParticles[k]]++] = sidx;
+        IX_TRY(deviceAlloc(ctx, "particleSiteStart", (size_t)ctx->n + 1, &ctx->dParticleSiteStart));
+        IX_TRY(deviceAlloc(ctx, "particleSites", std::max<size_t>(list.size(), 1), &ctx->dParticleSites));
+        IX_TRY(stageCopy(ctx, ctx->dParticleSiteStart, start.data(), start.size() * sizeof(int)));
+        IX_TRY(stageCopy(ctx, ctx->dParticleSites, list.data(), list.size() * sizeof(int)));
+    }
     IX_TRY(deviceAlloc(ctx, "atmParticleForce", 3 * (size_t)ctx->n, &A.particleForce));
     // accumulators start at zero here; afterwards the kernels that read them clear them
     IX_CUDA(ctx, cudaMemsetAsync(A.siteForce, 0, 3 * (size_t)ns * sizeof(long long), ctx->stream));
@@ -978,28 +994,41 @@ __global__ void kFinalize(int n, int np, const int* slotOf, long long* pairForce
 // accumulators) and resets the pair kernel's tile counter for the next evaluation.
 constexpr int kReduceBlocks = 64;
 
-__global__ void kReduceEnergies(const double* pairPartials, const int* numPairPartials, int pairCap,
-                                const double* atmPartials, int numAtmWarps, double lrcEnergy, double* outEnergy,
-                                double* blockSums, unsigned* ticket, unsigned long long* counts, int* taskCounter) {
+struct EnergyReduction {
+    const double* pairPartials;          // null: no pair terms
+    const int* numPairPartials;
+    int pairCap;
+    const double* atmPartials;           // null: no three-body term
+    int numAtmWarps;
+    double lrcEnergy;
+    double* outEnergy;
+    double* blockSums;
+    unsigned* ticket;
+    unsigned long long* counts;
+    int* taskCounter;
+};
+
+// One block (of `numBlocks`) of the energy reduction; 256 threads.
+__device__ void reduceEnergiesBlock(const EnergyReduction& R, int block, int numBlocks) {
     __shared__ double red[4][256];
     __shared__ bool last;
     const int t = threadIdx.x;
     // each block sums a fixed contiguous share of each array; the last block to finish adds the block sums in order
-    auto share = [](int total, int& lo, int& hi) {
-        const int per = (total + gridDim.x - 1) / gridDim.x;
-        lo = min((int)blockIdx.x * per, total);
+    auto share = [&](int total, int& lo, int& hi) {
+        const int per = (total + numBlocks - 1) / numBlocks;
+        lo = min(block * per, total);
         hi = min(lo + per, total);
     };
     double s[4] = {0.0, 0.0, 0.0, 0.0};
     int lo, hi;
-    if (pairPartials) {
-        share(min(*numPairPartials, pairCap), lo, hi);
+    if (R.pairPartials) {
+        share(min(*R.numPairPartials, R.pairCap), lo, hi);
         for (int w = lo + t; w < hi; w += 256)
-            for (int k = 0; k < 3; k++) s[k] += pairPartials[3 * w + k];
+            for (int k = 0; k < 3; k++) s[k] += R.pairPartials[3 * w + k];
     }
-    if (atmPartials) {
-        share(numAtmWarps, lo, hi);
-        for (int w = lo + t; w < hi; w += 256) s[3] += atmPartials[w];
+    if (R.atmPartials) {
+        share(R.numAtmWarps, lo, hi);
+        for (int w = lo + t; w < hi; w += 256) s[3] += R.atmPartials[w];
     }
     for (int k = 0; k < 4; k++) red[k][t] = s[k];
     __syncthreads();
@@ -1009,28 +1038,129 @@ __global__ void kReduceEnergies(const double* pairPartials, const int* numPairPa
         __syncthreads();
     }
     if (t == 0) {
-        for (int k = 0; k < 4; k++) blockSums[4 * blockIdx.x + k] = red[k][0];
+        for (int k = 0; k < 4; k++) R.blockSums[4 * block + k] = red[k][0];
         __threadfence();
         // wraps to 0 on the last block, ready for the next launch
-        last = atomicInc(ticket, gridDim.x - 1) == gridDim.x - 1;
+        last = atomicInc(R.ticket, numBlocks - 1) == (unsigned)(numBlocks - 1);
     }
     __syncthreads();
     if (last && t < 4) {
         __threadfence();
         double v = 0.0;
-        for (int b = 0; b < (int)gridDim.x; b++) v += ((volatile double*)blockSums)[4 * b + t];
-        if (t == 0) v += lrcEnergy;
-        if (outEnergy) outEnergy[t] = v;
+        for (int b = 0; b < numBlocks; b++) v += ((volatile double*)R.blockSums)[4 * b + t];
+        if (t == 0) v += R.lrcEnergy;
+        if (R.outEnergy) R.outEnergy[t] = v;
         if (t == 0) {
-            if (counts) {
-                counts[2] = counts[0];
-                counts[3] = counts[1];
-                counts[0] = 0;
-                counts[1] = 0;
+            if (R.counts) {
+                R.counts[2] = R.counts[0];
+                R.counts[3] = R.counts[1];
+                R.counts[0] = 0;
+                R.counts[1] = 0;
             }
-            if (taskCounter) *taskCounter = 0;
+            if (R.taskCounter) *R.taskCounter = 0;
         }
     }
+}
+
+__global__ void kReduceEnergies(const double* pairPartials, const int* numPairPartials, int pairCap,
+                                const double* atmPartials, int numAtmWarps, double lrcEnergy, double* outEnergy,
+                                double* blockSums, unsigned* ticket, unsigned long long* counts, int* taskCounter) {
+    const EnergyReduction R{pairPartials, numPairPartials, pairCap, atmPartials, numAtmWarps, lrcEnergy,
+                            outEnergy,    blockSums,       ticket,  counts,      taskCounter};
+    reduceEnergiesBlock(R, blockIdx.x, gridDim.x);
+}
+
+struct FinishForces {
+    int n, np;
+    const int* slotOf;
+    long long* pairForce;                // null: no pair terms; cleared as read
+    const long long* siteForce;          // null: no three-body term (cleared by the next evaluation's centroid kernel)
+    int numSites;
+    const int* siteOffsets;
+    const int* particleSiteStart;
+    const int* particleSites;
+    double* outForces;
+    long long* addFixed;
+    int stride;
+    const double* invMass;               // null: no velocity half kick
+    double* vel;
+    double halfDt;
+    int blocks;                          // blocks of 256 particles; the grid's remaining blocks reduce the energies
+};
+
+// The end of an evaluation in one launch: each particle's force (its pair force and its share of the forces on its
+// three-body sites, in 64-bit fixed point, so the sum is the same in any order) to the outputs, and in an MD step
+// the second velocity half kick; the grid's last kReduceBlocks blocks reduce the term energies.
+__global__ void kFinish(FinishForces F, EnergyReduction R) {
+    if ((int)blockIdx.x >= F.blocks) {
+        reduceEnergiesBlock(R, (int)blockIdx.x - F.blocks, (int)gridDim.x - F.blocks);
+        return;
+    }
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= F.n) return;
+    long long f[3] = {0, 0, 0};
+    if (F.pairForce) {
+        const int s = F.slotOf[i];
+        for (int d = 0; d < 3; d++) {
+            f[d] = F.pairForce[d * F.np + s];
+            F.pairForce[d * F.np + s] = 0;
+        }
+    }
+    if (F.siteForce)
+        for (int k = F.particleSiteStart[i]; k < F.particleSiteStart[i + 1]; k++) {
+            const int site = F.particleSites[k];
+            const double inv = 1.0 / (double)(F.siteOffsets[site + 1] - F.siteOffsets[site]);
+            for (int d = 0; d < 3; d++) {
+                const long long v = F.siteForce[d * F.numSites + site];
+                if (v != 0) f[d] += __double2ll_rn((double)v * inv);
+            }
+        }
+    const double inv = 1.0 / kFixedScale;
+    const double fx = (double)f[0] * inv, fy = (double)f[1] * inv, fz = (double)f[2] * inv;
+    if (F.outForces) {
+        F.outForces[3 * i] = fx;
+        F.outForces[3 * i + 1] = fy;
+        F.outForces[3 * i + 2] = fz;
+    }
+    if (F.addFixed) {
+        atomicAddFixed(F.addFixed + i, f[0]);
+        atomicAddFixed(F.addFixed + F.stride + i, f[1]);
+        atomicAddFixed(F.addFixed + 2 * F.stride + i, f[2]);
+    }
+    if (F.invMass) {
+        const double h = F.halfDt * F.invMass[i];
+        F.vel[3 * i] += h * fx;
+        F.vel[3 * i + 1] += h * fy;
+        F.vel[3 * i + 2] += h * fz;
+    }
+}
+
+// The start of an MD step over the pair list's sorted slots, in one launch: the first velocity half kick and the
+// drift of each particle, the displacement check that requests a list rebuild, and the refresh of its sorted
+// position (the rebuild, when it runs, sorts and refreshes again).
+__global__ void kStepStart(ListBuffers L, double* pos, double dt, const double* invMass, const double* force,
+                           double* vel, float maxMove2) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    bool moved = false;
+    if (s < L.n) {
+        const int i = L.sortedAtom[s];
+        const double h = 0.5 * dt * invMass[i];
+        double x[3];
+        for (int d = 0; d < 3; d++) {
+            const double v = vel[3 * i + d] + h * force[3 * i + d];
+            vel[3 * i + d] = v;
+            x[d] = pos[3 * i + d] + dt * v;
+            pos[3 * i + d] = x[d];
+        }
+        const double dx = x[0] - L.refPos[3 * i], dy = x[1] - L.refPos[3 * i + 1], dz = x[2] - L.refPos[3 * i + 2];
+        moved = (float)(dx * dx + dy * dy + dz * dz) > maxMove2;
+        const double sx = x[0] - L.shift[3 * s], sy = x[1] - L.shift[3 * s + 1], sz = x[2] - L.shift[3 * s + 2];
+        L.spos[3 * s] = sx;
+        L.spos[3 * s + 1] = sy;
+        L.spos[3 * s + 2] = sz;
+        L.sposf[s] = make_float4((float)sx, (float)sy, (float)sz, 0.0f);
+    }
+    if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(L.flag, 1);
 }
 
 // Which terms of the context are selected by a force-group mask.
@@ -1152,8 +1282,17 @@ static int launchIfElse(ix_ctx* ctx, cudaStream_t st, const int* flag, Body body
 
 // Launch the whole evaluation on the context's stream.  Forces go to outForces (device, n x 3 doubles) and/or are
 // added to addFixed; energies to outEnergy (device, 4 doubles).
+// The second velocity half kick of an MD step, done by the evaluation's finishing kernel.
+struct StepKick {
+    const double* invMass;
+    double* vel;
+    double halfDt;
+};
+
+// `kick`: an MD step whose first kernel (kStepStart) has already moved the particles, checked their displacement and
+// refreshed the pair list's sorted positions; the evaluation ends with the second half kick.
 static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, double* outEnergy, long long* addFixed,
-                            int stride) {
+                            int stride, const StepKick* kick = nullptr) {
     const int n = ctx->n;
     cudaStream_t st = ctx->stream;
     const bool doPair = (terms & 7u) != 0;
@@ -1184,30 +1323,23 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         C.maxMove2 = 0.25f * kSiteSkin * kSiteSkin;
         const int tpb = 256;
         const int gS = (C.numSites + tpb - 1) / tpb;
+        // the wide kernel's energy slots start at zero (it runs only while some list is long)
+        C.zeroSlots = ctx->atmGridBlocks * kAtmWarps;
+        C.zeroOffset = ctx->atmFastBlocks * kAtmFastWarps;
         kSiteCentroids<<<gS, tpb, 0, sa>>>(A, C, ctx->dPos);
-        ctx->launches += 1;
-        // site list rebuild (the centroid kernel set the flag); the long-list flag is recomputed with the lists
-        IX_TRY(launchIf(ctx, sa, A.flag, [&](cudaStream_t s) {
-            kClearFlagIf<<<1, 1, 0, s>>>(A.flag + 2, A.flag);
-            kSiteNeighbors<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, s>>>(A, C);
-            kClearFlag<<<1, 1, 0, s>>>(A.flag);
-            ctx->launches += 3;
-            return IX_OK;
-        }));
+        // site list rebuild when the centroid kernel set the flag: these kernels return at once otherwise (three
+        // short launches cost less than a conditional graph node); the long-list flag is recomputed with the lists
+        kClearFlagIf<<<1, 1, 0, sa>>>(A.flag + 2, A.flag);
+        kSiteNeighbors<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, sa>>>(A, C);
+        kClearFlag<<<1, 1, 0, sa>>>(A.flag);
         recordTiming(ctx, 2, sa);
         kTriplesFast<<<ctx->atmFastBlocks, 32 * kAtmFastWarps, 0, sa>>>(A, C);
-        ctx->launches += 1;
-        // the sites whose lists are too long for the fast kernel, if there are any
-        IX_TRY(launchIf(ctx, sa, A.flag + 2, [&](cudaStream_t s) {
-            const size_t smem = sizeof(AtmWarpStorage) * kAtmWarps;
-            kTriplesWide<<<ctx->atmGridBlocks, 32 * kAtmWarps, smem, s>>>(A, C, ctx->atmFastBlocks * kAtmFastWarps);
-            ctx->launches += 1;
-            return IX_OK;
-        }));
+        // the sites whose lists are too long for the fast kernel: the kernel returns at once when there are none
+        kTriplesWide<<<ctx->atmGridBlocks, 32 * kAtmWarps, sizeof(AtmWarpStorage) * kAtmWarps, sa>>>(
+            A, C, ctx->atmFastBlocks * kAtmFastWarps, A.flag + 2);
+        ctx->launches += 6;
         recordTiming(ctx, 3, sa);
         ctx->evAtm = ctx->profiling;
-        kSpreadSiteForces<<<gS, tpb, 0, sa>>>(A, C);
-        ctx->launches += 1;
         IX_CUDA(ctx, cudaGetLastError());
     }
     double lrcEnergy = 0.0;
@@ -1216,8 +1348,11 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         const int tpb = 256;
         const int gN = (n + tpb - 1) / tpb, gNp = (L.np + tpb - 1) / tpb;
         const int gCells = (L.numCells + tpb - 1) / tpb;
-        kCheckDisplacement<<<gN, tpb, 0, st>>>(L, 0.25f * kPairSkin * kPairSkin);
-        ctx->launches += 1;
+        const bool stepStarted = kick != nullptr;
+        if (!stepStarted) {
+            kCheckDisplacement<<<gN, tpb, 0, st>>>(L, 0.25f * kPairSkin * kPairSkin);
+            ctx->launches += 1;
+        }
         // the current positions in the build frame, every step
         auto refresh = [&](cudaStream_t s) {
             kUpdateSortedPositions<<<gNp, tpb, 0, s>>>(L);
@@ -1250,7 +1385,8 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
             ctx->launches += ctx->G.periodic ? 14 : 15;
             return IX_OK;
         };
-        IX_TRY(launchIfElse(ctx, st, L.flag, rebuild, refresh));
+        if (stepStarted) IX_TRY(launchIf(ctx, st, L.flag, rebuild));
+        else IX_TRY(launchIfElse(ctx, st, L.flag, rebuild, refresh));
         PairTermConfig C = pairConfig(ctx, terms);
         // the lean instantiation when no selected term has a soft core, a switching function or the order-2 overlap
         bool lean = true;
@@ -1280,14 +1416,30 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         IX_CUDA(ctx, cudaEventRecord(ctx->evJoin, sa));
         IX_CUDA(ctx, cudaStreamWaitEvent(st, ctx->evJoin, 0));
     }
-    kFinalize<<<(n + 255) / 256, 256, 0, st>>>(n, ctx->L.np, ctx->L.slotOf, doPair ? ctx->P.forceFixed : nullptr,
-                                              doAtm ? ctx->A.particleForce : nullptr, outForces, addFixed, stride);
-    kReduceEnergies<<<kReduceBlocks, 256, 0, st>>>(doPair ? ctx->dPairPartials : nullptr, ctx->L.numTiles,
-                                                   ctx->L.tileCap, doAtm ? ctx->dAtmPartials : nullptr,
-                                                   (int)atmPartialCount(ctx), lrcEnergy, outEnergy,
-                                                   ctx->dEnergyBlocks, ctx->dReduceTicket, ctx->dCounts,
-                                                   doPair ? ctx->L.taskCounter : nullptr);
-    ctx->launches += 2;
+    FinishForces F{};
+    F.n = n;
+    F.np = ctx->L.np;
+    F.slotOf = ctx->L.slotOf;
+    F.pairForce = doPair ? ctx->P.forceFixed : nullptr;
+    F.siteForce = doAtm ? ctx->A.siteForce : nullptr;
+    F.numSites = (int)ctx->siteParams.size() / 3;
+    F.siteOffsets = ctx->A.siteOffsets;
+    F.particleSiteStart = ctx->dParticleSiteStart;
+    F.particleSites = ctx->dParticleSites;
+    F.outForces = outForces;
+    F.addFixed = addFixed;
+    F.stride = stride;
+    if (kick) {
+        F.invMass = kick->invMass;
+        F.vel = kick->vel;
+        F.halfDt = kick->halfDt;
+    }
+    F.blocks = (n + 255) / 256;
+    EnergyReduction R{doPair ? ctx->dPairPartials : nullptr, ctx->L.numTiles, ctx->L.tileCap,
+                      doAtm ? ctx->dAtmPartials : nullptr, (int)atmPartialCount(ctx), lrcEnergy, outEnergy,
+                      ctx->dEnergyBlocks, ctx->dReduceTicket, ctx->dCounts, doPair ? ctx->L.taskCounter : nullptr};
+    kFinish<<<F.blocks + kReduceBlocks, 256, 0, st>>>(F, R);
+    ctx->launches += 1;
     IX_CUDA(ctx, cudaGetLastError());
     return IX_OK;
 }
@@ -1879,11 +2031,24 @@ int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt) {
     key.out0 = ctx->dOutForces;
     key.out1 = ctx->dOutEnergy;
     key.dt = dt;
+    // one step: the first half kick and drift (fused with the list's displacement check and position refresh when
+    // there are pair terms), the evaluation at the new positions, whose finishing kernel applies the second half kick
     auto step = [&]() -> int {
-        kVerletFirstHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos);
-        if (terms) IX_TRY(launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0));
-        kVerletSecondHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel);
-        ctx->launches += 2;
+        if (!terms) {
+            kVerletFirstHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos);
+            kVerletSecondHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel);
+            ctx->launches += 2;
+            IX_CUDA(ctx, cudaGetLastError());
+            return IX_OK;
+        }
+        if (terms & 7u)
+            kStepStart<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ctx->L, ctx->dPos, dt, ctx->dInvMass, ctx->dOutForces,
+                                                                ctx->dVel, 0.25f * kPairSkin * kPairSkin);
+        else
+            kVerletFirstHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos);
+        ctx->launches += 1;
+        const StepKick kick{ctx->dInvMass, ctx->dVel, 0.5 * dt};
+        IX_TRY(launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0, &kick));
         IX_CUDA(ctx, cudaGetLastError());
         return IX_OK;
     };
@@ -2307,7 +2472,8 @@ int ix_three_body_noalloc(int num_particles, const double* d_positions, const do
         const int blocks = std::max(1, std::min((num_sites + kAtmWarps - 1) / kAtmWarps, kNoAllocBlocks));
         kTriplesFast<<<fastBlocks, 32 * kAtmFastWarps, 0, st>>>(A, C);
         kTriplesWide<<<blocks, 32 * kAtmWarps, sizeof(AtmWarpStorage) * kAtmWarps, st>>>(A, C,
-                                                                                        fastBlocks * kAtmFastWarps);
+                                                                                        fastBlocks * kAtmFastWarps,
+                                                                                        nullptr);
         kNoAllocSpread<<<(num_sites + tpb - 1) / tpb, tpb, 0, st>>>(S, num_particles, num_sites, d_site_offsets,
                                                                    d_site_particles);
         kReduceEnergies<<<1, 256, 0, st>>>(nullptr, nullptr, 0, S->energyPartials,
