@@ -210,6 +210,7 @@ struct ix_ctx {
     DeviceArena* arena = nullptr;        // the owning server's device memory (null: cudaMalloc)
     std::vector<double> requestPos, requestVel, requestMass;   // starting state of a server request description
     char* uploadBuf = nullptr;           // pinned host staging of a server's context (null: pageable copies)
+    unsigned char* hostStatus = nullptr; // pinned host copy of the status block (flags, energies, counts)
     size_t uploadCap = 0, uploadUsed = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;      // the three-body chain, forked from and joined back into `stream`
@@ -1457,10 +1458,17 @@ static int prepare(ix_ctx* ctx, unsigned terms) {
 }
 
 // After a synchronized evaluation: grow the lists that overflowed.  Returns true if the evaluation must be redone.
+static int checkOverflowFlags(ix_ctx* ctx, unsigned terms, const int* flags, bool& redo);
+
 static int checkOverflow(ix_ctx* ctx, unsigned terms, bool& redo) {
-    redo = false;
     int flags[6];
     IX_CUDA(ctx, cudaMemcpy(flags, ctx->dFlags, sizeof(flags), cudaMemcpyDeviceToHost));
+    return checkOverflowFlags(ctx, terms, flags, redo);
+}
+
+// The same from flags already copied to the host (6 ints from ctx->dFlags).
+static int checkOverflowFlags(ix_ctx* ctx, unsigned terms, const int* flags, bool& redo) {
+    redo = false;
     if ((terms & 7u) && flags[1]) {
         long long tiles = 0;
         int cnt = 0;
@@ -1547,6 +1555,40 @@ static void releaseGraph(LaunchGraph& g) {
 // C ABI
 // ---------------------------------------------------------------------------------------------------------------------
 
+// The status block of a context (device, and a pinned host copy): flags (8 ints), term energies (4 doubles), counts
+// (4 unsigned long long).
+constexpr size_t kStatusBytes = 96;
+
+// Pinned host slots of 128 bytes for the status copies, carved from shared pinned pages (one cudaHostAlloc per
+// 64 KB); the pages live until the process exits.
+struct PinnedSlots {
+    std::mutex m;
+    std::vector<unsigned char*> free;
+    unsigned char* take() {
+        std::lock_guard<std::mutex> lock(m);
+        if (free.empty()) {
+            unsigned char* page = nullptr;
+            if (cudaHostAlloc(reinterpret_cast<void**>(&page), size_t(64) << 10, cudaHostAllocDefault) != cudaSuccess) {
+                cudaGetLastError();
+                return nullptr;
+            }
+            for (size_t off = 0; off + 128 <= (size_t(64) << 10); off += 128) free.push_back(page + off);
+        }
+        unsigned char* p = free.back();
+        free.pop_back();
+        return p;
+    }
+    void give(unsigned char* p) {
+        std::lock_guard<std::mutex> lock(m);
+        free.push_back(p);
+    }
+};
+
+static PinnedSlots& pinnedSlots() {
+    static PinnedSlots* slots = new PinnedSlots();
+    return *slots;
+}
+
 // The device side of a context: streams, events and the buffers every evaluation uses (through ctx->arena when a
 // server owns the context).  A context described on the host only (a server request) gets it on admission.
 static int ctxInitDevice(ix_ctx* ctx) {
@@ -1561,10 +1603,13 @@ static int ctxInitDevice(ix_ctx* ctx) {
         return fail(ctx, IX_ERR_CUDA, "cudaStreamCreate failed");
     const int n = ctx->n;
     IX_TRY(deviceAlloc(ctx, "pos", 3 * (size_t)n, &ctx->dPos));
-    IX_TRY(deviceAlloc(ctx, "counts", 4, &ctx->dCounts));
-    IX_TRY(deviceAlloc(ctx, "flags", 8, &ctx->dFlags));
+    // flags, term energies and interaction counts side by side, so that one copy brings them to the host
+    unsigned char* status = nullptr;
+    IX_TRY(deviceAlloc(ctx, "status", kStatusBytes, &status));
+    ctx->dFlags = reinterpret_cast<int*>(status);
+    ctx->dOutEnergy = reinterpret_cast<double*>(status + 32);
+    ctx->dCounts = reinterpret_cast<unsigned long long*>(status + 64);
     IX_TRY(deviceAlloc(ctx, "outForces", 3 * (size_t)n, &ctx->dOutForces));
-    IX_TRY(deviceAlloc(ctx, "outEnergy", 4, &ctx->dOutEnergy));
     IX_TRY(deviceAlloc(ctx, "energyBlocks", 4 * kReduceBlocks, &ctx->dEnergyBlocks));
     IX_TRY(deviceAlloc(ctx, "reduceTicket", 1, &ctx->dReduceTicket));
     int init[8] = {1, 0, 0, 0, 1, 0, 0, 0};
@@ -1656,6 +1701,7 @@ void ix_ctx_destroy(ix_ctx* ctx) {
     releaseGraph(ctx->graphMd);
     for (auto& g : ctx->graphWindows) releaseGraph(g);
     for (auto& kv : ctx->buffers) arenaFree(ctx->arena, kv.second.p);
+    if (ctx->hostStatus) pinnedSlots().give(ctx->hostStatus);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->evFork) cudaEventDestroy(ctx->evFork);
@@ -1849,19 +1895,37 @@ static int readCounts(ix_ctx* ctx, unsigned terms) {
 // One evaluation of the selected terms at the current positions and parameters, left on the device: forces in
 // dOutForces, term energies copied to e.  Grows the neighbor lists and repeats on an overflow.
 static int evaluateResident(ix_ctx* ctx, unsigned terms, double e[4], LaunchGraph* graph = nullptr,
-                            double param = 0.0) {
+                            double param = 0.0, double* hostForces = nullptr) {
     for (int t = 0; t < 4; t++) e[t] = 0.0;
     if (!terms) return IX_OK;
     IX_TRY(prepare(ctx, terms));
+    if (!ctx->hostStatus) ctx->hostStatus = pinnedSlots().take();
+    unsigned char* hs = ctx->hostStatus;
     for (int attempt = 0; attempt < 4; attempt++) {
         IX_TRY(enqueueResident(ctx, terms, graph ? *graph : ctx->graphCompute, param));
+        // the status block and the forces come back with the evaluation; one wait for all of it
+        if (hs)
+            IX_CUDA(ctx, cudaMemcpyAsync(hs, ctx->dFlags, kStatusBytes, cudaMemcpyDeviceToHost, ctx->stream));
+        if (hostForces)
+            IX_CUDA(ctx, cudaMemcpyAsync(hostForces, ctx->dOutForces, 3 * (size_t)ctx->n * sizeof(double),
+                                         cudaMemcpyDeviceToHost, ctx->stream));
         IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         bool redo = false;
-        IX_TRY(checkOverflow(ctx, terms, redo));
+        if (hs) IX_TRY(checkOverflowFlags(ctx, terms, reinterpret_cast<const int*>(hs), redo));
+        else IX_TRY(checkOverflow(ctx, terms, redo));
         if (!redo) break;
     }
-    IX_CUDA(ctx, cudaMemcpy(e, ctx->dOutEnergy, 4 * sizeof(double), cudaMemcpyDeviceToHost));
-    IX_TRY(readCounts(ctx, terms));
+    unsigned long long c[2];
+    if (hs) {
+        std::memcpy(e, hs + 32, 4 * sizeof(double));
+        std::memcpy(c, hs + 64 + 2 * sizeof(unsigned long long), sizeof(c));
+    }
+    else {
+        IX_CUDA(ctx, cudaMemcpy(e, ctx->dOutEnergy, 4 * sizeof(double), cudaMemcpyDeviceToHost));
+        IX_CUDA(ctx, cudaMemcpy(c, ctx->dCounts + 2, sizeof(c), cudaMemcpyDeviceToHost));
+    }
+    ctx->lastPairs = (terms & 7u) ? (long long)c[0] : 0;
+    ctx->lastTriples = (terms & 8u) ? (long long)c[1] : 0;
     for (int t = 0; t < 4; t++)
         if (!((terms >> t) & 1u)) e[t] = 0.0;
     return IX_OK;
@@ -1874,14 +1938,11 @@ int ix_compute(ix_ctx* ctx, int groups, int include_forces, int include_energy, 
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
     unsigned terms = selectedTerms(ctx, groups);
     double e[4];
-    IX_TRY(evaluateResident(ctx, terms, e));
+    const bool copyForces = forces && terms && include_forces;
+    IX_TRY(evaluateResident(ctx, terms, e, nullptr, 0.0, copyForces ? forces : nullptr));
     if (term_energies) std::memcpy(term_energies, e, sizeof(e));
     if (energy) *energy = e[0] + e[1] + e[2] + e[3];
-    if (forces) {
-        if (terms && include_forces)
-            IX_CUDA(ctx, cudaMemcpy(forces, ctx->dOutForces, 3 * (size_t)ctx->n * sizeof(double), cudaMemcpyDeviceToHost));
-        else std::memset(forces, 0, 3 * (size_t)ctx->n * sizeof(double));
-    }
+    if (forces && !copyForces) std::memset(forces, 0, 3 * (size_t)ctx->n * sizeof(double));
     (void)include_energy;
     return IX_OK;
 }
