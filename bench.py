@@ -442,7 +442,8 @@ def run_lambda(args, rank, world, num_windows=16, num_alchemical=30):
     with cutoff 0.8 nm) with 30 waters decoupled by lambda_sterics, evaluated at 16 windows linspace(0, 1, 16) per step
     (energies and forces of every window).  --config lambda has no soft core, so every window is E0 + lambda E1 and
     the 16 windows cost two evaluations plus an interpolation kernel; --config lambda-softcore (R = 0.1 nm) evaluates
-    the pair terms at every window and the three-body term (linear in lambda) at 0 and 1.  Each counts 16 full
+    the pair terms once at 0 (where the alchemical pairs contribute nothing), each window's alchemical pairs, and the
+    three-body term (linear in lambda) at 0 and 1.  Each counts 16 full
     energy+force evaluations per step.  Compared with the plain path: setParameter + getState
     per window."""
     import torch
@@ -531,7 +532,8 @@ def run_lambda(args, rank, world, num_windows=16, num_alchemical=30):
                                f"cutoff 0.8 nm), {num_alchemical} waters alchemical, {num_windows} lambda_sterics "
                                f"windows per step, soft-core radius {softcore} nm",
                    "windows_method": "two evaluations + linear interpolation (exact: no soft core)" if softcore == 0
-                   else "pair terms evaluated at every window (soft core); ATM and LRC from 0 and 1, interpolated",
+                   else "pair terms once at 0 plus each window's alchemical pairs (soft core); ATM and LRC from 0 "
+                        "and 1, interpolated",
                    "pairs_per_window": pairs, "triples_per_window": triples,
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
         "plain_per_window": {"value": plain, "unit": "evaluations/s",

@@ -2140,6 +2140,34 @@ __global__ void kWindowForces(size_t n3, int num_windows, const double* __restri
     }
 }
 
+// out[w] += base + a0 + lambda_w (a1 - a0) (a0, a1 may be null): the λ-independent and linear parts of the windows'
+// forces added to their alchemical-pair parts.
+__global__ void kWindowCombine(size_t n3, int num_windows, const double* __restrict__ lambdas,
+                               const double* __restrict__ base, const double* __restrict__ a0,
+                               const double* __restrict__ a1, double* __restrict__ out) {
+    for (int w = blockIdx.y; w < num_windows; w += gridDim.y) {
+        const double lam = lambdas[w];
+        double* o = out + (size_t)w * n3;
+        for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n3; k += (size_t)gridDim.x * blockDim.x) {
+            double v = base[k];
+            if (a0) v += fma(lam, a1[k] - a0[k], a0[k]);
+            o[k] += v;
+        }
+    }
+}
+
+// Tiles holding at least one particle that carries the alchemical flag `bit` (1 or 0 per tile).
+__global__ void kMarkAlchemicalTiles(ListBuffers L, const int* flags, int bit, unsigned char* out) {
+    const int numTiles = min(*L.numTiles, L.tileCap);
+    const int lane = threadIdx.x & 31;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < numTiles; t += (gridDim.x * blockDim.x) >> 5) {
+        const int si = L.tileIBlock[t] * 32 + lane, sj = L.tileJ[32 * t + lane];
+        const bool a = (flags[si] & bit) != 0 || (sj >= 0 && (flags[sj] & bit) != 0);
+        const bool any = __any_sync(0xffffffffu, a);
+        if (lane == 0) out[t] = any ? 1 : 0;
+    }
+}
+
 static const size_t kMaxWindowGraphs = 40;
 
 // The graph of an evaluation of the given terms at one value of the window parameter: the cached one, a new slot, or
@@ -2156,6 +2184,129 @@ static LaunchGraph& windowGraph(ix_ctx* ctx, unsigned terms, double value) {
 
 // One pass over the windows (see computeWindows).  redo: a neighbor list overflowed after the first window and was
 // grown; the pass must be repeated.
+// Soft-core windows when every pair term uses the window parameter with the same alchemical particles: the pair terms
+// are evaluated once at 0, where the alchemical pairs contribute nothing (their scale is the parameter), the
+// three-body term at 0 and 1 (it is linear), and each window adds only its alchemical pairs: the pair kernel over the
+// tiles that hold an alchemical particle, keeping the pairs with exactly one (the same kernel and terms as a full
+// evaluation at that value).  The long-range correction's alchemical part joins each window's energy.
+static int softcoreWindows(ix_ctx* ctx, const std::string& name, int num_windows, const double* values,
+                           double* energies, double* d_forces) {
+    const size_t n3 = 3 * (size_t)ctx->n;
+    const unsigned terms = selectedTerms(ctx, -1), pairTerms = terms & 7u;
+    const bool atmLinear = (terms & 8u) && ctx->atmAnyAlch && ctx->atmAlchName == name;
+    int bit = 0;
+    for (int t = 0; t < 3 && !bit; t++)
+        if ((pairTerms >> t) & 1u) bit = 1 << t;
+    double *dBase = nullptr, *dA0 = nullptr, *dA1 = nullptr, *dLambda = nullptr, *dWinEnergy = nullptr;
+    double* dAlchEnergy = nullptr;
+    int* dAlchCount = nullptr;
+    unsigned long long* dPairScratch = nullptr;
+    IX_TRY(deviceAlloc(ctx, "windowLambda", (size_t)num_windows, &dLambda));
+    IX_TRY(deviceAlloc(ctx, "windowEnergy", 4 * (size_t)num_windows, &dWinEnergy));
+    IX_TRY(deviceAlloc(ctx, "windowAlchCount", 1, &dAlchCount));
+    IX_TRY(deviceAlloc(ctx, "windowPairScratch", 1, &dPairScratch));
+    if (d_forces) {
+        IX_TRY(deviceAlloc(ctx, "windowBase", n3, &dBase));
+        if (terms & 8u) IX_TRY(deviceAlloc(ctx, "windowA0", n3, &dA0));
+        if (atmLinear) IX_TRY(deviceAlloc(ctx, "windowSlope", n3, &dA1));
+    }
+    // the pair terms at 0 (the lists are built for these positions here), the three-body term at 0 and 1
+    double eP[4], eA0[4] = {0, 0, 0, 0}, eA1[4] = {0, 0, 0, 0};
+    ctx->parameters[name] = 0.0;
+    IX_TRY(evaluateResident(ctx, pairTerms, eP, &windowGraph(ctx, pairTerms, 0.0), 0.0));
+    const long long pairs = ctx->lastPairs;
+    if (d_forces)
+        IX_CUDA(ctx, cudaMemcpyAsync(dBase, ctx->dOutForces, n3 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+    long long triples = 0;
+    if (terms & 8u) {
+        IX_TRY(evaluateResident(ctx, 8u, eA0, &windowGraph(ctx, 8u, 0.0), 0.0));
+        triples = ctx->lastTriples;
+        if (d_forces)
+            IX_CUDA(ctx, cudaMemcpyAsync(dA0, ctx->dOutForces, n3 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        if (atmLinear) {
+            ctx->parameters[name] = 1.0;
+            IX_TRY(evaluateResident(ctx, 8u, eA1, &windowGraph(ctx, 8u, 1.0), 1.0));
+            if (d_forces)
+                IX_CUDA(ctx, cudaMemcpyAsync(dA1, ctx->dOutForces, n3 * sizeof(double), cudaMemcpyDeviceToDevice,
+                                             ctx->stream));
+        }
+        else std::memcpy(eA1, eA0, sizeof(eA0));
+    }
+    // the tiles that hold an alchemical particle, in tile order
+    int numTiles = 0;
+    IX_CUDA(ctx, cudaMemcpy(&numTiles, ctx->L.numTiles, sizeof(int), cudaMemcpyDeviceToHost));
+    numTiles = std::min(numTiles, ctx->tileCap);
+    unsigned char* dMarks = nullptr;
+    IX_TRY(deviceAlloc(ctx, "windowTileMarks", std::max(numTiles, 1), &dMarks));
+    kMarkAlchemicalTiles<<<ctx->numSMs * 8, 256, 0, ctx->stream>>>(ctx->L, ctx->P.flags, bit, dMarks);
+    ctx->launches += 1;
+    std::vector<unsigned char> marks(std::max(numTiles, 1));
+    IX_CUDA(ctx, cudaMemcpyAsync(marks.data(), dMarks, numTiles, cudaMemcpyDeviceToHost, ctx->stream));
+    IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::vector<int> tiles;
+    for (int t = 0; t < numTiles; t++)
+        if (marks[t]) tiles.push_back(t);
+    const int numTasks = (int)tiles.size();
+    int* dTiles = nullptr;
+    IX_TRY(deviceAlloc(ctx, "windowTiles", std::max(numTasks, 1), &dTiles));
+    IX_TRY(deviceAlloc(ctx, "windowAlchEnergy", 3 * (size_t)std::max(numTasks, 1), &dAlchEnergy));
+    if (numTasks) IX_TRY(stageCopy(ctx, dTiles, tiles.data(), tiles.size() * sizeof(int)));
+    IX_TRY(stageCopy(ctx, dAlchCount, &numTasks, sizeof(int)));
+    // each window: its alchemical pairs, then their forces and energies
+    const PairTerm& D = ctx->term[0];
+    const double volume = ctx->box[0] * ctx->box[4] * ctx->box[8];
+    const int n = ctx->n;
+    for (int w = 0; w < num_windows; w++) {
+        ctx->parameters[name] = values[w];
+        PairTermConfig C = pairConfig(ctx, pairTerms);
+        C.alchOnlyBit = bit;
+        PairBuffers P = ctx->P;
+        P.taskTiles = dTiles;
+        P.numTasks = numTasks;
+        P.taskEnergy = dAlchEnergy;
+        P.pairCount = dPairScratch;
+        const bool table = P.coef != nullptr && C.overlapMethod[1] == 0 && C.overlapMethod[2] == 0;
+        if (numTasks) {
+            if (table) kPairTiles<false, true><<<ctx->pairGridBlocks, 32 * kPairWarps, 0, ctx->stream>>>(ctx->L, P, C);
+            else kPairTiles<false, false><<<ctx->pairGridBlocks, 32 * kPairWarps, 0, ctx->stream>>>(ctx->L, P, C);
+        }
+        FinishForces F{};
+        F.n = n;
+        F.np = ctx->L.np;
+        F.slotOf = ctx->L.slotOf;
+        F.pairForce = ctx->P.forceFixed;
+        F.outForces = d_forces ? d_forces + (size_t)w * n3 : nullptr;
+        F.blocks = (n + 255) / 256;
+        const double lrc = (D.present && (pairTerms & 1u) && D.lrcAlchCoef != 0) ? values[w] * D.lrcAlchCoef / volume
+                                                                                 : 0.0;
+        EnergyReduction R{dAlchEnergy, dAlchCount, std::max(numTasks, 1), nullptr, 0, lrc, dWinEnergy + 4 * (size_t)w,
+                          ctx->dEnergyBlocks, ctx->dReduceTicket, nullptr, ctx->L.taskCounter};
+        kFinish<<<F.blocks + kReduceBlocks, 256, 0, ctx->stream>>>(F, R);
+        ctx->launches += numTasks ? 2 : 1;
+        IX_CUDA(ctx, cudaGetLastError());
+    }
+    std::vector<double> alch(4 * (size_t)num_windows);
+    IX_CUDA(ctx, cudaMemcpyAsync(alch.data(), dWinEnergy, alch.size() * sizeof(double), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    if (d_forces) {
+        IX_TRY(stageCopy(ctx, dLambda, values, num_windows * sizeof(double)));
+        const unsigned bx = (unsigned)std::max<size_t>(std::min<size_t>((n3 + 255) / 256, 1184), 1);
+        const dim3 grid(bx, (unsigned)std::min(num_windows, 65535));
+        kWindowCombine<<<grid, 256, 0, ctx->stream>>>(n3, num_windows, dLambda, dBase, dA0, atmLinear ? dA1 : dA0,
+                                                      d_forces);
+        ctx->launches += 1;
+        IX_CUDA(ctx, cudaGetLastError());
+    }
+    IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int w = 0; w < num_windows; w++) {
+        for (int k = 0; k < 3; k++) energies[4 * w + k] = eP[k] + alch[4 * (size_t)w + k];
+        energies[4 * w + 3] = eA0[3] + values[w] * (eA1[3] - eA0[3]);
+    }
+    ctx->lastPairs = pairs;
+    ctx->lastTriples = triples;
+    return IX_OK;
+}
+
 static int windowsPass(ix_ctx* ctx, const std::string& name, int num_windows, const double* values, double* energies,
                        double* d_forces, bool& redo) {
     redo = false;
@@ -2167,6 +2318,19 @@ static int windowsPass(ix_ctx* ctx, const std::string& name, int num_windows, co
         pairNonlinear = pairNonlinear || (T.present && T.anyAlch && T.alchName == name && T.softcoreRadius > 0);
     }
     const unsigned pairTerms = terms & 7u;
+    if (pairNonlinear) {
+        // every pair term on the window parameter with a soft core and the same alchemical particles: only the
+        // alchemical pairs are evaluated per window
+        bool same = true;
+        const PairTerm* first = nullptr;
+        for (int t = 0; t < 3 && same; t++) {
+            const PairTerm& T = ctx->term[t];
+            if (!((pairTerms >> t) & 1u)) continue;
+            same = T.anyAlch && T.alchName == name && T.softcoreRadius > 0 && (!first || T.alch == first->alch);
+            if (!first) first = &T;
+        }
+        if (same) return softcoreWindows(ctx, name, num_windows, values, energies, d_forces);
+    }
     const unsigned linearTerms = pairNonlinear ? (terms & 8u) : terms;
     double *dLin0 = nullptr, *dLin1 = nullptr, *dLambda = nullptr, *dWinEnergy = nullptr;
     IX_TRY(deviceAlloc(ctx, "windowLambda", (size_t)num_windows, &dLambda));

@@ -48,6 +48,7 @@ struct PairTermConfig {
     double cutoff;
     Box box;
     BoxFF boxff;
+    int alchOnlyBit;             // nonzero: only the pairs with exactly one particle carrying this alchemical flag bit
 };
 
 struct PairBuffers {
@@ -61,6 +62,8 @@ struct PairBuffers {
     unsigned long long* pairCount;
     const PairCoef* coef;        // class-pair coefficients (numClasses^2), or null
     int numClasses;
+    const int* taskTiles;        // null: every tile is a task; else the tiles of the tasks (energies go to task slots)
+    int numTasks;
 };
 
 // Bits 8..15 of a particle's flags hold its parameter class when the class tables are in use.
@@ -334,14 +337,15 @@ __global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     PairWarpStorage& S = storage[warp];
-    const int numTiles = min(*L.numTiles, L.tileCap);
+    const int numTasks = P.taskTiles ? P.numTasks : min(*L.numTiles, L.tileCap);
     const unsigned ltMask = laneMaskLt();
     unsigned long long pairs = 0;
     for (;;) {
-        int t = 0;
-        if (lane == 0) t = atomicAdd(L.taskCounter, 1);
-        t = __shfl_sync(0xffffffffu, t, 0);
-        if (t >= numTiles) break;
+        int task = 0;
+        if (lane == 0) task = atomicAdd(L.taskCounter, 1);
+        task = __shfl_sync(0xffffffffu, task, 0);
+        if (task >= numTasks) break;
+        const int t = P.taskTiles ? P.taskTiles[task] : task;
         const int I = L.tileIBlock[t];
         const int iBase = I * 32;
         const float4 center = L.bbox[2 * I];
@@ -351,11 +355,18 @@ __global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, 
         float fi[3] = {0.0f, 0.0f, 0.0f};
         {
             const int jslot = L.tileJ[32 * t + lane];
-            const unsigned row = L.tileMask[64 * t + lane];
-            const unsigned column = L.tileMask[64 * t + 32 + lane];
+            unsigned row = L.tileMask[64 * t + lane];
+            unsigned column = L.tileMask[64 * t + 32 + lane];
             __syncwarp();
             stageParticle(S, 0, lane, iBase + lane, cx, cy, cz, false, C, L, P);
             stageParticle(S, 1, lane, jslot, cx, cy, cz, shiftImage, C, L, P);
+            if (C.alchOnlyBit) {
+                // keep the pairs with exactly one alchemical particle
+                const bool ia = (S.flags[0][lane] & C.alchOnlyBit) != 0, ja = (S.flags[1][lane] & C.alchOnlyBit) != 0;
+                const unsigned iAlch = __ballot_sync(0xffffffffu, ia), jAlch = __ballot_sync(0xffffffffu, ja);
+                row &= ia ? ~jAlch : jAlch;
+                column &= ja ? ~iAlch : iAlch;
+            }
             // queue the tile's candidate pairs row by row
             const int count = __popc(row);
             int start = count;
@@ -406,7 +417,7 @@ __global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, 
             // the tile's energies: a fixed reduction tree over the lanes, one slot per tile
             for (int k = 0; k < 3; k++) {
                 const double sum = warpSumD((double)e[k]);
-                if (lane == 0) P.taskEnergy[3 * t + k] = sum;
+                if (lane == 0) P.taskEnergy[3 * (P.taskTiles ? task : t) + k] = sum;
             }
         }
         flushForce(fi, iBase + lane, L.np, P.forceFixed);

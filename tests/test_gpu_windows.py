@@ -4,8 +4,8 @@ Each window must match the context evaluated at that value with setParameter + g
 same value (InteraxPairForce.cpp:138-146 define the parameter; the pair kernels scale pairs with one alchemical
 particle, kernels/interaxPairForce.cu, and the three-body kernel scales triples with an alchemical site,
 kernels/interaxThreeBodyForce.cu).  Without a soft core the energies and forces are linear in lambda and the windows
-come from two evaluations; with a soft core every window is a full evaluation and must be bitwise identical to
-getState at that value.
+come from two evaluations; with a soft core the pair terms are evaluated once at 0 and each window adds its alchemical
+pairs (the same pair kernel and terms), within the same tolerances of getState at that value.
 """
 import numpy as np
 import pytest
@@ -49,10 +49,6 @@ def test_windows_match_get_state(softcore_radius, three_body):
         assert energies.shape == (len(WINDOWS), 4) and forces.shape == (len(WINDOWS), len(pos), 3)
         assert ctx.getParameter("lambda_sterics") == 0.8
     ref_e, ref_f = _per_window(ctx, WINDOWS)
-    if softcore_radius > 0 and not three_body:
-        # pair terms with a soft core are evaluated at every window by the same kernels as getState
-        assert np.array_equal(energies, ref_e)
-        assert np.array_equal(forces, ref_f)
     for w in range(len(WINDOWS)):
         e_err, f_err = errors(energies[w].sum(), forces[w], ref_e[w].sum(), ref_f[w],
                               abs_energy=np.abs(ref_e[w]).sum())
