@@ -233,6 +233,9 @@ struct ix_ctx {
     double cutoff = 1.0;
     std::vector<std::pair<int, int>> exclusions;   // normalized (min, max), sorted unique
     bool pairDirty = true;               // parameters must be re-uploaded
+    unsigned pairGatesAll = 0;           // bit t: every particle takes part in pair term t
+    unsigned pairAlchAny = 0;            // bit t: some particle is alchemical in pair term t
+    int pairShareOverlap = 0;            // exchange and short-range widths agree for every particle
     bool pairAllocated = false;
 
     // three-body force
@@ -417,13 +420,40 @@ static double lambdaOf(const ix_ctx* ctx, const std::string& name, bool anyAlch)
     return it == ctx->parameters.end() ? 1.0 : it->second;
 }
 
-static unsigned mortonCode(unsigned x, unsigned y, unsigned z) {
-    auto spread = [](unsigned v) {
-        unsigned r = 0;
-        for (int b = 0; b < 10; b++) r |= ((v >> b) & 1u) << (3 * b);
-        return r;
-    };
-    return spread(x) | (spread(y) << 1) | (spread(z) << 2);
+// Position of cell (x, y, z) on the Hilbert curve through the 2^bits cube (the transpose algorithm of J. Skilling,
+// "Programming the Hilbert curve", AIP Conf. Proc. 707, 381 (2004)).  Consecutive cells of the curve are face
+// neighbours, so the 32-particle blocks cut from the particles in cell order are compact; a Z-order curve jumps at
+// its octant boundaries, and the blocks that straddle a jump span much of the box.
+static unsigned long long hilbertIndex(unsigned x, unsigned y, unsigned z, int bits) {
+    unsigned X[3] = {x, y, z};
+    const unsigned top = 1u << (bits - 1);
+    for (unsigned q = top; q > 1; q >>= 1) {
+        const unsigned p = q - 1;
+        for (int i = 0; i < 3; i++) {
+            if (X[i] & q) X[0] ^= p;
+            else {
+                const unsigned t = (X[0] ^ X[i]) & p;
+                X[0] ^= t;
+                X[i] ^= t;
+            }
+        }
+    }
+    for (int i = 1; i < 3; i++) X[i] ^= X[i - 1];
+    unsigned t = 0;
+    for (unsigned q = top; q > 1; q >>= 1)
+        if (X[2] & q) t ^= q - 1;
+    for (int i = 0; i < 3; i++) X[i] ^= t;
+    unsigned long long h = 0;
+    for (int b = bits - 1; b >= 0; b--)
+        for (int i = 0; i < 3; i++) h = (h << 1) | ((X[i] >> b) & 1u);
+    return h;
+}
+
+// The power of two nearest to v (in ratio), within [1, 1024].
+static int nearestPow2(double v) {
+    int p = 1;
+    while (p < 1024 && v >= p * std::sqrt(2.0)) p *= 2;
+    return p;
 }
 
 // ---------------------------------------------------------------------------------------------------------------------
@@ -672,6 +702,19 @@ static int uploadPairParams(ix_ctx* ctx) {
     std::vector<float4> p0, p1, p2, p3;
     std::vector<int> flags;
     packPairParams(ctx, p0, p1, p2, p3, flags);
+    ctx->pairGatesAll = 7u;
+    ctx->pairAlchAny = 0u;
+    for (int i = 0; i < n; i++) {
+        for (int t = 0; t < 3; t++)
+            if (!(flags[i] & (kFlagGateDisp << t))) ctx->pairGatesAll &= ~(1u << t);
+        ctx->pairAlchAny |= (unsigned)(flags[i] & 7);
+    }
+    ctx->pairShareOverlap = 0;
+    if (ctx->term[1].present && ctx->term[2].present) {
+        bool same = true;
+        for (int i = 0; i < n && same; i++) same = ctx->term[1].params[2 * i + 1] == ctx->term[2].params[3 * i + 2];
+        ctx->pairShareOverlap = same;
+    }
     IX_TRY(stageCopy(ctx, ctx->dP0o, p0.data(), n * sizeof(float4)));
     IX_TRY(stageCopy(ctx, ctx->dP1o, p1.data(), n * sizeof(float4)));
     IX_TRY(stageCopy(ctx, ctx->dP2o, p2.data(), n * sizeof(float4)));
@@ -746,20 +789,22 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
         double volume = ctx->box[0] * ctx->box[4] * ctx->box[8];
         double cell = std::cbrt(4.0 * volume / n);
         const double len[3] = {ctx->box[0], ctx->box[4], ctx->box[8]};
-        for (int d = 0; d < 3; d++) nc[d] = std::min(1024, std::max(1, (int)(len[d] / cell)));
+        for (int d = 0; d < 3; d++) nc[d] = nearestPow2(len[d] / cell);
     }
     else {
-        int m = std::min(1024, std::max(1, (int)std::lround(std::cbrt(n / 4.0))));
+        const int m = nearestPow2(std::cbrt(n / 4.0));
         nc[0] = nc[1] = nc[2] = m;
     }
     for (int d = 0; d < 3; d++) G.nc[d] = nc[d];
     const int numCells = nc[0] * nc[1] * nc[2];
-    std::vector<std::pair<unsigned, int>> order(numCells);
+    int bits = 1;
+    while ((1 << bits) < std::max(nc[0], std::max(nc[1], nc[2]))) bits++;
+    std::vector<std::pair<unsigned long long, int>> order(numCells);
     for (int z = 0; z < nc[2]; z++)
         for (int y = 0; y < nc[1]; y++)
             for (int x = 0; x < nc[0]; x++) {
                 int c = (z * nc[1] + y) * nc[0] + x;
-                order[c] = {mortonCode(x, y, z), c};
+                order[c] = {hilbertIndex(x, y, z, bits), c};
             }
     std::sort(order.begin(), order.end());
     std::vector<int> rank(numCells);
@@ -783,7 +828,6 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
     IX_TRY(deviceAlloc(ctx, "spos", 3 * (size_t)np, &L.spos));
     IX_TRY(deviceAlloc(ctx, "sposf", np, &L.sposf));
     IX_TRY(deviceAlloc(ctx, "bbox", 2 * (size_t)nb, &L.bbox));
-    IX_TRY(deviceAlloc(ctx, "partCount", (size_t)nb * kListParts, &L.partCount));
     IX_TRY(deviceAlloc(ctx, "blockAtoms", nb, &L.blockAtoms));
     IX_TRY(deviceAlloc(ctx, "blockTiles", nb + 1, &L.blockTiles));
     if (tileCap > (long long)1 << 26) return fail(ctx, IX_ERR_INVALID, "neighbor list too large (%lld tiles)", tileCap);
@@ -1188,12 +1232,7 @@ static PairTermConfig pairConfig(const ix_ctx* ctx, unsigned terms) {
     }
     C.twoBeta = (float)(2.0 * ctx->term[0].dampingScale);
     // the exchange and short-range terms share one overlap when their widths and methods agree for every particle
-    C.shareOverlap = 0;
-    if (ctx->term[1].present && ctx->term[2].present && ctx->term[1].overlapMethod == ctx->term[2].overlapMethod) {
-        bool same = true;
-        for (int i = 0; i < ctx->n && same; i++) same = ctx->term[1].params[2 * i + 1] == ctx->term[2].params[3 * i + 2];
-        C.shareOverlap = same;
-    }
+    C.shareOverlap = ctx->pairShareOverlap && ctx->term[1].overlapMethod == ctx->term[2].overlapMethod;
     C.useCutoff = ctx->method != IX_NO_CUTOFF;
     C.periodic = ctx->method == IX_CUTOFF_PERIODIC;
     C.cutoff = ctx->cutoff;
@@ -1374,16 +1413,12 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
                                               ctx->dP1, ctx->dP2, ctx->dP3, ctx->dFlagsSorted);
             refresh(s);
             kBlockBounds<<<(L.nb * 32 + tpb - 1) / tpb, tpb, 0, s>>>(L, ctx->G);
-            const int warpsPerBlock = 8;
-            const int gParts = (L.nb * kListParts + warpsPerBlock - 1) / warpsPerBlock;
-            const int gB = (L.nb + warpsPerBlock - 1) / warpsPerBlock;
-            kListAtoms<0><<<gParts, 32 * warpsPerBlock, 0, s>>>(L, ctx->G);
+            kListTiles<0><<<L.nb, kListThreads, 0, s>>>(L, ctx->G);
             kScanTiles<<<1, 1024, 0, s>>>(L);
-            kListAtoms<1><<<gParts, 32 * warpsPerBlock, 0, s>>>(L, ctx->G);
-            kTileHeaders<<<gB, 32 * warpsPerBlock, 0, s>>>(L);
-            kTileMasks<<<ctx->numSMs * 8, 32 * warpsPerBlock, 0, s>>>(L, ctx->G);
+            kListTiles<1><<<L.nb, kListThreads, 0, s>>>(L, ctx->G);
+            kTileMasks<<<ctx->numSMs * 8, kListThreads, 0, s>>>(L, ctx->G);
             kClearFlag<<<1, 1, 0, s>>>(L.flag);
-            ctx->launches += ctx->G.periodic ? 14 : 15;
+            ctx->launches += ctx->G.periodic ? 13 : 14;
             return IX_OK;
         };
         if (stepStarted) IX_TRY(launchIf(ctx, st, L.flag, rebuild));
@@ -1399,7 +1434,15 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         for (int t = 1; t < 3; t++)
             if ((terms >> t) & 1u) table = table && C.overlapMethod[t] == 0;
         const int grid = lean ? ctx->pairGridBlocksLean : ctx->pairGridBlocks;
-        if (lean && table) kPairTiles<true, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        // every pair of every selected term evaluated unscaled: no per-pair gate or scale tests
+        bool uniform = lean;
+        for (int t = 0; t < 3; t++)
+            if ((terms >> t) & 1u)
+                uniform = uniform && ((ctx->pairGatesAll >> t) & 1u) &&
+                          (!((ctx->pairAlchAny >> t) & 1u) || C.lambda[t] == 1.0f);
+        if (lean && table && uniform) kPairTiles<true, true, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        else if (lean && uniform) kPairTiles<true, false, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        else if (lean && table) kPairTiles<true, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
         else if (lean) kPairTiles<true, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
         else if (table) kPairTiles<false, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
         else kPairTiles<false, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);

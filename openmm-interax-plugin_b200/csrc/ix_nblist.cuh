@@ -17,7 +17,6 @@
 namespace ix {
 
 constexpr float kPairSkin = 0.1f;    // nm; rebuild when a particle has moved by more than half of it
-constexpr int kListParts = 8;        // warps sharing the candidate search of one i-block
 
 // Particle flags in the sorted parameter arrays.
 constexpr int kFlagReal = 1 << 3;
@@ -61,7 +60,6 @@ struct ListBuffers {
     float4* sposf;              // np
     float4* bbox;               // nb x 2: center (xyz), half extent (xyz)
     // tiles
-    int* partCount;             // nb x kListParts: candidates found by each part of a block's search, then offsets
     int* blockAtoms;            // nb: candidate j particles of each i-block
     int* blockTiles;            // nb + 1: exclusive scan of the tile counts, then the total
     int* tileJ;                 // tileCap x 32
@@ -334,50 +332,184 @@ __device__ __forceinline__ bool isExcluded(const ListBuffers& L, int oi, int oj)
     return false;
 }
 
-// Candidate j particles of one i-block, searched by kListParts warps that split the blocks J >= I into contiguous
-// ranges: the particles of blocks whose box is within the list cutoff of block I's box, and whose own position is
-// within it too.  PASS 0 counts each part's candidates; PASS 1 writes their slots to the i-block's tile rows, part
-// after part and in slot order within a part, so the lists do not depend on scheduling.
+constexpr int kListThreads = 256;                 // one thread block of 8 warps per i-block
+constexpr int kListWarps = kListThreads / 32;
+
+// Candidate j particles of one i-block (one thread block per i-block): the particles of the blocks J >= I whose box is
+// within the list cutoff of block I's box and whose own position is within it too, in the order (J, slot).  The blocks
+// are examined 256 at a time: each thread tests one block's box, the candidate blocks are compacted in block order, and
+// the warps take them round robin for the particle tests, so that the search of an i-block whose candidates crowd
+// into one index range is not serialised on one warp.  PASS 0 counts the candidates; PASS 1 writes their slots to the
+// i-block's tile rows and its tile headers.  Both passes make the same decisions, so the lists do not depend on
+// scheduling.
 template <int PASS>
-__global__ void kListAtoms(ListBuffers L, ListGeometry G) {
+__global__ void __launch_bounds__(kListThreads) kListTiles(ListBuffers L, ListGeometry G) {
     if (!rebuildRequested(L)) return;
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    const int I = w / kListParts, part = w % kListParts;
-    if (I >= L.nb) return;
-    const int span = L.nb - I;
-    const int J0 = I + (int)((long long)span * part / kListParts);
-    const int J1 = I + (int)((long long)span * (part + 1) / kListParts);
+    __shared__ int candJ[kListThreads];
+    __shared__ unsigned keep[kListThreads];
+    __shared__ int offset[kListThreads];
+    __shared__ int warpTotal[kListWarps];
+    const int I = blockIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const float4 ci = L.bbox[2 * I], ei = L.bbox[2 * I + 1];
     const float cut2 = G.useCutoff ? G.listCutoff * G.listCutoff : INFINITY;
-    long long base = 0;
-    if (PASS == 1) base = 32LL * L.blockTiles[I] + L.partCount[I * kListParts + part];
-    const long long end = 32LL * L.tileCap;
-    int count = 0;
-    for (int Jc = J0; Jc < J1; Jc += 32) {
-        const int Jl = Jc + lane;
-        const bool cand = Jl < J1 && boxBoxDist2(ci, ei, L.bbox[2 * Jl], L.bbox[2 * Jl + 1], G) < cut2;
-        unsigned cmask = __ballot_sync(0xffffffffu, cand);
-        while (cmask) {
-            const int J = Jc + __ffs(cmask) - 1;
-            cmask &= cmask - 1;
-            const int j = J * 32 + lane;
-            bool keep = L.sortedAtom[j] >= 0;
-            if (keep && G.useCutoff) keep = pointBoxDist2(L.sposf[j], ci, ei, G) < cut2;
-            const unsigned kmask = __ballot_sync(0xffffffffu, keep);
-            if (PASS == 1 && keep) {
-                const long long pos = base + count + __popc(kmask & laneMaskLt());
-                if (pos < end) L.tileJ[pos] = j;
-            }
-            count += __popc(kmask);
-        }
+    int t0 = 0, t1 = 0;
+    if (PASS == 1) {
+        t0 = L.blockTiles[I];
+        t1 = L.blockTiles[I + 1];
+        if (t1 > L.tileCap) return;   // overflow: nothing is scheduled, the host grows the buffers and builds again
     }
-    if (PASS == 0 && lane == 0) L.partCount[I * kListParts + part] = count;
+    const long long base = 32LL * t0, last = 32LL * t1;
+    int count = 0;
+    for (int Jc = I; Jc < L.nb; Jc += kListThreads) {
+        // the candidate blocks of this chunk, in block order
+        const int J = Jc + tid;
+        const bool cand = J < L.nb && boxBoxDist2(ci, ei, L.bbox[2 * J], L.bbox[2 * J + 1], G) < cut2;
+        const unsigned b = __ballot_sync(0xffffffffu, cand);
+        if (lane == 0) warpTotal[warp] = __popc(b);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int w = 0; w < kListWarps; w++) {
+            const int c = warpTotal[w];
+            before += w < warp ? c : 0;
+            total += c;
+        }
+        if (cand) candJ[before + __popc(b & laneMaskLt())] = J;
+        __syncthreads();
+        // the particle tests of the candidate blocks
+        for (int k = warp; k < total; k += kListWarps) {
+            const int j = candJ[k] * 32 + lane;
+            bool in = L.sortedAtom[j] >= 0;
+            if (in && G.useCutoff) in = pointBoxDist2(L.sposf[j], ci, ei, G) < cut2;
+            const unsigned m = __ballot_sync(0xffffffffu, in);
+            if (lane == 0) keep[k] = m;
+        }
+        __syncthreads();
+        // offsets of the candidate blocks' particles: exclusive scan over the chunk
+        const int v = tid < total ? __popc(keep[tid]) : 0;
+        int incl = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += u;
+        }
+        if (lane == 31) warpTotal[warp] = incl;
+        __syncthreads();
+        int wBefore = 0, chunkAtoms = 0;
+        for (int w = 0; w < kListWarps; w++) {
+            const int c = warpTotal[w];
+            wBefore += w < warp ? c : 0;
+            chunkAtoms += c;
+        }
+        if (tid < total) offset[tid] = count + wBefore + incl - v;
+        __syncthreads();
+        if (PASS == 1) {
+            for (int k = warp; k < total; k += kListWarps) {
+                const unsigned m = keep[k];
+                const long long pos = base + offset[k] + __popc(m & laneMaskLt());
+                if (((m >> lane) & 1u) && pos < last) L.tileJ[pos] = candJ[k] * 32 + lane;
+            }
+        }
+        count += chunkAtoms;
+        __syncthreads();   // the shared arrays are refilled by the next chunk
+    }
+    if (PASS == 0) {
+        if (tid == 0) L.blockAtoms[I] = count;
+    }
+    else {
+        // tile headers: the i-block of each tile, padding (-1) after the last candidate of the last tile
+        for (int t = t0 + tid; t < t1; t += kListThreads) L.tileIBlock[t] = I;
+        const int rest = count & 31;
+        if (t1 > t0 && rest != 0 && tid >= rest && tid < 32) L.tileJ[last - 32 + tid] = -1;
+    }
 }
 
-// Per i-block: the offsets of its parts' candidates, its candidate and tile counts; then the exclusive scan of the
-// tile counts over the blocks (one block of 1024 threads).  On overflow no tile is scheduled (nothing is written
-// beyond the buffers); the host grows them and evaluates again.
+// Pair masks of the tiles, one warp per tile over the whole list (the tiles of an i-block vary in number, so a
+// per-i-block distribution would wait on the largest); lane = the tile's j lane, the i particles from shared memory.
+// A pair's bit is set when j's slot follows i's (each pair once), both are real particles gated on for a common term,
+// the pair is not excluded and its build-time distance (minimum image) is within the list cutoff: then no pair outside
+// the masks can come within the cutoff before the displacement check requests the next build.  The tests that do not
+// depend on the distance are masks formed once per tile; where the i-block allows it (rectangular box, block small
+// against the box), j is placed at its image nearest the block's center once, as in the pair kernel, instead of a
+// minimum image per pair.  Exclusions are looked up only for the pairs whose i lies in j's exclusion range.  Row
+// masks: lane = i slot, bit k = the tile's j lane k; column masks: the transpose.
+__global__ void __launch_bounds__(kListThreads) kTileMasks(ListBuffers L, ListGeometry G) {
+    if (!rebuildRequested(L)) return;
+    __shared__ float4 ipos[kListWarps][32];   // xyz and the original index (as its bits)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // the margin covers the float rounding of the build-time distance
+    const float cut2 = G.useCutoff ? G.listCutoff * G.listCutoff * (1.0f + 1e-5f) : INFINITY;
+    const int numTiles = *L.numTiles;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < numTiles; t += warps) {
+        const int I = L.tileIBlock[t];
+        const int si = I * 32 + lane;
+        const int oi = L.sortedAtom[si];
+        const int fi = L.flags[si];
+        float4 p = L.sposf[si];
+        p.w = __int_as_float(oi);
+        __syncwarp();
+        ipos[warp][lane] = p;
+        __syncwarp();
+        const unsigned iReal = __ballot_sync(0xffffffffu, oi >= 0);
+        const unsigned gateD = __ballot_sync(0xffffffffu, (fi & kFlagGateDisp) != 0);
+        const unsigned gateE = __ballot_sync(0xffffffffu, (fi & kFlagGateExch) != 0);
+        const unsigned gateS = __ballot_sync(0xffffffffu, (fi & kFlagGateSr) != 0);
+        const int sj = L.tileJ[32LL * t + lane];
+        int oj = -1, fj = 0;
+        float4 pj = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        int2 jr = make_int2(1, 0);
+        if (sj >= 0) {
+            oj = L.sortedAtom[sj];
+            fj = L.flags[sj];
+            pj = L.sposf[sj];
+            if (oj >= 0) jr = L.exclRange[oj];
+        }
+        unsigned column = 0;
+        if (oj >= 0) {
+            column = iReal & (((fj & kFlagGateDisp) ? gateD : 0u) | ((fj & kFlagGateExch) ? gateE : 0u) |
+                              ((fj & kFlagGateSr) ? gateS : 0u));
+            const int d = sj - I * 32;   // the i slots of the block below j's
+            column &= d >= 32 ? 0xffffffffu : (d <= 0 ? 0u : (1u << d) - 1u);
+        }
+        if (G.useCutoff && __any_sync(0xffffffffu, column != 0)) {
+            bool perPair = G.periodic;
+            const float4 c = L.bbox[2 * I];
+            if (G.periodic && c.w != 0.0f) {
+                pj.x -= G.boxf.a[0] * rintf((pj.x - c.x) * G.boxf.inv[0]);
+                pj.y -= G.boxf.b[1] * rintf((pj.y - c.y) * G.boxf.inv[1]);
+                pj.z -= G.boxf.c[2] * rintf((pj.z - c.z) * G.boxf.inv[2]);
+                perPair = false;
+            }
+            unsigned in = 0;
+#pragma unroll
+            for (int i = 0; i < 32; i++) {
+                const float4 q = ipos[warp][i];
+                float dx = pj.x - q.x, dy = pj.y - q.y, dz = pj.z - q.z;
+                if (perPair) minimumImageF(dx, dy, dz, G.boxf);
+                if (fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < cut2) in |= 1u << i;
+            }
+            column &= in;
+        }
+        if (jr.x <= jr.y) {
+            for (unsigned m = column; m; m &= m - 1) {
+                const int i = __ffs(m) - 1;
+                const int o = __float_as_int(ipos[warp][i].w);
+                if (o >= jr.x && o <= jr.y && isExcluded(L, oj, o)) column &= ~(1u << i);
+            }
+        }
+        unsigned row = 0;
+        for (int i = 0; i < 32; i++) {
+            const unsigned bits = __ballot_sync(0xffffffffu, (column >> i) & 1u);
+            if (lane == i) row = bits;
+        }
+        L.tileMask[64LL * t + lane] = row;
+        L.tileMask[64LL * t + 32 + lane] = column;
+    }
+}
+
+// The exclusive scan of the i-blocks' tile counts (one block of 1024 threads).  On overflow no tile is scheduled
+// (nothing is written beyond the buffers); the host grows them and evaluates again.
 __global__ void kScanTiles(ListBuffers L) {
     if (!rebuildRequested(L)) return;
     __shared__ int partial[1024];
@@ -386,14 +518,7 @@ __global__ void kScanTiles(ListBuffers L) {
     const int begin = min(t * per, L.nb), end = min(begin + per, L.nb);
     int sum = 0;
     for (int c = begin; c < end; c++) {
-        int atoms = 0;
-        for (int p = 0; p < kListParts; p++) {
-            const int k = L.partCount[c * kListParts + p];
-            L.partCount[c * kListParts + p] = atoms;
-            atoms += k;
-        }
-        L.blockAtoms[c] = atoms;
-        const int tiles = (atoms + 31) / 32;
+        const int tiles = (L.blockAtoms[c] + 31) / 32;
         L.blockTiles[c] = tiles;
         sum += tiles;
     }
@@ -416,71 +541,6 @@ __global__ void kScanTiles(ListBuffers L) {
         L.blockTiles[L.nb] = total;
         *L.numTiles = total > L.tileCap ? 0 : total;
         if (total > L.tileCap) atomicOr(L.flag + 1, 1);
-    }
-}
-
-// Tile headers of one i-block (one warp): the i-block of each of its tiles, and padding (-1) after the last candidate
-// of its last tile.
-__global__ void kTileHeaders(ListBuffers L) {
-    if (!rebuildRequested(L)) return;
-    const int I = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (I >= L.nb) return;
-    const int t0 = L.blockTiles[I], t1 = L.blockTiles[I + 1];
-    if (t1 > L.tileCap) return;
-    for (int t = t0 + lane; t < t1; t += 32) L.tileIBlock[t] = I;
-    const int rest = L.blockAtoms[I] & 31;
-    if (t1 > t0 && rest != 0 && lane >= rest) L.tileJ[32 * (t1 - 1) + lane] = -1;
-}
-
-// Pair masks of the tiles (one warp per tile).  A pair's bit is set when j's slot follows i's (each pair once), both
-// are real particles gated on for a common term, the pair is not excluded and its build-time distance (minimum image)
-// is within the list cutoff: then no pair outside the masks can come within the cutoff before the displacement check
-// requests the next build.  Row masks: lane = i slot, bit k = the tile's j lane k; column masks: the transpose.
-__global__ void kTileMasks(ListBuffers L, ListGeometry G) {
-    if (!rebuildRequested(L)) return;
-    const int lane = threadIdx.x & 31;
-    const int numTiles = *L.numTiles;
-    // the margin covers the float rounding of the build-time distance
-    const float cut2 = G.useCutoff ? G.listCutoff * G.listCutoff * (1.0f + 1e-5f) : INFINITY;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; t < numTiles; t += warps) {
-        const int si = L.tileIBlock[t] * 32 + lane;
-        const int oi = L.sortedAtom[si];
-        const float4 pi = L.sposf[si];
-        const int fi = L.flags[si];
-        const int2 range = oi >= 0 ? L.exclRange[oi] : make_int2(1, 0);
-        const int sj = L.tileJ[32 * t + lane];
-        int oj = -1, fj = 0;
-        float4 pj = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        if (sj >= 0) {
-            oj = L.sortedAtom[sj];
-            fj = L.flags[sj];
-            pj = L.sposf[sj];
-        }
-        unsigned mask = 0;
-        for (int k = 0; k < 32; k++) {
-            const int sk = __shfl_sync(0xffffffffu, sj, k);
-            const int ok = __shfl_sync(0xffffffffu, oj, k);
-            const int fk = __shfl_sync(0xffffffffu, fj, k);
-            float dx = __shfl_sync(0xffffffffu, pj.x, k) - pi.x;
-            float dy = __shfl_sync(0xffffffffu, pj.y, k) - pi.y;
-            float dz = __shfl_sync(0xffffffffu, pj.z, k) - pi.z;
-            bool in = oi >= 0 && ok >= 0 && sk > si && (fi & fk & kFlagGates) != 0;
-            if (in && G.useCutoff) {
-                if (G.periodic) minimumImageF(dx, dy, dz, G.boxf);
-                in = fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < cut2;
-            }
-            if (in && ok >= range.x && ok <= range.y) in = !isExcluded(L, oi, ok);
-            if (in) mask |= 1u << k;
-        }
-        unsigned column = 0;
-        for (int k = 0; k < 32; k++) {
-            const unsigned b = __ballot_sync(0xffffffffu, (mask >> k) & 1u);
-            if (lane == k) column = b;
-        }
-        L.tileMask[64 * t + lane] = mask;
-        L.tileMask[64 * t + 32 + lane] = column;
     }
 }
 

@@ -71,8 +71,9 @@ constexpr int kClassShift = 8;
 
 // Every pair term of one pair.  r, invR: distance; fi, fj: flags.  Adds each term's scaled energy to e[] and returns
 // the scaled dE/dr of all terms.  LEAN: the configuration has no soft core, no switching function and no order-2
-// overlap, so those paths are compiled out.
-template <bool LEAN>
+// overlap, so those paths are compiled out.  UNIFORM: every particle takes part in every selected term and no pair
+// is scaled (no alchemical particle, or lambda = 1), so the per-pair gate and scale tests are compiled out.
+template <bool LEAN, bool UNIFORM>
 __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, float invR, const float4& a0,
                                            const float4& a1, const float4& a2, const float4& a3, int fi,
                                            const float4& b0, const float4& b1, const float4& b2, const float4& b3,
@@ -82,9 +83,11 @@ __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, flo
 #pragma unroll
     for (int t = 0; t < 3; t++) {
         if (!((C.termMask >> t) & 1)) continue;
-        const int gate = t == 0 ? kFlagGateDisp : (t == 1 ? kFlagGateExch : kFlagGateSr);
-        if (!(fi & fj & gate)) continue;
-        const bool alch = ((fi ^ fj) >> t) & 1;
+        if (!UNIFORM) {
+            const int gate = t == 0 ? kFlagGateDisp : (t == 1 ? kFlagGateExch : kFlagGateSr);
+            if (!(fi & fj & gate)) continue;
+        }
+        const bool alch = UNIFORM ? false : (((fi ^ fj) >> t) & 1) != 0;
         float rEff = r, invEff = invR, scR = 1.0f;
         if (!LEAN && alch && C.softShift[t] > 0.0f) {
             // r_eff = (r^6 + (1 - lambda) R^6)^(1/6), dE/dr picks up (r/r_eff)^5 (interaxPairBegin.cc, interaxPairEnd.cc)
@@ -151,7 +154,7 @@ __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, flo
 }
 
 // The same from the pair's class coefficients (see PairCoef).  Only the exact overlap method.
-template <bool LEAN>
+template <bool LEAN, bool UNIFORM>
 __device__ __forceinline__ float pairTermsTable(const PairTermConfig& C, float r, float invR, const PairCoef* K,
                                                 int fi, int fj, float e[3]) {
     float dTotal = 0.0f;
@@ -159,9 +162,11 @@ __device__ __forceinline__ float pairTermsTable(const PairTermConfig& C, float r
 #pragma unroll
     for (int t = 0; t < 3; t++) {
         if (!((C.termMask >> t) & 1)) continue;
-        const int gate = t == 0 ? kFlagGateDisp : (t == 1 ? kFlagGateExch : kFlagGateSr);
-        if (!(fi & fj & gate)) continue;
-        const bool alch = ((fi ^ fj) >> t) & 1;
+        if (!UNIFORM) {
+            const int gate = t == 0 ? kFlagGateDisp : (t == 1 ? kFlagGateExch : kFlagGateSr);
+            if (!(fi & fj & gate)) continue;
+        }
+        const bool alch = UNIFORM ? false : (((fi ^ fj) >> t) & 1) != 0;
         float rEff = r, invEff = invR, scR = 1.0f;
         if (!LEAN && alch && C.softShift[t] > 0.0f) {
             const float r2 = r * r;
@@ -285,10 +290,10 @@ __device__ __forceinline__ void flushForce(const float f[3], int s, int np, long
 }
 
 // One queued pair: displacement, exact cutoff test, the terms.  Returns the force on i (zero outside the cutoff).
-template <bool LEAN, bool TABLE>
+template <bool LEAN, bool TABLE, bool UNIFORM>
 __device__ __forceinline__ float4 computeQueuedPair(PairWarpStorage& S, int entry, int iBase, bool perPairImage,
                                                     const PairTermConfig& C, const ListBuffers& L,
-                                                    const PairBuffers& P, float e[3], unsigned long long& pairs) {
+                                                    const PairBuffers& P, float e[3], unsigned& pairs) {
     const int i = entry >> 5, j = entry & 31;
     const float4 hi_i = S.hi[0][i], hi_j = S.hi[1][j], lo_i = S.lo[0][i], lo_j = S.lo[1][j];
     float dxh = hi_j.x - hi_i.x, dyh = hi_j.y - hi_i.y, dzh = hi_j.z - hi_i.z;
@@ -316,7 +321,7 @@ __device__ __forceinline__ float4 computeQueuedPair(PairWarpStorage& S, int entr
     float dEdR;
     if (TABLE) {
         const int ci = (fi >> kClassShift) & 0xff, cj = (fj >> kClassShift) & 0xff;
-        dEdR = pairTermsTable<LEAN>(C, r, invR, P.coef + ci * P.numClasses + cj, fi, fj, e);
+        dEdR = pairTermsTable<LEAN, UNIFORM>(C, r, invR, P.coef + ci * P.numClasses + cj, fi, fj, e);
     }
     else {
         const int si = iBase + i, sj = S.jslot[j];
@@ -324,14 +329,14 @@ __device__ __forceinline__ float4 computeQueuedPair(PairWarpStorage& S, int entr
         const float4 b0 = __ldg(P.p0 + sj), b1 = __ldg(P.p1 + sj), b2 = __ldg(P.p2 + sj), b3 = __ldg(P.p3 + sj);
         // InteraxOrder2 expands about the width of the particle with the lower original index
         const bool iFirst = LEAN ? true : __ldg(L.sortedAtom + si) < __ldg(L.sortedAtom + sj);
-        dEdR = pairTerms<LEAN>(C, r, invR, a0, a1, a2, a3, fi, b0, b1, b2, b3, fj, iFirst, e);
+        dEdR = pairTerms<LEAN, UNIFORM>(C, r, invR, a0, a1, a2, a3, fi, b0, b1, b2, b3, fj, iFirst, e);
     }
     const float fs = dEdR * invR;
     pairs++;
     return make_float4(dx * fs, dy * fs, dz * fs, 0.0f);
 }
 
-template <bool LEAN, bool TABLE>
+template <bool LEAN, bool TABLE, bool UNIFORM = false>
 __global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, PairBuffers P, PairTermConfig C) {
     __shared__ PairWarpStorage storage[kPairWarps];
     const int warp = threadIdx.x >> 5;
@@ -384,11 +389,12 @@ __global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, 
             __syncwarp();
             float e[3] = {0.0f, 0.0f, 0.0f};
             float fj[3] = {0.0f, 0.0f, 0.0f};
+            unsigned tilePairs = 0;
             for (int base = 0; base < total; base += kPairRound) {
                 const int n = min(kPairRound, total - base);
                 for (int p = lane; p < n; p += 32)
-                    S.force[p] = computeQueuedPair<LEAN, TABLE>(S, S.queue[base + p], iBase, perPairImage, C, L, P,
-                                                                 e, pairs);
+                    S.force[p] = computeQueuedPair<LEAN, TABLE, UNIFORM>(S, S.queue[base + p], iBase, perPairImage,
+                                                                          C, L, P, e, tilePairs);
                 __syncwarp();
                 // i side: this lane's row, contiguous in the queue
                 const int a = max(start, base), b = min(start + count, base + n);
@@ -413,6 +419,7 @@ __global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, 
                 }
                 __syncwarp();
             }
+            pairs += tilePairs;
             flushForce(fj, jslot, L.np, P.forceFixed);
             // the tile's energies: a fixed reduction tree over the lanes, one slot per tile
             for (int k = 0; k < 3; k++) {
