@@ -1089,10 +1089,14 @@ __device__ void reduceEnergiesBlock(const EnergyReduction& R, int block, int num
         last = atomicInc(R.ticket, numBlocks - 1) == (unsigned)(numBlocks - 1);
     }
     __syncthreads();
-    if (last && t < 4) {
-        __threadfence();
+    if (!last) return;
+    // the block sums are loaded in parallel, then added in block order
+    __threadfence();
+    for (int k = t; k < 4 * numBlocks; k += 256) red[k & 3][k >> 2] = ((volatile double*)R.blockSums)[k];
+    __syncthreads();
+    if (t < 4) {
         double v = 0.0;
-        for (int b = 0; b < numBlocks; b++) v += ((volatile double*)R.blockSums)[4 * b + t];
+        for (int b = 0; b < numBlocks; b++) v += red[t][b];
         if (t == 0) v += R.lrcEnergy;
         if (R.outEnergy) R.outEnergy[t] = v;
         if (t == 0) {
