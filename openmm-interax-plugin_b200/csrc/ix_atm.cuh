@@ -45,6 +45,8 @@ struct AtmBuffers {
     const int* molecule;         // effective molecule (negative input already replaced by -1 - site)
     double* sitePos;             // numSites x 3
     double* siteRef;             // numSites x 3, at the last list build
+    float4* chunkBox;            // 2 per chunk of 32 consecutive sites: box center (w = 1: usable) and half extents,
+                                 // of the positions wrapped into a rectangular box; null: the list search scans all
     int* flag;                   // [0] rebuild, [1] neighbor overflow, [2] a list longer than kAtmFast
     int* nbrCount;               // numSites
     int* nbr;                    // numSites x cap
@@ -73,9 +75,36 @@ constexpr TrianglePairs makeTrianglePairs() {
 }
 __device__ const TrianglePairs kTrianglePairs = makeTrianglePairs();
 
+// A site position as float, wrapped into a rectangular periodic box (unchanged otherwise): the frame of the chunk
+// boxes, in which the minimum-image distance between a point and a box bounds that to every point in the box.
+__device__ __forceinline__ float3 siteWrapped(const AtmConfig& C, double x, double y, double z) {
+    float3 p = make_float3((float)x, (float)y, (float)z);
+    if (C.periodic && !C.box.triclinic) {
+        p.x -= C.boxf.a[0] * floorf(p.x * C.boxf.inv[0]);
+        p.y -= C.boxf.b[1] * floorf(p.y * C.boxf.inv[1]);
+        p.z -= C.boxf.c[2] * floorf(p.z * C.boxf.inv[2]);
+    }
+    return p;
+}
+
+// Squared minimum-image distance from a point to a box (0 inside it), both in the wrapped frame.
+__device__ __forceinline__ float siteBoxDist2(const AtmConfig& C, float3 p, float4 c, float4 e) {
+    float dx = c.x - p.x, dy = c.y - p.y, dz = c.z - p.z;
+    if (C.periodic) {
+        dx -= C.boxf.a[0] * rintf(dx * C.boxf.inv[0]);
+        dy -= C.boxf.b[1] * rintf(dy * C.boxf.inv[1]);
+        dz -= C.boxf.c[2] * rintf(dz * C.boxf.inv[2]);
+    }
+    dx = fmaxf(fabsf(dx) - e.x, 0.0f);
+    dy = fmaxf(fabsf(dy) - e.y, 0.0f);
+    dz = fmaxf(fabsf(dz) - e.z, 0.0f);
+    return dx * dx + dy * dy + dz * dz;
+}
+
 __global__ void kSiteCentroids(AtmBuffers A, AtmConfig C, const double* pos) {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     bool moved = false;
+    float3 w = make_float3(INFINITY, INFINITY, INFINITY), wMax = make_float3(-INFINITY, -INFINITY, -INFINITY);
     if (s < C.numSites) {
         double c[3] = {0.0, 0.0, 0.0};
         const int b = A.siteOffsets[s], e = A.siteOffsets[s + 1];
@@ -93,8 +122,25 @@ __global__ void kSiteCentroids(AtmBuffers A, AtmConfig C, const double* pos) {
         }
         const double dx = c[0] - A.siteRef[3 * s], dy = c[1] - A.siteRef[3 * s + 1], dz = c[2] - A.siteRef[3 * s + 2];
         moved = (float)(dx * dx + dy * dy + dz * dz) > C.maxMove2;
+        w = siteWrapped(C, c[0], c[1], c[2]);
+        wMax = w;
     }
     if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(A.flag, 1);
+    if (A.chunkBox) {
+        // the box of this warp's 32 sites (blocks are whole warps, so a warp is one chunk)
+        const float lo[3] = {warpMinF(w.x), warpMinF(w.y), warpMinF(w.z)};
+        const float hi[3] = {warpMaxF(wMax.x), warpMaxF(wMax.y), warpMaxF(wMax.z)};
+        const int chunk = s >> 5;
+        if ((threadIdx.x & 31) == 0 && 32 * chunk < C.numSites) {
+            // the margin covers the float rounding of the wrapped positions
+            const float m = 1e-4f;
+            const bool usable = !(C.periodic && C.box.triclinic);
+            A.chunkBox[2 * chunk] = make_float4(0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1]), 0.5f * (lo[2] + hi[2]),
+                                                usable ? 1.0f : 0.0f);
+            A.chunkBox[2 * chunk + 1] = make_float4(0.5f * (hi[0] - lo[0]) + m, 0.5f * (hi[1] - lo[1]) + m,
+                                                    0.5f * (hi[2] - lo[2]) + m, 0.0f);
+        }
+    }
 }
 
 __device__ __forceinline__ void siteDelta(const AtmBuffers& A, const AtmConfig& C, int from, int to, double d[3]) {
@@ -104,7 +150,8 @@ __device__ __forceinline__ void siteDelta(const AtmBuffers& A, const AtmConfig& 
     if (C.periodic) minimumImage(d[0], d[1], d[2], C.box);
 }
 
-// One warp per site A scans the sites above it.  The list is in increasing site order.
+// One warp per site A scans the sites above it, 32-site chunk by chunk, skipping the chunks whose box is farther
+// than the list cutoff from A (when the centroid kernel wrote the chunk boxes).  The list is in increasing site order.
 __global__ void kSiteNeighbors(AtmBuffers A, AtmConfig C) {
     if (*(volatile int*)A.flag == 0) return;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -112,11 +159,17 @@ __global__ void kSiteNeighbors(AtmBuffers A, AtmConfig C) {
     if (warp >= C.numSites) return;
     const int a = warp;
     const int molA = A.molecule[a];
+    const float3 pa = siteWrapped(C, A.sitePos[3 * a], A.sitePos[3 * a + 1], A.sitePos[3 * a + 2]);
+    const float skip2 = C.listCutoff2 * (1.0f + 1e-4f);
     int count = 0;
-    for (int b0 = a + 1; b0 < C.numSites; b0 += 32) {
+    for (int b0 = (a + 1) & ~31; b0 < C.numSites; b0 += 32) {
+        if (A.chunkBox) {
+            const float4 c = A.chunkBox[2 * (b0 >> 5)];
+            if (c.w != 0.0f && siteBoxDist2(C, pa, c, A.chunkBox[2 * (b0 >> 5) + 1]) >= skip2) continue;
+        }
         const int b = b0 + lane;
         bool near = false;
-        if (b < C.numSites && A.molecule[b] != molA) {
+        if (b > a && b < C.numSites && A.molecule[b] != molA) {
             double d[3];
             siteDelta(A, C, a, b, d);
             near = (float)(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) < C.listCutoff2;

@@ -934,6 +934,7 @@ static int allocateAtm(ix_ctx* ctx) {
     A.siteParams = dParams;
     IX_TRY(deviceAlloc(ctx, "sitePos", 3 * (size_t)ns, &A.sitePos));
     IX_TRY(deviceAlloc(ctx, "siteRef", 3 * (size_t)ns, &A.siteRef));
+    IX_TRY(deviceAlloc(ctx, "siteChunkBox", 2 * (size_t)((ns + 31) / 32), &A.chunkBox));
     IX_TRY(deviceAlloc(ctx, "nbrCount", ns, &A.nbrCount));
     IX_TRY(deviceAlloc(ctx, "siteForce", 3 * (size_t)ns, &A.siteForce));
     {
