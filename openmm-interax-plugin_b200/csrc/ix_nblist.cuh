@@ -64,6 +64,9 @@ struct ListBuffers {
     int* blockTiles;            // nb + 1: exclusive scan of the tile counts, then the total
     int* tileJ;                 // tileCap x 32
     int* tileIBlock;            // tileCap
+    int* tileBucket;            // tileCap: each tile's candidate pairs / 32
+    int* tileOrder;             // tileCap: the tiles by decreasing candidate count, the pair kernel's schedule (null:
+                                // list order), so that the last tiles the warps take are short
     unsigned* tileMask;         // tileCap x 64: row masks (per i lane, bit = j slot), then column masks (per j lane)
     int* numTiles;              // tiles to evaluate (0 after an overflow)
     int* taskCounter;           // next tile of the pair kernel's dynamic schedule (zeroed before each launch)
@@ -505,7 +508,32 @@ __global__ void __launch_bounds__(kListThreads) kTileMasks(ListBuffers L, ListGe
         }
         L.tileMask[64LL * t + lane] = row;
         L.tileMask[64LL * t + 32 + lane] = column;
+        const unsigned pairs = __reduce_add_sync(0xffffffffu, (unsigned)__popc(column));
+        if (lane == 0 && L.tileBucket) L.tileBucket[t] = (int)(pairs >> 5);
     }
+}
+
+// The pair kernel's schedule: the tiles by decreasing candidate count (a counting sort over 33 buckets of 32 pairs, one
+// block).  The warps take tiles from a shared counter, so the kernel ends when the last tile taken ends; short tiles
+// last keep that tail short.  The order within a bucket follows the atomics and varies from build to build, which
+// changes no result: forces are summed in fixed point and energies go to each tile's own slot.
+__global__ void kTileOrder(ListBuffers L) {
+    if (!rebuildRequested(L)) return;
+    __shared__ int count[33], start[33];
+    const int n = *L.numTiles;
+    if (threadIdx.x < 33) count[threadIdx.x] = 0;
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) atomicAdd(&count[L.tileBucket[t]], 1);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int b = 32; b >= 0; b--) {
+            start[b] = run;
+            run += count[b];
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n; t += blockDim.x) L.tileOrder[atomicAdd(&start[L.tileBucket[t]], 1)] = t;
 }
 
 // The exclusive scan of the i-blocks' tile counts (one block of 1024 threads).  On overflow no tile is scheduled

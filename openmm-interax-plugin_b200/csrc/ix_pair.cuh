@@ -350,7 +350,7 @@ __global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, 
         if (lane == 0) task = atomicAdd(L.taskCounter, 1);
         task = __shfl_sync(0xffffffffu, task, 0);
         if (task >= numTasks) break;
-        const int t = P.taskTiles ? P.taskTiles[task] : task;
+        const int t = P.taskTiles ? P.taskTiles[task] : (L.tileOrder ? L.tileOrder[task] : task);
         const int I = L.tileIBlock[t];
         const int iBase = I * 32;
         const float4 center = L.bbox[2 * I];
