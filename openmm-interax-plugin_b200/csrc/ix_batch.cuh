@@ -98,7 +98,8 @@ struct ix_batch {
     PairTermConfig pairC{};
     AtmConfig atmC{};
     unsigned terms = 0;
-    bool lean = true, table = false;
+    bool lean = true, table = false, uniform = false;
+    unsigned gatesAll = 0, alchAny = 0;  // bit t: every particle has term t's gate; some particle is alchemical in t
     int pairGrid = 0, numTiles = 0, numSites = 0, numParticles = 0;
     int atmFastBlocks = 0, atmWideBlocks = 0;
     int* tileStart = nullptr;            // numSystems + 1
@@ -285,6 +286,21 @@ int buildBatchPairs(ix_batch* b, const std::vector<int>& blockStart, int nb) {
     }
     tileStart[S] = (int)tileI.size();
     b->numTiles = (int)tileI.size();
+    b->gatesAll = 7u;
+    b->alchAny = 0u;
+    for (int k = 0; k < np; k++) {
+        if (sortedAtom[k] < 0) continue;
+        for (int t = 0; t < 3; t++)
+            if (!(flags[k] & (kFlagGateDisp << t))) b->gatesAll &= ~(1u << t);
+        b->alchAny |= (unsigned)(flags[k] & 7);
+    }
+    // the pair kernel takes the tiles largest first (see kTileOrder), here ordered once on the host
+    std::vector<int> tileOrder(b->numTiles), tilePairs(b->numTiles, 0);
+    for (int t = 0; t < b->numTiles; t++) {
+        tileOrder[t] = t;
+        for (int i = 0; i < 32; i++) tilePairs[t] += __builtin_popcount(masks[64 * (size_t)t + i]);
+    }
+    std::stable_sort(tileOrder.begin(), tileOrder.end(), [&](int x, int y) { return tilePairs[x] > tilePairs[y]; });
     ListBuffers& L = b->L;
     L.n = n;
     L.nb = nb;
@@ -299,6 +315,7 @@ int buildBatchPairs(ix_batch* b, const std::vector<int>& blockStart, int nb) {
     IX_TRY(batchUpload(b, "tileJ", tileJ, &L.tileJ));
     IX_TRY(batchUpload(b, "tileIBlock", tileI, &L.tileIBlock));
     IX_TRY(batchUpload(b, "tileMask", masks, &L.tileMask));
+    if (b->numTiles > 0) IX_TRY(batchUpload(b, "tileOrder", tileOrder, &L.tileOrder));
     IX_TRY(batchUpload(b, "numTiles", std::vector<int>{b->numTiles}, &L.numTiles));
     IX_TRY(batchUpload(b, "taskCounter", std::vector<int>{0}, &L.taskCounter));
     IX_TRY(batchUpload(b, "tileStart", tileStart, &b->tileStart));
@@ -430,7 +447,9 @@ int enqueueBatch(ix_batch* b) {
     kBlockBounds<<<(L.nb * 32 + tpb - 1) / tpb, tpb, 0, st>>>(L, G);
     if (b->numTiles > 0) {
         const PairTermConfig& C = b->pairC;
-        if (b->lean && b->table) kPairTiles<true, true><<<b->pairGrid, 32 * kPairWarps, 0, st>>>(L, b->P, C);
+        if (b->uniform && b->table) kPairTiles<true, true, true><<<b->pairGrid, 32 * kPairWarps, 0, st>>>(L, b->P, C);
+        else if (b->uniform) kPairTiles<true, false, true><<<b->pairGrid, 32 * kPairWarps, 0, st>>>(L, b->P, C);
+        else if (b->lean && b->table) kPairTiles<true, true><<<b->pairGrid, 32 * kPairWarps, 0, st>>>(L, b->P, C);
         else if (b->lean) kPairTiles<true, false><<<b->pairGrid, 32 * kPairWarps, 0, st>>>(L, b->P, C);
         else if (b->table) kPairTiles<false, true><<<b->pairGrid, 32 * kPairWarps, 0, st>>>(L, b->P, C);
         else kPairTiles<false, false><<<b->pairGrid, 32 * kPairWarps, 0, st>>>(L, b->P, C);
@@ -506,6 +525,12 @@ int buildBatch(ix_batch* b) {
     b->table = b->P.coef != nullptr;
     for (int t = 1; t < 3; t++)
         if ((b->terms >> t) & 1u) b->table = b->table && b->pairC.overlapMethod[t] == 0;
+    // every pair of every term evaluated unscaled: the instantiation without per-pair gate and scale tests
+    b->uniform = b->lean;
+    for (int t = 0; t < 3; t++)
+        if ((b->terms >> t) & 1u)
+            b->uniform = b->uniform && ((b->gatesAll >> t) & 1u) &&
+                         (!((b->alchAny >> t) & 1u) || b->pairC.lambda[t] == 1.0f);
     int perSM = 0;
     if (b->lean && b->table) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kPairTiles<true, true>, 32 * kPairWarps, 0);
     else if (b->lean) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kPairTiles<true, false>, 32 * kPairWarps, 0);

@@ -235,7 +235,7 @@ struct ix_ctx {
     bool pairDirty = true;               // parameters must be re-uploaded
     unsigned pairGatesAll = 0;           // bit t: every particle takes part in pair term t
     unsigned pairAlchAny = 0;            // bit t: some particle is alchemical in pair term t
-    int pairShareOverlap = 0;            // exchange and short-range widths agree for every particle
+    mutable int pairShareOverlap = -1;   // exchange and short-range widths agree for every particle (-1: not known)
     bool pairAllocated = false;
 
     // three-body force
@@ -524,6 +524,7 @@ static int addPairForce(ix_ctx* ctx, int t, const ix_pair_settings* s, const dou
     T.alch.assign(alch, alch + ctx->n);
     T.anyAlch = std::any_of(T.alch.begin(), T.alch.end(), [](unsigned char a) { return a != 0; });
     ctx->pairDirty = true;
+    ctx->pairShareOverlap = -1;
     bumpVersion(ctx);
     ctx->pairAllocated = false;
     return IX_OK;
@@ -708,12 +709,6 @@ static int uploadPairParams(ix_ctx* ctx) {
         for (int t = 0; t < 3; t++)
             if (!(flags[i] & (kFlagGateDisp << t))) ctx->pairGatesAll &= ~(1u << t);
         ctx->pairAlchAny |= (unsigned)(flags[i] & 7);
-    }
-    ctx->pairShareOverlap = 0;
-    if (ctx->term[1].present && ctx->term[2].present) {
-        bool same = true;
-        for (int i = 0; i < n && same; i++) same = ctx->term[1].params[2 * i + 1] == ctx->term[2].params[3 * i + 2];
-        ctx->pairShareOverlap = same;
     }
     IX_TRY(stageCopy(ctx, ctx->dP0o, p0.data(), n * sizeof(float4)));
     IX_TRY(stageCopy(ctx, ctx->dP1o, p1.data(), n * sizeof(float4)));
@@ -1239,6 +1234,11 @@ static PairTermConfig pairConfig(const ix_ctx* ctx, unsigned terms) {
     }
     C.twoBeta = (float)(2.0 * ctx->term[0].dampingScale);
     // the exchange and short-range terms share one overlap when their widths and methods agree for every particle
+    if (ctx->pairShareOverlap < 0) {
+        bool same = ctx->term[1].present && ctx->term[2].present;
+        for (int i = 0; i < ctx->n && same; i++) same = ctx->term[1].params[2 * i + 1] == ctx->term[2].params[3 * i + 2];
+        ctx->pairShareOverlap = same;
+    }
     C.shareOverlap = ctx->pairShareOverlap && ctx->term[1].overlapMethod == ctx->term[2].overlapMethod;
     C.useCutoff = ctx->method != IX_NO_CUTOFF;
     C.periodic = ctx->method == IX_CUTOFF_PERIODIC;
@@ -1845,6 +1845,7 @@ static int updatePair(ix_ctx* ctx, int t, const double* params, int stride) {
     if (!params) return fail(ctx, IX_ERR_INVALID, "%s: null argument", kTermNames[t]);
     ctx->term[t].params.assign(params, params + (size_t)ctx->n * stride);
     ctx->pairDirty = true;
+    ctx->pairShareOverlap = -1;
     bumpVersion(ctx);
     return IX_OK;
 }
