@@ -832,6 +832,7 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
     IX_TRY(deviceAlloc(ctx, "tileIBlock", L.tileCap, &L.tileIBlock));
     IX_TRY(deviceAlloc(ctx, "tileBucket", L.tileCap, &L.tileBucket));
     IX_TRY(deviceAlloc(ctx, "tileOrder", L.tileCap, &L.tileOrder));
+    IX_TRY(deviceAlloc(ctx, "bucketCount", 33, &L.bucketCount));
     IX_TRY(deviceAlloc(ctx, "tileMask", 64 * (size_t)L.tileCap, &L.tileMask));
     IX_TRY(deviceAlloc(ctx, "numTiles", 1, &L.numTiles));
     IX_TRY(deviceAlloc(ctx, "taskCounter", 1, &L.taskCounter));
@@ -1424,7 +1425,7 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
             kScanTiles<<<1, 1024, 0, s>>>(L);
             kListTiles<1><<<L.nb, kListThreads, 0, s>>>(L, ctx->G);
             kTileMasks<<<ctx->numSMs * 8, kListThreads, 0, s>>>(L, ctx->G);
-            kTileOrder<<<1, 1024, 0, s>>>(L);
+            kTileOrder<<<ctx->numSMs, 256, 0, s>>>(L);
             kClearFlag<<<1, 1, 0, s>>>(L.flag);
             ctx->launches += ctx->G.periodic ? 14 : 15;
             return IX_OK;

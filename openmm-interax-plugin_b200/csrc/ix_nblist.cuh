@@ -64,7 +64,8 @@ struct ListBuffers {
     int* blockTiles;            // nb + 1: exclusive scan of the tile counts, then the total
     int* tileJ;                 // tileCap x 32
     int* tileIBlock;            // tileCap
-    int* tileBucket;            // tileCap: each tile's candidate pairs / 32
+    int* tileBucket;            // tileCap: each tile's candidate pairs / 32 (bits 0..5) and its rank in that bucket
+    int* bucketCount;           // 33: tiles per bucket
     int* tileOrder;             // tileCap: the tiles by decreasing candidate count, the pair kernel's schedule (null:
                                 // list order), so that the last tiles the warps take are short
     unsigned* tileMask;         // tileCap x 64: row masks (per i lane, bit = j slot), then column masks (per j lane)
@@ -509,31 +510,34 @@ __global__ void __launch_bounds__(kListThreads) kTileMasks(ListBuffers L, ListGe
         L.tileMask[64LL * t + lane] = row;
         L.tileMask[64LL * t + 32 + lane] = column;
         const unsigned pairs = __reduce_add_sync(0xffffffffu, (unsigned)__popc(column));
-        if (lane == 0 && L.tileBucket) L.tileBucket[t] = (int)(pairs >> 5);
+        if (lane == 0 && L.tileBucket) {
+            const int b = (int)(pairs >> 5);
+            L.tileBucket[t] = (int)((unsigned)b | ((unsigned)atomicAdd(L.bucketCount + b, 1) << 6));
+        }
     }
 }
 
-// The pair kernel's schedule: the tiles by decreasing candidate count (a counting sort over 33 buckets of 32 pairs, one
-// block).  The warps take tiles from a shared counter, so the kernel ends when the last tile taken ends; short tiles
+// The pair kernel's schedule: the tiles by decreasing candidate count (a counting sort over 33 buckets of 32 pairs:
+// the mask kernel counted each bucket and gave each tile its rank in it; here each tile goes to its bucket's start plus
+// its rank).  The warps take tiles from a shared counter, so the kernel ends when the last tile taken ends; short tiles
 // last keep that tail short.  The order within a bucket follows the atomics and varies from build to build, which
 // changes no result: forces are summed in fixed point and energies go to each tile's own slot.
 __global__ void kTileOrder(ListBuffers L) {
     if (!rebuildRequested(L)) return;
-    __shared__ int count[33], start[33];
-    const int n = *L.numTiles;
-    if (threadIdx.x < 33) count[threadIdx.x] = 0;
-    __syncthreads();
-    for (int t = threadIdx.x; t < n; t += blockDim.x) atomicAdd(&count[L.tileBucket[t]], 1);
-    __syncthreads();
+    __shared__ int start[33];
     if (threadIdx.x == 0) {
         int run = 0;
         for (int b = 32; b >= 0; b--) {
             start[b] = run;
-            run += count[b];
+            run += L.bucketCount[b];
         }
     }
     __syncthreads();
-    for (int t = threadIdx.x; t < n; t += blockDim.x) L.tileOrder[atomicAdd(&start[L.tileBucket[t]], 1)] = t;
+    const int n = *L.numTiles;
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+        const unsigned v = (unsigned)L.tileBucket[t];
+        L.tileOrder[start[v & 63u] + (int)(v >> 6)] = t;
+    }
 }
 
 // The exclusive scan of the i-blocks' tile counts (one block of 1024 threads).  On overflow no tile is scheduled
@@ -564,6 +568,7 @@ __global__ void kScanTiles(ListBuffers L) {
         L.blockTiles[c] = run;
         run += k;
     }
+    if (t < 33 && L.bucketCount) L.bucketCount[t] = 0;   // for the mask kernel's tile counts
     if (t == 1023) {
         const int total = partial[1023];
         L.blockTiles[L.nb] = total;
