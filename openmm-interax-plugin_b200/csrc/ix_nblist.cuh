@@ -50,7 +50,7 @@ struct ListBuffers {
     int* cellStart;             // numCells + 1
     int* cellFill;              // numCells
     int* order;                 // n: particles in cell order (within a cell by index after the per-cell sort)
-    const int* cellRank;        // dense cell index -> Morton rank
+    const int* cellRank;        // dense cell index -> rank along the Hilbert curve
     int numCells;
     // sorted particles
     int* sortedAtom;            // np: original index, -1 for padding
