@@ -1370,11 +1370,11 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         C.invCentroidRadius = ctx->atmCentroidRadius > 0 ? (float)(1.0 / ctx->atmCentroidRadius) : 0.0f;
         C.maxMove2 = 0.25f * kSiteSkin * kSiteSkin;
         const int tpb = 256;
-        const int gS = (C.numSites + tpb - 1) / tpb;
+        const int gS = (C.numSites + 63) / 64;   // 64-thread blocks, so that a few thousand sites reach every SM
         // the wide kernel's energy slots start at zero (it runs only while some list is long)
         C.zeroSlots = ctx->atmGridBlocks * kAtmWarps;
         C.zeroOffset = ctx->atmFastBlocks * kAtmFastWarps;
-        kSiteCentroids<<<gS, tpb, 0, sa>>>(A, C, ctx->dPos);
+        kSiteCentroids<<<gS, 64, 0, sa>>>(A, C, ctx->dPos);
         // site list rebuild when the centroid kernel set the flag: these kernels return at once otherwise (three
         // short launches cost less than a conditional graph node); the long-list flag is recomputed with the lists
         kClearFlagIf<<<1, 1, 0, sa>>>(A.flag + 2, A.flag);
@@ -2156,7 +2156,8 @@ int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt) {
             return IX_OK;
         }
         if (terms & 7u)
-            kStepStart<<<(n + 255) / 256, 256, 0, ctx->stream>>>(ctx->L, ctx->dPos, dt, ctx->dInvMass, ctx->dOutForces,
+            // 128-thread blocks: a latency-bound gather by particle, spread over every SM
+            kStepStart<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->L, ctx->dPos, dt, ctx->dInvMass, ctx->dOutForces,
                                                                 ctx->dVel, 0.25f * kPairSkin * kPairSkin);
         else
             kVerletFirstHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos);
