@@ -638,7 +638,7 @@ static int buildClassTable(ix_ctx* ctx, std::vector<int>& flags) {
     std::vector<PairCoef> table;
     const int T = classTableHost(sys, fl, table);
     if (T == 0) return IX_OK;
-    PairCoef* dTable;
+    PairCoef* dTable = nullptr;
     IX_TRY(deviceAlloc(ctx, "classTable", table.size(), &dTable));
     IX_TRY(stageCopy(ctx, dTable, table.data(), table.size() * sizeof(PairCoef)));
     ctx->P.coef = dTable;
@@ -855,8 +855,8 @@ static int allocatePair(ix_ctx* ctx, long long tileCap) {
         range[i] = part[i].empty() ? make_int2(1, 0) : make_int2(part[i].front(), part[i].back());
     }
     start[n] = (int)list.size();
-    int *dStart, *dList;
-    int2* dRange;
+    int *dStart = nullptr, *dList = nullptr;
+    int2* dRange = nullptr;
     IX_TRY(deviceAlloc(ctx, "exclStart", n + 1, &dStart));
     IX_TRY(deviceAlloc(ctx, "exclList", std::max<size_t>(list.size(), 1), &dList));
     IX_TRY(deviceAlloc(ctx, "exclRange", n, &dRange));
