@@ -38,7 +38,7 @@ F_PAIR = 612.4
 F_TRIPLE = 151.0
 # DRAM bytes (read + write) of one pair-kernel launch on this workload, from one ncu capture of an MD-step launch
 # (dram__bytes_read.sum + dram__bytes_write.sum); the kernel is FP32-issue bound, the traffic is reported beside it
-PAIR_TRAFFIC_BYTES = 12737280
+PAIR_TRAFFIC_BYTES = 10082304
 METRIC = "interactions/s"
 WORKLOAD = "water box 24,000 atoms (8,000 rigid-geometry waters, 6.208 nm periodic, cutoff 1.0 nm) + ATM on " \
            "8,000 molecular sites (cutoff 0.6 nm); velocity-Verlet 1 fs"
