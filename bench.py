@@ -66,16 +66,42 @@ def parse():
 
 
 def dist_init(args):
-    """One process per GPU under torchrun; returns (rank, world)."""
+    """One process per GPU under torchrun (NCCL); on a host without GPUs (the CPU tests of the rank logic) the ranks
+    use gloo.  Returns (rank, world)."""
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if world > 1:
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        backend = "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+            backend = "nccl"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world
+
+
+def _rank_reduce(x, world, op):
+    if world == 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device="cuda" if torch.cuda.is_available() else "cpu")
+    dist.all_reduce(t, op=op)
+    return float(t.item())
+
+
+def rank_max(x, world):
+    """x's maximum over the ranks: a timed region lasts as long as its slowest rank."""
+    import torch.distributed as dist
+    return _rank_reduce(x, world, dist.ReduceOp.MAX)
+
+
+def rank_sum(x, world):
+    """x summed over the ranks (work done by the whole job)."""
+    import torch.distributed as dist
+    return _rank_reduce(x, world, dist.ReduceOp.SUM)
 
 
 def build_system(args, rank):
@@ -262,14 +288,8 @@ def run_ours(args, rank, world):
     ctx._check(L.ix_set_profiling(ctx._ctx, 2))
     kernel_rows = np.array([md_step() for _ in range(args.warmup + args.steps)][args.warmup:])
     ctx._check(L.ix_set_profiling(ctx._ctx, 0))
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([step_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms = float(t.item())
-        c = torch.tensor([interactions], dtype=torch.float64, device="cuda")
-        dist.all_reduce(c, op=dist.ReduceOp.SUM)
-        interactions = float(c.item())
+    step_ms = rank_max(step_ms, world)
+    interactions = rank_sum(interactions, world)
     value = interactions / (step_ms * 1e-3)
     ms_per_step = step_ms / args.steps
 
@@ -388,11 +408,7 @@ def run_clusters(args, rank, world, num_clusters=4096, plain_sample=128):
     with ClockSampler(device) as clocks:
         ms = [device_step() for _ in range(args.steps)]
     step_ms = float(np.sum(ms))
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([step_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms = float(t.item())
+    step_ms = rank_max(step_ms, world)
     value = world * num_clusters * args.steps / (step_ms * 1e-3)
     # e2e: host positions in, host forces and energies out, per step
     e2e_t = 0.0
@@ -493,11 +509,7 @@ def run_lambda(args, rank, world, num_windows=16, num_alchemical=30):
     launches1 = ctypes.c_longlong()
     ctx._check(L.ix_get_launch_count(ctx._ctx, ctypes.byref(launches1)))
     step_ms = float(np.sum(ms))
-    if world > 1:
-        import torch.distributed as dist
-        t = torch.tensor([step_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        step_ms = float(t.item())
+    step_ms = rank_max(step_ms, world)
     value = world * num_windows * args.steps / (step_ms * 1e-3)
     # e2e: host positions in (pinned), every window's energies and forces out to host memory, per step
     hpos = torch.from_numpy(np.ascontiguousarray(pos)).pin_memory()
