@@ -709,10 +709,14 @@ def main():
             run_reference(args, rank, world)
         else:
             run_ours(args, rank, world)
+        if world > 1:
+            # the ranks leave together only when every rank succeeded; a failing rank skips this barrier, and the
+            # others' next collective ends with the process group's timeout instead of hiding its traceback
+            import torch.distributed as dist
+            dist.barrier()
     finally:
         if world > 1:
             import torch.distributed as dist
-            dist.barrier()
             dist.destroy_process_group()
 
 

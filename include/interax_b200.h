@@ -115,6 +115,16 @@ int ix_update_short_range(ix_ctx* ctx, const double* params, int overlap_method)
 int ix_update_three_body(ix_ctx* ctx, const double* site_params, double scale_factor, double damping_scale,
                          double centroid_damping_radius);
 
+/* Long-range dispersion correction coefficients of a dispersion force, as
+ * InteraxDispersionForceImpl::calcLongRangeCorrection (openmmapi/src/InteraxDispersionForceImpl.cpp:86-149): the
+ * correction energy is (coefficient + lambda alchemical_coefficient) / V.  Both are 0 unless the method is
+ * IX_CUTOFF_PERIODIC and use_long_range_correction is set.  params and is_alchemical as in ix_add_dispersion.  Host
+ * only (FP64); needs no GPU. */
+int ix_dispersion_long_range_correction(int num_particles, const double* params, const uint8_t* is_alchemical,
+                                        const ix_pair_settings* settings, double damping_scale,
+                                        int use_long_range_correction, double* coefficient,
+                                        double* alchemical_coefficient);
+
 /* Set a context parameter (the alchemical parameters; ContextImpl::setParameter in OpenMM).  Parameters that no
  * force uses are accepted and ignored. */
 int ix_set_parameter(ix_ctx* ctx, const char* name, double value);
@@ -131,19 +141,57 @@ int ix_compute(ix_ctx* ctx, int groups, int include_forces, int include_energy, 
                double* energy, double* forces);
 
 /* Device-resident variant for integration into a GPU engine: evaluate on the context's stream using the positions
- * already on the device, and ADD the forces to d_force_fixed, an int64 fixed-point buffer (scale 2^32,
- * layout x[0..stride), y[stride..2 stride), z[...]) as OpenMM's CUDA platform keeps them
+ * already on the device (ix_set_positions), and ADD the forces to d_force_fixed, an int64 fixed-point buffer (scale
+ * 2^32, layout x[0..stride), y[stride..2 stride), z[...]) as OpenMM's CUDA platform keeps them
  * (platforms/common/src/kernels/interaxThreeBody.cc:644-652), in original particle order.  d_term_energies
  * (device, IX_NUM_TERMS doubles, may be NULL) receives the term energies.  Nothing is copied to the host and the
- * call does not synchronize. */
+ * call does not synchronize; its list-overflow status is read with ix_get_device_status. */
 int ix_compute_device(ix_ctx* ctx, int groups, long long* d_force_fixed, int force_stride,
                       double* d_term_energies);
 
 /* Device positions in and device forces out, for callers that keep their state on the GPU: d_positions is
  * num_particles x 3 doubles on the device (copied device-to-device on the context's stream), d_forces receives
- * num_particles x 3 doubles (overwritten) and d_term_energies IX_NUM_TERMS doubles.  Does not synchronize. */
+ * num_particles x 3 doubles (overwritten) and d_term_energies IX_NUM_TERMS doubles.  `box` (host, 9 doubles, may be
+ * NULL to keep the previous box).  Does not synchronize; status as ix_compute_device. */
 int ix_compute_device_f64(ix_ctx* ctx, int groups, const double* d_positions, const double* box,
                           double* d_forces, double* d_term_energies);
+
+/* Position formats of ix_compute_device_posq: OpenMM's posq array in single precision (float4 x, y, z, charge), in
+ * mixed precision (float4 posq plus the float4 posqCorrection that holds the rounding, x = posq.x + correction.x) and
+ * in double precision (double4). */
+#define IX_POSQ_FLOAT4 0
+#define IX_POSQ_FLOAT4_CORRECTED 1
+#define IX_POSQ_DOUBLE4 2
+
+/* The drop-in for OpenMM's CUDA platform: what CalcInterax*ForceKernel::execute does there
+ * (platforms/common/src/CommonInteraxKernels.cpp:251-259 for the pair forces, 631-646 for the three-body force), with
+ * positions and forces in the platform's own device arrays and nothing copied through the host.
+ *   d_posq, d_posq_correction: the platform's position array(s) in its slot order (posq_format above); slot k holds
+ *       particle d_atom_index[k] (the platform's atom index array; NULL: slot k holds particle k).
+ *   box: host, 9 doubles, NULL to keep the previous box (the platform's periodic box vectors).
+ *   d_force_fixed: the platform's int64 force buffer (scale 2^32, x/y/z rows of force_stride, the padded atom count):
+ *       the forces are ADDED at each particle's slot.
+ *   d_energy: a device double to which the total energy of the selected terms is ADDED (may be NULL).
+ *   d_status: a device int (may be NULL) written with the list status of this call: bit 0 = the pair list
+ *       overflowed and the forces and energy are incomplete; bit 1 = a three-body list overflowed (the results are
+ *       complete).  After bit 0, call again: the next call (or ix_get_device_status) grows the list first.
+ * Asynchronous on the context's stream (order the caller's own work with ix_get_stream).  The box, the parameter
+ * values and the force-group mask are read on the host at each call. */
+int ix_compute_device_posq(ix_ctx* ctx, int groups, int posq_format, const void* d_posq,
+                           const void* d_posq_correction, const int32_t* d_atom_index, const double* box,
+                           long long* d_force_fixed, int force_stride, double* d_energy, int* d_status);
+
+/* Wait for the last device call of `ctx` (ix_compute_device, ix_compute_device_f64, ix_compute_device_posq) and
+ * return its list status (the bits of d_status above); lists that overflowed are grown, so a repeated call is
+ * complete. */
+int ix_get_device_status(ix_ctx* ctx, int* status);
+
+/* Capacities of the neighbor lists at their next allocation: pair_tiles tiles of the pair list and site_neighbors
+ * entries per site of the three-body list (0: estimated from the density, the default).  Lists grow when they
+ * overflow; a small capacity forces that path (the tests use it).  ix_get_list_stats returns the current capacities
+ * and how many times MD steps were rerun after a pair-list overflow.  No counterpart in the reference. */
+int ix_set_list_capacity(ix_ctx* ctx, long long pair_tiles, int site_neighbors);
+int ix_get_list_stats(ix_ctx* ctx, long long* pair_tiles, int* site_neighbors, long long* md_reruns);
 
 /* Counts of the last evaluation: interacting pairs (non-excluded, within the cutoff, gate true, counted once) and
  * interacting triples.  Counting costs an extra reduction, so it is done only after ix_set_counting(ctx, 1). */
@@ -159,8 +207,9 @@ int ix_md_run(ix_ctx* ctx, int num_steps, double dt, double* positions, double* 
 
 /* The same split in two: ix_md_steps_async enqueues `num_steps` steps on the context's stream and returns at once
  * (ix_md_run or ix_md_set_masses plus a first ix_md_run must have set the masses and velocities); ix_md_finish
- * synchronizes, checks the neighbor lists (an overflow during the steps makes it return IX_ERR_STATE after growing
- * them: the steps must be rerun) and copies the state out (any pointer may be NULL). */
+ * synchronizes, checks the neighbor lists and copies the state out (any pointer may be NULL).  When the pair list
+ * overflowed during the steps, ix_md_finish grows it, restores the state saved before the first unfinished
+ * ix_md_steps_async and runs the steps again, so the trajectory is the one a large enough list gives. */
 int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt);
 int ix_md_finish(ix_ctx* ctx, double* positions, double* velocities, double* energy);
 
@@ -210,14 +259,18 @@ int ix_measure_fp32_peak(int device, double* tflops);
  * their own pool, and step loops that must not allocate.  All working memory is one fixed file-scope __device__
  * array (about 2.7 MB on every GPU that loads the library, held until the process exits) that every call shares:
  * calls that overlap on the GPU race on it, so the caller must serialize them (one stream per device, or an event
- * between them).  Limits: 16384 particles, 4096 sites, 128 sites above any site within the cutoff (more are dropped
- * and reported by ix_three_body_noalloc_overflow); larger inputs are rejected with IX_ERR_INVALID.
+ * between them).  Limits: 16384 particles and 4096 sites (larger inputs are rejected with IX_ERR_INVALID); a site
+ * with more than 128 sites above it within the cutoff does not fit its neighbor list and is evaluated by scanning
+ * every later site instead (slower, same result), which ix_three_body_noalloc_overflow reports.
  * Inputs and outputs are device pointers on the current CUDA device: d_positions (num_particles x 3 doubles), the
  * sites as in ix_add_three_body (site particle indices outside [0, num_particles) are ignored), d_forces
  * (num_particles x 3 doubles, overwritten with the three-body forces) and d_energy (one double).  `box` is a host
- * pointer (9 doubles, may be NULL when not periodic) and `stream` a cudaStream_t (NULL: the default stream).  The
- * first call on a device looks up the array's device address (cudaGetSymbolAddress) once; make that first call
- * before any stream capture.  The call is asynchronous on `stream`. */
+ * pointer (9 doubles, may be NULL when not periodic) and `stream` a cudaStream_t (NULL: the default stream).  The box
+ * and the scalar arguments (cutoff, lambda, ...) are passed to the kernels by value when the call is made: a call
+ * captured into a CUDA graph keeps them, and a graph replayed after the box or lambda changed uses the old values,
+ * so capture it again after such a change.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) once and keeps it for the life of the process; make that first call before any stream
+ * capture, and make no call after a cudaDeviceReset of that device.  The call is asynchronous on `stream`. */
 int ix_three_body_noalloc(int num_particles, const double* d_positions, const double* box, int num_sites,
                           const int32_t* d_site_offsets, const int32_t* d_site_particles,
                           const double* d_site_params, const int32_t* d_molecule, const uint8_t* d_is_alchemical,
@@ -225,7 +278,9 @@ int ix_three_body_noalloc(int num_particles, const double* d_positions, const do
                           double centroid_damping_radius, int periodic, double lambda, double* d_forces,
                           double* d_energy, void* stream);
 
-/* Whether the last ix_three_body_noalloc call on the current device dropped neighbors (synchronizes the device). */
+/* Whether a site of the last ix_three_body_noalloc call on the current device had more neighbors than its list holds
+ * (its triples were found by a full scan, so the results are complete).  Waits for the whole device
+ * (cudaDeviceSynchronize), so that the flag of a call made on any stream has been written. */
 int ix_three_body_noalloc_overflow(int* overflow);
 
 /* Library version string. */

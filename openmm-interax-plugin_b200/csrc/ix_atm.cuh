@@ -12,7 +12,9 @@
 //                        lowest) and evaluated in float; the forces on B and C of each pair are stored and gathered
 //                        per staged neighbor in a fixed order (no atomics)
 //   kTriplesWide         the same for the rare sites with longer lists (chunked beyond kAtmMaxStaged within the
-//                        cutoff, so any length), with the B and C forces accumulated by shared-memory atomics
+//                        cutoff, so any length), with the B and C forces accumulated by shared-memory atomics; a
+//                        site whose list overflowed its capacity scans every later site instead, so an overflow
+//                        never drops a triple
 //   kSpreadSiteForces    the site forces, shared equally among each site's particles, into the particle forces
 #pragma once
 
@@ -182,10 +184,12 @@ __global__ void kSiteNeighbors(AtmBuffers A, AtmConfig C) {
         count += __popc(bal);
     }
     if (lane == 0) {
-        A.nbrCount[a] = min(count, A.cap);
+        // the full count: a site whose list overflowed its capacity is found by the wide triple kernel, which then
+        // scans every later site instead of reading the list
+        A.nbrCount[a] = count;
         if (count > A.cap) atomicOr(A.flag + 1, 1);
-        // flag[2]: some list is longer than the fast triple kernel takes (cleared before each build)
-        if (count > kAtmFast) atomicOr(A.flag + 2, 1);
+        // flag[2]: some site needs the wide triple kernel (cleared before each build)
+        if (count > kAtmFast || count > A.cap) atomicOr(A.flag + 2, 1);
     }
     for (int d = 0; d < 3; d++)
         if (lane == 0) A.siteRef[3 * a + d] = A.sitePos[3 * a + d];
@@ -334,6 +338,33 @@ __device__ __forceinline__ int stageTripleNeighbors(const AtmBuffers& A, const A
     return m;
 }
 
+// The same for a site whose list overflowed its capacity: every later site of another molecule is tested against the
+// cutoff, which gives the list's neighbors within the cutoff in the same (increasing) order, so the triples and their
+// evaluation order are those of a list that fitted.  The reference falls back the same way
+// (platforms/common/src/kernels/interaxThreeBody.cc:111-112, 437-438).
+template <class Store>
+__device__ __forceinline__ int stageTripleNeighborsScan(const AtmBuffers& A, const AtmConfig& C, int a, int lane,
+                                                        int first, int capacity, Store store) {
+    const int molA = A.molecule[a];
+    int m = 0;
+    for (int b0 = a + 1; b0 < C.numSites; b0 += 32) {
+        const int b = b0 + lane;
+        bool in = false;
+        double d[3];
+        if (b < C.numSites && A.molecule[b] != molA) {
+            siteDelta(A, C, a, b, d);
+            in = (float)(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) < C.cutoff2;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, in);
+        if (in) {
+            const int slot = m + __popc(bal & laneMaskLt()) - first;
+            if (slot >= 0 && slot < capacity) store(slot, b, (float)d[0], (float)d[1], (float)d[2]);
+        }
+        m += __popc(bal);
+    }
+    return m;
+}
+
 struct AtmFastStorage {
     float4 pos[kAtmFast];        // displacement from A; w holds the molecule (int bits)
     float4 params[kAtmFast];
@@ -354,7 +385,7 @@ __global__ void __launch_bounds__(32 * kAtmFastWarps, 7) kTriplesFast(AtmBuffers
     unsigned long long triples = 0;
     for (int a = warp; a < C.numSites; a += gridDim.x * kAtmFastWarps) {
         const int n = A.nbrCount[a];
-        if (n > kAtmFast) continue;      // the wide kernel takes this site
+        if (n > kAtmFast || n > A.cap) continue;      // the wide kernel takes this site
         const float4 pa = A.siteParams[a];
         __syncwarp();
         const int m = stageTripleNeighbors(A, C, a, n, lane, 0, kAtmFast,
@@ -473,22 +504,24 @@ __global__ void __launch_bounds__(32 * kAtmWarps) kTriplesWide(AtmBuffers A, Atm
     unsigned long long triples = 0;
     for (int a = blockIdx.x * kAtmWarps + (threadIdx.x >> 5); a < C.numSites; a += gridDim.x * kAtmWarps) {
         const int n = A.nbrCount[a];
-        if (n <= kAtmFast) continue;     // the fast kernel takes this site
+        if (n <= kAtmFast && n <= A.cap) continue;     // the fast kernel takes this site
         const float4 pa = A.siteParams[a];
+        const bool scan = n > A.cap;                   // the list overflowed: scan every later site
         auto stage = [&](int first, int base, int capacity) {
-            return stageTripleNeighbors(A, C, a, n, lane, first, capacity,
-                                        [&](int slot, int b, float x, float y, float z) {
-                                            const int k = base + slot;
-                                            S.dx[k] = x;
-                                            S.dy[k] = y;
-                                            S.dz[k] = z;
-                                            S.params[k] = A.siteParams[b];
-                                            S.mol[k] = A.molecule[b];
-                                            S.site[k] = b;
-                                            S.fx[k] = 0.0f;
-                                            S.fy[k] = 0.0f;
-                                            S.fz[k] = 0.0f;
-                                        });
+            auto store = [&](int slot, int b, float x, float y, float z) {
+                const int k = base + slot;
+                S.dx[k] = x;
+                S.dy[k] = y;
+                S.dz[k] = z;
+                S.params[k] = A.siteParams[b];
+                S.mol[k] = A.molecule[b];
+                S.site[k] = b;
+                S.fx[k] = 0.0f;
+                S.fy[k] = 0.0f;
+                S.fz[k] = 0.0f;
+            };
+            return scan ? stageTripleNeighborsScan(A, C, a, lane, first, capacity, store)
+                        : stageTripleNeighbors(A, C, a, n, lane, first, capacity, store);
         };
         float fax = 0.0f, fay = 0.0f, faz = 0.0f;
         auto pair = [&](int b, int c) {

@@ -186,11 +186,17 @@ struct GraphKey {
     const void* out0 = nullptr;
     const void* out1 = nullptr;
     const void* out2 = nullptr;
+    const void* out3 = nullptr;
+    const void* in0 = nullptr;           // device inputs read by a captured gather (positions in a caller's layout)
+    const void* in1 = nullptr;
+    const void* in2 = nullptr;
+    int format = 0;
     int stride = 0;
     double dt = 0.0;
     double param = 0.0;                  // value of the window parameter a window graph was captured with
     bool operator==(const GraphKey& o) const {
-        return terms == o.terms && out0 == o.out0 && out1 == o.out1 && out2 == o.out2 && stride == o.stride &&
+        return terms == o.terms && out0 == o.out0 && out1 == o.out1 && out2 == o.out2 && out3 == o.out3 &&
+               in0 == o.in0 && in1 == o.in1 && in2 == o.in2 && format == o.format && stride == o.stride &&
                dt == o.dt && std::memcmp(&param, &o.param, sizeof(param)) == 0;
     }
 };
@@ -237,6 +243,7 @@ struct ix_ctx {
     unsigned pairAlchAny = 0;            // bit t: some particle is alchemical in pair term t
     mutable int pairShareOverlap = -1;   // exchange and short-range widths agree for every particle (-1: not known)
     bool pairAllocated = false;
+    long long tileCapRequest = 0;        // ix_set_list_capacity: tile capacity of the next allocation (0: estimated)
 
     // three-body force
     bool atmPresent = false;
@@ -287,6 +294,19 @@ struct ix_ctx {
     double* dInvMass = nullptr;
     bool haveMasses = false;
     bool mdForcesValid = false;          // dOutForces holds all-group forces of the current positions
+    // the state before the enqueued steps not yet finished (positions, velocities, forces: 3n each; energies: 4), so
+    // that steps run with an overflowed pair list are rerun from it after the list has grown
+    double* dMdSave = nullptr;
+    bool mdRollback = true;              // a server's contexts rerun a whole request instead
+    long long mdReruns = 0;              // steps rerun after an overflow (ix_get_list_stats)
+    bool mdSavedForcesValid = false;
+    std::vector<std::pair<int, double>> mdPending;   // steps and dt of each ix_md_steps_async since the save
+    // device entry points: the flags of the last call, copied to pinned memory, and the event after the copy
+    unsigned char* deviceStatus = nullptr;
+    cudaEvent_t evStatus = nullptr;
+    bool statusPending = false;
+    int lastDeviceStatus = 0;
+    int* dAddSlot = nullptr;             // slot in the caller's force buffer of each particle (ix_compute_device_posq)
     // optional CUDA-event timing of the pair and triple kernels (ix_set_profiling)
     bool profiling = false;
     bool serialize = false;              // profiling level 2: the three-body chain runs after the pair chain
@@ -297,7 +317,7 @@ struct ix_ctx {
     // state that a captured launch depends on (parameters, box, buffers, settings) bumps the version
     bool useGraphs = true;
     unsigned long long version = 1;
-    LaunchGraph graphCompute, graphDevice, graphMd;
+    LaunchGraph graphCompute, graphDevice, graphMd, graphPosq;
     std::vector<LaunchGraph> graphWindows;  // evaluations at window values of one parameter, one graph per value
     size_t windowNext = 0;                  // slot replaced next when graphWindows is full
 };
@@ -601,13 +621,10 @@ static int classTableHost(const std::vector<const ix_ctx*>& sys, std::vector<std
             if (ctx->term[0].present) {
                 const double* p = &ctx->term[0].params[5 * i];
                 const double* q = &ctxJ->term[0].params[5 * j];
-                // InteraxPairTerms.h:274-279
-                const double pref = p[3] * q[3] / std::max(p[3] * q[0] + q[3] * p[0], 1e-30);
-                const double c6 = pref * p[0] * q[0];
-                const double c8 = 1.5 * pref * (p[0] * q[1] + p[1] * q[0]);
-                const double c10 = pref * (2.0 * (p[0] * q[2] + p[2] * q[0]) + 4.2 * p[1] * q[1]);
+                double c[3];
+                ixhost::xdmCoefficients(p, q, c);
                 const double ws = p[4] + q[4];
-                K.disp = make_float4((float)c6, (float)c8, (float)c10, ws != 0 ? (float)(2.0 * beta / ws) : 0.0f);
+                K.disp = make_float4((float)c[0], (float)c[1], (float)c[2], ws != 0 ? (float)(2.0 * beta / ws) : 0.0f);
             }
             if (ctx->term[1].present) {
                 const double* p = &ctx->term[1].params[2 * i];
@@ -1130,6 +1147,7 @@ struct FinishForces {
     double* outForces;
     long long* addFixed;
     int stride;
+    const int* addSlot;                  // row of each particle in addFixed (null: its index)
     const double* invMass;               // null: no velocity half kick
     double* vel;
     double halfDt;
@@ -1171,9 +1189,13 @@ __global__ void kFinish(FinishForces F, EnergyReduction R) {
         F.outForces[3 * i + 2] = fz;
     }
     if (F.addFixed) {
-        atomicAddFixed(F.addFixed + i, f[0]);
-        atomicAddFixed(F.addFixed + F.stride + i, f[1]);
-        atomicAddFixed(F.addFixed + 2 * F.stride + i, f[2]);
+        // a slot map that did not name this particle (not a permutation) leaves it out rather than write elsewhere
+        const int row = F.addSlot ? F.addSlot[i] : i;
+        if (row >= 0 && row < F.stride) {
+            atomicAddFixed(F.addFixed + row, f[0]);
+            atomicAddFixed(F.addFixed + F.stride + row, f[1]);
+            atomicAddFixed(F.addFixed + 2 * F.stride + row, f[2]);
+        }
     }
     if (F.invMass) {
         const double h = F.halfDt * F.invMass[i];
@@ -1340,7 +1362,7 @@ struct StepKick {
 // `kick`: an MD step whose first kernel (kStepStart) has already moved the particles, checked their displacement and
 // refreshed the pair list's sorted positions; the evaluation ends with the second half kick.
 static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, double* outEnergy, long long* addFixed,
-                            int stride, const StepKick* kick = nullptr) {
+                            int stride, const StepKick* kick = nullptr, const int* addSlot = nullptr) {
     const int n = ctx->n;
     cudaStream_t st = ctx->stream;
     const bool doPair = (terms & 7u) != 0;
@@ -1482,6 +1504,7 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
     F.outForces = outForces;
     F.addFixed = addFixed;
     F.stride = stride;
+    F.addSlot = addSlot;
     if (kick) {
         F.invMass = kick->invMass;
         F.vel = kick->vel;
@@ -1503,7 +1526,7 @@ static int prepare(ix_ctx* ctx, unsigned terms) {
     if ((terms & 7u) && !ctx->pairAllocated) {
         updateGeometry(ctx);
         const int nb = (ctx->n + 31) / 32;
-        IX_TRY(allocatePair(ctx, estimateTiles(ctx, nb)));
+        IX_TRY(allocatePair(ctx, ctx->tileCapRequest > 0 ? ctx->tileCapRequest : estimateTiles(ctx, nb)));
     }
     if ((terms & 8u) && !ctx->atmAllocated) IX_TRY(allocateAtm(ctx));
     return IX_OK;
@@ -1534,12 +1557,21 @@ static int checkOverflowFlags(ix_ctx* ctx, unsigned terms, const int* flags, boo
         bumpVersion(ctx);
     }
     if ((terms & 8u) && flags[5]) {
-        ctx->atmCap = std::min(2 * ctx->atmCap, (((int)ctx->siteParams.size() / 3 + 31) / 32) * 32 + 32);
+        // the sites whose lists overflowed were evaluated by scanning every later site, so the results stand; the
+        // lists grow for the next evaluations
+        int cap = 0;
+        {
+            std::vector<int> counts(ctx->siteParams.size() / 3);
+            IX_CUDA(ctx, cudaMemcpy(counts.data(), ctx->A.nbrCount, counts.size() * sizeof(int),
+                                    cudaMemcpyDeviceToHost));
+            for (int c : counts) cap = std::max(cap, c);
+        }
+        const int allSites = (((int)ctx->siteParams.size() / 3 + 31) / 32) * 32 + 32;
+        ctx->atmCap = std::min(std::max(2 * ctx->atmCap, ((cap * 5 / 4 + 31) / 32) * 32), allSites);
         int f[2] = {1, 0};
         IX_CUDA(ctx, cudaMemcpy(ctx->dFlags + 4, f, sizeof(f), cudaMemcpyHostToDevice));
         IX_TRY(allocateAtm(ctx));
         IX_TRY(uploadAtmParams(ctx));
-        redo = true;
         bumpVersion(ctx);
     }
     return IX_OK;
@@ -1751,9 +1783,12 @@ void ix_ctx_destroy(ix_ctx* ctx) {
     releaseGraph(ctx->graphCompute);
     releaseGraph(ctx->graphDevice);
     releaseGraph(ctx->graphMd);
+    releaseGraph(ctx->graphPosq);
     for (auto& g : ctx->graphWindows) releaseGraph(g);
     for (auto& kv : ctx->buffers) arenaFree(ctx->arena, kv.second.p);
     if (ctx->hostStatus) pinnedSlots().give(ctx->hostStatus);
+    if (ctx->deviceStatus) pinnedSlots().give(ctx->deviceStatus);
+    if (ctx->evStatus) cudaEventDestroy(ctx->evStatus);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     if (ctx->evFork) cudaEventDestroy(ctx->evFork);
@@ -1895,6 +1930,21 @@ int ix_update_three_body(ix_ctx* ctx, const double* site_params, double scale_fa
     return IX_OK;
 }
 
+int ix_dispersion_long_range_correction(int num_particles, const double* params, const uint8_t* is_alchemical,
+                                        const ix_pair_settings* settings, double damping_scale,
+                                        int use_long_range_correction, double* coefficient,
+                                        double* alchemical_coefficient) {
+    if (!coefficient || !alchemical_coefficient || !settings || num_particles < 0 ||
+        (num_particles > 0 && (!params || !is_alchemical)))
+        return fail(nullptr, IX_ERR_INVALID, "ix_dispersion_long_range_correction: invalid argument");
+    *coefficient = *alchemical_coefficient = 0.0;
+    if (settings->nonbonded_method != IX_CUTOFF_PERIODIC || !use_long_range_correction) return IX_OK;
+    ixhost::longRangeCorrection(num_particles, params, is_alchemical, settings->cutoff,
+                                settings->use_switching_function != 0, settings->switching_distance, damping_scale,
+                                *coefficient, *alchemical_coefficient);
+    return IX_OK;
+}
+
 int ix_set_parameter(ix_ctx* ctx, const char* name, double value) {
     if (!ctx || !name) return IX_ERR_INVALID;
     ctx->mdForcesValid = false;
@@ -1919,6 +1969,7 @@ int ix_set_positions(ix_ctx* ctx, const double* positions, const double* box) {
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
     IX_TRY(stageCopy(ctx, ctx->dPos, positions, 3 * (size_t)ctx->n * sizeof(double)));
     ctx->havePositions = true;
+    ctx->mdPending.clear();
     return IX_OK;
 }
 
@@ -2000,10 +2051,179 @@ int ix_compute(ix_ctx* ctx, int groups, int include_forces, int include_energy, 
     return IX_OK;
 }
 
+}  // extern "C"
+
+// The device entry points do not wait for their work.  Each records its flags (list overflows) into pinned memory
+// with an event after them; the next device call, or ix_get_device_status, waits for that event and grows the lists
+// that overflowed, so that a call repeated after an overflow is complete (as OpenMM repeats a force evaluation whose
+// neighbor list overflowed).
+static int deviceStatusCheck(ix_ctx* ctx) {
+    if (!ctx->statusPending) return IX_OK;
+    IX_CUDA(ctx, cudaEventSynchronize(ctx->evStatus));
+    ctx->statusPending = false;
+    const int* flags = reinterpret_cast<const int*>(ctx->deviceStatus);
+    ctx->lastDeviceStatus = (flags[1] ? 1 : 0) | (flags[5] ? 2 : 0);
+    if (ctx->lastDeviceStatus) {
+        bool redo = false;
+        IX_TRY(checkOverflowFlags(ctx, selectedTerms(ctx, -1), flags, redo));
+    }
+    return IX_OK;
+}
+
+__global__ void kDeviceStatus(const int* flags, const double* termEnergies, unsigned terms, double* addEnergy,
+                              int* status) {
+    if (status) *status = (flags[1] ? 1 : 0) | (flags[5] ? 2 : 0);
+    if (addEnergy) {
+        double e = 0.0;
+        for (int t = 0; t < 4; t++)
+            if ((terms >> t) & 1u) e += termEnergies[t];
+        *addEnergy += e;
+    }
+}
+
+static int deviceStatusRecord(ix_ctx* ctx) {
+    if (!ctx->deviceStatus) ctx->deviceStatus = pinnedSlots().take();
+    if (!ctx->evStatus) IX_CUDA(ctx, cudaEventCreateWithFlags(&ctx->evStatus, cudaEventDisableTiming));
+    if (!ctx->deviceStatus) return fail(ctx, IX_ERR_CUDA, "pinned host memory for the status is not available");
+    IX_CUDA(ctx, cudaMemcpyAsync(ctx->deviceStatus, ctx->dFlags, 8 * sizeof(int), cudaMemcpyDeviceToHost,
+                                 ctx->stream));
+    IX_CUDA(ctx, cudaEventRecord(ctx->evStatus, ctx->stream));
+    ctx->statusPending = true;
+    return IX_OK;
+}
+
+// Positions of a caller's device array in its slot order (slot k holds particle atomIndex[k], or k) into the
+// context's FP64 positions, and the slot of each particle for the force rows.  FORMAT: IX_POSQ_FLOAT4,
+// IX_POSQ_FLOAT4_CORRECTED (x = posq.x + correction.x, OpenMM's mixed precision), IX_POSQ_DOUBLE4.
+template <int FORMAT>
+__global__ void kGatherPosq(int n, const void* posq, const float4* correction, const int* atomIndex, double* pos,
+                            int* slotOfParticle) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int i = atomIndex ? atomIndex[k] : k;
+    if (i < 0 || i >= n) return;
+    double x, y, z;
+    if (FORMAT == IX_POSQ_DOUBLE4) {
+        const double4 p = reinterpret_cast<const double4*>(posq)[k];
+        x = p.x;
+        y = p.y;
+        z = p.z;
+    }
+    else {
+        const float4 p = reinterpret_cast<const float4*>(posq)[k];
+        x = p.x;
+        y = p.y;
+        z = p.z;
+        if (FORMAT == IX_POSQ_FLOAT4_CORRECTED) {
+            const float4 c = correction[k];
+            x += c.x;
+            y += c.y;
+            z += c.z;
+        }
+    }
+    pos[3 * i] = x;
+    pos[3 * i + 1] = y;
+    pos[3 * i + 2] = z;
+    slotOfParticle[i] = k;
+}
+
+extern "C" {
+
+int ix_set_list_capacity(ix_ctx* ctx, long long pair_tiles, int site_neighbors) {
+    if (!ctx) return IX_ERR_INVALID;
+    if (pair_tiles < 0 || site_neighbors < 0) return fail(ctx, IX_ERR_INVALID, "ix_set_list_capacity: negative capacity");
+    ctx->tileCapRequest = pair_tiles;
+    ctx->atmCap = site_neighbors;
+    ctx->pairAllocated = false;
+    ctx->atmAllocated = false;
+    bumpVersion(ctx);
+    return IX_OK;
+}
+
+int ix_get_list_stats(ix_ctx* ctx, long long* pair_tiles, int* site_neighbors, long long* md_reruns) {
+    if (!ctx) return IX_ERR_INVALID;
+    if (pair_tiles) *pair_tiles = ctx->pairAllocated ? ctx->tileCap : 0;
+    if (site_neighbors) *site_neighbors = ctx->atmAllocated ? ctx->atmCap : 0;
+    if (md_reruns) *md_reruns = ctx->mdReruns;
+    return IX_OK;
+}
+
+int ix_get_device_status(ix_ctx* ctx, int* status) {
+    if (!ctx || !status) return IX_ERR_INVALID;
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    IX_TRY(deviceStatusCheck(ctx));
+    *status = ctx->lastDeviceStatus;
+    return IX_OK;
+}
+
+int ix_compute_device_posq(ix_ctx* ctx, int groups, int posq_format, const void* d_posq,
+                           const void* d_posq_correction, const int32_t* d_atom_index, const double* box,
+                           long long* d_force_fixed, int force_stride, double* d_energy, int* d_status) {
+    if (!ctx) return IX_ERR_INVALID;
+    if (posq_format != IX_POSQ_FLOAT4 && posq_format != IX_POSQ_FLOAT4_CORRECTED && posq_format != IX_POSQ_DOUBLE4)
+        return fail(ctx, IX_ERR_INVALID, "ix_compute_device_posq: unknown position format %d", posq_format);
+    if (!d_posq || (posq_format == IX_POSQ_FLOAT4_CORRECTED && !d_posq_correction))
+        return fail(ctx, IX_ERR_INVALID, "ix_compute_device_posq: positions are NULL");
+    if (d_force_fixed && force_stride < ctx->n)
+        return fail(ctx, IX_ERR_INVALID, "ix_compute_device_posq: stride smaller than the particle count");
+    ctx->mdForcesValid = false;
+    ctx->mdPending.clear();
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    IX_TRY(deviceStatusCheck(ctx));
+    if (box) {
+        if (box[0] <= 0 || box[4] <= 0 || box[8] <= 0) return fail(ctx, IX_ERR_INVALID, "Illegal periodic box vectors");
+        if (std::memcmp(ctx->box, box, sizeof(ctx->box)) != 0) bumpVersion(ctx);
+        std::memcpy(ctx->box, box, sizeof(ctx->box));
+    }
+    ctx->havePositions = true;
+    unsigned terms = selectedTerms(ctx, groups);
+    if (!ctx->dAddSlot) {
+        IX_TRY(deviceAlloc(ctx, "addSlot", ctx->n, &ctx->dAddSlot));
+        IX_CUDA(ctx, cudaMemsetAsync(ctx->dAddSlot, 0xff, ctx->n * sizeof(int), ctx->stream));   // -1: no slot yet
+    }
+    if (terms) {
+        IX_TRY(prepare(ctx, terms));
+        IX_TRY(stageUploads(ctx, terms));
+    }
+    GraphKey key;
+    key.terms = terms;
+    key.out0 = d_energy;
+    key.out2 = d_force_fixed;
+    key.out3 = d_status;
+    key.in0 = d_posq;
+    key.in1 = d_posq_correction;
+    key.in2 = d_atom_index;
+    key.format = posq_format;
+    key.stride = force_stride;
+    IX_TRY(launchGraph(ctx, ctx->graphPosq, key, [&]() -> int {
+        const int blocks = (ctx->n + 255) / 256;
+        const float4* corr = reinterpret_cast<const float4*>(d_posq_correction);
+        if (posq_format == IX_POSQ_DOUBLE4)
+            kGatherPosq<IX_POSQ_DOUBLE4><<<blocks, 256, 0, ctx->stream>>>(ctx->n, d_posq, corr, d_atom_index,
+                                                                           ctx->dPos, ctx->dAddSlot);
+        else if (posq_format == IX_POSQ_FLOAT4_CORRECTED)
+            kGatherPosq<IX_POSQ_FLOAT4_CORRECTED><<<blocks, 256, 0, ctx->stream>>>(ctx->n, d_posq, corr, d_atom_index,
+                                                                                    ctx->dPos, ctx->dAddSlot);
+        else
+            kGatherPosq<IX_POSQ_FLOAT4><<<blocks, 256, 0, ctx->stream>>>(ctx->n, d_posq, corr, d_atom_index,
+                                                                          ctx->dPos, ctx->dAddSlot);
+        ctx->launches += 1;
+        if (terms)
+            IX_TRY(launchEvaluation(ctx, terms, nullptr, ctx->dOutEnergy, d_force_fixed, force_stride, nullptr,
+                                    ctx->dAddSlot));
+        kDeviceStatus<<<1, 1, 0, ctx->stream>>>(ctx->dFlags, ctx->dOutEnergy, terms, d_energy, d_status);
+        ctx->launches += 1;
+        IX_CUDA(ctx, cudaGetLastError());
+        return IX_OK;
+    }));
+    return deviceStatusRecord(ctx);
+}
+
 int ix_compute_device(ix_ctx* ctx, int groups, long long* d_force_fixed, int force_stride, double* d_term_energies) {
     if (!ctx) return IX_ERR_INVALID;
     if (force_stride < ctx->n) return fail(ctx, IX_ERR_INVALID, "ix_compute_device: stride smaller than the particle count");
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    IX_TRY(deviceStatusCheck(ctx));
     unsigned terms = selectedTerms(ctx, groups);
     if (!terms) return IX_OK;
     IX_TRY(prepare(ctx, terms));
@@ -2013,17 +2233,21 @@ int ix_compute_device(ix_ctx* ctx, int groups, long long* d_force_fixed, int for
     key.out1 = d_term_energies;
     key.out2 = d_force_fixed;
     key.stride = force_stride;
-    return launchGraph(ctx, ctx->graphDevice, key, [&]() {
+    IX_TRY(launchGraph(ctx, ctx->graphDevice, key, [&]() {
         return launchEvaluation(ctx, terms, nullptr, d_term_energies, d_force_fixed, force_stride);
-    });
+    }));
+    return deviceStatusRecord(ctx);
 }
 
 int ix_compute_device_f64(ix_ctx* ctx, int groups, const double* d_positions, const double* box, double* d_forces,
                           double* d_term_energies) {
     if (!ctx) return IX_ERR_INVALID;
     ctx->mdForcesValid = false;
+    ctx->mdPending.clear();
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    IX_TRY(deviceStatusCheck(ctx));
     if (box) {
+        if (box[0] <= 0 || box[4] <= 0 || box[8] <= 0) return fail(ctx, IX_ERR_INVALID, "Illegal periodic box vectors");
         if (std::memcmp(ctx->box, box, sizeof(ctx->box)) != 0) bumpVersion(ctx);
         std::memcpy(ctx->box, box, sizeof(ctx->box));
     }
@@ -2044,8 +2268,9 @@ int ix_compute_device_f64(ix_ctx* ctx, int groups, const double* d_positions, co
     key.terms = terms;
     key.out0 = d_forces;
     key.out1 = d_term_energies;
-    return launchGraph(ctx, ctx->graphDevice, key,
-                       [&]() { return launchEvaluation(ctx, terms, d_forces, d_term_energies, nullptr, 0); });
+    IX_TRY(launchGraph(ctx, ctx->graphDevice, key,
+                       [&]() { return launchEvaluation(ctx, terms, d_forces, d_term_energies, nullptr, 0); }));
+    return deviceStatusRecord(ctx);
 }
 
 int ix_set_counting(ix_ctx* ctx, int enable) {
@@ -2082,6 +2307,7 @@ int ix_md_set_masses(ix_ctx* ctx, const double* masses) {
     IX_TRY(deviceAlloc(ctx, "vel", 3 * (size_t)ctx->n, &ctx->dVel));
     IX_TRY(stageCopy(ctx, ctx->dInvMass, inv.data(), ctx->n * sizeof(double)));
     ctx->haveMasses = true;
+    ctx->mdPending.clear();
     bumpVersion(ctx);
     return IX_OK;
 }
@@ -2120,13 +2346,10 @@ int ix_get_kernel_times(ix_ctx* ctx, double* pair_ms, double* three_body_ms) {
     return IX_OK;
 }
 
-// Enqueue velocity-Verlet steps without synchronizing (masses and velocities must have been set by ix_md_run or
-// ix_md_set_state).
-int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt) {
-    if (!ctx) return IX_ERR_INVALID;
-    if (!ctx->haveMasses) return fail(ctx, IX_ERR_STATE, "ix_md_steps_async: masses have not been set");
-    if (!ctx->havePositions) return fail(ctx, IX_ERR_STATE, "positions have not been set");
-    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+}  // extern "C"
+
+// Enqueue velocity-Verlet steps on the context's stream without synchronizing.
+static int enqueueSteps(ix_ctx* ctx, int num_steps, double dt) {
     unsigned terms = selectedTerms(ctx, -1);
     if (terms) {
         IX_TRY(prepare(ctx, terms));
@@ -2170,6 +2393,43 @@ int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt) {
     for (int s = 0; s < num_steps; s++) IX_TRY(launchGraph(ctx, ctx->graphMd, key, step));
     IX_CUDA(ctx, cudaGetLastError());
     return IX_OK;
+}
+
+// The MD state (positions, velocities, forces, energies) copied to or from the save area, in stream order.
+static int mdStateCopy(ix_ctx* ctx, bool save) {
+    const size_t n3 = 3 * (size_t)ctx->n;
+    IX_TRY(deviceAlloc(ctx, "mdSave", 3 * n3 + 4, &ctx->dMdSave));
+    double* live[4] = {ctx->dPos, ctx->dVel, ctx->dOutForces, ctx->dOutEnergy};
+    const size_t count[4] = {n3, n3, n3, 4};
+    size_t off = 0;
+    for (int k = 0; k < 4; k++) {
+        double* kept = ctx->dMdSave + off;
+        IX_CUDA(ctx, cudaMemcpyAsync(save ? kept : live[k], save ? live[k] : kept, count[k] * sizeof(double),
+                                     cudaMemcpyDeviceToDevice, ctx->stream));
+        off += count[k];
+    }
+    return IX_OK;
+}
+
+extern "C" {
+
+// Enqueue velocity-Verlet steps without synchronizing (masses and velocities must have been set by ix_md_run or
+// ix_md_set_state).  The first call after a finish saves the state, so that ix_md_finish can rerun the steps after a
+// neighbor-list overflow.
+int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt) {
+    if (!ctx) return IX_ERR_INVALID;
+    if (!ctx->haveMasses) return fail(ctx, IX_ERR_STATE, "ix_md_steps_async: masses have not been set");
+    if (!ctx->havePositions) return fail(ctx, IX_ERR_STATE, "positions have not been set");
+    if (num_steps < 0) return fail(ctx, IX_ERR_INVALID, "ix_md_steps_async: negative step count");
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (ctx->mdRollback && (selectedTerms(ctx, -1) & 7u)) {
+        if (ctx->mdPending.empty()) {
+            IX_TRY(mdStateCopy(ctx, true));
+            ctx->mdSavedForcesValid = ctx->mdForcesValid;
+        }
+        ctx->mdPending.push_back({num_steps, dt});
+    }
+    return enqueueSteps(ctx, num_steps, dt);
 }
 
 int ix_set_graphs(ix_ctx* ctx, int enable) {
@@ -2511,19 +2771,30 @@ int ix_get_launch_count(ix_ctx* ctx, long long* launches) {
     return IX_OK;
 }
 
-// Finish enqueued MD steps: synchronize, check the neighbor lists (an overflow during the steps invalidates them:
-// the lists are grown and IX_ERR_STATE is returned), record the counts of the last evaluation, copy the state out.
+// Finish enqueued MD steps: synchronize, check the neighbor lists, record the counts of the last evaluation, copy the
+// state out.  When the pair list overflowed during the steps (their forces missed pairs), the list is grown, the
+// state saved before the steps is restored and the steps are run again, as OpenMM recomputes a step whose neighbor
+// list overflowed; a three-body list overflow needs no rerun (those sites scan every later site).
 int ix_md_finish(ix_ctx* ctx, double* positions, double* velocities, double* energy) {
     if (!ctx) return IX_ERR_INVALID;
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
-    IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     unsigned terms = selectedTerms(ctx, -1);
-    bool redo = false;
-    if (terms) IX_TRY(checkOverflow(ctx, terms, redo));
-    if (redo) {
-        ctx->mdForcesValid = false;
-        return fail(ctx, IX_ERR_STATE, "neighbor list overflow during MD; the lists were grown, rerun the steps");
+    for (int attempt = 0;; attempt++) {
+        IX_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        bool redo = false;
+        if (terms) IX_TRY(checkOverflow(ctx, terms, redo));
+        if (!redo) break;
+        if (ctx->mdPending.empty() || attempt == 4) {
+            ctx->mdPending.clear();
+            ctx->mdForcesValid = false;
+            return fail(ctx, IX_ERR_STATE, "neighbor list overflow during MD; the lists were grown, rerun the steps");
+        }
+        IX_TRY(mdStateCopy(ctx, false));
+        ctx->mdForcesValid = ctx->mdSavedForcesValid;
+        for (const auto& seg : ctx->mdPending) IX_TRY(enqueueSteps(ctx, seg.first, seg.second));
+        ctx->mdReruns++;
     }
+    ctx->mdPending.clear();
     unsigned long long c[2] = {0, 0};
     IX_CUDA(ctx, cudaMemcpy(c, ctx->dCounts + 2, sizeof(c), cudaMemcpyDeviceToHost));
     ctx->lastPairs = (terms & 7u) ? (long long)c[0] : 0;
@@ -2560,8 +2831,8 @@ int ix_md_run(ix_ctx* ctx, int num_steps, double dt, double* positions, double* 
 // allocation inside stream capture is not allowed), an engine whose device memory is owned by its own pool, or a
 // real-time loop that must not allocate.  For them ix_three_body_noalloc evaluates the three-body force with all its
 // working memory in one file-scope __device__ array of fixed size; the caller passes only its inputs and outputs.
-// Limits: kNoAllocMaxParticles particles, kNoAllocMaxSites sites, kNoAllocMaxNeighbors sites above any site within
-// the cutoff.  The array is allocated by the CUDA runtime when the library is loaded, on every GPU that loads it
+// Limits: kNoAllocMaxParticles particles, kNoAllocMaxSites sites; a site with more than kNoAllocMaxNeighbors sites
+// above it within the cutoff is evaluated by a scan of every later site (reported by the overflow query).  The array is allocated by the CUDA runtime when the library is loaded, on every GPU that loads it
 // (about 2.7 MB), and stays until the process exits.  Every call shares it: two calls that overlap on the GPU (on
 // different streams, or from different host threads on one device) race on it and must be serialized by the caller.
 // ---------------------------------------------------------------------------------------------------------------------
@@ -2778,6 +3049,10 @@ int ix_three_body_noalloc_overflow(int* overflow) {
     if (e != cudaSuccess) return fail(nullptr, IX_ERR_NO_DEVICE, "cudaGetDevice failed: %s", cudaGetErrorString(e));
     NoAllocScratch* S = nullptr;
     IX_TRY(noAllocScratch(device, &S));
+    // the flag is written by the last call's kernels on the caller's stream, which may be a non-blocking stream that a
+    // plain copy does not wait for: wait for the whole device first
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return fail(nullptr, IX_ERR_CUDA, "ix_three_body_noalloc_overflow: %s", cudaGetErrorString(e));
     int flags[2] = {0, 0};
     e = cudaMemcpy(flags, S->flag, sizeof(flags), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return fail(nullptr, IX_ERR_CUDA, "ix_three_body_noalloc_overflow: %s", cudaGetErrorString(e));

@@ -318,6 +318,7 @@ void launchContext(ix_server* S, ServerShard* H, ServerRequest* r) {
     c->arena = &S->arena;
     c->device = S->device;
     c->useGraphs = r->steps >= kServerGraphSteps;
+    c->mdRollback = false;   // an overflow reruns the whole request from its description
     if (!H->streams.empty()) {
         const StreamSet set = H->streams.back();
         H->streams.pop_back();
@@ -549,18 +550,22 @@ bool collect(ix_server* S, ServerShard* H) {
                 int flags[8];
                 std::memcpy(flags, st + 3 * n3 + 4, sizeof(flags));
                 if (flags[1] || flags[5]) {
+                    // a pair-list overflow: grow the list and run the request again; a three-body list overflow
+                    // needs no rerun (those sites were scanned in full), the list only grows
                     bool redo = false;
                     int rc = checkOverflow(u->ctx, selectedTerms(u->ctx, -1), redo);
-                    if (rc == IX_OK && ++u->restarts <= 3) {
+                    if (rc == IX_OK && redo && ++u->restarts <= 3) {
                         H->freeEvents.push_back(mk.event);
                         u->marks.clear();
                         u->ctx->uploadUsed = 0;   // the stream has run every earlier upload
                         rc = enqueueContextRun(H, u);
                         if (rc == IX_OK) continue;
                     }
-                    failCode = rc != IX_OK ? rc : IX_ERR_STATE;
-                    msg = rc != IX_OK ? u->ctx->error : "neighbor lists kept overflowing";
-                    break;
+                    if (rc != IX_OK || redo) {
+                        failCode = rc != IX_OK ? rc : IX_ERR_STATE;
+                        msg = rc != IX_OK ? u->ctx->error : "neighbor lists kept overflowing";
+                        break;
+                    }
                 }
                 ServerRequest* r = u->members[0];
                 r->pos.assign(st, st + n3);

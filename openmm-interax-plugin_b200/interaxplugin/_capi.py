@@ -8,6 +8,7 @@ _PKG = Path(__file__).resolve().parent.parent
 LIB_PATH = _PKG / "libinterax_b200.so"
 
 IX_OK = 0
+IX_POSQ_FLOAT4, IX_POSQ_FLOAT4_CORRECTED, IX_POSQ_DOUBLE4 = 0, 1, 2
 P = ctypes.c_void_p
 
 
@@ -52,10 +53,18 @@ def lib():
             "ix_update_short_range": (ctypes.c_int, [P, P, ctypes.c_int]),
             "ix_update_three_body": (ctypes.c_int, [P, P, ctypes.c_double, ctypes.c_double, ctypes.c_double]),
             "ix_set_parameter": (ctypes.c_int, [P, ctypes.c_char_p, ctypes.c_double]),
+            "ix_dispersion_long_range_correction": (ctypes.c_int, [ctypes.c_int, P, P, ctypes.POINTER(PairSettings),
+                                                                   ctypes.c_double, ctypes.c_int, P, P]),
             "ix_set_positions": (ctypes.c_int, [P, P, P]),
             "ix_compute": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, P, P, P]),
             "ix_compute_device": (ctypes.c_int, [P, ctypes.c_int, P, ctypes.c_int, P]),
             "ix_compute_device_f64": (ctypes.c_int, [P, ctypes.c_int, P, P, P, P]),
+            "ix_compute_device_posq": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_int, P, P, P, P, P, ctypes.c_int, P,
+                                                      P]),
+            "ix_get_device_status": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_int)]),
+            "ix_set_list_capacity": (ctypes.c_int, [P, ctypes.c_longlong, ctypes.c_int]),
+            "ix_get_list_stats": (ctypes.c_int, [P, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_int),
+                                                 ctypes.POINTER(ctypes.c_longlong)]),
             "ix_set_counting": (ctypes.c_int, [P, ctypes.c_int]),
             "ix_get_counts": (ctypes.c_int, [P, P, P]),
             "ix_md_set_masses": (ctypes.c_int, [P, P]),

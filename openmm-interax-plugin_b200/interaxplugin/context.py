@@ -70,6 +70,24 @@ def _pair_settings(force, n):
     return s, ex
 
 
+def calcLongRangeCorrection(force):
+    """Long-range correction coefficients (coefficient, alchemicalCoefficient) of an InteraxDispersionForce, as
+    InteraxDispersionForceImpl::calcLongRangeCorrection (openmmapi/src/InteraxDispersionForceImpl.cpp:86-149): the
+    correction energy is (coefficient + lambda alchemicalCoefficient) / V.  Host-side FP64; needs no GPU."""
+    lib = _capi.lib()
+    n = force.getNumParticles()
+    s, ex = _pair_settings(force, n)
+    params = _capi.arr(force._params_array(), np.float64)
+    alch = _capi.arr(force._alch_array(), np.uint8)
+    coef, alch_coef = ctypes.c_double(), ctypes.c_double()
+    rc = lib.ix_dispersion_long_range_correction(n, _capi.ptr(params), _capi.ptr(alch), ctypes.byref(s),
+                                                 force.getDampingScale(), int(force.getUseLongRangeCorrection()),
+                                                 ctypes.byref(coef), ctypes.byref(alch_coef))
+    if rc != 0:
+        raise OpenMMException(lib.ix_last_error(None).decode())
+    return coef.value, alch_coef.value
+
+
 def describe_forces(lib, handle, system, check, keep=None):
     """Describe a System's InteraxFF forces to a context or request handle with the ix_add_* functions (what the
     reference's kernels' initialize() receive, InteraxKernels.h:64-67, 99-102, 134-137, 169-172).  Returns
@@ -204,6 +222,18 @@ class Context:
                                          ctypes.byref(energy), _capi.ptr(forces)))
         return State(energy.value if getEnergy else None, forces, terms,
                      self._positions.copy() if getPositions else None)
+
+    def setListCapacity(self, pairTiles=0, siteNeighbors=0):
+        """Capacities of the pair list (tiles) and of the three-body lists (entries per site) at their next
+        allocation; 0 = estimated from the density.  The lists grow when they overflow, and a small capacity forces
+        that path (ix_set_list_capacity)."""
+        self._check(self._lib.ix_set_list_capacity(self._ctx, int(pairTiles), int(siteNeighbors)))
+
+    def getListStats(self):
+        """(pair-list tiles, three-body entries per site, MD steps reruns after an overflow) (ix_get_list_stats)."""
+        a, b, c = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_longlong()
+        self._check(self._lib.ix_get_list_stats(self._ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return a.value, b.value, c.value
 
     def getCounts(self):
         """Interacting pairs and triples of the last evaluation."""

@@ -70,9 +70,10 @@ class Server:
             self._templates[id(system)] = t
         return t
 
-    def submit(self, system, positions, velocities=None, steps=0, dt=0.001, parameters=None):
+    def submit(self, system, positions, velocities=None, steps=0, dt=0.001, parameters=None, list_capacity=None):
         """Queue `steps` velocity-Verlet steps of `dt` ps of `system` from the given state (0 steps: one energy+force
-        evaluation).  Masses come from the System.  Returns the request id."""
+        evaluation).  Masses come from the System.  list_capacity: (pair tiles, three-body entries per site) of the
+        request's neighbor lists at admission (ix_set_list_capacity; None = estimated).  Returns the request id."""
         L = self._lib
         _, n, box, mass, calls, _ = self._template(system)
         req = ctypes.c_void_p()
@@ -87,6 +88,8 @@ class Server:
                 check(getattr(L, name)(req, *args))
             for k, v in (parameters or {}).items():
                 check(L.ix_set_parameter(req, k.encode(), float(v)))
+            if list_capacity is not None:
+                check(L.ix_set_list_capacity(req, int(list_capacity[0]), int(list_capacity[1])))
             pos = _capi.arr(np.asarray(positions, dtype=np.float64).reshape(n, 3), np.float64)
             vel = None if velocities is None else _capi.arr(np.asarray(velocities).reshape(n, 3), np.float64)
             check(L.ix_request_set_state(req, _capi.ptr(pos), _capi.ptr(vel), _capi.ptr(mass)))

@@ -174,6 +174,24 @@ def water_cluster(num_waters, seed=0, params=None, three_body=True):
     return system, pos, None
 
 
+def cluster_set(num_clusters, seed=1, stream=0):
+    """The batched workload: num_clusters water clusters of 2..32 waters (configuration 2 of the benchmark), cluster k
+    drawn from its own seed so that any subset can be rebuilt alone.  Returns (systems, positions)."""
+    rng = np.random.default_rng(seed + 7919 * stream)
+    sizes = rng.integers(2, 33, size=num_clusters)
+    systems, positions = [], []
+    for k in range(num_clusters):
+        s, p, _ = water_cluster(int(sizes[k]), seed=seed * 100003 + 7919 * stream + k)
+        systems.append(s)
+        positions.append(p)
+    return systems, positions
+
+
+def cluster_sizes(num_clusters, seed=1, stream=0):
+    """The water counts of cluster_set's clusters, without building them."""
+    return np.random.default_rng(seed + 7919 * stream).integers(2, 33, size=num_clusters)
+
+
 def box_length_for(num_waters):
     return (num_waters / WATERS_PER_NM3) ** (1.0 / 3.0)
 

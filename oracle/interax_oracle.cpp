@@ -4,8 +4,10 @@
 // The product never links or loads it.
 #include "interax_oracle.hpp"
 
+#include <algorithm>
 #include <cstring>
 #include <numeric>
+#include <thread>
 #include <set>
 #include <unordered_map>
 
@@ -15,6 +17,14 @@ namespace ixo {
 static double& lastAbsEnergy() {
     static thread_local double value = 0.0;
     return value;
+}
+
+// Threads for a loop of `work` items: every hardware thread for large loops (the split is fixed for a given thread
+// count, so the sums are reproducible), one below 100000 items.
+static int oracleThreads(size_t work) {
+    if (work < 100000) return 1;
+    const unsigned hw = std::thread::hardware_concurrency();
+    return (int)std::max(1u, std::min(hw ? hw : 1u, 64u));
 }
 
 static bool isRectangular(const Vec3* box) {
@@ -81,23 +91,39 @@ void candidatePairs(int n, const std::vector<Vec3>& pos, const Vec3* box, const 
         cellIndex[i] = (c[2] * nc[1] + c[1]) * nc[0] + c[0];
         cells[cellIndex[i]].push_back(i);
     }
-    for (int i = 0; i < n; i++) {
-        int c[3] = {cellIndex[i] % nc[0], (cellIndex[i] / nc[0]) % nc[1], cellIndex[i] / (nc[0] * nc[1])};
-        for (int dz = -1; dz <= 1; dz++)
-            for (int dy = -1; dy <= 1; dy++)
-                for (int dx = -1; dx <= 1; dx++) {
-                    int cc[3] = {c[0] + dx, c[1] + dy, c[2] + dz};
-                    bool skip = false;
-                    for (int k = 0; k < 3; k++) {
-                        if (periodic) cc[k] = (cc[k] + nc[k]) % nc[k];
-                        else if (cc[k] < 0 || cc[k] >= nc[k]) skip = true;
+    // the particles split over threads in contiguous ranges; each range's pairs sorted by (i, j), so the ranges
+    // joined in order give the pairs in (i, j) order
+    auto range = [&](int first, int last, std::vector<std::pair<int, int>>& dst) {
+        std::vector<int> js;
+        for (int i = first; i < last; i++) {
+            int c[3] = {cellIndex[i] % nc[0], (cellIndex[i] / nc[0]) % nc[1], cellIndex[i] / (nc[0] * nc[1])};
+            js.clear();
+            for (int dz = -1; dz <= 1; dz++)
+                for (int dy = -1; dy <= 1; dy++)
+                    for (int dx = -1; dx <= 1; dx++) {
+                        int cc[3] = {c[0] + dx, c[1] + dy, c[2] + dz};
+                        bool skip = false;
+                        for (int k = 0; k < 3; k++) {
+                            if (periodic) cc[k] = (cc[k] + nc[k]) % nc[k];
+                            else if (cc[k] < 0 || cc[k] >= nc[k]) skip = true;
+                        }
+                        if (skip) continue;
+                        for (int j : cells[(cc[2] * nc[1] + cc[1]) * nc[0] + cc[0]])
+                            if (j > i && !excluded(i, j)) js.push_back(j);
                     }
-                    if (skip) continue;
-                    for (int j : cells[(cc[2] * nc[1] + cc[1]) * nc[0] + cc[0]])
-                        if (j > i && !excluded(i, j)) out.push_back({i, j});
-                }
-    }
-    std::sort(out.begin(), out.end());
+            std::sort(js.begin(), js.end());
+            js.erase(std::unique(js.begin(), js.end()), js.end());   // small grids visit a cell more than once
+            for (int j : js) dst.push_back({i, j});
+        }
+    };
+    const int threads = oracleThreads((size_t)n * 50);
+    std::vector<std::vector<std::pair<int, int>>> parts(threads);
+    std::vector<std::thread> pool;
+    for (int t = 0; t < threads; t++)
+        pool.emplace_back([&, t]() { range((int)((long long)n * t / threads), (int)((long long)n * (t + 1) / threads),
+                                           parts[t]); });
+    for (auto& th : pool) th.join();
+    for (auto& part : parts) out.insert(out.end(), part.begin(), part.end());
 }
 
 double computePairForce(PairTerm term, const std::vector<Vec3>& pos, const Vec3* box, const PairSettings& s,
@@ -118,13 +144,12 @@ double computePairForce(PairTerm term, const std::vector<Vec3>& pos, const Vec3*
     candidatePairs(n, pos, box, s, pairs);
     const int st = params.stride;
     const double* P = params.p.data();
-    double total = 0;
-    int64_t count = 0;
-    for (auto& pr : pairs) {
+    // one pair; the pair loop is split over threads in fixed contiguous shares (below), each with its own sums
+    auto evalPair = [&](const std::pair<int, int>& pr, Vec3* F, double& total, double& absSum, int64_t& count) {
         int i = pr.first, j = pr.second;
         Vec3 d = periodic ? periodicDelta(pos[i], pos[j], box) : pos[j] - pos[i];
         double r = std::sqrt(d.dot(d));
-        if (useCutoff && r >= s.cutoff) continue;
+        if (useCutoff && r >= s.cutoff) return;
         bool alchPair = (params.alch[i] != 0) != (params.alch[j] != 0);
         double rEff = r;
         if (alchPair && s.softcoreRadius > 0) {
@@ -137,16 +162,16 @@ double computePairForce(PairTerm term, const std::vector<Vec3>& pos, const Vec3*
         const double* a = P + size_t(i) * st;
         const double* b = P + size_t(j) * st;
         if (term == kDispersion) {
-            if (a[3] * b[3] == 0) continue;
+            if (a[3] * b[3] == 0) return;
             dispersionPair(rEff, a[0], a[1], a[2], a[3], a[4], b[0], b[1], b[2], b[3], b[4], params.dampingScale, e,
                            dEdR);
         }
         else if (term == kExchange) {
-            if (a[1] * b[1] == 0) continue;
+            if (a[1] * b[1] == 0) return;
             exchangePair(rEff, a[0], a[1], b[0], b[1], scheme, e, dEdR);
         }
         else {
-            if (a[2] * b[2] == 0) continue;
+            if (a[2] * b[2] == 0) return;
             shortRangePair(rEff, a[0], a[1], a[2], b[0], b[1], b[2], scheme, e, dEdR);
         }
         count++;
@@ -165,7 +190,7 @@ double computePairForce(PairTerm term, const std::vector<Vec3>& pos, const Vec3*
         }
         if (rEff != r) dEdR *= std::pow(r / rEff, 5);
         // sum of |pair energies| before switching: the error scale of tests/TestInteraxPairForce.h:105-142
-        lastAbsEnergy() += std::fabs((alchPair ? lambda : 1.0) * e);
+        absSum += std::fabs((alchPair ? lambda : 1.0) * e);
         if (useSwitch && r > s.switchDistance) {
             double t = (r - s.switchDistance) / (s.cutoff - s.switchDistance);
             double sv = 1 + t * t * t * (-10 + t * (15 - t * 6));
@@ -177,9 +202,35 @@ double computePairForce(PairTerm term, const std::vector<Vec3>& pos, const Vec3*
         total += scale * e;
         double fs = scale * dEdR / r;
         Vec3 f(d.x * fs, d.y * fs, d.z * fs);
-        forces[i] += f;
-        forces[j] -= f;
+        F[i] += f;
+        F[j] -= f;
+    };
+    double total = 0, absSum = 0;
+    int64_t count = 0;
+    const size_t numPairs = pairs.size();
+    const int threads = ops ? 1 : oracleThreads(numPairs);
+    if (threads <= 1) {
+        for (auto& pr : pairs) evalPair(pr, forces.data(), total, absSum, count);
     }
+    else {
+        std::vector<std::vector<Vec3>> F(threads, std::vector<Vec3>(n));
+        std::vector<double> tot(threads, 0.0), abss(threads, 0.0);
+        std::vector<int64_t> cnt(threads, 0);
+        std::vector<std::thread> pool;
+        for (int t = 0; t < threads; t++)
+            pool.emplace_back([&, t]() {
+                const size_t b = numPairs * t / threads, e = numPairs * (t + 1) / threads;
+                for (size_t k = b; k < e; k++) evalPair(pairs[k], F[t].data(), tot[t], abss[t], cnt[t]);
+            });
+        for (auto& th : pool) th.join();
+        for (int t = 0; t < threads; t++) {
+            total += tot[t];
+            absSum += abss[t];
+            count += cnt[t];
+            for (int i = 0; i < n; i++) forces[i] += F[t][i];
+        }
+    }
+    lastAbsEnergy() = absSum;
     if (term == kDispersion && params.useLongRangeCorrection && s.method == 2) {
         double coef, alchCoef;
         longRangeCorrection(s, params, coef, alchCoef);

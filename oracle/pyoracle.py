@@ -59,6 +59,20 @@ def _c(a, dtype):
     return np.ascontiguousarray(a, dtype=dtype)
 
 
+def long_range_coefficients(force):
+    """The oracle's long-range correction coefficients (coefficient, alchemical coefficient) of a dispersion force."""
+    ex = _c(force._exclusion_array(), np.int32)
+    s = _PairSettings(force.getNonbondedMethod(), force.getCutoffDistance(), int(force.getUseSwitchingFunction()),
+                      force.getSwitchingDistance(), force.getSoftcoreRadius(), len(ex), _ptr(ex))
+    params = _c(force._params_array(), np.float64)
+    alch = _c(force._alch_array(), np.uint8)
+    coef, alch_coef = ctypes.c_double(), ctypes.c_double()
+    lib().ox_long_range_coefficients(force.getNumParticles(), ctypes.byref(s), _ptr(params), _ptr(alch),
+                                     force.getDampingScale(), int(force.getUseLongRangeCorrection()),
+                                     ctypes.byref(coef), ctypes.byref(alch_coef))
+    return coef.value, alch_coef.value
+
+
 def pair_force(term, force, positions, box, lam=1.0, counts=None, overlap_method=None):
     """Energy and forces (N x 3) of one pair force.  term: 0 dispersion, 1 exchange, 2 short range."""
     pos = _c(positions, np.float64)
