@@ -14,9 +14,11 @@
 //     all-pairs neighbor search split over the threads, then the triples by marking (a site C is a neighbor of A and
 //     of B < C when it carries A's mark and appears in B's list), sites taken from an atomic counter, per-thread site
 //     forces combined at the end.
-// The reference evaluates eight pairs at once with SIMD (fvec8); this restatement evaluates one pair at a time per
-// thread, so it is slower per core than the reference's own CPU platform.
+// Like the reference with AVX (fvec8, CpuInteraxPairForceAvx.cpp:44-48), each block of eight is evaluated against
+// each listed neighbor with one eight-lane vector (cpu_simd.h): the block's particles in the lanes, the neighbor
+// broadcast, exclusions as a per-neighbor lane mask built with the list.
 #include "interax_oracle.hpp"
+#include "cpu_simd.h"
 
 #include <algorithm>
 #include <atomic>
@@ -140,6 +142,7 @@ struct CpuPairForce {
     std::vector<float> pos;                 // n x 3
     std::vector<int> sorted, sortedPos;
     std::vector<std::vector<int>> blockNbrs;
+    std::vector<std::vector<uint8_t>> blockExcl;   // per listed neighbor: the block lanes it is excluded from
     std::vector<std::vector<float>> threadForce;
     std::vector<double> threadEnergy;
     std::vector<long long> threadCount;
@@ -157,13 +160,23 @@ void buildNeighborList(CpuPairForce& F, const float box[3][3], const float invDi
     F.sortedPos.resize(n);
     const int nb = (n + kBlock - 1) / kBlock;
     F.blockNbrs.assign(nb, {});
+    F.blockExcl.assign(nb, {});
     if (!useCutoff) {
         for (int i = 0; i < n; i++) F.sorted[i] = F.sortedPos[i] = i;
         std::atomic<int> next(0);
         tp.run([&](int) {
+            std::vector<uint8_t> exclMark(n, 0);
             for (int b = next++; b < nb; b = next++) {
+                const int k0 = b * kBlock, k1 = std::min(n, k0 + kBlock);
+                for (int k = k0; k < k1; k++)
+                    for (int j : F.excl[k]) exclMark[j] |= (uint8_t)(1u << (k - k0));
                 auto& list = F.blockNbrs[b];
-                for (int j = b * kBlock + 1; j < n; j++) list.push_back(j);
+                for (int j = k0 + 1; j < n; j++) {
+                    list.push_back(j);
+                    F.blockExcl[b].push_back(exclMark[j]);
+                }
+                for (int k = k0; k < k1; k++)
+                    for (int j : F.excl[k]) exclMark[j] = 0;
             }
         });
         return;
@@ -185,7 +198,7 @@ void buildNeighborList(CpuPairForce& F, const float box[3][3], const float invDi
             lo[d] = mn;
             ext[d] = std::max(mx - mn, 1e-6f);
         }
-        nc[d] = std::max(1, std::min(1024, (int)(ext[d] / cutoff)));
+        nc[d] = std::max(1, std::min(1024, (int)(2.0f * ext[d] / cutoff)));   // cells of at least half the cutoff
     }
     const int numCells = nc[0] * nc[1] * nc[2];
     std::vector<int> cellOf(n), cellCount(numCells + 1, 0);
@@ -213,8 +226,11 @@ void buildNeighborList(CpuPairForce& F, const float box[3][3], const float invDi
     std::atomic<int> next(0);
     tp.run([&](int) {
         std::vector<int> stamp(numCells, -1);
+        std::vector<uint8_t> exclMark(n, 0);     // lanes of the current block that exclude each particle
         for (int b = next++; b < nb; b = next++) {
             const int k0 = b * kBlock, k1 = std::min(n, k0 + kBlock);
+            for (int k = k0; k < k1; k++)
+                for (int j : F.excl[F.sorted[k]]) exclMark[j] |= (uint8_t)(1u << (k - k0));
             // block center and half extents (minimum image from the first member when periodic)
             const int i0 = F.sorted[k0];
             float mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
@@ -228,45 +244,59 @@ void buildNeighborList(CpuPairForce& F, const float box[3][3], const float invDi
                     mx[e] = std::max(mx[e], d[e]);
                 }
             }
+            float center[3], half[3];
+            for (int e = 0; e < 3; e++) {
+                center[e] = F.pos[3 * i0 + e] + 0.5f * (mn[e] + mx[e]);
+                half[e] = 0.5f * (mx[e] - mn[e]);
+            }
             auto& list = F.blockNbrs[b];
+            auto& exclOut = F.blockExcl[b];
             auto scanCell = [&](int cell) {
                 if (stamp[cell] == b) return;
                 stamp[cell] = b;
-                for (int q = cellCount[cell]; q < cellCount[cell + 1]; q++) {
+                for (int q = std::max(cellCount[cell], k0 + 1); q < cellCount[cell + 1]; q++) {
+                    // only particles later in the sorted order
                     const int j = F.sorted[q];
-                    if (q <= k0) continue;   // only particles later in the sorted order
-                    float d[3] = {F.pos[3 * j] - F.pos[3 * i0], F.pos[3 * j + 1] - F.pos[3 * i0 + 1],
-                                  F.pos[3 * j + 2] - F.pos[3 * i0 + 2]};
-                    if (triclinic) {
-                        list.push_back(j);   // every candidate; the pair loop applies the cutoff
-                        continue;
-                    }
-                    if (periodic) minimumImage(d[0], d[1], d[2], box, invDiag, triclinic);
-                    // distance to the block's box, over the periodic images of j along each axis
-                    float r2 = 0.0f;
-                    for (int e = 0; e < 3; e++) {
-                        float out = 3.0e38f;
-                        for (int k = periodic ? -1 : 0; k <= (periodic ? 1 : 0); k++) {
-                            const float v = d[e] + k * box[e][e];
-                            out = std::min(out, v < mn[e] ? mn[e] - v : (v > mx[e] ? v - mx[e] : 0.0f));
+                    if (!triclinic) {
+                        // distance from j's nearest image to the block's box (the box is far smaller than half the
+                        // periodic box, so the image nearest the center is the nearest to the box)
+                        float r2 = 0.0f;
+                        for (int e = 0; e < 3; e++) {
+                            float d = F.pos[3 * j + e] - center[e];
+                            if (periodic) d -= box[e][e] * std::nearbyint(d * invDiag[e]);
+                            const float out = std::max(std::fabs(d) - half[e], 0.0f);
+                            r2 += out * out;
                         }
-                        r2 += out * out;
+                        if (r2 >= cutoff2) continue;
                     }
-                    if (r2 < cutoff2) list.push_back(j);
+                    // triclinic: every candidate; the pair loop applies the cutoff
+                    list.push_back(j);
+                    exclOut.push_back(exclMark[j]);
                 }
             };
             if (triclinic) {
                 // the images across a tilted face are shifted by whole cells: every cell is a candidate
                 for (int c = 0; c < numCells; c++) scanCell(c);
-                continue;
             }
-            for (int k = k0; k < k1; k++) {
-                const int c = cellOf[F.sorted[k]];
-                const int cx = c % nc[0], cy = (c / nc[0]) % nc[1], cz = c / (nc[0] * nc[1]);
-                for (int dz = -1; dz <= 1; dz++)
-                    for (int dy = -1; dy <= 1; dy++)
-                        for (int dx = -1; dx <= 1; dx++) {
-                            int x = cx + dx, y = cy + dy, z = cz + dz;
+            else {
+                // the cells that overlap the block's box grown by the cutoff, per axis (every cell of an axis whose
+                // range would wrap onto itself)
+                int from[3], count[3];
+                for (int e = 0; e < 3; e++) {
+                    const float cell = ext[e] / nc[e];
+                    const float a = (center[e] - half[e] - cutoff - lo[e]) / cell;
+                    const float z = (center[e] + half[e] + cutoff - lo[e]) / cell;
+                    from[e] = (int)std::floor(a);
+                    count[e] = (int)std::floor(z) - from[e] + 1;
+                    if (periodic && count[e] >= nc[e]) {
+                        from[e] = 0;
+                        count[e] = nc[e];
+                    }
+                }
+                for (int cz = from[2]; cz < from[2] + count[2]; cz++)
+                    for (int cy = from[1]; cy < from[1] + count[1]; cy++)
+                        for (int cx = from[0]; cx < from[0] + count[0]; cx++) {
+                            int x = cx, y = cy, z = cz;
                             if (periodic) {
                                 x = ((x % nc[0]) + nc[0]) % nc[0];
                                 y = ((y % nc[1]) + nc[1]) % nc[1];
@@ -277,6 +307,8 @@ void buildNeighborList(CpuPairForce& F, const float box[3][3], const float invDi
                             scanCell((z * nc[1] + y) * nc[0] + x);
                         }
             }
+            for (int k = k0; k < k1; k++)
+                for (int j : F.excl[F.sorted[k]]) exclMark[j] = 0;
         }
     });
 }
@@ -309,66 +341,128 @@ double evaluatePairForce(CpuPairForce& F, const double* xyz, const double* box9,
     F.threadEnergy.assign(T, 0.0);
     F.threadCount.assign(T, 0);
     const int nb = (n + kBlock - 1) / kBlock, st = F.stride;
+    const bool orderByIndex = !F.scheme.aboutSmallerWidth;
     std::atomic<int> next(0);
     tp.run([&](int t) {
+        using namespace simd;
         std::vector<float>& fo = F.threadForce[t];
         fo.assign(3 * (size_t)n, 0.0f);
         double energy = 0.0;
         long long count = 0;
+        const V8 cut2(cutoff2);
         for (int b = next++; b < nb; b = next++) {
             const int k0 = b * kBlock, k1 = std::min(n, k0 + kBlock);
-            for (int j : F.blockNbrs[b]) {
+            // the block's particles, one lane each (padding lanes repeat the last particle and stay masked)
+            float bx[kBlock], by[kBlock], bz[kBlock], bi[kBlock], ba[kBlock], bp[5][kBlock];
+            for (int l = 0; l < kBlock; l++) {
+                const int i = F.sorted[std::min(k0 + l, k1 - 1)];
+                bx[l] = F.pos[3 * i];
+                by[l] = F.pos[3 * i + 1];
+                bz[l] = F.pos[3 * i + 2];
+                bi[l] = (float)i;
+                ba[l] = (float)F.alch[i];
+                for (int k = 0; k < st; k++) bp[k][l] = F.params[(size_t)i * st + k];
+            }
+            const V8 X = V8::load(bx), Y = V8::load(by), Z = V8::load(bz), I = V8::load(bi), AL = V8::load(ba);
+            V8 P[5];
+            for (int k = 0; k < st; k++) P[k] = V8::load(bp[k]);
+            V8 fX, fY, fZ, eBlock;
+            const unsigned valid = (1u << (k1 - k0)) - 1u;
+            const std::vector<int>& list = F.blockNbrs[b];
+            const std::vector<uint8_t>& exclBits = F.blockExcl[b];
+            for (size_t q = 0; q < list.size(); q++) {
+                const int j = list[q];
                 const int sj = F.sortedPos[j];
-                const float xj = F.pos[3 * j], yj = F.pos[3 * j + 1], zj = F.pos[3 * j + 2];
-                const float* pj = &F.params[(size_t)j * st];
-                for (int k = k0; k < k1; k++) {     // one lane per block member
-                    if (sj <= k) continue;
-                    const int i = F.sorted[k];
-                    float dx = xj - F.pos[3 * i], dy = yj - F.pos[3 * i + 1], dz = zj - F.pos[3 * i + 2];
-                    if (periodic) minimumImage(dx, dy, dz, box, invDiag, triclinic);
-                    const float r2 = dx * dx + dy * dy + dz * dz;
-                    if (useCutoff && r2 >= cutoff2) continue;
-                    const std::vector<int>& ex = F.excl[i];
-                    if (!ex.empty() && std::binary_search(ex.begin(), ex.end(), j)) continue;
-                    const float* pi = &F.params[(size_t)i * st];
-                    // the lower particle index first (the order-2 overlap expands about its width)
-                    const float* a = i < j ? pi : pj;
-                    const float* c = i < j ? pj : pi;
-                    if (F.term == kDispersion ? a[3] * c[3] == 0.0f
-                                              : (F.term == kExchange ? a[1] * c[1] == 0.0f : a[2] * c[2] == 0.0f))
-                        continue;
-                    const float r = std::sqrt(r2);
-                    const bool alchPair = (F.alch[i] != 0) != (F.alch[j] != 0);
-                    float rEff = r;
-                    if (alchPair && soft6 > 0) rEff = std::pow(r2 * r2 * r2 + (1.0f - lam) * soft6, 1.0f / 6.0f);
-                    float e, dEdR;
-                    if (F.term == kDispersion)
-                        dispersionPair<float>(rEff, a[0], a[1], a[2], a[3], a[4], c[0], c[1], c[2], c[3], c[4],
-                                              F.dampingScale, e, dEdR);
-                    else if (F.term == kExchange) exchangePair<float>(rEff, a[0], a[1], c[0], c[1], F.scheme, e, dEdR);
-                    else shortRangePair<float>(rEff, a[0], a[1], a[2], c[0], c[1], c[2], F.scheme, e, dEdR);
-                    if (rEff != r) {
-                        const float q = r / rEff;
-                        dEdR *= q * q * q * q * q;
+                // lanes before j in the sorted order (each pair once), not excluded
+                const unsigned later = sj - k0 >= kBlock ? 0xffu : ((1u << (sj - k0)) - 1u);
+                const unsigned lanes = valid & later & ~(unsigned)exclBits[q];
+                if (!lanes) continue;
+                V8 dx = V8(F.pos[3 * j]) - X, dy = V8(F.pos[3 * j + 1]) - Y, dz = V8(F.pos[3 * j + 2]) - Z;
+                if (periodic) {
+                    if (triclinic) {
+                        V8 s3 = vround(dz * V8(invDiag[2]));
+                        dx -= s3 * V8(box[2][0]);
+                        dy -= s3 * V8(box[2][1]);
+                        dz -= s3 * V8(box[2][2]);
+                        V8 s2 = vround(dy * V8(invDiag[1]));
+                        dx -= s2 * V8(box[1][0]);
+                        dy -= s2 * V8(box[1][1]);
+                        dx -= vround(dx * V8(invDiag[0])) * V8(box[0][0]);
                     }
-                    if (useSwitch && r > sw) {
-                        const float u = (r - sw) * invSwitchWidth;
-                        const float sv = 1.0f + u * u * u * (-10.0f + u * (15.0f - u * 6.0f));
-                        const float sd = u * u * (-30.0f + u * (60.0f - u * 30.0f)) * invSwitchWidth;
-                        dEdR = dEdR * sv + e * sd;
-                        e *= sv;
+                    else {
+                        dx -= vround(dx * V8(invDiag[0])) * V8(box[0][0]);
+                        dy -= vround(dy * V8(invDiag[1])) * V8(box[1][1]);
+                        dz -= vround(dz * V8(invDiag[2])) * V8(box[2][2]);
                     }
-                    const float scale = alchPair ? lam : 1.0f;
-                    energy += (double)(scale * e);
-                    const float fs = scale * dEdR / r;
-                    fo[3 * i] += dx * fs;
-                    fo[3 * i + 1] += dy * fs;
-                    fo[3 * i + 2] += dz * fs;
-                    fo[3 * j] -= dx * fs;
-                    fo[3 * j + 1] -= dy * fs;
-                    fo[3 * j + 2] -= dz * fs;
-                    count++;
                 }
+                const V8 r2 = dx * dx + dy * dy + dz * dz;
+                V8 include = laneMask(lanes);
+                if (useCutoff) include = include & (r2 < cut2);
+                const float* pj = &F.params[(size_t)j * st];
+                V8 Q[5];
+                for (int k = 0; k < st; k++) Q[k] = V8(pj[k]);
+                const int gate = F.term == kDispersion ? 3 : (F.term == kExchange ? 1 : 2);
+                include = include & (P[gate] * Q[gate] > V8(0.0f));
+                if (!any(include)) continue;
+                const V8 r = vsqrt(r2);
+                const V8 alchLane = vabs(AL - V8((float)F.alch[j])) > V8(0.5f);
+                V8 rEff = r, softFactor(1.0f);
+                if (soft6 > 0 && any(alchLane & include)) {
+                    // per lane, as the reference does for the soft-core distance
+                    float rv[kBlock], av[kBlock], re[kBlock], fa[kBlock];
+                    r.store(rv);
+                    select(alchLane, V8(1.0f), V8(0.0f)).store(av);
+                    for (int l = 0; l < kBlock; l++) {
+                        re[l] = av[l] != 0 ? std::pow(rv[l] * rv[l] * rv[l] * rv[l] * rv[l] * rv[l] + (1.0f - lam) *
+                                                      soft6, 1.0f / 6.0f) : rv[l];
+                        const float qr = rv[l] / re[l];
+                        fa[l] = av[l] != 0 ? qr * qr * qr * qr * qr : 1.0f;
+                    }
+                    rEff = V8::load(re);
+                    softFactor = V8::load(fa);
+                }
+                // the order-2 overlap expands about the width of the particle with the lower index: it goes first
+                V8 A[5], C[5];
+                const V8 blockFirst = I < V8((float)j);
+                for (int k = 0; k < st; k++) {
+                    A[k] = orderByIndex ? select(blockFirst, P[k], Q[k]) : P[k];
+                    C[k] = orderByIndex ? select(blockFirst, Q[k], P[k]) : Q[k];
+                }
+                V8 e, dEdR;
+                if (F.term == kDispersion) dispersionPair(rEff, A, C, F.dampingScale, e, dEdR);
+                else if (F.term == kExchange) exchangePair(rEff, A, C, F.scheme, e, dEdR);
+                else shortRangePair(rEff, A, C, F.scheme, e, dEdR);
+                dEdR *= softFactor;
+                if (useSwitch) {
+                    const V8 u = zeroUnless(r > V8(sw), (r - V8(sw)) * V8(invSwitchWidth));
+                    const V8 sv = V8(1.0f) + u * u * u * (V8(-10.0f) + u * (V8(15.0f) - u * V8(6.0f)));
+                    const V8 sd = u * u * (V8(-30.0f) + u * (V8(60.0f) - u * V8(30.0f))) * V8(invSwitchWidth);
+                    dEdR = dEdR * sv + e * sd;
+                    e *= sv;
+                }
+                const V8 scale = select(alchLane, V8(lam), V8(1.0f));
+                eBlock += zeroUnless(include, scale * e);
+                // force on the block particle i: dE/dr (x_j - x_i)/r
+                const V8 fs = zeroUnless(include, scale * dEdR / r);
+                const V8 fx = dx * fs, fy = dy * fs, fz = dz * fs;
+                fX += fx;
+                fY += fy;
+                fZ += fz;
+                fo[3 * j] -= sum(fx);
+                fo[3 * j + 1] -= sum(fy);
+                fo[3 * j + 2] -= sum(fz);
+                count += __builtin_popcount((unsigned)_mm256_movemask_ps(include.v));
+            }
+            energy += (double)sum(eBlock);
+            float ox[kBlock], oy[kBlock], oz[kBlock];
+            fX.store(ox);
+            fY.store(oy);
+            fZ.store(oz);
+            for (int k = k0; k < k1; k++) {
+                const int i = F.sorted[k];
+                fo[3 * i] += ox[k - k0];
+                fo[3 * i + 1] += oy[k - k0];
+                fo[3 * i + 2] += oz[k - k0];
             }
         }
         F.threadEnergy[t] = energy;
