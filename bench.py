@@ -360,18 +360,22 @@ def run_ours(args, rank, world):
 def run_clusters(args, rank, world, num_clusters=4096, plain_sample=128):
     """Batched configuration: 4,096 water clusters of 2..32 waters (NoCutoff pair forces, ATM without cutoff), one
     energy+force evaluation of all of them per step through one CUDA graph, against the plain per-system path (one
-    Context per cluster, evaluated one after the other) on a sample of the same clusters.  Each rank evaluates its own
-    set of clusters (no collective)."""
+    Context per cluster, evaluated one after the other) on a sample of the same clusters.  With several GPUs the
+    4,096 clusters are partitioned over the ranks by a greedy balance of their work (interaxplugin.partition; no
+    collective on the data path) and each rank's energies are gathered on rank 0's host after the timed steps."""
     import torch
     from interaxplugin import BatchContext, Context
+    from interaxplugin import partition as PT
     from interaxplugin import workloads as W
 
     device = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(device)
-    rng = np.random.default_rng(args.seed + 7919 * rank)
+    sizes = W.cluster_sizes(num_clusters, args.seed)
+    shares = PT.assign([PT.cluster_cost(3 * int(w), int(w)) for w in sizes], world)
+    mine = shares[rank]
     systems, positions = [], []
-    for k in range(num_clusters):
-        s, p, _ = W.water_cluster(int(rng.integers(2, 33)), seed=args.seed * 100003 + 7919 * rank + k)
+    for k in mine:
+        s, p = W.cluster_of_set(k, sizes, args.seed)
         systems.append(s)
         positions.append(p)
     batch = BatchContext(systems, device=device)
@@ -379,12 +383,12 @@ def run_clusters(args, rank, world, num_clusters=4096, plain_sample=128):
     pos = np.ascontiguousarray(np.concatenate(positions))
     hpos = torch.from_numpy(pos).pin_memory()
     hfor = torch.empty(pos.shape, dtype=torch.float64).pin_memory()
-    hen = torch.empty((num_clusters, 4), dtype=torch.float64).pin_memory()
+    hen = torch.empty((len(mine), 4), dtype=torch.float64).pin_memory()
     batch.compute(positions)
     pairs, triples = batch.getCounts()
     dpos = torch.from_numpy(pos).cuda()
     dfor = torch.empty(pos.shape, dtype=torch.float64, device="cuda")
-    den = torch.empty((num_clusters, 4), dtype=torch.float64, device="cuda")
+    den = torch.empty((len(mine), 4), dtype=torch.float64, device="cuda")
     stream = torch.cuda.ExternalStream(L.ix_batch_get_stream(batch._batch))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
 
@@ -409,7 +413,9 @@ def run_clusters(args, rank, world, num_clusters=4096, plain_sample=128):
         ms = [device_step() for _ in range(args.steps)]
     step_ms = float(np.sum(ms))
     step_ms = rank_max(step_ms, world)
-    value = world * num_clusters * args.steps / (step_ms * 1e-3)
+    pairs = int(rank_sum(pairs, world))
+    triples = int(rank_sum(triples, world))
+    value = num_clusters * args.steps / (step_ms * 1e-3)
     # e2e: host positions in, host forces and energies out, per step
     e2e_t = 0.0
     for k in range(args.warmup + args.steps):
@@ -419,7 +425,9 @@ def run_clusters(args, rank, world, num_clusters=4096, plain_sample=128):
                                         ctypes.c_void_p(hfor.data_ptr()), ctypes.c_void_p(hen.data_ptr())))
         if k >= args.warmup:
             e2e_t += time.perf_counter() - t0
-    e2e = world * num_clusters * args.steps / e2e_t
+    e2e = num_clusters * args.steps / rank_max(e2e_t, world)
+    # the systems' energies gathered on rank 0's host, in cluster order
+    gathered = PT.gather(list(hen.numpy().sum(1)), shares, rank, world, PT.host_group(world))
     # the plain per-system drop-in: one Context per cluster, host API, on a sample of the clusters
     ctxs = [Context(systems[k], properties={"DeviceIndex": device}) for k in range(plain_sample)]
     for k, c in enumerate(ctxs):
@@ -435,19 +443,21 @@ def run_clusters(args, rank, world, num_clusters=4096, plain_sample=128):
         return
     line = {
         "metric": "evaluations/s", "value": value, "unit": "evaluations/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"{num_clusters} non-periodic water clusters of 2..32 waters per GPU, all four forces "
+        "config": {"workload": f"{num_clusters} non-periodic water clusters of 2..32 waters in all, all four forces "
                                "(NoCutoff pairs, ATM without cutoff), one batched evaluation per step",
-                   "atoms": int(pos.shape[0]), "pairs_per_step": pairs, "triples_per_step": triples,
-                   "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+                   "atoms_rank0": int(pos.shape[0]), "pairs_per_step": pairs, "triples_per_step": triples,
+                   "l2": "flushed between steps (256 MB write)",
+                   "parallelism": f"clusters partitioned over {world} GPUs by work" if world > 1 else "1 GPU"},
+        "gathered_systems": len(gathered),
         "plain_per_system": {"value": plain, "unit": "evaluations/s",
                              "sample": f"{plain_sample} of the clusters, one Context each, positions in and "
                                        "forces out per evaluation"},
         "batched_over_plain": e2e / plain,
         "e2e": {"value": e2e, "unit": "evaluations/s", "h2d_bytes_per_step": int(pos.nbytes),
                 "d2h_bytes_per_step": int(pos.nbytes + num_clusters * 4 * 8)},
-        "interactions_per_s": world * (pairs + triples) / (step_ms / args.steps * 1e-3),
+        "interactions_per_s": (pairs + triples) / (step_ms / args.steps * 1e-3),
         "clocks": clocks.summary(),
     }
     print(json.dumps(line))
@@ -461,25 +471,30 @@ def run_lambda(args, rank, world, num_windows=16, num_alchemical=30):
     the pair terms once at 0 (where the alchemical pairs contribute nothing), each window's alchemical pairs, and the
     three-body term (linear in lambda) at 0 and 1.  Each counts 16 full
     energy+force evaluations per step.  Compared with the plain path: setParameter + getState
-    per window."""
+    per window.  With several GPUs the windows are partitioned over the ranks (each rank holds the whole box and
+    evaluates its share of the windows; the window energies are gathered on rank 0's host)."""
     import torch
     from interaxplugin import Context, _capi
+    from interaxplugin import partition as PT
     from interaxplugin import workloads as W
 
     softcore = 0.1 if args.config == "lambda-softcore" else 0.0
     device = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(device)
     cfg = W.CONFIGS["96k"]
-    system, pos, box = W.water_box(cfg["num_waters"], cfg["box_length"], cfg["cutoff"], seed=args.seed + rank,
+    system, pos, box = W.water_box(cfg["num_waters"], cfg["box_length"], cfg["cutoff"], seed=args.seed,
                                    three_body_cutoff=cfg["three_body_cutoff"],
                                    alchemical_waters=range(num_alchemical), softcore_radius=softcore)
     ctx = Context(system, properties={"DeviceIndex": device})
     L = _capi.lib()
     n = system.getNumParticles()
     ctx.setPositions(pos)
-    values = np.linspace(0.0, 1.0, num_windows)
-    energies = np.zeros((num_windows, 4))
-    dfor = torch.empty((num_windows, n, 3), dtype=torch.float64, device="cuda")
+    all_values = np.linspace(0.0, 1.0, num_windows)
+    shares = PT.assign([1.0] * num_windows, world)
+    values = np.ascontiguousarray(all_values[shares[rank]])
+    local_windows = len(values)
+    energies = np.zeros((local_windows, 4))
+    dfor = torch.empty((local_windows, n, 3), dtype=torch.float64, device="cuda")
     stream = torch.cuda.ExternalStream(L.ix_get_stream(ctx._ctx))
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
     name = b"lambda_sterics"
@@ -489,8 +504,8 @@ def run_lambda(args, rank, world, num_windows=16, num_alchemical=30):
             flush.zero_()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        ctx._check(L.ix_compute_windows_device(ctx._ctx, name, num_windows, _capi.ptr(values), _capi.ptr(energies),
-                                               ctypes.c_void_p(dfor.data_ptr())))
+        ctx._check(L.ix_compute_windows_device(ctx._ctx, name, local_windows, _capi.ptr(values),
+                                               _capi.ptr(energies), ctypes.c_void_p(dfor.data_ptr())))
         b.record(stream)
         b.synchronize()
         return a.elapsed_time(b)
@@ -510,27 +525,28 @@ def run_lambda(args, rank, world, num_windows=16, num_alchemical=30):
     ctx._check(L.ix_get_launch_count(ctx._ctx, ctypes.byref(launches1)))
     step_ms = float(np.sum(ms))
     step_ms = rank_max(step_ms, world)
-    value = world * num_windows * args.steps / (step_ms * 1e-3)
+    value = num_windows * args.steps / (step_ms * 1e-3)
     # e2e: host positions in (pinned), every window's energies and forces out to host memory, per step
     hpos = torch.from_numpy(np.ascontiguousarray(pos)).pin_memory()
-    hfor = np.zeros((num_windows, n, 3))
+    hfor = np.zeros((local_windows, n, 3))
     e2e_t = 0.0
     for k in range(args.warmup + args.steps):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         ctx._check(L.ix_set_positions(ctx._ctx, ctypes.c_void_p(hpos.data_ptr()), None))
-        ctx._check(L.ix_compute_windows(ctx._ctx, name, num_windows, _capi.ptr(values), _capi.ptr(energies),
+        ctx._check(L.ix_compute_windows(ctx._ctx, name, local_windows, _capi.ptr(values), _capi.ptr(energies),
                                         _capi.ptr(hfor)))
         if k >= args.warmup:
             e2e_t += time.perf_counter() - t0
-    e2e = world * num_windows * args.steps / e2e_t
+    e2e = num_windows * args.steps / rank_max(e2e_t, world)
+    window_energies = PT.gather(list(energies.sum(1)), shares, rank, world, PT.host_group(world))
     # the plain path: one setParameter + getState per window
     reps = 2
     ctx.setParameter("lambda_sterics", 0.5)
     ctx.getState()
     t0 = time.perf_counter()
     for _ in range(reps):
-        for lam in values:
+        for lam in all_values:
             ctx.setParameter("lambda_sterics", lam)
             ctx.getState()
     plain = reps * num_windows / (time.perf_counter() - t0)
@@ -538,7 +554,7 @@ def run_lambda(args, rank, world, num_windows=16, num_alchemical=30):
         return
     line = {
         "metric": "evaluations/s", "value": value, "unit": "evaluations/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": step_ms / args.steps, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"96,000-atom water box (32,000 waters, 9.855 nm, cutoff 1.0 nm, ATM on 32,000 sites "
                                f"cutoff 0.8 nm), {num_alchemical} waters alchemical, {num_windows} lambda_sterics "
@@ -547,11 +563,13 @@ def run_lambda(args, rank, world, num_windows=16, num_alchemical=30):
                    else "pair terms once at 0 plus each window's alchemical pairs (soft core); ATM and LRC from 0 "
                         "and 1, interpolated",
                    "pairs_per_window": pairs, "triples_per_window": triples,
-                   "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
+                   "l2": "flushed between steps (256 MB write)",
+                   "parallelism": f"windows partitioned over {world} GPUs" if world > 1 else "1 GPU"},
+        "gathered_windows": len(window_energies),
         "plain_per_window": {"value": plain, "unit": "evaluations/s",
                              "sample": "setParameter + getState (forces to host) per window"},
         "windows_over_plain": e2e / plain,
-        "interactions_per_s": world * num_windows * (pairs + triples) / (step_ms / args.steps * 1e-3),
+        "interactions_per_s": num_windows * (pairs + triples) / (step_ms / args.steps * 1e-3),
         "e2e": {"value": e2e, "unit": "evaluations/s", "h2d_bytes_per_step": int(n * 3 * 8),
                 "d2h_bytes_per_step": int(num_windows * (n * 3 + 4) * 8)},
         "gpu_launches": int(launches1.value - launches0.value),
@@ -583,14 +601,17 @@ def run_served(args, rank, world, num_requests=20000, budget=120e9, plain_sample
     atoms, clusters below), each 1..50 velocity-Verlet steps of 1 fs, through the request server with a 120 GB device
     budget.  Evaluations = initial evaluation + one per step.  Throughput (`value`): the whole stream arriving at once.
     Latency: Poisson arrivals at --rate (below the capacity) for the first --latency-requests requests, from the
-    scheduled arrival to the completion seen by the server."""
+    scheduled arrival to the completion seen by the server.  With several GPUs the stream's requests are partitioned
+    over the ranks by a greedy balance of their estimated work (interaxplugin.partition), each rank serving its share
+    with its own server; throughput is the whole stream over the slowest rank's time."""
     import torch
     from interaxplugin import Context, Server
+    from interaxplugin import partition as PT
 
     device = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(device)
-    rng = np.random.default_rng(args.seed + 7919 * rank)
-    boxes, clusters = served_pool(args.seed + 100 * rank)
+    rng = np.random.default_rng(args.seed)
+    boxes, clusters = served_pool(args.seed)
     sizes_b = np.log([s.getNumParticles() for s, _, _ in boxes])
     sizes_c = np.log([s.getNumParticles() for s, _, _ in clusters])
     reqs = []
@@ -601,6 +622,12 @@ def run_served(args, rank, world, num_requests=20000, budget=120e9, plain_sample
         else:
             tpl = clusters[int(np.abs(sizes_c - a).argmin())]
         reqs.append((tpl, int(rng.integers(1, 51))))
+    all_requests = len(reqs)
+    all_evals = sum(n + 1 for _, n in reqs)
+    shares = PT.assign([PT.request_cost(t[0].getNumParticles(), n, t[0] in [b[0] for b in boxes]) for t, n in reqs],
+                       world)
+    reqs = [reqs[i] for i in shares[rank]]
+    num_requests = len(reqs)
     evals = sum(n + 1 for _, n in reqs)
     atoms = sum(t[0].getNumParticles() for t, _ in reqs)
     srv = Server(device=device, budget_bytes=budget, max_running=args.max_running, threads=args.server_threads,
@@ -647,7 +674,8 @@ def run_served(args, rank, world, num_requests=20000, budget=120e9, plain_sample
     wall_p, lat = stream(reqs[:m], np.cumsum(rng.exponential(1.0 / args.rate, m)))
     stats = srv.stats()
     srv.close()
-    value = world * evals / wall
+    wall = rank_max(wall, world)
+    value = all_evals / wall
     # the plain per-system path on a sample of the same requests: one Context per request, positions and
     # velocities in, steps, state out
     t_plain, e_plain = 0.0, 0
@@ -664,32 +692,32 @@ def run_served(args, rank, world, num_requests=20000, budget=120e9, plain_sample
     if rank != 0:
         return
     line = {
-        "metric": "evaluations/s", "value": value, "unit": "evaluations/s", "n_gpus": world, "steps": num_requests,
-        "warmup": 4, "ms_per_step": 1000 * wall / num_requests, "higher_is_better": True, "scaling": "weak",
+        "metric": "evaluations/s", "value": value, "unit": "evaluations/s", "n_gpus": world, "steps": all_requests,
+        "warmup": 4, "ms_per_step": 1000 * wall / all_requests, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": f"served stream of {num_requests} energy+force requests, sizes log-uniform 50..20,000 "
+        "config": {"workload": f"served stream of {all_requests} energy+force requests, sizes log-uniform 50..20,000 "
                                "atoms (periodic water boxes from 1,000 atoms, cutoff 1.0 nm, ATM 0.6 nm; clusters "
                                "below, NoCutoff), 1..50 velocity-Verlet steps of 1 fs each, 120 GB device budget; "
                                "throughput with the whole stream arriving at once; a step = one request",
-                   "evaluations": evals, "atoms_total": atoms, "wall_s": wall,
+                   "evaluations": all_evals, "atoms_rank0": atoms, "wall_s": wall,
                    "templates": f"{len(boxes)} box and {len(clusters)} cluster sizes, relaxed",
                    "max_running": args.max_running, "server_threads": args.server_threads,
                    "cohort_window_s": args.cohort_window,
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": f"requests partitioned over {world} GPUs by work" if world > 1 else "1 GPU"},
         "latency_ms": {"arrivals": f"Poisson at {args.rate:g} requests/s, the first {m} requests of the stream",
                        "p50": 1000 * float(np.percentile(lat, 50)), "p99": 1000 * float(np.percentile(lat, 99)),
                        "mean": 1000 * float(lat.mean()), "max": 1000 * float(lat.max()),
                        "requests_per_s": m / wall_p},
         "latency_at_saturation_ms": {"p50": 1000 * float(np.percentile(sat_lat, 50)),
                                      "p99": 1000 * float(np.percentile(sat_lat, 99))},
-        "requests_per_s": world * num_requests / wall,
+        "requests_per_s": all_requests / wall,
         "server": {k: stats[k] for k in ("contexts", "cohorts", "peak_reserved_bytes", "peak_arena_bytes",
                                          "worker_seconds")},
         "plain_per_system": {"value": plain, "unit": "evaluations/s",
                              "sample": f"the first {plain_sample} requests, one Context each, sequentially"},
         "served_over_plain": value / world / plain,
-        "e2e": {"value": value, "unit": "evaluations/s", "h2d_bytes_per_step": int(48 * atoms / num_requests),
-                "d2h_bytes_per_step": int(72 * atoms / num_requests + 32)},
+        "e2e": {"value": value, "unit": "evaluations/s", "h2d_bytes_per_step": int(48 * atoms / max(num_requests, 1)),
+                "d2h_bytes_per_step": int(72 * atoms / max(num_requests, 1) + 32)},
         "clocks": clocks.summary(),
     }
     print(json.dumps(line))

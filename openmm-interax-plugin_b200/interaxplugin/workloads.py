@@ -177,14 +177,19 @@ def water_cluster(num_waters, seed=0, params=None, three_body=True):
 def cluster_set(num_clusters, seed=1, stream=0):
     """The batched workload: num_clusters water clusters of 2..32 waters (configuration 2 of the benchmark), cluster k
     drawn from its own seed so that any subset can be rebuilt alone.  Returns (systems, positions)."""
-    rng = np.random.default_rng(seed + 7919 * stream)
-    sizes = rng.integers(2, 33, size=num_clusters)
+    sizes = cluster_sizes(num_clusters, seed, stream)
     systems, positions = [], []
     for k in range(num_clusters):
-        s, p, _ = water_cluster(int(sizes[k]), seed=seed * 100003 + 7919 * stream + k)
+        s, p = cluster_of_set(k, sizes, seed, stream)
         systems.append(s)
         positions.append(p)
     return systems, positions
+
+
+def cluster_of_set(k, sizes, seed=1, stream=0):
+    """Cluster k of cluster_set (sizes from cluster_sizes), built alone: (system, positions)."""
+    s, p, _ = water_cluster(int(sizes[k]), seed=seed * 100003 + 7919 * stream + k)
+    return s, p
 
 
 def cluster_sizes(num_clusters, seed=1, stream=0):
