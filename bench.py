@@ -40,8 +40,8 @@ F_TRIPLE = 151.0
 # (dram__bytes_read.sum + dram__bytes_write.sum); the kernel is FP32-issue bound, the traffic is reported beside it
 PAIR_TRAFFIC_BYTES = 10082304
 METRIC = "interactions/s"
-WORKLOAD = "water box 24,000 atoms (8,000 rigid-geometry waters, 6.208 nm periodic, cutoff 1.0 nm) + ATM on " \
-           "8,000 molecular sites (cutoff 0.6 nm); velocity-Verlet 1 fs"
+WORKLOAD = "water box 24,000 atoms (8,000 rigid 3-site waters, constrained, 6.208 nm periodic, cutoff 1.0 nm) + ATM " \
+           "on 8,000 molecular sites (cutoff 0.6 nm); velocity-Verlet 1 fs with SHAKE/RATTLE"
 
 
 def parse():
@@ -104,20 +104,25 @@ def rank_sum(x, world):
     return _rank_reduce(x, world, dist.ReduceOp.SUM)
 
 
-def build_system(args, rank):
+def build_system(args, rank, rigid=True):
     from interaxplugin import workloads as W
     cfg = W.CONFIGS[args.config]
-    # every rank runs an independent replica (a single box does not shard; see the design notes)
+    # every rank runs an independent replica (a single box does not shard)
     return W.water_box(cfg["num_waters"], cfg["box_length"], cfg["cutoff"], seed=args.seed + rank,
-                       three_body_cutoff=cfg["three_body_cutoff"])
+                       three_body_cutoff=cfg["three_body_cutoff"], rigid=rigid)
 
 
 def relax(ctx, system, positions, iterations=60, max_step=0.01):
-    """Steepest descent with a capped step, so that 1 fs velocity Verlet starts without the lattice's hot contacts."""
+    """Steepest descent with a capped step, so that 1 fs velocity Verlet starts without the lattice's hot contacts.
+    A System with constraints (rigid waters, three consecutive particles) moves each molecule as a whole along its
+    total force, so that its geometry is kept."""
     pos = positions.copy()
+    rigid = system.getNumConstraints() > 0
     for _ in range(iterations):
         ctx.setPositions(pos)
         f = ctx.getState(getEnergy=False).getForces()
+        if rigid:
+            f = np.repeat(f.reshape(-1, 3, 3).sum(1), 3, axis=0)
         fmax = np.sqrt((f ** 2).sum(1)).max()
         pos = pos + f * (max_step / max(fmax, 1e-12))
     ctx.setPositions(pos)
@@ -224,6 +229,36 @@ def run_reference(args, rank, world):
     print(json.dumps(line))
 
 
+def md_ns_per_day(args, built, device, dt_ps):
+    """ns/day of velocity-Verlet on a (system, positions, box) from build_system (relaxed first), over the bench's
+    step count: mean step time by CUDA events on the context's stream, L2 flushed between steps."""
+    import torch
+    from interaxplugin import Context, _capi
+    from interaxplugin import workloads as W
+    system, pos0, _ = built
+    ctx = Context(system, properties={"DeviceIndex": device})
+    L = _capi.lib()
+    pos = relax(ctx, system, pos0)
+    vel = np.ascontiguousarray(W.initial_velocities(system, 300.0, seed=0))
+    masses = np.array([system.getParticleMass(i) for i in range(system.getNumParticles())])
+    ctx._check(L.ix_md_set_masses(ctx._ctx, _capi.ptr(masses)))
+    ctx._check(L.ix_md_run(ctx._ctx, 1, dt_ps, None, _capi.ptr(vel), None))
+    stream = torch.cuda.ExternalStream(L.ix_get_stream(ctx._ctx))
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    ms = []
+    for step in range(args.warmup + args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        ctx._check(L.ix_md_steps_async(ctx._ctx, 1, dt_ps))
+        b.record(stream)
+        ctx._check(L.ix_md_finish(ctx._ctx, None, None, None))
+        if step >= args.warmup:
+            ms.append(a.elapsed_time(b))
+    return 86400 * dt_ps * 1e-3 / (float(np.mean(ms)) * 1e-3)
+
+
 def run_ours(args, rank, world):
     import torch
     from interaxplugin import Context, _capi
@@ -325,6 +360,23 @@ def run_ours(args, rank, world):
 
     if rank != 0:
         return
+    # the error of this run against the FP64 oracle: the last e2e frame, evaluated by both (outside the timed region)
+    import pyoracle
+    last = frames[-1].numpy()
+    e_or, f_or = pyoracle.evaluate(system, last, box)
+    f_gpu = hfor.numpy()
+    oracle_error = {"energy_rel": abs(energy.value - e_or) / abs(e_or),
+                    "force_rms_rel": float(np.sqrt(((f_gpu - f_or) ** 2).mean() / (f_or ** 2).mean())),
+                    "frame": "the last configuration of the e2e pass (rigid-water MD trajectory)"}
+    # the same box without constraints (flexible waters whose intramolecular pairs are excluded), for comparison
+    flex = md_ns_per_day(args, build_system(args, rank, rigid=False), device, dt_ps)
+    # the batched workload's evaluations/s beside the plain per-system path (one GPU)
+    batched = None
+    if world == 1:
+        cl = clusters_measure(argparse.Namespace(**{**vars(args), "steps": 10, "warmup": 3}), 0, 1)
+        batched = {"value": cl["value"], "unit": "evaluations/s", "e2e": cl["e2e"]["value"],
+                   "plain_per_system": cl["plain_per_system"]["value"], "batched_over_plain": cl["batched_over_plain"],
+                   "workload": cl["config"]["workload"]}
     pair_ms = float(np.mean(kernel_rows[:, 1]))
     atm_ms = float(np.mean(kernel_rows[:, 2]))
     pairs_per_launch = float(np.mean(kernel_rows[:, 3]))
@@ -338,6 +390,7 @@ def run_ours(args, rank, world):
         "config": {"workload": WORKLOAD, "atoms": n, "sites": system.getForce(3).getNumSites(),
                    "pairs_per_step": float(np.mean(rows[:, 3])), "triples_per_step": float(np.mean(rows[:, 4])),
                    "ns_per_day": 86400 * dt_ps * 1e-3 / (ms_per_step * 1e-3),
+                   "ns_per_day_unconstrained": flex,
                    "l2": "flushed between steps (256 MB write)", "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                      "frac": achieved / peak.value, "traffic": PAIR_TRAFFIC_BYTES,
@@ -349,6 +402,8 @@ def run_ours(args, rank, world):
                      "three_body_kernels_ms": atm_ms, "ops_per_triple": F_TRIPLE,
                      "three_body_achieved": triples_per_launch * F_TRIPLE / (atm_ms * 1e-3) / 1e12},
         "cpu_baseline": base,
+        "oracle_error": oracle_error,
+        "batched": batched,
         "e2e": {"value": e2e_value, "unit": METRIC, "h2d_bytes_per_step": n * 3 * 8,
                 "d2h_bytes_per_step": n * 3 * 8 + 4 * 8 + 8},
         "gpu_launches": int(launches1.value - launches0.value),
@@ -357,7 +412,13 @@ def run_ours(args, rank, world):
     print(json.dumps(line))
 
 
-def run_clusters(args, rank, world, num_clusters=4096, plain_sample=128):
+def run_clusters(args, rank, world):
+    line = clusters_measure(args, rank, world)
+    if rank == 0:
+        print(json.dumps(line))
+
+
+def clusters_measure(args, rank, world, num_clusters=4096, plain_sample=128):
     """Batched configuration: 4,096 water clusters of 2..32 waters (NoCutoff pair forces, ATM without cutoff), one
     energy+force evaluation of all of them per step through one CUDA graph, against the plain per-system path (one
     Context per cluster, evaluated one after the other) on a sample of the same clusters.  With several GPUs the
@@ -460,7 +521,7 @@ def run_clusters(args, rank, world, num_clusters=4096, plain_sample=128):
         "interactions_per_s": (pairs + triples) / (step_ms / args.steps * 1e-3),
         "clocks": clocks.summary(),
     }
-    print(json.dumps(line))
+    return line
 
 
 def run_lambda(args, rank, world, num_windows=16, num_alchemical=30):

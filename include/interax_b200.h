@@ -205,6 +205,14 @@ int ix_get_counts(ix_ctx* ctx, long long* num_pairs, long long* num_triples);
 int ix_md_set_masses(ix_ctx* ctx, const double* masses);
 int ix_md_run(ix_ctx* ctx, int num_steps, double dt, double* positions, double* velocities, double* energy);
 
+/* Distance constraints of the MD loop (OpenMM's System::addConstraint; the rigid 3-site waters of the benchmark):
+ * particles pairs[2k], pairs[2k+1] kept at distances[k] nm.  Each connected cluster of constrained particles (at most
+ * 8 particles) is solved by SHAKE after the drift and by RATTLE's velocity stage after the second half kick, to the
+ * relative tolerance given (on the squared distance, and on the stretching rate per ps).  num_constraints = 0 removes
+ * them.  A step whose constraints did not converge makes ix_md_finish return IX_ERR_STATE. */
+int ix_md_set_constraints(ix_ctx* ctx, int num_constraints, const int32_t* pairs, const double* distances,
+                          double tolerance);
+
 /* The same split in two: ix_md_steps_async enqueues `num_steps` steps on the context's stream and returns at once
  * (ix_md_run or ix_md_set_masses plus a first ix_md_run must have set the masses and velocities); ix_md_finish
  * synchronizes, checks the neighbor lists and copies the state out (any pointer may be NULL).  When the pair list

@@ -22,7 +22,7 @@
 
 namespace ix {
 
-constexpr float kSiteSkin = 0.1f;
+constexpr float kSiteSkin = IX_TUNE_SITE_SKIN;
 
 struct AtmConfig {
     int numSites;
@@ -60,8 +60,8 @@ struct AtmBuffers {
     unsigned long long* tripleCount;
 };
 
-constexpr int kAtmFast = 64;         // neighbor lists up to this length take the fast triple kernel
-constexpr int kAtmRound = 64;        // (B, C) pairs evaluated before their forces are gathered
+constexpr int kAtmFast = IX_TUNE_ATM_FAST;     // neighbor lists up to this length take the fast triple kernel
+constexpr int kAtmRound = IX_TUNE_ATM_ROUND;   // (B, C) pairs evaluated before their forces are gathered
 constexpr int kAtmFastWarps = 4;
 
 // The flat triangular index p = c (c - 1) / 2 + b of the pairs b < c < kAtmFast, decoded: b | c << 8.

@@ -751,6 +751,7 @@ int ix_batch_num_particles(const ix_batch* b, int* num_particles, int* num_syste
 void* ix_batch_get_stream(ix_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 int ix_batch_compute_device(ix_batch* b, const double* d_positions, double* d_forces, double* d_energies) {
+    NvtxRange nvtxRange("ix_batch_compute_device");
     if (!b) return IX_ERR_INVALID;
     IX_BCUDA(b, cudaSetDevice(b->device));
     if (!b->built || b->dirty) IX_TRY(buildBatch(b));
@@ -767,6 +768,7 @@ int ix_batch_compute_device(ix_batch* b, const double* d_positions, double* d_fo
 }
 
 int ix_batch_compute(ix_batch* b, const double* positions, double* forces, double* energies) {
+    NvtxRange nvtxRange("ix_batch_compute");
     if (!b) return IX_ERR_INVALID;
     if (!positions) return batchFail(b, IX_ERR_INVALID, "ix_batch_compute: positions is NULL");
     const size_t n3 = 3 * (size_t)b->particleStart.back();

@@ -4,6 +4,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <nvtx3/nvToolsExt.h>
+
+#include "ix_tuning.h"
+
 namespace ix {
 
 constexpr int kWarp = 32;
@@ -140,5 +144,14 @@ __device__ __forceinline__ float warpMinF(float v) {
     for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
+
+// A named NVTX range over a host scope (the API calls, graph captures and list growth), visible in Nsight Systems
+// timelines; with no profiler attached NVTX does nothing.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 }  // namespace ix

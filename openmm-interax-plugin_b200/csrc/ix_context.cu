@@ -307,6 +307,9 @@ struct ix_ctx {
     bool statusPending = false;
     int lastDeviceStatus = 0;
     int* dAddSlot = nullptr;             // slot in the caller's force buffer of each particle (ix_compute_device_posq)
+    // distance constraints of the MD loop (ix_md_set_constraints), as clusters solved by one thread each
+    int numConstraints = 0;
+    ConstraintClusters K{};
     // optional CUDA-event timing of the pair and triple kernels (ix_set_profiling)
     bool profiling = false;
     bool serialize = false;              // profiling level 2: the three-body chain runs after the pair chain
@@ -1357,6 +1360,7 @@ struct StepKick {
     const double* invMass;
     double* vel;
     double halfDt;
+    bool started = true;     // the step's first kernel checked the displacement and refreshed the sorted positions
 };
 
 // `kick`: an MD step whose first kernel (kStepStart) has already moved the particles, checked their displacement and
@@ -1418,7 +1422,7 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         const int tpb = 256;
         const int gN = (n + tpb - 1) / tpb, gNp = (L.np + tpb - 1) / tpb;
         const int gCells = (L.numCells + tpb - 1) / tpb;
-        const bool stepStarted = kick != nullptr;
+        const bool stepStarted = kick != nullptr && kick->started;
         if (!stepStarted) {
             kCheckDisplacement<<<gN, tpb, 0, st>>>(L, 0.25f * kPairSkin * kPairSkin);
             ctx->launches += 1;
@@ -1471,12 +1475,17 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
             if ((terms >> t) & 1u)
                 uniform = uniform && ((ctx->pairGatesAll >> t) & 1u) &&
                           (!((ctx->pairAlchAny >> t) & 1u) || C.lambda[t] == 1.0f);
-        if (lean && table && uniform) kPairTiles<true, true, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
-        else if (lean && uniform) kPairTiles<true, false, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
-        else if (lean && table) kPairTiles<true, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
-        else if (lean) kPairTiles<true, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
-        else if (table) kPairTiles<false, true><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
-        else kPairTiles<false, false><<<grid, 32 * kPairWarps, 0, st>>>(L, ctx->P, C);
+        // a small class-pair table is staged in shared memory by each block
+        PairBuffers P = ctx->P;
+        const size_t tableBytes = (size_t)P.numClasses * P.numClasses * sizeof(PairCoef);
+        const size_t dyn = table && tableBytes <= (size_t)IX_TUNE_PAIR_SHARED_TABLE_BYTES ? tableBytes : 0;
+        P.coefShared = dyn > 0;
+        if (lean && table && uniform) kPairTiles<true, true, true><<<grid, 32 * kPairWarps, dyn, st>>>(L, P, C);
+        else if (lean && uniform) kPairTiles<true, false, true><<<grid, 32 * kPairWarps, 0, st>>>(L, P, C);
+        else if (lean && table) kPairTiles<true, true><<<grid, 32 * kPairWarps, dyn, st>>>(L, P, C);
+        else if (lean) kPairTiles<true, false><<<grid, 32 * kPairWarps, 0, st>>>(L, P, C);
+        else if (table) kPairTiles<false, true><<<grid, 32 * kPairWarps, dyn, st>>>(L, P, C);
+        else kPairTiles<false, false><<<grid, 32 * kPairWarps, 0, st>>>(L, P, C);
         ctx->launches += 1;
         recordTiming(ctx, 1, st);
         ctx->evPair = ctx->profiling;
@@ -1543,6 +1552,7 @@ static int checkOverflow(ix_ctx* ctx, unsigned terms, bool& redo) {
 
 // The same from flags already copied to the host (6 ints from ctx->dFlags).
 static int checkOverflowFlags(ix_ctx* ctx, unsigned terms, const int* flags, bool& redo) {
+    NvtxRange nvtxRange("list overflow check");
     redo = false;
     if ((terms & 7u) && flags[1]) {
         long long tiles = 0;
@@ -1592,6 +1602,7 @@ static int launchGraph(ix_ctx* ctx, LaunchGraph& g, const GraphKey& key, F&& enq
     if (!ctx->useGraphs) return enqueue();
     if (!g.exec || g.version != ctx->version || !(g.key == key)) {
         const long long before = ctx->launches;
+        NvtxRange nvtxRange("graph capture");
         IX_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
         ctx->capturing = true;
         const int rc = enqueue();
@@ -1954,6 +1965,7 @@ int ix_set_parameter(ix_ctx* ctx, const char* name, double value) {
 }
 
 int ix_set_positions(ix_ctx* ctx, const double* positions, const double* box) {
+    NvtxRange nvtxRange("ix_set_positions");
     if (!ctx) return IX_ERR_INVALID;
     ctx->mdForcesValid = false;
     if (!positions) return fail(ctx, IX_ERR_INVALID, "ix_set_positions: positions is NULL");
@@ -2037,6 +2049,7 @@ static int evaluateResident(ix_ctx* ctx, unsigned terms, double e[4], LaunchGrap
 
 int ix_compute(ix_ctx* ctx, int groups, int include_forces, int include_energy, double* term_energies,
                double* energy, double* forces) {
+    NvtxRange nvtxRange("ix_compute");
     if (!ctx) return IX_ERR_INVALID;
     ctx->mdForcesValid = false;
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -2159,6 +2172,7 @@ int ix_get_device_status(ix_ctx* ctx, int* status) {
 int ix_compute_device_posq(ix_ctx* ctx, int groups, int posq_format, const void* d_posq,
                            const void* d_posq_correction, const int32_t* d_atom_index, const double* box,
                            long long* d_force_fixed, int force_stride, double* d_energy, int* d_status) {
+    NvtxRange nvtxRange("ix_compute_device_posq");
     if (!ctx) return IX_ERR_INVALID;
     if (posq_format != IX_POSQ_FLOAT4 && posq_format != IX_POSQ_FLOAT4_CORRECTED && posq_format != IX_POSQ_DOUBLE4)
         return fail(ctx, IX_ERR_INVALID, "ix_compute_device_posq: unknown position format %d", posq_format);
@@ -2220,6 +2234,7 @@ int ix_compute_device_posq(ix_ctx* ctx, int groups, int posq_format, const void*
 }
 
 int ix_compute_device(ix_ctx* ctx, int groups, long long* d_force_fixed, int force_stride, double* d_term_energies) {
+    NvtxRange nvtxRange("ix_compute_device");
     if (!ctx) return IX_ERR_INVALID;
     if (force_stride < ctx->n) return fail(ctx, IX_ERR_INVALID, "ix_compute_device: stride smaller than the particle count");
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -2241,6 +2256,7 @@ int ix_compute_device(ix_ctx* ctx, int groups, long long* d_force_fixed, int for
 
 int ix_compute_device_f64(ix_ctx* ctx, int groups, const double* d_positions, const double* box, double* d_forces,
                           double* d_term_energies) {
+    NvtxRange nvtxRange("ix_compute_device_f64");
     if (!ctx) return IX_ERR_INVALID;
     ctx->mdForcesValid = false;
     ctx->mdPending.clear();
@@ -2372,21 +2388,43 @@ static int enqueueSteps(ix_ctx* ctx, int num_steps, double dt) {
     // there are pair terms), the evaluation at the new positions, whose finishing kernel applies the second half kick
     auto step = [&]() -> int {
         if (!terms) {
-            kVerletFirstHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos);
+            if (ctx->numConstraints)
+                kConstrainedDrift<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(ctx->K, dt, ctx->dInvMass,
+                                                                                    ctx->dOutForces, ctx->dVel,
+                                                                                    ctx->dPos);
+            else
+                kVerletFirstHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel,
+                                                             ctx->dPos);
             kVerletSecondHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel);
             ctx->launches += 2;
+            if (ctx->numConstraints) {
+                kConstrainVelocities<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(ctx->K, ctx->dInvMass,
+                                                                                       ctx->dPos, ctx->dVel);
+                ctx->launches += 1;
+            }
             IX_CUDA(ctx, cudaGetLastError());
             return IX_OK;
         }
-        if (terms & 7u)
+        StepKick kick{ctx->dInvMass, ctx->dVel, 0.5 * dt};
+        if (ctx->numConstraints) {
+            // the constrained clusters move together; the evaluation then checks the displacements itself
+            kConstrainedDrift<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(ctx->K, dt, ctx->dInvMass,
+                                                                                ctx->dOutForces, ctx->dVel, ctx->dPos);
+            kick.started = false;
+        }
+        else if (terms & 7u)
             // 128-thread blocks: a latency-bound gather by particle, spread over every SM
             kStepStart<<<(n + 127) / 128, 128, 0, ctx->stream>>>(ctx->L, ctx->dPos, dt, ctx->dInvMass, ctx->dOutForces,
                                                                 ctx->dVel, 0.25f * kPairSkin * kPairSkin);
         else
             kVerletFirstHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos);
         ctx->launches += 1;
-        const StepKick kick{ctx->dInvMass, ctx->dVel, 0.5 * dt};
         IX_TRY(launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0, &kick));
+        if (ctx->numConstraints) {
+            kConstrainVelocities<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(ctx->K, ctx->dInvMass, ctx->dPos,
+                                                                                   ctx->dVel);
+            ctx->launches += 1;
+        }
         IX_CUDA(ctx, cudaGetLastError());
         return IX_OK;
     };
@@ -2417,6 +2455,7 @@ extern "C" {
 // ix_md_set_state).  The first call after a finish saves the state, so that ix_md_finish can rerun the steps after a
 // neighbor-list overflow.
 int ix_md_steps_async(ix_ctx* ctx, int num_steps, double dt) {
+    NvtxRange nvtxRange("ix_md_steps_async");
     if (!ctx) return IX_ERR_INVALID;
     if (!ctx->haveMasses) return fail(ctx, IX_ERR_STATE, "ix_md_steps_async: masses have not been set");
     if (!ctx->havePositions) return fail(ctx, IX_ERR_STATE, "positions have not been set");
@@ -2724,6 +2763,7 @@ static int windowsPass(ix_ctx* ctx, const std::string& name, int num_windows, co
 // has its own cached graph, so repeated window sets replay without capturing.  The parameter keeps its value.
 static int computeWindows(ix_ctx* ctx, const char* parameter, int num_windows, const double* values, double* energies,
                           double* d_forces) {
+    NvtxRange nvtxRange("ix_compute_windows");
     if (!parameter || num_windows < 0 || (num_windows > 0 && (!values || !energies)))
         return fail(ctx, IX_ERR_INVALID, "ix_compute_windows: null argument");
     for (int w = 0; w < num_windows; w++)
@@ -2776,6 +2816,7 @@ int ix_get_launch_count(ix_ctx* ctx, long long* launches) {
 // state saved before the steps is restored and the steps are run again, as OpenMM recomputes a step whose neighbor
 // list overflowed; a three-body list overflow needs no rerun (those sites scan every later site).
 int ix_md_finish(ix_ctx* ctx, double* positions, double* velocities, double* energy) {
+    NvtxRange nvtxRange("ix_md_finish");
     if (!ctx) return IX_ERR_INVALID;
     IX_CUDA(ctx, cudaSetDevice(ctx->device));
     unsigned terms = selectedTerms(ctx, -1);
@@ -2795,6 +2836,15 @@ int ix_md_finish(ix_ctx* ctx, double* positions, double* velocities, double* ene
         ctx->mdReruns++;
     }
     ctx->mdPending.clear();
+    if (ctx->numConstraints) {
+        int failed = 0;
+        IX_CUDA(ctx, cudaMemcpy(&failed, ctx->K.fail, sizeof(int), cudaMemcpyDeviceToHost));
+        if (failed) {
+            const int zero = 0;
+            IX_CUDA(ctx, cudaMemcpy(ctx->K.fail, &zero, sizeof(int), cudaMemcpyHostToDevice));
+            return fail(ctx, IX_ERR_STATE, "the constraints did not converge during the MD steps");
+        }
+    }
     unsigned long long c[2] = {0, 0};
     IX_CUDA(ctx, cudaMemcpy(c, ctx->dCounts + 2, sizeof(c), cudaMemcpyDeviceToHost));
     ctx->lastPairs = (terms & 7u) ? (long long)c[0] : 0;
@@ -2809,6 +2859,84 @@ int ix_md_finish(ix_ctx* ctx, double* positions, double* velocities, double* ene
         if (terms) IX_CUDA(ctx, cudaMemcpy(e, ctx->dOutEnergy, sizeof(e), cudaMemcpyDeviceToHost));
         *energy = e[0] + e[1] + e[2] + e[3];
     }
+    return IX_OK;
+}
+
+int ix_md_set_constraints(ix_ctx* ctx, int num_constraints, const int32_t* pairs, const double* distances,
+                          double tolerance) {
+    if (!ctx) return IX_ERR_INVALID;
+    if (num_constraints < 0 || (num_constraints > 0 && (!pairs || !distances)))
+        return fail(ctx, IX_ERR_INVALID, "ix_md_set_constraints: invalid arguments");
+    if (!(tolerance > 0.0)) return fail(ctx, IX_ERR_INVALID, "ix_md_set_constraints: the tolerance must be positive");
+    const int n = ctx->n;
+    // clusters: the connected components of the constraint graph (union-find), single particles as their own
+    std::vector<int> parent(n);
+    for (int i = 0; i < n; i++) parent[i] = i;
+    auto root = [&](int i) {
+        while (parent[i] != i) i = parent[i] = parent[parent[i]];
+        return i;
+    };
+    for (int k = 0; k < num_constraints; k++) {
+        const int a = pairs[2 * k], b = pairs[2 * k + 1];
+        if (a < 0 || b < 0 || a >= n || b >= n || a == b)
+            return fail(ctx, IX_ERR_INVALID, "Illegal particle index for a constraint: %d, %d", a, b);
+        if (!(distances[k] > 0.0)) return fail(ctx, IX_ERR_INVALID, "Illegal constraint distance: %g", distances[k]);
+        const int ra = root(a), rb = root(b);
+        if (ra != rb) parent[std::max(ra, rb)] = std::min(ra, rb);
+    }
+    std::vector<int> clusterOf(n, -1), particleStart{0}, particles, members;
+    std::vector<std::vector<int>> byRoot(n);
+    for (int i = 0; i < n; i++) byRoot[root(i)].push_back(i);
+    std::vector<int> local(n, 0);
+    for (int r = 0; r < n; r++) {
+        if (byRoot[r].empty()) continue;
+        if ((int)byRoot[r].size() > kMaxClusterParticles)
+            return fail(ctx, IX_ERR_INVALID, "a cluster of %zu constrained particles (the limit is %d)",
+                        byRoot[r].size(), kMaxClusterParticles);
+        const int c = (int)particleStart.size() - 1;
+        for (size_t k = 0; k < byRoot[r].size(); k++) {
+            clusterOf[byRoot[r][k]] = c;
+            local[byRoot[r][k]] = (int)k;
+            particles.push_back(byRoot[r][k]);
+        }
+        particleStart.push_back((int)particles.size());
+    }
+    const int numClusters = (int)particleStart.size() - 1;
+    std::vector<std::vector<int>> consOf(numClusters);
+    for (int k = 0; k < num_constraints; k++) consOf[clusterOf[pairs[2 * k]]].push_back(k);
+    std::vector<int> consStart{0};
+    std::vector<int2> pair;
+    std::vector<double> dist2;
+    for (int c = 0; c < numClusters; c++) {
+        for (int k : consOf[c]) {
+            pair.push_back(make_int2(local[pairs[2 * k]], local[pairs[2 * k + 1]]));
+            dist2.push_back(distances[k] * distances[k]);
+        }
+        consStart.push_back((int)pair.size());
+    }
+    IX_CUDA(ctx, cudaSetDevice(ctx->device));
+    int *dPS, *dP, *dCS, *dFail;
+    int2* dPair;
+    double* dD2;
+    IX_TRY(deviceAlloc(ctx, "clusterParticleStart", particleStart.size(), &dPS));
+    IX_TRY(deviceAlloc(ctx, "clusterParticles", particles.size(), &dP));
+    IX_TRY(deviceAlloc(ctx, "clusterConstraintStart", consStart.size(), &dCS));
+    IX_TRY(deviceAlloc(ctx, "constraintPairs", std::max<size_t>(pair.size(), 1), &dPair));
+    IX_TRY(deviceAlloc(ctx, "constraintDist2", std::max<size_t>(dist2.size(), 1), &dD2));
+    IX_TRY(deviceAlloc(ctx, "constraintFail", 1, &dFail));
+    IX_TRY(stageCopy(ctx, dPS, particleStart.data(), particleStart.size() * sizeof(int)));
+    IX_TRY(stageCopy(ctx, dP, particles.data(), particles.size() * sizeof(int)));
+    IX_TRY(stageCopy(ctx, dCS, consStart.data(), consStart.size() * sizeof(int)));
+    if (!pair.empty()) {
+        IX_TRY(stageCopy(ctx, dPair, pair.data(), pair.size() * sizeof(int2)));
+        IX_TRY(stageCopy(ctx, dD2, dist2.data(), dist2.size() * sizeof(double)));
+    }
+    IX_CUDA(ctx, cudaMemsetAsync(dFail, 0, sizeof(int), ctx->stream));
+    IX_TRY(uploadsDone(ctx));
+    ctx->K = ConstraintClusters{numClusters, dPS, dP, dCS, dPair, dD2, tolerance, dFail};
+    ctx->numConstraints = num_constraints;
+    ctx->mdPending.clear();
+    bumpVersion(ctx);
     return IX_OK;
 }
 
@@ -2962,6 +3090,7 @@ int ix_three_body_noalloc(int num_particles, const double* d_positions, const do
                           double cutoff, double scale_factor, int damping_method, double damping_scale,
                           double centroid_damping_radius, int periodic, double lambda, double* d_forces,
                           double* d_energy, void* stream) {
+    NvtxRange nvtxRange("ix_three_body_noalloc");
     if (num_particles <= 0 || num_particles > kNoAllocMaxParticles)
         return fail(nullptr, IX_ERR_INVALID, "ix_three_body_noalloc: %d particles (the limit is %d)", num_particles,
                     kNoAllocMaxParticles);

@@ -16,7 +16,7 @@
 
 namespace ix {
 
-constexpr float kPairSkin = 0.1f;    // nm; rebuild when a particle has moved by more than half of it
+constexpr float kPairSkin = IX_TUNE_PAIR_SKIN;   // nm; rebuild when a particle has moved by more than half of it
 
 // Particle flags in the sorted parameter arrays.
 constexpr int kFlagReal = 1 << 3;

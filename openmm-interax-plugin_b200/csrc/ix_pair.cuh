@@ -62,6 +62,7 @@ struct PairBuffers {
     unsigned long long* pairCount;
     const PairCoef* coef;        // class-pair coefficients (numClasses^2), or null
     int numClasses;
+    int coefShared;              // the launch gives dynamic shared memory for the table: it is staged there
     const int* taskTiles;        // null: every tile is a task; else the tiles of the tasks (energies go to task slots)
     int numTasks;
 };
@@ -242,8 +243,11 @@ __device__ __forceinline__ void minimumImageFF(float& xh, float& xl, float& yh, 
 }
 
 
-constexpr int kPairWarps = 4;
-constexpr int kPairRound = 128;  // queued pairs computed before their forces are gathered
+constexpr int kPairWarps = IX_TUNE_PAIR_WARPS;
+// 1: each tile's column lists (the queue positions of each column's pairs) are built once with the queue, and the
+// column forces of every round are read along them; 0: each round finds them from the row masks
+constexpr int kPairColumnLists = IX_TUNE_PAIR_COLUMN_LISTS;
+constexpr int kPairRound = IX_TUNE_PAIR_ROUND;   // queued pairs computed before their forces are gathered
 
 // Per-warp shared memory of the pair kernel (about 6.8 KB, so that eight 4-warp blocks fit on an SM).  Parameters
 // are not staged: the compute phase reads them through the read-only cache by sorted slot.
@@ -256,6 +260,7 @@ struct PairWarpStorage {
     unsigned rowMask[32];
     unsigned short queue[1024];  // the tile's candidate pairs, row by row: (i << 5) | j
     float4 force[kPairRound];    // force on i of each pair of the current round (j receives the opposite)
+    unsigned short colList[kPairColumnLists ? 1024 : 1];   // queue positions of each column's pairs, column by column
 };
 
 __device__ __forceinline__ void stageParticle(PairWarpStorage& S, int side, int lane, int s, double cx, double cy,
@@ -293,7 +298,8 @@ __device__ __forceinline__ void flushForce(const float f[3], int s, int np, long
 template <bool LEAN, bool TABLE, bool UNIFORM>
 __device__ __forceinline__ float4 computeQueuedPair(PairWarpStorage& S, int entry, int iBase, bool perPairImage,
                                                     const PairTermConfig& C, const ListBuffers& L,
-                                                    const PairBuffers& P, float e[3], unsigned& pairs) {
+                                                    const PairBuffers& P, const PairCoef* coef, float e[3],
+                                                    unsigned& pairs) {
     const int i = entry >> 5, j = entry & 31;
     const float4 hi_i = S.hi[0][i], hi_j = S.hi[1][j], lo_i = S.lo[0][i], lo_j = S.lo[1][j];
     float dxh = hi_j.x - hi_i.x, dyh = hi_j.y - hi_i.y, dzh = hi_j.z - hi_i.z;
@@ -321,7 +327,7 @@ __device__ __forceinline__ float4 computeQueuedPair(PairWarpStorage& S, int entr
     float dEdR;
     if (TABLE) {
         const int ci = (fi >> kClassShift) & 0xff, cj = (fj >> kClassShift) & 0xff;
-        dEdR = pairTermsTable<LEAN, UNIFORM>(C, r, invR, P.coef + ci * P.numClasses + cj, fi, fj, e);
+        dEdR = pairTermsTable<LEAN, UNIFORM>(C, r, invR, coef + ci * P.numClasses + cj, fi, fj, e);
     }
     else {
         const int si = iBase + i, sj = S.jslot[j];
@@ -337,11 +343,21 @@ __device__ __forceinline__ float4 computeQueuedPair(PairWarpStorage& S, int entr
 }
 
 template <bool LEAN, bool TABLE, bool UNIFORM = false>
-__global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, PairBuffers P, PairTermConfig C) {
+__global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPairTiles(ListBuffers L, PairBuffers P, PairTermConfig C) {
     __shared__ PairWarpStorage storage[kPairWarps];
+    extern __shared__ float4 pairShared[];
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     PairWarpStorage& S = storage[warp];
+    // the class-pair table, staged in shared memory when the launch gives room for it
+    const PairCoef* coef = P.coef;
+    if (TABLE && P.coefShared) {
+        const int words = P.numClasses * P.numClasses * (int)(sizeof(PairCoef) / sizeof(float4));
+        const float4* src = reinterpret_cast<const float4*>(P.coef);
+        for (int k = threadIdx.x; k < words; k += blockDim.x) pairShared[k] = __ldg(src + k);
+        __syncthreads();
+        coef = reinterpret_cast<const PairCoef*>(pairShared);
+    }
     const int numTasks = P.taskTiles ? P.numTasks : min(*L.numTiles, L.tileCap);
     const unsigned ltMask = laneMaskLt();
     unsigned long long pairs = 0;
@@ -387,6 +403,25 @@ __global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, 
             for (unsigned m = row, q = start; m; m &= m - 1, q++)
                 S.queue[q] = (unsigned short)((lane << 5) | (__ffs(m) - 1));
             __syncwarp();
+            // column lists: for each row i of this lane's column, the position of (i, lane) in the queue (rising)
+            int colPtr = 0, colEnd = 0;
+            if (kPairColumnLists) {
+                const int ccount = __popc(column);
+                int cstart = ccount;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(0xffffffffu, cstart, o);
+                    if (lane >= o) cstart += v;
+                }
+                cstart -= ccount;
+                colPtr = cstart;
+                colEnd = cstart + ccount;
+                for (unsigned m = column, q = cstart; m; m &= m - 1, q++) {
+                    const int i = __ffs(m) - 1;
+                    S.colList[q] = (unsigned short)(S.rowStart[i] + __popc(S.rowMask[i] & ltMask));
+                }
+                __syncwarp();
+            }
             float e[3] = {0.0f, 0.0f, 0.0f};
             float fj[3] = {0.0f, 0.0f, 0.0f};
             unsigned tilePairs = 0;
@@ -394,7 +429,7 @@ __global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, 
                 const int n = min(kPairRound, total - base);
                 for (int p = lane; p < n; p += 32)
                     S.force[p] = computeQueuedPair<LEAN, TABLE, UNIFORM>(S, S.queue[base + p], iBase, perPairImage,
-                                                                          C, L, P, e, tilePairs);
+                                                                          C, L, P, coef, e, tilePairs);
                 __syncwarp();
                 // i side: this lane's row, contiguous in the queue
                 const int a = max(start, base), b = min(start + count, base + n);
@@ -404,17 +439,30 @@ __global__ void __launch_bounds__(32 * kPairWarps, 8) kPairTiles(ListBuffers L, 
                     fi[1] += f.y;
                     fi[2] += f.z;
                 }
-                // j side: the pair (i, lane) of each row i of this round that holds it
-                unsigned rows = column & __ballot_sync(0xffffffffu, start < base + n && start + count > base);
-                while (rows) {
-                    const int i = __ffs(rows) - 1;
-                    rows &= rows - 1;
-                    const int q = S.rowStart[i] + __popc(S.rowMask[i] & ltMask) - base;
-                    if (q >= 0 && q < n) {
+                if (kPairColumnLists) {
+                    // j side: along this lane's column list, the positions inside this round
+                    for (; colPtr < colEnd; colPtr++) {
+                        const int q = S.colList[colPtr] - base;
+                        if (q >= n) break;
                         const float4 f = S.force[q];
                         fj[0] -= f.x;
                         fj[1] -= f.y;
                         fj[2] -= f.z;
+                    }
+                }
+                else {
+                    // j side: the pair (i, lane) of each row i of this round that holds it
+                    unsigned rows = column & __ballot_sync(0xffffffffu, start < base + n && start + count > base);
+                    while (rows) {
+                        const int i = __ffs(rows) - 1;
+                        rows &= rows - 1;
+                        const int q = S.rowStart[i] + __popc(S.rowMask[i] & ltMask) - base;
+                        if (q >= 0 && q < n) {
+                            const float4 f = S.force[q];
+                            fj[0] -= f.x;
+                            fj[1] -= f.y;
+                            fj[2] -= f.z;
+                        }
                     }
                 }
                 __syncwarp();

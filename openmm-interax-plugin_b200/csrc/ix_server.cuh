@@ -884,6 +884,7 @@ void ix_server_destroy(ix_server* S) {
 const char* ix_server_last_error(const ix_server* S) { return S ? S->error.c_str() : g_createError.c_str(); }
 
 int ix_server_submit(ix_server* S, ix_ctx* request, int steps, double dt, long long* id) {
+    NvtxRange nvtxRange("ix_server_submit");
     if (!S || !request) return IX_ERR_INVALID;
     if (request->stream || request->device != -1)
         return serverFail(S, IX_ERR_INVALID, "ix_server_submit: not a request description (use ix_request_create)");

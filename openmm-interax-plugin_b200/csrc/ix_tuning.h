@@ -1,0 +1,39 @@
+// Tile and schedule constants of the kernels.  The autotuner (openmm-interax-plugin_b200/tune.py) times candidate
+// values on the benchmark's shapes on the GPU and records the chosen ones in openmm-interax-plugin_b200/tuning.json;
+// the build passes them to the compiler as the IX_TUNE_* macros below.  The defaults here are used only when a build
+// is made without that file.
+#pragma once
+
+// pair kernel: warps per thread block, queued pairs evaluated before their forces are gathered, and the minimum
+// resident blocks per SM the compiler is told to fit (which bounds its registers per thread)
+#ifndef IX_TUNE_PAIR_WARPS
+#define IX_TUNE_PAIR_WARPS 4
+#endif
+#ifndef IX_TUNE_PAIR_ROUND
+#define IX_TUNE_PAIR_ROUND 128
+#endif
+#ifndef IX_TUNE_PAIR_MIN_BLOCKS
+#define IX_TUNE_PAIR_MIN_BLOCKS 8
+#endif
+// pair kernel: 1 = per-tile column lists for the column-force gather, 0 = found from the row masks each round
+#ifndef IX_TUNE_PAIR_COLUMN_LISTS
+#define IX_TUNE_PAIR_COLUMN_LISTS 0
+#endif
+// pair kernel: largest class-pair table (bytes) staged in shared memory; larger tables are read through the cache
+#ifndef IX_TUNE_PAIR_SHARED_TABLE_BYTES
+#define IX_TUNE_PAIR_SHARED_TABLE_BYTES 0
+#endif
+// pair list: skin (nm) of the list cutoff; the list is rebuilt when a particle has moved by half of it
+#ifndef IX_TUNE_PAIR_SKIN
+#define IX_TUNE_PAIR_SKIN 0.1f
+#endif
+// three-body: skin of the site lists, the longest list the fast triple kernel takes, (B, C) pairs per round
+#ifndef IX_TUNE_SITE_SKIN
+#define IX_TUNE_SITE_SKIN 0.1f
+#endif
+#ifndef IX_TUNE_ATM_FAST
+#define IX_TUNE_ATM_FAST 64
+#endif
+#ifndef IX_TUNE_ATM_ROUND
+#define IX_TUNE_ATM_ROUND 64
+#endif

@@ -1,11 +1,13 @@
 """ctypes binding of the C ABI in include/interax_b200.h (libinterax_b200.so, built in-tree)."""
 import ctypes
+import os
 from pathlib import Path
 
 import numpy as np
 
 _PKG = Path(__file__).resolve().parent.parent
-LIB_PATH = _PKG / "libinterax_b200.so"
+# IX_B200_LIBRARY names another build of the library (the autotuner's candidates); the default is the in-tree build
+LIB_PATH = Path(os.environ.get("IX_B200_LIBRARY", str(_PKG / "libinterax_b200.so")))
 
 IX_OK = 0
 IX_POSQ_FLOAT4, IX_POSQ_FLOAT4_CORRECTED, IX_POSQ_DOUBLE4 = 0, 1, 2
@@ -69,6 +71,7 @@ def lib():
             "ix_get_counts": (ctypes.c_int, [P, P, P]),
             "ix_md_set_masses": (ctypes.c_int, [P, P]),
             "ix_md_run": (ctypes.c_int, [P, ctypes.c_int, ctypes.c_double, P, P, P]),
+            "ix_md_set_constraints": (ctypes.c_int, [P, ctypes.c_int, P, P, ctypes.c_double]),
             "ix_get_stream": (P, [P]),
             "ix_synchronize": (ctypes.c_int, [P]),
             "ix_version": (ctypes.c_char_p, []),

@@ -133,6 +133,9 @@ def describe_forces(lib, handle, system, check, keep=None):
 
 
 class Context:
+    # relative tolerance of the MD loop's constraints (squared distances, stretching rate per ps)
+    constraintTolerance = 1e-10
+
     def __init__(self, system, integrator=None, platform=None, properties=None):
         self._system = system
         self._platform = platform if isinstance(platform, Platform) else Platform(
@@ -163,6 +166,12 @@ class Context:
         self._forces, names = describe_forces(self._lib, self._ctx, system, self._check)
         for name in names:
             self._parameters.setdefault(name, 1.0)
+        if system.getNumConstraints():
+            cons = [system.getConstraintParameters(i) for i in range(system.getNumConstraints())]
+            pairs = _capi.arr([(a, b) for a, b, _ in cons], np.int32)
+            dist = _capi.arr([d for _, _, d in cons], np.float64)
+            self._check(self._lib.ix_md_set_constraints(self._ctx, len(cons), _capi.ptr(pairs), _capi.ptr(dist),
+                                                        self.constraintTolerance))
 
     def __del__(self):
         if getattr(self, "_ctx", None) and self._ctx.value:

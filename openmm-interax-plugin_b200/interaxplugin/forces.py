@@ -320,7 +320,19 @@ class System:
     def __init__(self):
         self._masses = []
         self._forces = []
+        self._constraints = []
         self._box = [(2.0, 0.0, 0.0), (0.0, 2.0, 0.0), (0.0, 0.0, 2.0)]
+
+    def addConstraint(self, particle1, particle2, distance):
+        """A distance constraint, as OpenMM's System::addConstraint; applied by the MD loop of a Context."""
+        self._constraints.append((int(particle1), int(particle2), float(distance)))
+        return len(self._constraints) - 1
+
+    def getNumConstraints(self):
+        return len(self._constraints)
+
+    def getConstraintParameters(self, index):
+        return self._constraints[index]
 
     def addParticle(self, mass):
         self._masses.append(float(mass))

@@ -107,8 +107,9 @@ def cluster_waters(num_waters, rng, min_dist=0.26):
 
 def build_water_system(positions, params, rng, method, cutoff, box_length=None, three_body_cutoff=None,
                        three_body=True, alchemical_waters=(), use_lrc=None, softcore_radius=0.0,
-                       use_switch=False, switch_distance=-1.0, overlap_method=0, site_rng=None):
-    """A System of waters with the three pair forces and (optionally) the three-body force."""
+                       use_switch=False, switch_distance=-1.0, overlap_method=0, site_rng=None, rigid=False):
+    """A System of waters with the three pair forces and (optionally) the three-body force; rigid: each water's
+    O-H, O-H and H-H distances constrained to the model geometry (the benchmark's rigid 3-site water)."""
     num_waters = len(positions) // 3
     alch_set = set(int(w) for w in alchemical_waters)
     system = System()
@@ -123,6 +124,12 @@ def build_water_system(positions, params, rng, method, cutoff, box_length=None, 
             disp.addParticle(p["m1"], p["m2"], p["m3"], p["alpha"], p["disp_width"], alch)
             exch.addParticle(p["amplitude"], p["width"], alch)
             sr.addParticle(p["k"], p["l"], p["width"], alch)
+    if rigid:
+        hh = 2.0 * OH * math.sin(HOH / 2.0)
+        for w in range(num_waters):
+            system.addConstraint(3 * w, 3 * w + 1, OH)
+            system.addConstraint(3 * w, 3 * w + 2, OH)
+            system.addConstraint(3 * w + 1, 3 * w + 2, hh)
     for f, group in ((disp, 0), (exch, 1), (sr, 2)):
         f.setNonbondedMethod(method)
         f.setCutoffDistance(cutoff)

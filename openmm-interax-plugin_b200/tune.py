@@ -1,0 +1,190 @@
+"""Autotuner of the kernels' tile and schedule constants (the IX_TUNE_* macros of csrc/ix_tuning.h).
+
+Run on the GPU:  python openmm-interax-plugin_b200/tune.py [--out tuning.json] [--steps 200]
+
+Each candidate set of values is compiled into its own copy of the library (in parallel, with nvcc), and timed in a
+fresh process that loads that copy (IX_B200_LIBRARY) on the benchmark's shapes:
+
+* the 24,000-atom rigid-water box with the three-body term: the mean velocity-Verlet step time over `--steps` steps
+  (list rebuilds included, so the pair skin's trade-off between candidate pairs and rebuild frequency is measured),
+  and the pair kernel's and the three-body kernels' own times (CUDA events, the chains serialised);
+* the 4,096 water clusters of the batched workload: the time of one batched evaluation.
+
+The search is coordinate-wise: starting from the current values, each group of constants is varied over its
+candidates with the others fixed, and the best by the objective (the MD step time, plus the batched evaluation time
+for the groups that change it) is kept before the next group.  The chosen values and every measurement are written to
+tuning.json, which the build (build_lib.py) turns into compiler definitions.
+"""
+import argparse
+import concurrent.futures
+import hashlib
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+sys.path.insert(0, str(PKG))
+import build_lib  # noqa: E402
+
+DEFAULTS = {"IX_TUNE_PAIR_WARPS": 4, "IX_TUNE_PAIR_ROUND": 128, "IX_TUNE_PAIR_MIN_BLOCKS": 8,
+            "IX_TUNE_PAIR_COLUMN_LISTS": 0, "IX_TUNE_PAIR_SHARED_TABLE_BYTES": 0, "IX_TUNE_PAIR_SKIN": 0.1,
+            "IX_TUNE_SITE_SKIN": 0.1, "IX_TUNE_ATM_FAST": 64, "IX_TUNE_ATM_ROUND": 64}
+
+# groups of constants searched together, each with its candidate values (dicts of the group's macros)
+GROUPS = [
+    ("pair tiles", [dict(IX_TUNE_PAIR_WARPS=w, IX_TUNE_PAIR_ROUND=r, IX_TUNE_PAIR_MIN_BLOCKS=b,
+                         IX_TUNE_PAIR_COLUMN_LISTS=c)
+                    for w, r, b, c in ((4, 128, 8, 0), (4, 64, 8, 0), (4, 256, 6, 0), (2, 128, 16, 0),
+                                       (4, 64, 7, 1), (4, 128, 6, 1), (2, 64, 14, 1))]),
+    ("pair table", [dict(IX_TUNE_PAIR_SHARED_TABLE_BYTES=b) for b in (0, 1024, 2048)]),
+    ("pair skin", [dict(IX_TUNE_PAIR_SKIN=s) for s in (0.06, 0.08, 0.1, 0.12)]),
+    ("three-body", [dict(IX_TUNE_ATM_FAST=f, IX_TUNE_ATM_ROUND=r) for f, r in ((64, 64), (32, 32), (64, 32), (64, 128))]),
+    ("site skin", [dict(IX_TUNE_SITE_SKIN=s) for s in (0.05, 0.1, 0.15)]),
+]
+
+
+def _key(values):
+    return hashlib.sha1(json.dumps(sorted(values.items())).encode()).hexdigest()[:12]
+
+
+def compile_candidates(candidates, workdir, jobs=4):
+    """Compile each candidate (a full dict of values) into workdir; returns {key: path}."""
+    out = {}
+    Path(workdir).mkdir(parents=True, exist_ok=True)
+
+    def one(values):
+        path = Path(workdir) / f"libinterax_b200_{_key(values)}.so"
+        if not path.exists():
+            build_lib.compile_library(path, values)
+        return _key(values), path
+
+    with concurrent.futures.ThreadPoolExecutor(jobs) as pool:
+        for key, path in pool.map(one, candidates):
+            out[key] = path
+    return out
+
+
+def measure(steps, clusters=True):
+    """Timings of the library named by IX_B200_LIBRARY (run in a fresh process)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    sys.path.insert(0, str(PKG.parent))
+    import bench  # the benchmark's relaxation
+    from interaxplugin import BatchContext, Context, _capi
+    from interaxplugin import workloads as W
+
+    cfg = W.CONFIGS["24k"]
+    system, pos, box = W.water_box(cfg["num_waters"], cfg["box_length"], cfg["cutoff"], seed=1,
+                                   three_body_cutoff=cfg["three_body_cutoff"], rigid=True)
+    ctx = Context(system)
+    L = _capi.lib()
+    pos = bench.relax(ctx, system, pos, iterations=30)
+    vel = np.ascontiguousarray(W.initial_velocities(system, 300.0, seed=0))
+    masses = np.array([system.getParticleMass(i) for i in range(system.getNumParticles())])
+    ctx._check(L.ix_md_set_masses(ctx._ctx, _capi.ptr(masses)))
+    ctx._check(L.ix_md_run(ctx._ctx, 20, 0.001, None, _capi.ptr(vel), None))
+    stream = torch.cuda.ExternalStream(L.ix_get_stream(ctx._ctx))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    ctx._check(L.ix_md_steps_async(ctx._ctx, steps, 0.001))
+    b.record(stream)
+    ctx._check(L.ix_md_finish(ctx._ctx, None, None, None))
+    step_ms = a.elapsed_time(b) / steps
+    # the kernels alone: the three-body chain after the pair chain, events around each
+    ctx._check(L.ix_set_profiling(ctx._ctx, 2))
+    pair, atm = [], []
+    for _ in range(30):
+        ctx._check(L.ix_md_steps_async(ctx._ctx, 1, 0.001))
+        ctx._check(L.ix_md_finish(ctx._ctx, None, None, None))
+        p, t = ctypes.c_double(), ctypes.c_double()
+        ctx._check(L.ix_get_kernel_times(ctx._ctx, ctypes.byref(p), ctypes.byref(t)))
+        pair.append(p.value)
+        atm.append(t.value)
+    out = {"md_step_ms": step_ms, "pair_kernel_ms": float(np.median(pair)), "three_body_ms": float(np.median(atm))}
+    if clusters:
+        systems, positions = W.cluster_set(4096, seed=1)
+        batch = BatchContext(systems)
+        batch.compute(positions)
+        dpos = torch.from_numpy(np.ascontiguousarray(np.concatenate(positions))).cuda()
+        dfor = torch.empty_like(dpos)
+        den = torch.empty((4096, 4), dtype=torch.float64, device="cuda")
+        bstream = torch.cuda.ExternalStream(L.ix_batch_get_stream(batch._batch))
+        times = []
+        for k in range(13):
+            torch.cuda.synchronize()
+            a.record(bstream)
+            batch._check(L.ix_batch_compute_device(batch._batch, ctypes.c_void_p(dpos.data_ptr()),
+                                                   ctypes.c_void_p(dfor.data_ptr()), ctypes.c_void_p(den.data_ptr())))
+            b.record(bstream)
+            b.synchronize()
+            if k >= 3:
+                times.append(a.elapsed_time(b))
+        out["clusters_ms"] = float(np.median(times))
+    return out
+
+
+def run_candidate(path, steps, clusters):
+    env = dict(os.environ, IX_B200_LIBRARY=str(path))
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--measure", "--steps", str(steps)]
+    if not clusters:
+        cmd.append("--no-clusters")
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        return {"error": r.stderr[-2000:]}
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def objective(m, with_clusters):
+    if "error" in m:
+        return float("inf")
+    return m["md_step_ms"] + (m["clusters_ms"] if with_clusters else 0.0)
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--out", default=str(build_lib.TUNING))
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--measure", action="store_true", help=argparse.SUPPRESS)
+    p.add_argument("--no-clusters", action="store_true", help=argparse.SUPPRESS)
+    args = p.parse_args()
+    if args.measure:
+        print(json.dumps(measure(args.steps, clusters=not args.no_clusters)))
+        return
+    import torch
+    current = dict(DEFAULTS)
+    current.update(build_lib.tuned_values())
+    record = []
+    workdir = tempfile.mkdtemp(prefix="ix_tune_")
+    t0 = time.time()
+    for name, options in GROUPS:
+        # the batched workload has no pair list and no site lists to rebuild: the skins do not change it
+        clusters = name not in ("pair skin", "site skin", "pair table")
+        candidates = [dict(current, **o) for o in options]
+        libs = compile_candidates(candidates, workdir)
+        results = []
+        for values in candidates:
+            m = run_candidate(libs[_key(values)], args.steps, clusters)
+            results.append((objective(m, clusters), values, m))
+            record.append({"group": name, "values": {k: values[k] for k in options[0]}, "measured": m})
+            print(name, {k: values[k] for k in options[0]}, m, flush=True)
+        best = min(results, key=lambda r: r[0])
+        current = dict(best[1])
+    out = {"chosen": current, "device": torch.cuda.get_device_name(0), "steps": args.steps,
+           "objective": "mean velocity-Verlet step of the 24,000-atom rigid-water box (ms), plus one batched "
+                        "evaluation of the 4,096 clusters (ms) for the groups that change it",
+           "command": "python openmm-interax-plugin_b200/tune.py", "seconds": time.time() - t0,
+           "measurements": record}
+    Path(args.out).write_text(json.dumps(out, indent=1) + "\n")
+    print("chosen", current)
+
+
+if __name__ == "__main__":
+    main()
