@@ -40,6 +40,17 @@ struct AtmConfig {
     int zeroSlots, zeroOffset;   // energy slots the fast kernel clears (those of a wide kernel that may not run)
 };
 
+// Cell grid of the site-list search in a rectangular periodic box whose edges hold at least three cells as wide as
+// the list cutoff: every site within the list cutoff of a site lies in its cell or the 26 around it.
+struct SiteCells {
+    int nc[3];                   // cells per axis; nc[0] = 0: no grid (the chunk scan is used)
+    float cellsPerNm[3];
+    int* cellStart;              // numCells + 1
+    int* cellSites;              // the sites by cell, each cell's in increasing order
+    int* siteCell;               // numSites
+};
+constexpr int kSiteCellMax = 8192;   // cells the one-block sort holds in shared memory
+
 struct AtmBuffers {
     const int* siteOffsets;      // numSites + 1
     const int* siteParticles;
@@ -58,6 +69,7 @@ struct AtmBuffers {
     int numParticles;
     double* energyPartials;      // one per warp of the fast triple kernel's grid, then one per warp of the wide one
     unsigned long long* tripleCount;
+    SiteCells cells;
 };
 
 constexpr int kAtmFast = IX_TUNE_ATM_FAST;     // neighbor lists up to this length take the fast triple kernel
@@ -193,6 +205,114 @@ __global__ void kSiteNeighbors(AtmBuffers A, AtmConfig C) {
     }
     for (int d = 0; d < 3; d++)
         if (lane == 0) A.siteRef[3 * a + d] = A.sitePos[3 * a + d];
+}
+
+// The sites binned into the cell grid (rebuild only), in one block: each site's cell from its wrapped position, the
+// cell counts in shared memory, their scan, the scatter, and each cell's sites put in increasing order (so that the
+// lists built from the cells come out the same on every run).
+__global__ void __launch_bounds__(1024) kSiteCellSort(AtmBuffers A, AtmConfig C) {
+    if (*(volatile int*)A.flag == 0) return;
+    __shared__ int count[kSiteCellMax];
+    __shared__ int threadSum[1024];
+    const SiteCells& G = A.cells;
+    const int numCells = G.nc[0] * G.nc[1] * G.nc[2];
+    const int t = threadIdx.x, T = blockDim.x;
+    for (int c = t; c < numCells; c += T) count[c] = 0;
+    __syncthreads();
+    for (int s = t; s < C.numSites; s += T) {
+        const float3 p = siteWrapped(C, A.sitePos[3 * s], A.sitePos[3 * s + 1], A.sitePos[3 * s + 2]);
+        const int cx = min(max((int)(p.x * G.cellsPerNm[0]), 0), G.nc[0] - 1);
+        const int cy = min(max((int)(p.y * G.cellsPerNm[1]), 0), G.nc[1] - 1);
+        const int cz = min(max((int)(p.z * G.cellsPerNm[2]), 0), G.nc[2] - 1);
+        const int cell = (cz * G.nc[1] + cy) * G.nc[0] + cx;
+        G.siteCell[s] = cell;
+        atomicAdd(&count[cell], 1);
+    }
+    __syncthreads();
+    // exclusive scan: each thread a contiguous chunk of cells, then the chunk sums
+    const int per = (numCells + T - 1) / T;
+    const int c0 = min(t * per, numCells), c1 = min(c0 + per, numCells);
+    int sum = 0;
+    for (int c = c0; c < c1; c++) sum += count[c];
+    threadSum[t] = sum;
+    __syncthreads();
+    for (int o = 1; o < T; o <<= 1) {
+        const int v = t >= o ? threadSum[t - o] : 0;
+        __syncthreads();
+        threadSum[t] += v;
+        __syncthreads();
+    }
+    int run = threadSum[t] - sum;
+    for (int c = c0; c < c1; c++) {
+        const int n = count[c];
+        G.cellStart[c] = run;
+        count[c] = run;          // the fill position from here on
+        run += n;
+    }
+    if (t == T - 1) G.cellStart[numCells] = run;
+    __syncthreads();
+    for (int s = t; s < C.numSites; s += T) G.cellSites[atomicAdd(&count[G.siteCell[s]], 1)] = s;
+    __syncthreads();
+    // insertion sort of each cell's sites (a few dozen at most)
+    for (int c = t; c < numCells; c += T) {
+        int* v = G.cellSites + G.cellStart[c];
+        const int n = G.cellStart[c + 1] - G.cellStart[c];
+        for (int i = 1; i < n; i++) {
+            const int x = v[i];
+            int j = i - 1;
+            while (j >= 0 && v[j] > x) {
+                v[j + 1] = v[j];
+                j--;
+            }
+            v[j + 1] = x;
+        }
+    }
+}
+
+// The list search over the cell grid (rebuild only): one warp per site A takes the sites B > A of other molecules
+// within the list cutoff from the 27 cells around A's cell, in cell order.  The counts and flags are those of
+// kSiteNeighbors.
+__global__ void kSiteNeighborsCells(AtmBuffers A, AtmConfig C) {
+    if (*(volatile int*)A.flag == 0) return;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= C.numSites) return;
+    const int a = warp;
+    const int molA = A.molecule[a];
+    const SiteCells& G = A.cells;
+    const int cell = G.siteCell[a];
+    const int cx = cell % G.nc[0], cy = (cell / G.nc[0]) % G.nc[1], cz = cell / (G.nc[0] * G.nc[1]);
+    int count = 0;
+    for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dx = -1; dx <= 1; dx++) {
+                const int x = (cx + dx + G.nc[0]) % G.nc[0], y = (cy + dy + G.nc[1]) % G.nc[1],
+                          z = (cz + dz + G.nc[2]) % G.nc[2];
+                const int c = (z * G.nc[1] + y) * G.nc[0] + x;
+                const int end = G.cellStart[c + 1];
+                for (int k0 = G.cellStart[c]; k0 < end; k0 += 32) {
+                    const int k = k0 + lane;
+                    const int b = k < end ? G.cellSites[k] : -1;
+                    bool near = false;
+                    if (b > a && A.molecule[b] != molA) {
+                        double d[3];
+                        siteDelta(A, C, a, b, d);
+                        near = (float)(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) < C.listCutoff2;
+                    }
+                    const unsigned bal = __ballot_sync(0xffffffffu, near);
+                    if (near) {
+                        const int slot = count + __popc(bal & laneMaskLt());
+                        if (slot < A.cap) A.nbr[(size_t)a * A.cap + slot] = b;
+                    }
+                    count += __popc(bal);
+                }
+            }
+    if (lane == 0) {
+        A.nbrCount[a] = count;
+        if (count > A.cap) atomicOr(A.flag + 1, 1);
+        if (count > kAtmFast || count > A.cap) atomicOr(A.flag + 2, 1);
+        for (int d = 0; d < 3; d++) A.siteRef[3 * a + d] = A.sitePos[3 * a + d];
+    }
 }
 
 // Tang-Toennies f_3 and its derivative (InteraxThreeBodyTerms.h:51-65); the series is exact to float for x < 2 at
@@ -339,8 +459,8 @@ __device__ __forceinline__ int stageTripleNeighbors(const AtmBuffers& A, const A
 }
 
 // The same for a site whose list overflowed its capacity: every later site of another molecule is tested against the
-// cutoff, which gives the list's neighbors within the cutoff in the same (increasing) order, so the triples and their
-// evaluation order are those of a list that fitted.  The reference falls back the same way
+// cutoff, which gives the same neighbors within the cutoff (in increasing order), so the same triples are evaluated.
+// The reference falls back the same way
 // (platforms/common/src/kernels/interaxThreeBody.cc:111-112, 437-438).
 template <class Store>
 __device__ __forceinline__ int stageTripleNeighborsScan(const AtmBuffers& A, const AtmConfig& C, int a, int lane,
@@ -373,8 +493,7 @@ struct AtmFastStorage {
     float4 fc[kAtmRound];        // force on C
 };
 
-// 72 registers (7 blocks of 4 warps per SM)
-__global__ void __launch_bounds__(32 * kAtmFastWarps, 7) kTriplesFast(AtmBuffers A, AtmConfig C) {
+__global__ void __launch_bounds__(32 * kAtmFastWarps, IX_TUNE_ATM_MIN_BLOCKS) kTriplesFast(AtmBuffers A, AtmConfig C) {
     __shared__ AtmFastStorage storage[kAtmFastWarps];
     for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < C.zeroSlots; k += gridDim.x * blockDim.x)
         A.energyPartials[C.zeroOffset + k] = 0.0;

@@ -955,6 +955,12 @@ static int allocateAtm(ix_ctx* ctx) {
     IX_TRY(deviceAlloc(ctx, "siteChunkBox", 2 * (size_t)((ns + 31) / 32), &A.chunkBox));
     IX_TRY(deviceAlloc(ctx, "nbrCount", ns, &A.nbrCount));
     IX_TRY(deviceAlloc(ctx, "siteForce", 3 * (size_t)ns, &A.siteForce));
+    if (ctx->atmPeriodic) {
+        // the cell grid of the list search (its shape follows the box at each evaluation)
+        IX_TRY(deviceAlloc(ctx, "siteCellStart", kSiteCellMax + 1, &A.cells.cellStart));
+        IX_TRY(deviceAlloc(ctx, "siteCellSites", ns, &A.cells.cellSites));
+        IX_TRY(deviceAlloc(ctx, "siteCell", ns, &A.cells.siteCell));
+    }
     {
         // the sites of each particle, so that the finishing kernel gives each particle its share of its sites' forces
         std::vector<int> start(ctx->n + 1, 0), list(ctx->siteParticles.size());
@@ -1400,11 +1406,29 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         // the wide kernel's energy slots start at zero (it runs only while some list is long)
         C.zeroSlots = ctx->atmGridBlocks * kAtmWarps;
         C.zeroOffset = ctx->atmFastBlocks * kAtmFastWarps;
+        // the cell grid of the list search in a rectangular periodic box with at least three cells per edge
+        A.cells.nc[0] = A.cells.nc[1] = A.cells.nc[2] = 0;
+        if (C.periodic && !C.box.triclinic && A.cells.cellStart) {
+            const double width = ctx->atmCutoff + kSiteSkin + 1e-3;   // room for the float rounding of the binning
+            const double len[3] = {ctx->box[0], ctx->box[4], ctx->box[8]};
+            int nc[3];
+            for (int d = 0; d < 3; d++) nc[d] = (int)std::floor(len[d] / width);
+            if (nc[0] >= 3 && nc[1] >= 3 && nc[2] >= 3 && (long long)nc[0] * nc[1] * nc[2] <= kSiteCellMax)
+                for (int d = 0; d < 3; d++) {
+                    A.cells.nc[d] = nc[d];
+                    A.cells.cellsPerNm[d] = (float)(nc[d] / len[d]);
+                }
+        }
         kSiteCentroids<<<gS, 64, 0, sa>>>(A, C, ctx->dPos);
-        // site list rebuild when the centroid kernel set the flag: these kernels return at once otherwise (three
-        // short launches cost less than a conditional graph node); the long-list flag is recomputed with the lists
+        // site list rebuild when the centroid kernel set the flag: these kernels return at once otherwise (short
+        // launches cost less than a conditional graph node); the long-list flag is recomputed with the lists
         kClearFlagIf<<<1, 1, 0, sa>>>(A.flag + 2, A.flag);
-        kSiteNeighbors<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, sa>>>(A, C);
+        if (A.cells.nc[0]) {
+            kSiteCellSort<<<1, 1024, 0, sa>>>(A, C);
+            kSiteNeighborsCells<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, sa>>>(A, C);
+            ctx->launches += 1;
+        }
+        else kSiteNeighbors<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, sa>>>(A, C);
         kClearFlag<<<1, 1, 0, sa>>>(A.flag);
         recordTiming(ctx, 2, sa);
         kTriplesFast<<<ctx->atmFastBlocks, 32 * kAtmFastWarps, 0, sa>>>(A, C);

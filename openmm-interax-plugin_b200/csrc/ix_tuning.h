@@ -37,3 +37,7 @@
 #ifndef IX_TUNE_ATM_ROUND
 #define IX_TUNE_ATM_ROUND 64
 #endif
+// three-body: minimum resident blocks of the fast triple kernel per SM (bounds its registers per thread)
+#ifndef IX_TUNE_ATM_MIN_BLOCKS
+#define IX_TUNE_ATM_MIN_BLOCKS 7
+#endif
