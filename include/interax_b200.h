@@ -358,6 +358,7 @@ typedef struct {
      * checks, admission scans, idle waits; within set-up and enqueue: pinned staging, device set-up, state uploads,
      * the steps' launches */
     double worker_seconds[12];
+    long long contexts_reused;                /* contexts taken from the pool of finished requests' contexts */
 } ix_server_stats;
 
 /* A host-only request description of num_particles particles (box: 9 doubles, NULL for non-periodic). */

@@ -26,6 +26,7 @@
 #include <deque>
 #include <memory>
 #include <thread>
+#include <unordered_map>
 
 namespace {
 
@@ -85,6 +86,8 @@ struct ServerRequest {
     double tSubmit = 0.0, tDone = 0.0;
     size_t estimate = 0;
     bool small = false;
+    std::string desc;                    // a periodic request's System, serialized: the key of the context pool
+    unsigned long long key = 0;          // its hash
     int status = IX_OK;
     std::string error;
 };
@@ -111,8 +114,19 @@ struct StreamSet {
     cudaEvent_t fork = nullptr, join = nullptr;
 };
 
+// A context whose request finished, kept with its device arrays, streams and CUDA graphs for the next request of the
+// same System (the same particles, forces, parameters and masses; only the state differs).
+struct PooledContext {
+    ix_ctx* ctx = nullptr;
+    std::string desc;
+    size_t reserved = 0;                 // device bytes it holds, still reserved against the budget
+    double lastUse = 0.0;
+};
+
 struct ServerShard {
     int index = 0;
+    std::unordered_multimap<unsigned long long, PooledContext> pool;
+    size_t poolBytes = 0;
     std::thread worker;
     std::deque<ServerRequest*> incoming;     // guarded by the server's mutex
     std::deque<ServerRequest*> pending;
@@ -139,6 +153,7 @@ struct ix_server {
     int maxCohort = 512;
     double window = 200e-6;
     std::vector<std::unique_ptr<ServerShard>> shards;
+    size_t maxPooled = 64;                   // idle contexts kept per shard for reuse
     std::mutex m;                        // guards the shards' incoming queues, done, doneIds, error, stats, stop
     std::condition_variable cvSubmit, cvDone;
     bool stop = false;
@@ -157,6 +172,82 @@ struct ix_server {
 };
 
 namespace {
+
+// A periodic request's System serialized for the context pool: everything a context's device arrays and graphs
+// depend on (particle count, box, masses, parameter values, every force's settings and per-particle parameters,
+// exclusions, sites), so that equal strings mean a context can be reused as it is.
+template <class T>
+void putBytes(std::string& out, const T* p, size_t count) {
+    out.append(reinterpret_cast<const char*>(p), count * sizeof(T));
+}
+template <class T>
+void putValue(std::string& out, const T& v) {
+    putBytes(out, &v, 1);
+}
+template <class T>
+void putVector(std::string& out, const std::vector<T>& v) {
+    putValue(out, v.size());
+    putBytes(out, v.data(), v.size());
+}
+
+std::string poolDescription(const ix_ctx* c, const std::vector<double>& mass) {
+    std::string d;
+    putValue(d, c->n);
+    putBytes(d, c->box, 9);
+    putVector(d, mass);
+    for (const auto& kv : c->parameters) {
+        d += kv.first;
+        putValue(d, kv.second);
+    }
+    putValue(d, c->method);
+    putValue(d, c->cutoff);
+    putValue(d, c->exclusions.size());
+    for (const auto& e : c->exclusions) {
+        putValue(d, e.first);
+        putValue(d, e.second);
+    }
+    for (const PairTerm& T : c->term) {
+        putValue(d, T.present);
+        if (!T.present) continue;
+        putValue(d, T.group);
+        d += T.alchName;
+        putValue(d, T.useSwitch);
+        putValue(d, T.switchDistance);
+        putValue(d, T.softcoreRadius);
+        putValue(d, T.overlapMethod);
+        putValue(d, T.dampingScale);
+        putValue(d, T.useLrc);
+        putVector(d, T.params);
+        putVector(d, T.alch);
+    }
+    putValue(d, c->atmPresent);
+    if (c->atmPresent) {
+        putValue(d, c->atmGroup);
+        d += c->atmAlchName;
+        putVector(d, c->siteOffsets);
+        putVector(d, c->siteParticles);
+        putVector(d, c->molecule);
+        putVector(d, c->siteParams);
+        putVector(d, c->siteAlch);
+        putValue(d, c->atmCutoff);
+        putValue(d, c->atmScale);
+        putValue(d, c->atmDampingScale);
+        putValue(d, c->atmCentroidRadius);
+        putValue(d, c->atmDamping);
+        putValue(d, c->atmPeriodic);
+    }
+    return d;
+}
+
+// FNV-1a, 64 bits.
+unsigned long long hashBytes(const std::string& s) {
+    unsigned long long h = 1469598103934665603ull;
+    for (unsigned char ch : s) {
+        h ^= ch;
+        h *= 1099511628211ull;
+    }
+    return h;
+}
 
 // Device bytes a request will hold, an upper bound used for admission (the unit's actual bytes replace it once it
 // is launched).  A periodic context holds per-particle arrays, the pair tiles (a few hundred bytes per tile, ~75 tiles
@@ -183,6 +274,42 @@ bool reserveBytes(ix_server* S, size_t bytes) {
 }
 
 void unreserveBytes(ix_server* S, size_t bytes) { S->reserved -= (long long)bytes; }
+
+void retireContext(ix_server* S, ServerShard* H, ix_ctx* c);
+
+// An idle context of the shard's pool for request r (nullptr: none), taken out of the pool.
+PooledContext takePooled(ServerShard* H, const ServerRequest* r) {
+    auto range = H->pool.equal_range(r->key);
+    for (auto it = range.first; it != range.second; ++it)
+        if (it->second.desc == r->desc) {
+            PooledContext p = std::move(it->second);
+            H->pool.erase(it);
+            H->poolBytes -= p.reserved;
+            return p;
+        }
+    return PooledContext{};
+}
+
+bool hasPooled(const ServerShard* H, const ServerRequest* r) {
+    auto range = H->pool.equal_range(r->key);
+    for (auto it = range.first; it != range.second; ++it)
+        if (it->second.desc == r->desc) return true;
+    return false;
+}
+
+// Retire the shard's least recently used idle context; false when the pool is empty.
+bool evictPooled(ix_server* S, ServerShard* H) {
+    if (H->pool.empty()) return false;
+    auto oldest = H->pool.begin();
+    for (auto it = H->pool.begin(); it != H->pool.end(); ++it)
+        if (it->second.lastUse < oldest->second.lastUse) oldest = it;
+    PooledContext p = std::move(oldest->second);
+    H->pool.erase(oldest);
+    H->poolBytes -= p.reserved;
+    retireContext(S, H, p.ctx);
+    unreserveBytes(S, p.reserved);
+    return true;
+}
 
 size_t bufferBytes(const std::map<std::string, DeviceBuffer>& buffers) {
     size_t total = 0;
@@ -275,7 +402,7 @@ constexpr int kServerGraphSteps = IX_SERVER_GRAPH_STEPS;
 
 // Enqueue a periodic request's whole run on its context's stream: positions, masses and velocities in, the first
 // evaluation and every step, then the final state copied into the pinned staging, and the event that marks it done.
-int enqueueContextRun(ServerShard* H, ServerUnit* u) {
+int enqueueContextRun(ServerShard* H, ServerUnit* u, bool reused = false) {
     ServerRequest* r = u->members[0];
     ix_ctx* c = u->ctx;
     const size_t n3 = 3 * (size_t)c->n;
@@ -283,7 +410,15 @@ int enqueueContextRun(ServerShard* H, ServerUnit* u) {
         PhaseTimer t(H->workerSec[10]);
         IX_TRY(ix_set_positions(c, r->pos.data(), nullptr));
         if (r->mass.empty()) r->mass.assign(c->n, 1.0);
-        IX_TRY(ix_md_set_masses(c, r->mass.data()));
+        // a pooled context has these masses already (they are part of its description); setting them again would
+        // invalidate its CUDA graphs
+        if (!reused) IX_TRY(ix_md_set_masses(c, r->mass.data()));
+        else {
+            // rebuild both neighbor lists from the new positions, so that the request runs exactly as on a new context
+            const int rebuild = 1;
+            IX_TRY(stageCopy(c, c->dFlags, &rebuild, sizeof(int)));
+            if (c->atmAllocated) IX_TRY(stageCopy(c, c->dFlags + 4, &rebuild, sizeof(int)));
+        }
         if (r->vel.empty()) IX_CUDA(c, cudaMemsetAsync(c->dVel, 0, n3 * sizeof(double), c->stream));
         else IX_TRY(stageCopy(c, c->dVel, r->vel.data(), n3 * sizeof(double)));
     }
@@ -314,6 +449,51 @@ void launchContext(ix_server* S, ServerShard* H, ServerRequest* r) {
     ServerUnit* u = new ServerUnit();
     u->members.push_back(r);
     u->reserved = r->estimate;
+    {
+        // an idle context of the same System: its arrays, lists and graphs are reused, only the state is uploaded
+        PooledContext p = takePooled(H, r);
+        if (p.ctx) {
+            int rc = IX_OK;
+            ix_ctx_destroy(r->sys);         // the description is no longer needed
+            r->sys = p.ctx;
+            u->ctx = p.ctx;
+            unreserveBytes(S, u->reserved);   // the pooled context's bytes are reserved already
+            u->reserved = p.reserved;
+            p.ctx->useGraphs = r->steps >= kServerGraphSteps;
+            {
+                PhaseTimer t(H->workerSec[0]);
+                const size_t results = (9 * (size_t)p.ctx->n + 8) * sizeof(double);
+                u->staging = S->pinned.alloc(results + 320 * (size_t)p.ctx->n + (size_t(64) << 10));
+                if (!u->staging) rc = fail(p.ctx, IX_ERR_MEMORY, "pinned host staging could not be allocated");
+                else {
+                    p.ctx->uploadBuf = u->staging + results;
+                    p.ctx->uploadCap = 320 * (size_t)p.ctx->n + (size_t(64) << 10);
+                    p.ctx->uploadUsed = 0;
+                }
+            }
+            if (rc == IX_OK) {
+                PhaseTimer t(H->workerSec[1]);
+                rc = enqueueContextRun(H, u, true);
+            }
+            if (rc != IX_OK) {
+                const std::string msg = p.ctx->error;
+                for (auto& mk : u->marks) H->freeEvents.push_back(mk.event);
+                if (u->staging) S->pinned.release(u->staging);
+                r->sys = nullptr;
+                retireContext(S, H, p.ctx);
+                unreserveBytes(S, u->reserved);
+                delete u;
+                serverFinish(S, H, r, rc, msg);
+                return;
+            }
+            H->units.push_back(u);
+            std::lock_guard<std::mutex> lock(S->m);
+            S->stats.contexts++;
+            S->stats.contexts_reused++;
+            S->stats.admitted++;
+            return;
+        }
+    }
     ix_ctx* c = r->sys;
     c->arena = &S->arena;
     c->device = S->device;
@@ -505,16 +685,40 @@ void unpackCohortMark(ix_server* S, ServerShard* H, ServerUnit* u, const ServerU
     }
 }
 
-// Release a unit whose requests are all finished (or failed).
-void releaseUnit(ix_server* S, ServerShard* H, ServerUnit* u) {
+// Release a unit whose requests are all finished (or failed).  A context whose request succeeded goes to the shard's
+// pool, keeping its memory reserved, for the next request of the same System.
+void releaseUnit(ix_server* S, ServerShard* H, ServerUnit* u, bool succeeded = false) {
     for (auto& mk : u->marks) H->freeEvents.push_back(mk.event);
     u->marks.clear();
     if (u->staging) S->pinned.release(u->staging);
     u->staging = nullptr;
     if (u->ctx) {
-        u->members[0]->sys = nullptr;
-        retireContext(S, H, u->ctx);
-        u->ctx = nullptr;
+        ServerRequest* r = u->members[0];
+        r->sys = nullptr;
+        if (succeeded && S->maxPooled > 0 && !r->desc.empty()) {
+            ix_ctx* c = u->ctx;
+            c->uploadBuf = nullptr;          // the staging went back to the pinned pool
+            c->uploadCap = c->uploadUsed = 0;
+            const size_t actual = bufferBytes(c->buffers);
+            if (actual > u->reserved) {
+                S->reserved += (long long)(actual - u->reserved);
+                u->reserved = actual;
+            }
+            PooledContext p;
+            p.ctx = c;
+            p.desc = std::move(r->desc);
+            p.reserved = u->reserved;
+            p.lastUse = serverNow();
+            H->poolBytes += p.reserved;
+            H->pool.emplace(r->key, std::move(p));
+            u->ctx = nullptr;
+            u->reserved = 0;
+            while (H->pool.size() > S->maxPooled) evictPooled(S, H);
+        }
+        else {
+            retireContext(S, H, u->ctx);
+            u->ctx = nullptr;
+        }
     }
     if (u->batch) {
         cudaStreamSynchronize(u->batch->stream);
@@ -589,7 +793,7 @@ bool collect(ix_server* S, ServerShard* H) {
             else if (failCode != IX_OK)
                 for (size_t m = (size_t)u->marks[u->next].first; m < u->members.size(); m++)
                     rest.push_back(u->members[m]);
-            releaseUnit(S, H, u);
+            releaseUnit(S, H, u, failCode == IX_OK);
             for (ServerRequest* r : rest) serverFinish(S, H, r, failCode, msg);
         }
         delete u;
@@ -635,12 +839,21 @@ bool admit(ix_server* S, ServerShard* H) {
                 continue;
             }
         }
-        else if (reserveBytes(S, r->estimate)) {
-            it = H->pending.erase(it);
-            H->running++;
-            launchContext(S, H, r);
-            launched = true;
-            continue;
+        else {
+            bool fits = hasPooled(H, r);
+            if (fits) fits = reserveBytes(S, 0);
+            else {
+                fits = reserveBytes(S, r->estimate);
+                while (!fits && evictPooled(S, H)) fits = reserveBytes(S, r->estimate);
+            }
+            if (fits) {
+                if (hasPooled(H, r)) r->estimate = 0;   // launchContext releases nothing for it
+                it = H->pending.erase(it);
+                H->running++;
+                launchContext(S, H, r);
+                launched = true;
+                continue;
+            }
         }
         if (taken) {
             H->running++;
@@ -712,6 +925,8 @@ void shardLoop(ix_server* S, ServerShard* H) {
         delete u;
     }
     H->units.clear();
+    while (evictPooled(S, H)) {
+    }
     for (ServerRequest* r : H->pending) serverFinish(S, nullptr, r, IX_ERR_STATE, "the server was destroyed");
     H->pending.clear();
     for (const StreamSet& set : H->streams) {
@@ -904,13 +1119,20 @@ int ix_server_submit(ix_server* S, ix_ctx* request, int steps, double dt, long l
     r->steps = steps;
     r->dt = steps > 0 ? dt : 0.0;
     r->tSubmit = serverNow();
+    const bool small = batchable(request) && request->n <= S->smallAtoms;
+    if (!small) {
+        // serialized on the submitting thread: the key of the shard's context pool
+        r->desc = poolDescription(request, r->mass);
+        r->key = hashBytes(r->desc);
+    }
     {
         std::lock_guard<std::mutex> lock(S->m);
-        r->small = batchable(request) && request->n <= S->smallAtoms;
+        r->small = small;
         r->estimate = estimateRequestBytes(request, r->small);
         r->id = S->nextId++;
-        // small requests gather on shard 0 (larger cohorts); the others go round the shards
-        ServerShard* H = r->small ? S->shards[0].get() : S->shards[S->nextShard++ % S->shards.size()].get();
+        // small requests gather on shard 0 (larger cohorts); the others go to the shard that pools their System's
+        // contexts
+        ServerShard* H = r->small ? S->shards[0].get() : S->shards[r->key % S->shards.size()].get();
         H->incoming.push_back(r);
         S->stats.submitted++;
         if (id) *id = r->id;

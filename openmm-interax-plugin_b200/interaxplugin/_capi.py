@@ -26,7 +26,8 @@ class ServerStats(ctypes.Structure):
     _fields_ = [(k, ctypes.c_longlong) for k in ("submitted", "admitted", "completed", "failed", "contexts", "cohorts",
                                                   "pending", "running")] + \
                [(k, ctypes.c_double) for k in ("budget_bytes", "reserved_bytes", "peak_reserved_bytes", "arena_bytes",
-                                               "peak_arena_bytes")] + [("worker_seconds", ctypes.c_double * 12)]
+                                               "peak_arena_bytes")] + [("worker_seconds", ctypes.c_double * 12)] + \
+               [("contexts_reused", ctypes.c_longlong)]
 
 
 _lib = None

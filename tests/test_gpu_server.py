@@ -125,3 +125,22 @@ def test_server_admission_budget():
     big = [(*_box(2000, seed=9), None, 0)]
     results, stats = _serve(big, budget_bytes=budget)
     assert results[0].status == 5 and "budget" in results[0].error
+
+
+def test_server_reuses_contexts_of_the_same_system():
+    """Requests of one System that come one after the other run on the same pooled context (its arrays, lists and
+    graphs kept from the previous request), with results bitwise equal to the request run on a new server."""
+    s, p = _box(300, seed=21)
+    reqs = [(s, p, W.initial_velocities(s, 300.0, seed=k), 3 + k % 3) for k in range(4)]
+    srv = Server()
+    got = []
+    for system, pos, vel, n in reqs:
+        rid = srv.submit(system, pos, vel, steps=n, dt=DT)
+        got.append(srv.run_all(timeout=120)[rid])
+    stats = srv.stats()
+    srv.close()
+    assert stats["contexts_reused"] >= 3, stats
+    for req, m in zip(reqs, got):
+        (a,), _ = _serve([req])
+        assert np.array_equal(a.positions, m.positions) and np.array_equal(a.velocities, m.velocities)
+        assert np.array_equal(a.forces, m.forces) and np.array_equal(a.term_energies, m.term_energies)
