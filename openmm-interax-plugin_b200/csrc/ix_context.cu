@@ -1504,6 +1504,7 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         const size_t tableBytes = (size_t)P.numClasses * P.numClasses * sizeof(PairCoef);
         const size_t dyn = table && tableBytes <= (size_t)IX_TUNE_PAIR_SHARED_TABLE_BYTES ? tableBytes : 0;
         P.coefShared = dyn > 0;
+        C.coefShared = P.coefShared;
         if (lean && table && uniform) kPairTiles<true, true, true><<<grid, 32 * kPairWarps, dyn, st>>>(L, P, C);
         else if (lean && uniform) kPairTiles<true, false, true><<<grid, 32 * kPairWarps, 0, st>>>(L, P, C);
         else if (lean && table) kPairTiles<true, true><<<grid, 32 * kPairWarps, dyn, st>>>(L, P, C);

@@ -49,6 +49,7 @@ struct PairTermConfig {
     Box box;
     BoxFF boxff;
     int alchOnlyBit;             // nonzero: only the pairs with exactly one particle carrying this alchemical flag bit
+    int coefShared;              // the class-pair table is read from its copy in shared memory
 };
 
 struct PairBuffers {
@@ -154,6 +155,10 @@ __device__ __forceinline__ float pairTerms(const PairTermConfig& C, float r, flo
     return dTotal;
 }
 
+// A class-pair coefficient: through the read-only cache from the global table, or a plain load from the copy staged
+// in shared memory (the read-only path cannot address shared memory).  `shared` is the same for the whole launch.
+__device__ __forceinline__ float4 ldCoef(const float4* p, bool shared) { return shared ? *p : __ldg(p); }
+
 // The same from the pair's class coefficients (see PairCoef).  Only the exact overlap method.
 template <bool LEAN, bool UNIFORM>
 __device__ __forceinline__ float pairTermsTable(const PairTermConfig& C, float r, float invR, const PairCoef* K,
@@ -180,12 +185,12 @@ __device__ __forceinline__ float pairTermsTable(const PairTermConfig& C, float r
         }
         float E, D;
         if (t == 0) {
-            dispersionFromCoef(rEff, invEff, __ldg(&K->disp), E, D);
+            dispersionFromCoef(rEff, invEff, ldCoef(&K->disp, C.coefShared), E, D);
         }
         else if (t == 1) {
-            const float4 c = __ldg(&K->ovC);
+            const float4 c = ldCoef(&K->ovC, C.coefShared);
             float s8pi, ds8pi;
-            overlapFromCoef(rEff, __ldg(&K->ovA), __ldg(&K->ovB), c.x, c.y, s8pi, ds8pi);
+            overlapFromCoef(rEff, ldCoef(&K->ovA, C.coefShared), ldCoef(&K->ovB, C.coefShared), c.x, c.y, s8pi, ds8pi);
             shared8pi = s8pi;
             sharedD8pi = ds8pi;
             sharedR = rEff;
@@ -193,13 +198,13 @@ __device__ __forceinline__ float pairTermsTable(const PairTermConfig& C, float r
             D = c.z * ds8pi;
         }
         else {
-            const float4 c = __ldg(&K->srC), kl = __ldg(&K->srK);
+            const float4 c = ldCoef(&K->srC, C.coefShared), kl = ldCoef(&K->srK, C.coefShared);
             float s8pi, ds8pi;
             if (C.shareOverlap && rEff == sharedR) {
                 s8pi = shared8pi;
                 ds8pi = sharedD8pi;
             }
-            else overlapFromCoef(rEff, __ldg(&K->srA), __ldg(&K->srB), c.x, c.y, s8pi, ds8pi);
+            else overlapFromCoef(rEff, ldCoef(&K->srA, C.coefShared), ldCoef(&K->srB, C.coefShared), c.x, c.y, s8pi, ds8pi);
             const float st = c.z * s8pi;
             E = fmaf(kl.y, st, kl.x) * st;
             D = fmaf(2.0f * kl.y, st, kl.x) * c.z * ds8pi;
@@ -247,6 +252,8 @@ constexpr int kPairWarps = IX_TUNE_PAIR_WARPS;
 // 1: each tile's column lists (the queue positions of each column's pairs) are built once with the queue, and the
 // column forces of every round are read along them; 0: each round finds them from the row masks
 constexpr int kPairColumnLists = IX_TUNE_PAIR_COLUMN_LISTS;
+// 1: the class-table path without per-pair tests evaluates two queued pairs per lane at a time (computeQueuedPair2)
+constexpr int kPairIlp = IX_TUNE_PAIR_ILP;
 constexpr int kPairRound = IX_TUNE_PAIR_ROUND;   // queued pairs computed before their forces are gathered
 
 // Per-warp shared memory of the pair kernel (about 6.8 KB, so that eight 4-warp blocks fit on an SM).  Parameters
@@ -342,6 +349,102 @@ __device__ __forceinline__ float4 computeQueuedPair(PairWarpStorage& S, int entr
     return make_float4(dx * fs, dy * fs, dz * fs, 0.0f);
 }
 
+// Two queued pairs of the class-table path without per-pair tests (LEAN and UNIFORM: no soft core, switch, order-2
+// overlap, gate or scale), their arithmetic in one straight sequence so that each lane keeps two independent chains in
+// flight; a pair outside the cutoff is evaluated at a harmless distance and masked.  The results are those of
+// computeQueuedPair, operation for operation.  `two`: the second entry is a real pair.
+__device__ __forceinline__ void computeQueuedPair2(PairWarpStorage& S, int entry0, int entry1, bool two,
+                                                   bool perPairImage, const PairTermConfig& C, const PairBuffers& P,
+                                                   const PairCoef* coef, float e[3], unsigned& pairs,
+                                                   float4& out0, float4& out1) {
+    const int entry[2] = {entry0, entry1};
+    float dx[2], dy[2], dz[2], r[2], invR[2];
+    bool inside[2];
+    const PairCoef* K[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const int i = entry[k] >> 5, j = entry[k] & 31;
+        const float4 hi_i = S.hi[0][i], hi_j = S.hi[1][j], lo_i = S.lo[0][i], lo_j = S.lo[1][j];
+        float dxh = hi_j.x - hi_i.x, dyh = hi_j.y - hi_i.y, dzh = hi_j.z - hi_i.z;
+        float dxl = lo_j.x - lo_i.x, dyl = lo_j.y - lo_i.y, dzl = lo_j.z - lo_i.z;
+        if (perPairImage) minimumImageFF(dxh, dxl, dyh, dyl, dzh, dzl, C.boxff);
+        dx[k] = dxh + dxl;
+        dy[k] = dyh + dyl;
+        dz[k] = dzh + dzl;
+        const float r2 = fmaf(dx[k], dx[k], fmaf(dy[k], dy[k], dz[k] * dz[k]));
+        bool in = k == 0 || two;
+        if (C.useCutoff) {
+            bool within = r2 < C.cutoff2;
+            if (fabsf(r2 - C.cutoff2) < 1e-5f * C.cutoff2) {
+                double ddx = ((double)hi_j.x - (double)hi_i.x) + ((double)lo_j.x - (double)lo_i.x);
+                double ddy = ((double)hi_j.y - (double)hi_i.y) + ((double)lo_j.y - (double)lo_i.y);
+                double ddz = ((double)hi_j.z - (double)hi_i.z) + ((double)lo_j.z - (double)lo_i.z);
+                if (perPairImage) minimumImage(ddx, ddy, ddz, C.box);
+                const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz));
+                within = sqrt(r2d) < C.cutoff;
+            }
+            in = in && within;
+        }
+        inside[k] = in;
+        // a pair left out is evaluated at half the cutoff, where every term is finite, and its results dropped
+        r[k] = sqrtRefined(in ? r2 : 0.25f * C.cutoff2, invR[k]);
+        const int fi = S.flags[0][i], fj = S.flags[1][j];
+        const int ci = (fi >> kClassShift) & 0xff, cj = (fj >> kClassShift) & 0xff;
+        K[k] = coef + ci * P.numClasses + cj;
+    }
+    float dTotal[2] = {0.0f, 0.0f};
+    float s8[2] = {0.0f, 0.0f}, ds8[2] = {0.0f, 0.0f};
+    if (C.termMask & 1) {
+        const float4 kd[2] = {ldCoef(&K[0]->disp, C.coefShared), ldCoef(&K[1]->disp, C.coefShared)};
+        float E[2], D[2];
+        dispersionFromCoef2(r, invR, kd, E, D);
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            e[0] += inside[k] ? E[k] : 0.0f;
+            dTotal[k] += D[k];
+        }
+    }
+    if (C.termMask & 2) {
+        const float4 a[2] = {ldCoef(&K[0]->ovA, C.coefShared), ldCoef(&K[1]->ovA, C.coefShared)};
+        const float4 b[2] = {ldCoef(&K[0]->ovB, C.coefShared), ldCoef(&K[1]->ovB, C.coefShared)};
+        const float4 c[2] = {ldCoef(&K[0]->ovC, C.coefShared), ldCoef(&K[1]->ovC, C.coefShared)};
+        const float k1[2] = {c[0].x, c[1].x}, k2[2] = {c[0].y, c[1].y};
+        overlapFromCoef2(r, a, b, k1, k2, s8, ds8);
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            e[1] += inside[k] ? c[k].z * s8[k] : 0.0f;
+            dTotal[k] = fmaf(1.0f, c[k].z * ds8[k], dTotal[k]);
+        }
+    }
+    if (C.termMask & 4) {
+        const float4 c[2] = {ldCoef(&K[0]->srC, C.coefShared), ldCoef(&K[1]->srC, C.coefShared)};
+        const float4 kl[2] = {ldCoef(&K[0]->srK, C.coefShared), ldCoef(&K[1]->srK, C.coefShared)};
+        if (!(C.shareOverlap && (C.termMask & 2))) {
+            const float4 a[2] = {ldCoef(&K[0]->srA, C.coefShared), ldCoef(&K[1]->srA, C.coefShared)};
+            const float4 b[2] = {ldCoef(&K[0]->srB, C.coefShared), ldCoef(&K[1]->srB, C.coefShared)};
+            const float k1[2] = {c[0].x, c[1].x}, k2[2] = {c[0].y, c[1].y};
+            overlapFromCoef2(r, a, b, k1, k2, s8, ds8);
+        }
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const float st = c[k].z * s8[k];
+            const float E = fmaf(kl[k].y, st, kl[k].x) * st;
+            const float D = fmaf(2.0f * kl[k].y, st, kl[k].x) * c[k].z * ds8[k];
+            e[2] += inside[k] ? E : 0.0f;
+            dTotal[k] += D;
+        }
+    }
+    float4 out[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const float fs = inside[k] ? dTotal[k] * invR[k] : 0.0f;
+        out[k] = make_float4(dx[k] * fs, dy[k] * fs, dz[k] * fs, 0.0f);
+        pairs += inside[k];
+    }
+    out0 = out[0];
+    out1 = out[1];
+}
+
 template <bool LEAN, bool TABLE, bool UNIFORM = false>
 __global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPairTiles(ListBuffers L, PairBuffers P, PairTermConfig C) {
     __shared__ PairWarpStorage storage[kPairWarps];
@@ -427,9 +530,22 @@ __global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPai
             unsigned tilePairs = 0;
             for (int base = 0; base < total; base += kPairRound) {
                 const int n = min(kPairRound, total - base);
-                for (int p = lane; p < n; p += 32)
-                    S.force[p] = computeQueuedPair<LEAN, TABLE, UNIFORM>(S, S.queue[base + p], iBase, perPairImage,
-                                                                          C, L, P, coef, e, tilePairs);
+                if (kPairIlp && LEAN && TABLE && UNIFORM) {
+                    // two pairs per lane at a time: p and p + 32
+                    for (int p = lane; p < n; p += 64) {
+                        const bool two = p + 32 < n;
+                        float4 f0, f1;
+                        computeQueuedPair2(S, S.queue[base + p], S.queue[base + (two ? p + 32 : p)], two,
+                                           perPairImage, C, P, coef, e, tilePairs, f0, f1);
+                        S.force[p] = f0;
+                        if (two) S.force[p + 32] = f1;
+                    }
+                }
+                else
+                    for (int p = lane; p < n; p += 32)
+                        S.force[p] = computeQueuedPair<LEAN, TABLE, UNIFORM>(S, S.queue[base + p], iBase,
+                                                                              perPairImage, C, L, P, coef, e,
+                                                                              tilePairs);
                 __syncwarp();
                 // i side: this lane's row, contiguous in the queue
                 const int a = max(start, base), b = min(start + count, base + n);

@@ -229,6 +229,123 @@ __device__ __forceinline__ void dispersionFromCoef(float r, float invR, const fl
              e10 * fmaf(g, t10, -10.0f * f10 * invR));
 }
 
+// dispersionFromCoef for two pairs at once: the closed forms of both as one straight sequence (two independent
+// chains for the scheduler to interleave), then the series form of f_n for a pair below x = (n+1)/2 (rare at
+// interacting distances).
+__device__ __forceinline__ void dispersionFromCoef2(const float r[2], const float invR[2], const float4 K[2],
+                                                    float energy[2], float dEdR[2]) {
+    float x[2], expX[2], t6[2], t7[2], t8[2], t9[2], t10[2], f6[2], f8[2], f10[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        x[k] = K[k].w * r[k];
+        expX[k] = expNeg(x[k]);
+        const float x2 = x[k] * x[k];
+        const float x3 = x2 * x[k];
+        t6[k] = x3 * x3 * (1.0f / 720.0f);
+        t7[k] = t6[k] * x[k] * (1.0f / 7.0f);
+        t8[k] = t7[k] * x[k] * (1.0f / 8.0f);
+        t9[k] = t8[k] * x[k] * (1.0f / 9.0f);
+        t10[k] = t9[k] * x[k] * (1.0f / 10.0f);
+        float s6 = fmaf(x[k], 1.0f / 720.0f, 1.0f / 120.0f);
+        s6 = fmaf(s6, x[k], 1.0f / 24.0f);
+        s6 = fmaf(s6, x[k], 1.0f / 6.0f);
+        s6 = fmaf(s6, x[k], 0.5f);
+        s6 = fmaf(s6, x[k], 1.0f);
+        s6 = fmaf(s6, x[k], 1.0f);
+        const float s8 = (s6 + t7[k]) + t8[k];
+        const float s10 = (s8 + t9[k]) + t10[k];
+        f6[k] = fmaf(-expX[k], s6, 1.0f);
+        f8[k] = fmaf(-expX[k], s8, 1.0f);
+        f10[k] = fmaf(-expX[k], s10, 1.0f);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+        if (x[k] < 5.5f) {
+            float term = t10[k], tail = 0.0f;
+#pragma unroll 1
+            for (int m = 11; m <= 28; m++) {
+                term = term * x[k] * __fdividef(1.0f, (float)m);
+                tail += term;
+            }
+            const float tail8 = (tail + t10[k]) + t9[k];
+            f10[k] = expX[k] * tail;
+            if (x[k] < 4.5f) f8[k] = expX[k] * tail8;
+            if (x[k] < 3.5f) f6[k] = expX[k] * ((tail8 + t8[k]) + t7[k]);
+        }
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const float invR2 = invR[k] * invR[k];
+        const float e6 = K[k].x * invR2 * invR2 * invR2;
+        const float e8 = K[k].y * invR2 * invR2 * invR2 * invR2;
+        const float e10 = K[k].z * invR2 * invR2 * invR2 * invR2 * invR2;
+        energy[k] = -fmaf(f6[k], e6, fmaf(f8[k], e8, f10[k] * e10));
+        const float g = expX[k] * K[k].w;
+        dEdR[k] = -(e6 * fmaf(g, t6[k], -6.0f * f6[k] * invR[k]) + e8 * fmaf(g, t8[k], -8.0f * f8[k] * invR[k]) +
+                    e10 * fmaf(g, t10[k], -10.0f * f10[k] * invR[k]));
+    }
+}
+
+// overlapFromCoef for two pairs at once.  Where the warp holds both sides of the series/closed-form switch, both are
+// evaluated and each pair takes its own, so that the two chains stay one straight sequence.
+__device__ __forceinline__ void overlapFromCoef2(const float r[2], const float4 A[2], const float4 B[2],
+                                                 const float k1[2], const float k2[2], float s8pi[2],
+                                                 float ds8pi[2]) {
+    float ea[2], d[2], eP3[2], eP4[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        ea[k] = expNegScaled(r[k], A[k].x, A[k].y);
+        d[k] = r[k] * B[k].x;
+    }
+    const unsigned active = __activemask();
+    const bool anySeries = __any_sync(active, d[0] < 2.0f || d[1] < 2.0f);
+    const bool anyClosed = __any_sync(active, d[0] >= 2.0f || d[1] >= 2.0f);
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        float sP3 = 0.0f, sP4 = 0.0f, cP3 = 0.0f, cP4 = 0.0f;
+        if (anySeries) {
+            const float dd = fminf(d[k], 2.0f);
+            float p4 = 1.0f / 1307674368000.0f;
+            p4 = fmaf(p4, dd, 1.0f / 87178291200.0f);
+            p4 = fmaf(p4, dd, 1.0f / 6227020800.0f);
+            p4 = fmaf(p4, dd, 1.0f / 479001600.0f);
+            p4 = fmaf(p4, dd, 1.0f / 39916800.0f);
+            p4 = fmaf(p4, dd, 1.0f / 3628800.0f);
+            p4 = fmaf(p4, dd, 1.0f / 362880.0f);
+            p4 = fmaf(p4, dd, 1.0f / 40320.0f);
+            p4 = fmaf(p4, dd, 1.0f / 5040.0f);
+            p4 = fmaf(p4, dd, 1.0f / 720.0f);
+            p4 = fmaf(p4, dd, 1.0f / 120.0f);
+            p4 = fmaf(p4, dd, 1.0f / 24.0f);
+            sP3 = ea[k] * fmaf(dd, p4, 1.0f / 6.0f);
+            sP4 = ea[k] * p4;
+        }
+        if (anyClosed) {
+            const float dd = fmaxf(d[k], 2.0f);
+            const float eb = expNegScaled(r[k], A[k].z, A[k].w);
+            float id = rcpApprox(dd);
+            id = fmaf(id, fmaf(-dd, id, 1.0f), id);
+            cP3 = (eb - ea[k] * fmaf(dd, fmaf(0.5f, dd, 1.0f), 1.0f)) * id * id * id;
+            cP4 = fmaf(ea[k], -1.0f / 6.0f, cP3) * id;
+        }
+        const bool series = d[k] < 2.0f;
+        eP3[k] = series ? sP3 : cP3;
+        eP4[k] = series ? sP4 : cP4;
+    }
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const float ia = A[k].x, hab = B[k].x, is3 = B[k].y, c2 = B[k].z, c3 = B[k].w;
+        const float rk1 = r[k] * k1[k];
+        const float br = r[k] * r[k] * (rk1 - k2[k]);
+        const float dbr = r[k] * fmaf(3.0f, rk1, -2.0f * k2[k]);
+        const float poly = fmaf(r[k], fmaf(r[k], c3, c2), is3);
+        const float dpoly = fmaf(2.0f * r[k], c3, c2);
+        const float eg = fmaf(eP3[k], br, ea[k] * poly);
+        const float egp = fmaf(eP3[k], dbr, fmaf(fmaf(-3.0f, eP4[k], eP3[k]) * hab, br, ea[k] * dpoly));
+        s8pi[k] = eg;
+        ds8pi[k] = fmaf(-eg, ia, egp);
+    }
+}
+
 // Tang-Toennies damped C6/C8/C10 dispersion (InteraxPairTerms.h:267-293).  p = (m1, m2, m3, alpha), w the widths.
 __device__ __forceinline__ void dispersionEnergy(float r, float invR, float4 pi, float4 pj, float wi, float wj,
                                                  float twoBeta, float& energy, float& dEdR) {

@@ -19,6 +19,10 @@
 #ifndef IX_TUNE_PAIR_COLUMN_LISTS
 #define IX_TUNE_PAIR_COLUMN_LISTS 0
 #endif
+// pair kernel: 1 = two queued pairs per lane at a time on the class-table path without per-pair tests
+#ifndef IX_TUNE_PAIR_ILP
+#define IX_TUNE_PAIR_ILP 0
+#endif
 // pair kernel: largest class-pair table (bytes) staged in shared memory; larger tables are read through the cache
 #ifndef IX_TUNE_PAIR_SHARED_TABLE_BYTES
 #define IX_TUNE_PAIR_SHARED_TABLE_BYTES 0

@@ -31,15 +31,17 @@ sys.path.insert(0, str(PKG))
 import build_lib  # noqa: E402
 
 DEFAULTS = {"IX_TUNE_PAIR_WARPS": 4, "IX_TUNE_PAIR_ROUND": 128, "IX_TUNE_PAIR_MIN_BLOCKS": 8,
-            "IX_TUNE_PAIR_COLUMN_LISTS": 0, "IX_TUNE_PAIR_SHARED_TABLE_BYTES": 0, "IX_TUNE_PAIR_SKIN": 0.1,
+            "IX_TUNE_PAIR_COLUMN_LISTS": 0, "IX_TUNE_PAIR_ILP": 0, "IX_TUNE_PAIR_SHARED_TABLE_BYTES": 0,
+            "IX_TUNE_PAIR_SKIN": 0.1,
             "IX_TUNE_SITE_SKIN": 0.1, "IX_TUNE_ATM_FAST": 64, "IX_TUNE_ATM_ROUND": 64, "IX_TUNE_ATM_MIN_BLOCKS": 7}
 
 # groups of constants searched together, each with its candidate values (dicts of the group's macros)
 GROUPS = [
     ("pair tiles", [dict(IX_TUNE_PAIR_WARPS=w, IX_TUNE_PAIR_ROUND=r, IX_TUNE_PAIR_MIN_BLOCKS=b,
-                         IX_TUNE_PAIR_COLUMN_LISTS=c)
-                    for w, r, b, c in ((4, 128, 8, 0), (4, 64, 8, 0), (4, 256, 6, 0), (2, 128, 16, 0),
-                                       (4, 64, 7, 1), (4, 128, 6, 1), (2, 64, 14, 1))]),
+                         IX_TUNE_PAIR_COLUMN_LISTS=c, IX_TUNE_PAIR_ILP=i)
+                    for w, r, b, c, i in ((4, 128, 8, 0, 0), (4, 64, 8, 0, 0), (4, 256, 6, 0, 0), (2, 128, 16, 0, 0),
+                                          (4, 64, 7, 1, 0), (4, 128, 6, 1, 0), (4, 128, 8, 0, 1), (4, 128, 6, 0, 1),
+                                          (4, 128, 6, 1, 1), (4, 64, 7, 1, 1))]),
     ("pair table", [dict(IX_TUNE_PAIR_SHARED_TABLE_BYTES=b) for b in (0, 1024, 2048)]),
     ("pair skin", [dict(IX_TUNE_PAIR_SKIN=s) for s in (0.06, 0.08, 0.1, 0.12)]),
     ("three-body", [dict(IX_TUNE_ATM_FAST=f, IX_TUNE_ATM_ROUND=r, IX_TUNE_ATM_MIN_BLOCKS=b)
