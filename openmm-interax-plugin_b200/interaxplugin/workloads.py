@@ -107,19 +107,27 @@ def cluster_waters(num_waters, rng, min_dist=0.26):
 
 def build_water_system(positions, params, rng, method, cutoff, box_length=None, three_body_cutoff=None,
                        three_body=True, alchemical_waters=(), use_lrc=None, softcore_radius=0.0,
-                       use_switch=False, switch_distance=-1.0, overlap_method=0, site_rng=None, rigid=False):
+                       use_switch=False, switch_distance=-1.0, overlap_method=0, site_rng=None, rigid=False,
+                       distinct=False):
     """A System of waters with the three pair forces and (optionally) the three-body force; rigid: each water's
-    O-H, O-H and H-H distances constrained to the model geometry (the benchmark's rigid 3-site water)."""
+    O-H, O-H and H-H distances constrained to the model geometry (the benchmark's rigid 3-site water); distinct:
+    every water's parameters scaled by its own factors within 1% (every atom its own parameter class, as in a system of
+    many atom types, where the kernels cannot use per-class coefficient tables)."""
     num_waters = len(positions) // 3
     alch_set = set(int(w) for w in alchemical_waters)
     system = System()
     if box_length is not None:
         system.setDefaultPeriodicBoxVectors((box_length, 0, 0), (0, box_length, 0), (0, 0, box_length))
     disp, exch, sr = InteraxDispersionForce(), InteraxExchangeForce(), InteraxShortRangeForce()
+    drng = np.random.default_rng(777)
     for w in range(num_waters):
         alch = w in alch_set
         for t in ("O", "H", "H"):
             p = params[t]
+            if distinct:
+                f = 1.0 + 0.01 * drng.uniform(-1.0, 1.0, size=4)
+                p = dict(p, m1=p["m1"] * f[0], m2=p["m2"] * f[0], m3=p["m3"] * f[0], disp_width=p["disp_width"] * f[1],
+                         width=p["width"] * f[2], amplitude=p["amplitude"] * f[3], k=p["k"] * f[3], l=p["l"] * f[3])
             system.addParticle(MASS[t])
             disp.addParticle(p["m1"], p["m2"], p["m3"], p["alpha"], p["disp_width"], alch)
             exch.addParticle(p["amplitude"], p["width"], alch)

@@ -747,3 +747,11 @@ def test_neighbor_list_follows_motion():
     for step in range(4):
         moved = pos + rng.normal(scale=0.03 * step, size=pos.shape)
         compare(system, moved, box, context=ctx, scale="abs")
+
+
+def test_distinct_parameters_take_the_per_particle_path():
+    """Every water's parameters perturbed within 1% (every atom its own class, beyond the 16 classes of the
+    coefficient tables): the general pair kernel, against the oracle at the target bar."""
+    system, pos, box = W.water_box(216, 1.865, 0.9, seed=17, three_body_cutoff=0.6, distinct=True)
+    assert len({tuple(system.getForce(0).getParticleParameters(i)) for i in range(system.getNumParticles())}) > 16
+    compare(system, pos, box)
