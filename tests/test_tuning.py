@@ -1,0 +1,54 @@
+"""The autotuner's plumbing on the host: the constants it searches are exactly the IX_TUNE_* macros of
+csrc/ix_tuning.h, its candidates stay within what the kernels accept, and the build turns tuning.json into compiler
+definitions."""
+import json
+import re
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parents[1]
+PKG = ROOT / "openmm-interax-plugin_b200"
+sys.path.insert(0, str(PKG))
+
+import build_lib  # noqa: E402
+import tune  # noqa: E402
+
+
+def header_macros():
+    text = (PKG / "csrc" / "ix_tuning.h").read_text()
+    return dict(re.findall(r"#define (IX_TUNE_\w+) (\S+)", text))
+
+
+def test_tuner_covers_every_macro_with_the_header_defaults():
+    macros = header_macros()
+    assert set(tune.DEFAULTS) == set(macros)
+    for name, value in tune.DEFAULTS.items():
+        assert float(macros[name].rstrip("f")) == float(value), name
+    for _, options in tune.GROUPS:
+        for o in options:
+            assert set(o) <= set(macros)
+
+
+def test_candidates_respect_the_kernels_limits():
+    for _, options in tune.GROUPS:
+        for o in options:
+            v = dict(tune.DEFAULTS, **o)
+            # the fast triple kernel gathers at most two staged neighbors per lane
+            assert v["IX_TUNE_ATM_FAST"] in (32, 64)
+            assert v["IX_TUNE_PAIR_ROUND"] % 32 == 0 and v["IX_TUNE_ATM_ROUND"] % 32 == 0
+            # per-block static shared memory of the pair kernel stays within 48 KB
+            per_warp = 1024 + 1024 + 256 + 384 + 2048 + 16 * v["IX_TUNE_PAIR_ROUND"] + \
+                (2048 if v["IX_TUNE_PAIR_COLUMN_LISTS"] else 2)
+            assert per_warp * v["IX_TUNE_PAIR_WARPS"] <= 48 * 1024
+            assert 0.0 < v["IX_TUNE_PAIR_SKIN"] < 0.5 and 0.0 < v["IX_TUNE_SITE_SKIN"] < 0.5
+
+
+def test_build_passes_the_tuned_values(tmp_path, monkeypatch):
+    tuning = tmp_path / "tuning.json"
+    tuning.write_text(json.dumps({"chosen": {"IX_TUNE_PAIR_ROUND": 64, "IX_TUNE_PAIR_SKIN": 0.08}}))
+    monkeypatch.setattr(build_lib, "TUNING", tuning)
+    cmd = build_lib.compile_command(tmp_path / "lib.so")
+    assert "-DIX_TUNE_PAIR_ROUND=64" in cmd and "-DIX_TUNE_PAIR_SKIN=0.08f" in cmd
+    assert "arch=compute_100a,code=sm_100a" in " ".join(cmd)
+    explicit = build_lib.compile_command(tmp_path / "lib.so", {"IX_TUNE_PAIR_ILP": 1})
+    assert "-DIX_TUNE_PAIR_ILP=1" in explicit and not any("PAIR_ROUND" in a for a in explicit)
