@@ -2414,9 +2414,8 @@ static int enqueueSteps(ix_ctx* ctx, int num_steps, double dt) {
     auto step = [&]() -> int {
         if (!terms) {
             if (ctx->numConstraints)
-                kConstrainedDrift<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(ctx->K, dt, ctx->dInvMass,
-                                                                                    ctx->dOutForces, ctx->dVel,
-                                                                                    ctx->dPos);
+                kConstrainedDrift<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(
+                    ctx->K, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos, ctx->L, false, 0.0f);
             else
                 kVerletFirstHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel,
                                                              ctx->dPos);
@@ -2432,10 +2431,11 @@ static int enqueueSteps(ix_ctx* ctx, int num_steps, double dt) {
         }
         StepKick kick{ctx->dInvMass, ctx->dVel, 0.5 * dt};
         if (ctx->numConstraints) {
-            // the constrained clusters move together; the evaluation then checks the displacements itself
-            kConstrainedDrift<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(ctx->K, dt, ctx->dInvMass,
-                                                                                ctx->dOutForces, ctx->dVel, ctx->dPos);
-            kick.started = false;
+            // the constrained clusters move together, and refresh the pair list's sorted positions with the
+            // displacement check as kStepStart does
+            kConstrainedDrift<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(
+                ctx->K, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos, ctx->L, (terms & 7u) != 0,
+                0.25f * kPairSkin * kPairSkin);
         }
         else if (terms & 7u)
             // 128-thread blocks: a latency-bound gather by particle, spread over every SM

@@ -1,6 +1,8 @@
 // Velocity-Verlet integration on the device (units nm, ps, amu, kJ/mol: a = F/m in nm/ps^2).
 #pragma once
 
+#include "ix_nblist.cuh"
+
 namespace ix {
 
 // v += dt/2 F/m; x += dt v
@@ -42,26 +44,40 @@ struct ConstraintClusters {
     int* fail;                   // set when a cluster did not converge
 };
 
-// First half kick and drift of every particle, then SHAKE: the constrained particles of each cluster are moved along
-// the bonds of the positions before the drift until every distance is met; their velocities become the constrained
-// displacement over dt.
-__global__ void kConstrainedDrift(ConstraintClusters K, double dt, const double* invMass, const double* force,
-                                  double* vel, double* pos) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= K.num) return;
+// A particle's new position into the pair list's sorted slots (the list's build frame), with the displacement check
+// that requests a rebuild: the work kStepStart does for an unconstrained step.  Returns whether it moved too far.
+__device__ __forceinline__ bool refreshSlot(const ListBuffers& L, int i, const double x[3], float maxMove2) {
+    const int s = L.slotOf[i];
+    const double sx = x[0] - L.shift[3 * s], sy = x[1] - L.shift[3 * s + 1], sz = x[2] - L.shift[3 * s + 2];
+    L.spos[3 * s] = sx;
+    L.spos[3 * s + 1] = sy;
+    L.spos[3 * s + 2] = sz;
+    L.sposf[s] = make_float4((float)sx, (float)sy, (float)sz, 0.0f);
+    const double dx = x[0] - L.refPos[3 * i], dy = x[1] - L.refPos[3 * i + 1], dz = x[2] - L.refPos[3 * i + 2];
+    return (float)(dx * dx + dy * dy + dz * dz) > maxMove2;
+}
+
+// One cluster of kConstrainedDrift; returns whether one of its particles moved more than the list allows.
+__device__ __forceinline__ bool constrainedDriftCluster(ConstraintClusters K, int c, double dt, const double* invMass,
+                                                        const double* force, double* vel, double* pos,
+                                                        const ListBuffers& L, bool refresh, float maxMove2) {
     const int p0 = K.particleStart[c], np = K.particleStart[c + 1] - p0;
     const int c0 = K.constraintStart[c], nc = K.constraintStart[c + 1] - c0;
     const double h = 0.5 * dt;
+    bool moved = false;
     if (nc == 0) {
         for (int k = 0; k < np; k++) {
             const int i = K.particles[p0 + k];
+            double x[3];
             for (int d = 0; d < 3; d++) {
                 const double v = vel[3 * i + d] + h * invMass[i] * force[3 * i + d];
                 vel[3 * i + d] = v;
-                pos[3 * i + d] += dt * v;
+                x[d] = pos[3 * i + d] + dt * v;
+                pos[3 * i + d] = x[d];
             }
+            if (refresh) moved |= refreshSlot(L, i, x, maxMove2);
         }
-        return;
+        return moved;
     }
     double old[kMaxClusterParticles][3], x[kMaxClusterParticles][3], w[kMaxClusterParticles];
     for (int k = 0; k < np; k++) {
@@ -102,7 +118,21 @@ __global__ void kConstrainedDrift(ConstraintClusters K, double dt, const double*
             vel[3 * i + d] = (x[k][d] - old[k][d]) * invDt;
             pos[3 * i + d] = x[k][d];
         }
+        if (refresh) moved |= refreshSlot(L, i, x[k], maxMove2);
     }
+    return moved;
+}
+
+// First half kick and drift of every particle, then SHAKE: the constrained particles of each cluster are moved along
+// the bonds of the positions before the drift until every distance is met; their velocities become the constrained
+// displacement over dt.  With `refresh` (a pair list exists) the new positions also go to the list's sorted slots,
+// and a particle that moved more than the list allows requests a rebuild.
+__global__ void kConstrainedDrift(ConstraintClusters K, double dt, const double* invMass, const double* force,
+                                  double* vel, double* pos, ListBuffers L, bool refresh, float maxMove2) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    bool moved = false;
+    if (c < K.num) moved = constrainedDriftCluster(K, c, dt, invMass, force, vel, pos, L, refresh, maxMove2);
+    if (refresh && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(L.flag, 1);
 }
 
 // Velocities of each constrained cluster with the components along its bonds removed (no bond stretches), after the
