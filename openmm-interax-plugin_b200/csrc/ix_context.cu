@@ -2857,6 +2857,12 @@ int ix_md_finish(ix_ctx* ctx, double* positions, double* velocities, double* ene
         }
         IX_TRY(mdStateCopy(ctx, false));
         ctx->mdForcesValid = ctx->mdSavedForcesValid;
+        // both lists are rebuilt from the restored positions (the pair list's flag is set by its growth), so that
+        // the rerun is the run a large enough list gives, list for list
+        if (ctx->atmAllocated) {
+            const int one = 1;
+            IX_CUDA(ctx, cudaMemcpy(ctx->dFlags + 4, &one, sizeof(int), cudaMemcpyHostToDevice));
+        }
         for (const auto& seg : ctx->mdPending) IX_TRY(enqueueSteps(ctx, seg.first, seg.second));
         ctx->mdReruns++;
     }

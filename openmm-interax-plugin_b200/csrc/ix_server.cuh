@@ -413,12 +413,11 @@ int enqueueContextRun(ServerShard* H, ServerUnit* u, bool reused = false) {
         // a pooled context has these masses already (they are part of its description); setting them again would
         // invalidate its CUDA graphs
         if (!reused) IX_TRY(ix_md_set_masses(c, r->mass.data()));
-        else {
-            // rebuild both neighbor lists from the new positions, so that the request runs exactly as on a new context
-            const int rebuild = 1;
-            IX_TRY(stageCopy(c, c->dFlags, &rebuild, sizeof(int)));
-            if (c->atmAllocated) IX_TRY(stageCopy(c, c->dFlags + 4, &rebuild, sizeof(int)));
-        }
+        // both neighbor lists are rebuilt from the starting positions (a pooled context or a rerun after an overflow
+        // holds lists of other positions), so that the request runs exactly as on a new context
+        const int rebuild = 1;
+        IX_TRY(stageCopy(c, c->dFlags, &rebuild, sizeof(int)));
+        if (c->atmAllocated) IX_TRY(stageCopy(c, c->dFlags + 4, &rebuild, sizeof(int)));
         if (r->vel.empty()) IX_CUDA(c, cudaMemsetAsync(c->dVel, 0, n3 * sizeof(double), c->stream));
         else IX_TRY(stageCopy(c, c->dVel, r->vel.data(), n3 * sizeof(double)));
     }
