@@ -1814,7 +1814,9 @@ int ix_ctx_create(int num_particles, int device, const double* default_box, ix_c
 
 void ix_ctx_destroy(ix_ctx* ctx) {
     if (!ctx) return;
-    cudaSetDevice(ctx->device);
+    // a request described on the host only (device -1) has no device side: selecting device -1 would leave an
+    // "invalid device" error for the next cudaGetLastError of whatever runs on this thread
+    if (ctx->device >= 0) cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     releaseGraph(ctx->graphCompute);
     releaseGraph(ctx->graphDevice);

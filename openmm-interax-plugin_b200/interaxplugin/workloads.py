@@ -110,9 +110,10 @@ def build_water_system(positions, params, rng, method, cutoff, box_length=None, 
                        use_switch=False, switch_distance=-1.0, overlap_method=0, site_rng=None, rigid=False,
                        distinct=False):
     """A System of waters with the three pair forces and (optionally) the three-body force; rigid: each water's
-    O-H, O-H and H-H distances constrained to the model geometry (the benchmark's rigid 3-site water); distinct:
-    every water's parameters scaled by its own factors within 1% (every atom its own parameter class, as in a system of
-    many atom types, where the kernels cannot use per-class coefficient tables)."""
+    O-H, O-H and H-H distances constrained to the model geometry (the benchmark's rigid 3-site water); distinct: a
+    number of variants of each atom type, every variant's parameters scaled by its own factors within 1%, and each
+    water one variant (2 x distinct parameter classes, as in a system of many atom types: beyond the 16 classes of the
+    kernels' per-class coefficient tables)."""
     num_waters = len(positions) // 3
     alch_set = set(int(w) for w in alchemical_waters)
     system = System()
@@ -120,14 +121,21 @@ def build_water_system(positions, params, rng, method, cutoff, box_length=None, 
         system.setDefaultPeriodicBoxVectors((box_length, 0, 0), (0, box_length, 0), (0, 0, box_length))
     disp, exch, sr = InteraxDispersionForce(), InteraxExchangeForce(), InteraxShortRangeForce()
     drng = np.random.default_rng(777)
+    variants = {}
+    if distinct:
+        for t in ("O", "H"):
+            variants[t] = []
+            for _ in range(int(distinct)):
+                f = 1.0 + 0.01 * drng.uniform(-1.0, 1.0, size=4)
+                p = params[t]
+                variants[t].append(dict(p, m1=p["m1"] * f[0], m2=p["m2"] * f[0], m3=p["m3"] * f[0],
+                                        disp_width=p["disp_width"] * f[1], width=p["width"] * f[2],
+                                        amplitude=p["amplitude"] * f[3], k=p["k"] * f[3], l=p["l"] * f[3]))
     for w in range(num_waters):
         alch = w in alch_set
+        v = int(drng.integers(int(distinct))) if distinct else 0
         for t in ("O", "H", "H"):
-            p = params[t]
-            if distinct:
-                f = 1.0 + 0.01 * drng.uniform(-1.0, 1.0, size=4)
-                p = dict(p, m1=p["m1"] * f[0], m2=p["m2"] * f[0], m3=p["m3"] * f[0], disp_width=p["disp_width"] * f[1],
-                         width=p["width"] * f[2], amplitude=p["amplitude"] * f[3], k=p["k"] * f[3], l=p["l"] * f[3])
+            p = variants[t][v] if distinct else params[t]
             system.addParticle(MASS[t])
             disp.addParticle(p["m1"], p["m2"], p["m3"], p["alpha"], p["disp_width"], alch)
             exch.addParticle(p["amplitude"], p["width"], alch)

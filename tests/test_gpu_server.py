@@ -139,6 +139,7 @@ def test_server_reuses_contexts_of_the_same_system():
         got.append(srv.run_all(timeout=120)[rid])
     stats = srv.stats()
     srv.close()
+    assert all(r.status == 0 for r in got), [r.error for r in got]
     assert stats["contexts_reused"] >= 3, stats
     for req, m in zip(reqs, got):
         (a,), _ = _serve([req])
