@@ -65,6 +65,14 @@ def parse():
     return p.parse_args()
 
 
+_T0 = time.time()
+
+
+def progress(msg):
+    """A stage of the run on stderr (the JSON line alone goes to stdout)."""
+    print(f"[bench {time.time() - _T0:7.1f} s] {msg}", file=sys.stderr, flush=True)
+
+
 def dist_init(args):
     """One process per GPU under torchrun (NCCL); on a host without GPUs (the CPU tests of the rank logic) the ranks
     use gloo.  Returns (rank, world)."""
@@ -299,6 +307,7 @@ def run_ours(args, rank, world):
 
     device = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(device)
+    progress("building the 24k box")
     system, pos0, box = build_system(args, rank)
     ctx = Context(system, properties={"DeviceIndex": device})
     L = _capi.lib()
@@ -333,12 +342,14 @@ def run_ours(args, rank, world):
         pairs, triples = ctx.getCounts()
         return start.elapsed_time(end), pair_ms.value, atm_ms.value, pairs, triples
 
+    progress("relaxed; MD warm-up")
     for _ in range(args.warmup):
         md_step()
     if world > 1:
         import torch.distributed as dist
         dist.barrier()
     torch.cuda.synchronize()
+    progress("timed MD steps")
     rows = []
     launches0 = ctypes.c_longlong()
     ctx._check(L.ix_get_launch_count(ctx._ctx, ctypes.byref(launches0)))
@@ -393,6 +404,7 @@ def run_ours(args, rank, world):
 
     if rank != 0:
         return
+    progress("timed steps and e2e done; oracle error")
     # the error of this run against the FP64 oracle: the last e2e frame, evaluated by both (outside the timed region)
     import pyoracle
     last = frames[-1].numpy()
@@ -402,11 +414,14 @@ def run_ours(args, rank, world):
                     "force_rms_rel": float(np.sqrt(((f_gpu - f_or) ** 2).mean() / (f_or ** 2).mean())),
                     "frame": "the last configuration of the e2e pass (rigid-water MD trajectory)"}
     # the same box without constraints (flexible waters whose intramolecular pairs are excluded), for comparison
+    progress("unconstrained ns/day")
     flex = md_ns_per_day(args, build_system(args, rank, rigid=False), device, dt_ps)
+    progress("general pair-kernel instance")
     # the pair kernel's general instance: the same box with every atom its own parameter class
     general = general_pair_kernel(args, device, peak.value)
     # the batched workload's evaluations/s beside the plain per-system path (one GPU)
     batched = None
+    progress("batched workload")
     if world == 1:
         cl = clusters_measure(argparse.Namespace(**{**vars(args), "steps": 10, "warmup": 3}), 0, 1)
         batched = {"value": cl["value"], "unit": "evaluations/s", "e2e": cl["e2e"]["value"],
@@ -417,6 +432,7 @@ def run_ours(args, rank, world):
     pairs_per_launch = float(np.mean(kernel_rows[:, 3]))
     triples_per_launch = float(np.mean(kernel_rows[:, 4]))
     achieved = pairs_per_launch * F_PAIR / (pair_ms * 1e-3) / 1e12
+    progress("CPU baseline")
     base = cpu_baseline(system, cur, box)
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": args.steps,
