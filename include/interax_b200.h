@@ -207,9 +207,9 @@ int ix_md_run(ix_ctx* ctx, int num_steps, double dt, double* positions, double* 
 
 /* Distance constraints of the MD loop (OpenMM's System::addConstraint; the rigid 3-site waters of the benchmark):
  * particles pairs[2k], pairs[2k+1] kept at distances[k] nm.  Each connected cluster of constrained particles (at most
- * 8 particles) is solved by SHAKE after the drift and by RATTLE's velocity stage after the second half kick, to the
- * relative tolerance given (on the squared distance, and on the stretching rate per ps).  num_constraints = 0 removes
- * them.  A step whose constraints did not converge makes ix_md_finish return IX_ERR_STATE. */
+ * 8 particles and 12 constraints) is solved by SHAKE after the drift (Newton on all of the cluster's multipliers) and
+ * by RATTLE's velocity stage after the second half kick (a direct linear solve), to the relative tolerance given (on
+ * the squared distance, and on the stretching rate per ps).  num_constraints = 0 removes them.  A step whose constraints did not converge makes ix_md_finish return IX_ERR_STATE. */
 int ix_md_set_constraints(ix_ctx* ctx, int num_constraints, const int32_t* pairs, const double* distances,
                           double tolerance);
 

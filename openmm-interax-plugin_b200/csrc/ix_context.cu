@@ -2413,10 +2413,11 @@ static int enqueueSteps(ix_ctx* ctx, int num_steps, double dt) {
     key.dt = dt;
     // one step: the first half kick and drift (fused with the list's displacement check and position refresh when
     // there are pair terms), the evaluation at the new positions, whose finishing kernel applies the second half kick
+    const int clusterGrid = (ctx->K.num + kClusterBlock - 1) / kClusterBlock;
     auto step = [&]() -> int {
         if (!terms) {
             if (ctx->numConstraints)
-                kConstrainedDrift<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(
+                kConstrainedDrift<<<clusterGrid, kClusterBlock, 0, ctx->stream>>>(
                     ctx->K, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos, ctx->L, false, 0.0f);
             else
                 kVerletFirstHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel,
@@ -2424,8 +2425,8 @@ static int enqueueSteps(ix_ctx* ctx, int num_steps, double dt) {
             kVerletSecondHalf<<<g, 256, 0, ctx->stream>>>(n, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel);
             ctx->launches += 2;
             if (ctx->numConstraints) {
-                kConstrainVelocities<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(ctx->K, ctx->dInvMass,
-                                                                                       ctx->dPos, ctx->dVel);
+                kConstrainVelocities<<<clusterGrid, kClusterBlock, 0, ctx->stream>>>(ctx->K, ctx->dInvMass,
+                                                                                    ctx->dPos, ctx->dVel);
                 ctx->launches += 1;
             }
             IX_CUDA(ctx, cudaGetLastError());
@@ -2435,7 +2436,7 @@ static int enqueueSteps(ix_ctx* ctx, int num_steps, double dt) {
         if (ctx->numConstraints) {
             // the constrained clusters move together, and refresh the pair list's sorted positions with the
             // displacement check as kStepStart does
-            kConstrainedDrift<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(
+            kConstrainedDrift<<<clusterGrid, kClusterBlock, 0, ctx->stream>>>(
                 ctx->K, dt, ctx->dInvMass, ctx->dOutForces, ctx->dVel, ctx->dPos, ctx->L, (terms & 7u) != 0,
                 0.25f * kPairSkin * kPairSkin);
         }
@@ -2448,8 +2449,8 @@ static int enqueueSteps(ix_ctx* ctx, int num_steps, double dt) {
         ctx->launches += 1;
         IX_TRY(launchEvaluation(ctx, terms, ctx->dOutForces, ctx->dOutEnergy, nullptr, 0, &kick));
         if (ctx->numConstraints) {
-            kConstrainVelocities<<<(ctx->K.num + 127) / 128, 128, 0, ctx->stream>>>(ctx->K, ctx->dInvMass, ctx->dPos,
-                                                                                   ctx->dVel);
+            kConstrainVelocities<<<clusterGrid, kClusterBlock, 0, ctx->stream>>>(ctx->K, ctx->dInvMass, ctx->dPos,
+                                                                                ctx->dVel);
             ctx->launches += 1;
         }
         IX_CUDA(ctx, cudaGetLastError());
@@ -2941,6 +2942,9 @@ int ix_md_set_constraints(ix_ctx* ctx, int num_constraints, const int32_t* pairs
     std::vector<int2> pair;
     std::vector<double> dist2;
     for (int c = 0; c < numClusters; c++) {
+        if ((int)consOf[c].size() > kMaxClusterConstraints)
+            return fail(ctx, IX_ERR_INVALID, "a cluster of %zu constraints (the limit is %d)", consOf[c].size(),
+                        kMaxClusterConstraints);
         for (int k : consOf[c]) {
             pair.push_back(make_int2(local[pairs[2 * k]], local[pairs[2 * k + 1]]));
             dist2.push_back(distances[k] * distances[k]);

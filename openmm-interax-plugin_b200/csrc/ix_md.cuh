@@ -27,11 +27,60 @@ __global__ void kVerletSecondHalf(int n, double dt, const double* invMass, const
 }
 
 // Distance constraints (OpenMM's System::addConstraint; the benchmark's rigid 3-site waters), solved per connected
-// cluster of constrained particles by one thread: positions by SHAKE (J.-P. Ryckaert, G. Ciccotti and H. J. C.
-// Berendsen, J. Comput. Phys. 23, 327 (1977)), velocities by the second stage of RATTLE (H. C. Andersen, J. Comput.
-// Phys. 52, 24 (1983)), both iterated over the cluster's constraints until every one holds to the tolerance.  A
-// particle without constraints is a cluster of one, so the cluster kernels move every particle.
+// cluster of constrained particles by one thread.  Positions: the SHAKE equations (J.-P. Ryckaert, G. Ciccotti and
+// H. J. C. Berendsen, J. Comput. Phys. 23, 327 (1977): each particle moved along the cluster's bonds before the
+// drift) solved for all the cluster's multipliers at once by Newton's method, as in M-SHAKE (A. Kraeutler, W. F. van
+// Gunsteren and P. H. Huenenberger, J. Comput. Chem. 22, 501 (2001)), which converges quadratically where a sweep
+// over the constraints one by one converges slowly for coupled bonds.  Velocities: the second stage of RATTLE
+// (H. C. Andersen, J. Comput. Phys. 52, 24 (1983)), whose conditions are linear in the multipliers, solved in one step
+// with one refinement.  A particle without constraints is a cluster of one, so the cluster kernels move every particle.
 constexpr int kMaxClusterParticles = 8;
+constexpr int kMaxClusterConstraints = 12;
+// one thread per cluster in blocks of one warp: a few thousand clusters still spread over every SM
+constexpr int kClusterBlock = 32;
+
+// Solve the n x n system a x = b in place (b becomes x) by Gaussian elimination with partial pivoting; a row-major
+// with a leading dimension of kMaxClusterConstraints.  Returns false for a singular matrix.
+__device__ __forceinline__ bool solveSmall(double (&a)[kMaxClusterConstraints][kMaxClusterConstraints],
+                                           double (&b)[kMaxClusterConstraints], int n) {
+    for (int col = 0; col < n; col++) {
+        int piv = col;
+        for (int r = col + 1; r < n; r++)
+            if (fabs(a[r][col]) > fabs(a[piv][col])) piv = r;
+        if (a[piv][col] == 0.0) return false;
+        if (piv != col) {
+            for (int k = 0; k < n; k++) {
+                const double t = a[col][k];
+                a[col][k] = a[piv][k];
+                a[piv][k] = t;
+            }
+            const double t = b[col];
+            b[col] = b[piv];
+            b[piv] = t;
+        }
+        const double inv = 1.0 / a[col][col];
+        for (int r = col + 1; r < n; r++) {
+            const double f = a[r][col] * inv;
+            if (f == 0.0) continue;
+            for (int k = col; k < n; k++) a[r][k] -= f * a[col][k];
+            b[r] -= f * b[col];
+        }
+    }
+    for (int r = n - 1; r >= 0; r--) {
+        double sum = b[r];
+        for (int k = r + 1; k < n; k++) sum -= a[r][k] * b[k];
+        b[r] = sum / a[r][r];
+    }
+    return true;
+}
+
+// The coupling of constraint l's multiplier to constraint k's bond: how the bond vector of k changes per unit of l's
+// multiplier, as the coefficient of l's direction (w_p for the first particle of l, -w_q for its second).
+__device__ __forceinline__ double constraintCoupling(int2 k, int2 l, const double* w) {
+    const double ap = (k.x == l.x ? w[k.x] : 0.0) - (k.x == l.y ? w[k.x] : 0.0);
+    const double aq = (k.y == l.x ? w[k.y] : 0.0) - (k.y == l.y ? w[k.y] : 0.0);
+    return ap - aq;
+}
 
 struct ConstraintClusters {
     int num;                     // clusters, including the single particles
@@ -88,27 +137,40 @@ __device__ __forceinline__ bool constrainedDriftCluster(ConstraintClusters K, in
             x[k][d] = old[k][d] + dt * (vel[3 * i + d] + h * w[k] * force[3 * i + d]);
         }
     }
+    // Newton on g_k(lambda) = d_k^2 - |s_k|^2 = 0, s_k the bond of constraint k, each particle moved along the
+    // pre-drift bonds r_l: x_p += w_p lambda_l r_l, x_q -= w_q lambda_l r_l
+    int2 pair[kMaxClusterConstraints];
+    double r0[kMaxClusterConstraints][3], d2[kMaxClusterConstraints];
+    for (int q = 0; q < nc; q++) {
+        pair[q] = K.pair[c0 + q];
+        d2[q] = K.dist2[c0 + q];
+        for (int d = 0; d < 3; d++) r0[q][d] = old[pair[q].x][d] - old[pair[q].y][d];
+    }
     bool converged = false;
-    for (int iteration = 0; iteration < 1000 && !converged; iteration++) {
-        converged = true;
-        for (int q = 0; q < nc; q++) {
-            const int2 pq = K.pair[c0 + q];
-            const double d2 = K.dist2[c0 + q];
-            double s[3], r[3];
-            for (int d = 0; d < 3; d++) {
-                s[d] = x[pq.x][d] - x[pq.y][d];
-                r[d] = old[pq.x][d] - old[pq.y][d];
-            }
-            const double diff = d2 - (s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
-            if (fabs(diff) > K.tolerance * d2) converged = false;
-            const double denom = 2.0 * (s[0] * r[0] + s[1] * r[1] + s[2] * r[2]) * (w[pq.x] + w[pq.y]);
-            if (denom == 0.0) continue;
-            const double g = diff / denom;
-            for (int d = 0; d < 3; d++) {
-                x[pq.x][d] += g * w[pq.x] * r[d];
-                x[pq.y][d] -= g * w[pq.y] * r[d];
-            }
+    for (int iteration = 0; iteration < 30; iteration++) {
+        double s[kMaxClusterConstraints][3], g[kMaxClusterConstraints];
+        double worst = 0.0;
+        for (int k = 0; k < nc; k++) {
+            for (int d = 0; d < 3; d++) s[k][d] = x[pair[k].x][d] - x[pair[k].y][d];
+            g[k] = d2[k] - (s[k][0] * s[k][0] + s[k][1] * s[k][1] + s[k][2] * s[k][2]);
+            worst = fmax(worst, fabs(g[k]) / d2[k]);
         }
+        if (worst <= K.tolerance) {
+            converged = true;
+            break;
+        }
+        double J[kMaxClusterConstraints][kMaxClusterConstraints];
+        for (int k = 0; k < nc; k++)
+            for (int l = 0; l < nc; l++) {
+                const double c = constraintCoupling(pair[k], pair[l], w);
+                J[k][l] = c == 0.0 ? 0.0 : 2.0 * c * (s[k][0] * r0[l][0] + s[k][1] * r0[l][1] + s[k][2] * r0[l][2]);
+            }
+        if (!solveSmall(J, g, nc)) break;
+        for (int l = 0; l < nc; l++)
+            for (int d = 0; d < 3; d++) {
+                x[pair[l].x][d] += g[l] * w[pair[l].x] * r0[l][d];
+                x[pair[l].y][d] -= g[l] * w[pair[l].y] * r0[l][d];
+            }
     }
     if (!converged) atomicOr(K.fail, 1);
     const double invDt = 1.0 / dt;
@@ -124,8 +186,9 @@ __device__ __forceinline__ bool constrainedDriftCluster(ConstraintClusters K, in
 }
 
 // First half kick and drift of every particle, then SHAKE: the constrained particles of each cluster are moved along
-// the bonds of the positions before the drift until every distance is met; their velocities become the constrained
-// displacement over dt.  With `refresh` (a pair list exists) the new positions also go to the list's sorted slots,
+// the bonds of the positions before the drift until every distance is met (Newton on all of the cluster's
+// multipliers, at most 30 iterations; quadratic convergence takes 3 to 4 from a 1 fs drift); their velocities become
+// the constrained displacement over dt.  With `refresh` (a pair list exists) the new positions also go to the list's sorted slots,
 // and a particle that moved more than the list allows requests a rebuild.
 __global__ void kConstrainedDrift(ConstraintClusters K, double dt, const double* invMass, const double* force,
                                   double* vel, double* pos, ListBuffers L, bool refresh, float maxMove2) {
@@ -136,7 +199,7 @@ __global__ void kConstrainedDrift(ConstraintClusters K, double dt, const double*
 }
 
 // Velocities of each constrained cluster with the components along its bonds removed (no bond stretches), after the
-// second half kick.
+// second half kick: one linear solve of the cluster's multipliers and at most two refinements of the residual.
 __global__ void kConstrainVelocities(ConstraintClusters K, const double* invMass, const double* pos, double* vel) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= K.num) return;
@@ -152,27 +215,41 @@ __global__ void kConstrainVelocities(ConstraintClusters K, const double* invMass
             v[k][d] = vel[3 * i + d];
         }
     }
+    // conditions r_k . (v_p - v_q) = 0 after v_i += sum_l a_{l,i} mu_l r_l: linear in mu, solved directly, then
+    // once more on the residual (rounding)
+    int2 pair[kMaxClusterConstraints];
+    double r[kMaxClusterConstraints][3];
+    for (int q = 0; q < nc; q++) {
+        pair[q] = K.pair[c0 + q];
+        for (int d = 0; d < 3; d++) r[q][d] = x[pair[q].x][d] - x[pair[q].y][d];
+    }
     bool converged = false;
-    for (int iteration = 0; iteration < 1000 && !converged; iteration++) {
-        converged = true;
-        for (int q = 0; q < nc; q++) {
-            const int2 pq = K.pair[c0 + q];
-            double r[3], dv[3];
-            for (int d = 0; d < 3; d++) {
-                r[d] = x[pq.x][d] - x[pq.y][d];
-                dv[d] = v[pq.x][d] - v[pq.y][d];
-            }
-            const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-            const double rate = (dv[0] * r[0] + dv[1] * r[1] + dv[2] * r[2]) / r2;   // d|r|/dt / |r|
-            if (fabs(rate) > K.tolerance) converged = false;
-            const double wsum = w[pq.x] + w[pq.y];
-            if (wsum == 0.0) continue;
-            const double k = rate / wsum;
-            for (int d = 0; d < 3; d++) {
-                v[pq.x][d] -= k * w[pq.x] * r[d];
-                v[pq.y][d] += k * w[pq.y] * r[d];
-            }
+    for (int pass = 0; pass < 3; pass++) {
+        double rhs[kMaxClusterConstraints];
+        double worst = 0.0;
+        for (int k = 0; k < nc; k++) {
+            const double r2 = r[k][0] * r[k][0] + r[k][1] * r[k][1] + r[k][2] * r[k][2];
+            double dot = 0.0;
+            for (int d = 0; d < 3; d++) dot += r[k][d] * (v[pair[k].x][d] - v[pair[k].y][d]);
+            rhs[k] = -dot;
+            worst = fmax(worst, fabs(dot) / r2);    // stretching rate per ps
         }
+        if (worst <= K.tolerance) {
+            converged = true;
+            break;
+        }
+        double M[kMaxClusterConstraints][kMaxClusterConstraints];
+        for (int k = 0; k < nc; k++)
+            for (int l = 0; l < nc; l++) {
+                const double c = constraintCoupling(pair[k], pair[l], w);
+                M[k][l] = c == 0.0 ? 0.0 : c * (r[k][0] * r[l][0] + r[k][1] * r[l][1] + r[k][2] * r[l][2]);
+            }
+        if (!solveSmall(M, rhs, nc)) break;
+        for (int l = 0; l < nc; l++)
+            for (int d = 0; d < 3; d++) {
+                v[pair[l].x][d] += rhs[l] * w[pair[l].x] * r[l][d];
+                v[pair[l].y][d] -= rhs[l] * w[pair[l].y] * r[l][d];
+            }
     }
     if (!converged) atomicOr(K.fail, 1);
     for (int k = 0; k < np; k++) {

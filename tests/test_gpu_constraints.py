@@ -1,5 +1,6 @@
-"""Rigid water in the device MD loop (ix_md_set_constraints): SHAKE after the drift, RATTLE's velocity stage after the
-second half kick, per cluster of constrained particles.
+"""Rigid water in the device MD loop (ix_md_set_constraints): SHAKE after the drift (Newton on each cluster's
+multipliers), RATTLE's velocity stage after the second half kick (a direct solve), per cluster of constrained
+particles.
 
 The reference's ns/day comes from OpenMM's integrator on systems whose waters are rigid (tests/python/benchmark.py:
 88-97 with the force field's rigid water); here the constraints keep every O-H and H-H distance of the 3-site waters
