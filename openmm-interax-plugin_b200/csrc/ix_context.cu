@@ -563,7 +563,8 @@ static void computeLrc(ix_ctx* ctx) {
 
 // Per-particle float parameters in original order, with the term flags.
 // Coefficients of one ordered pair of overlap widths (w1, w2 > 0), double precision, rounded once to float.
-static void overlapCoefficients(double w1, double w2, float4& A, float4& B, float& k1, float& k2) {
+static void overlapCoefficients(double w1, double w2, float4& A, float4& B, float& k1, float& k2, float4& Q,
+                                float4& R) {
     const double a = std::min(w1, w2), b = std::max(w1, w2);
     const double ia = 1.0 / a, ib = 1.0 / b, h = b - a, s = a + b;
     const double is3 = 1.0 / (s * s * s);
@@ -576,6 +577,12 @@ static void overlapCoefficients(double w1, double w2, float4& A, float4& B, floa
     B = make_float4((float)(ia - ib), (float)is3, (float)(ia * is3), (float)(0.5 * ia * ia * ib / (s * s)));
     k1 = (float)(h * ia * ia * ia * ib * ib / (s * s));
     k2 = (float)(4.0 * ia * ib * is3);
+    // the exponential rates log2(e)/a and log2(e)/b as float-float, for the packed path
+    float qaHi, qaLo, qbHi, qbLo;
+    split(ia * M_LOG2E, qaHi, qaLo);
+    split(ib * M_LOG2E, qbHi, qbLo);
+    Q = make_float4(-qaHi, qaHi, qaLo, -qbHi);
+    R = make_float4(qbHi, qbLo, 0.0f, 0.0f);
 }
 
 // Particles with identical parameters of all pair forces form a class; with at most kMaxClasses classes the kernel
@@ -632,13 +639,13 @@ static int classTableHost(const std::vector<const ix_ctx*>& sys, std::vector<std
             if (ctx->term[1].present) {
                 const double* p = &ctx->term[1].params[2 * i];
                 const double* q = &ctxJ->term[1].params[2 * j];
-                if (p[1] != 0 && q[1] != 0) overlapCoefficients(p[1], q[1], K.ovA, K.ovB, K.ovC.x, K.ovC.y);
+                if (p[1] != 0 && q[1] != 0) overlapCoefficients(p[1], q[1], K.ovA, K.ovB, K.ovC.x, K.ovC.y, K.ovQ, K.ovR);
                 K.ovC.z = (float)(p[0] * q[0] / (8.0 * M_PI));
             }
             if (ctx->term[2].present) {
                 const double* p = &ctx->term[2].params[3 * i];
                 const double* q = &ctxJ->term[2].params[3 * j];
-                if (p[2] != 0 && q[2] != 0) overlapCoefficients(p[2], q[2], K.srA, K.srB, K.srC.x, K.srC.y);
+                if (p[2] != 0 && q[2] != 0) overlapCoefficients(p[2], q[2], K.srA, K.srB, K.srC.x, K.srC.y, K.srQ, K.srR);
                 const double ws = p[2] + q[2];
                 K.srC.z = (float)(ws * ws * ws);
                 K.srK = make_float4((float)(0.5 * (p[0] + q[0])), (float)(0.5 * (p[1] + q[1])), 0.0f, 0.0f);
@@ -1752,7 +1759,7 @@ int ix_measure_fp32_peak(int device, double* tflops) {
     cudaGetDeviceProperties(&prop, device);
     int perSM = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSM, kFmaPeak, 256, 0);
-    const int blocks = prop.multiProcessorCount * std::max(1, perSM) * 4;
+    const int blocks = prop.multiProcessorCount * std::max(1, perSM);
     float* sink = nullptr;
     if (cudaMalloc(&sink, 256 * sizeof(float)) != cudaSuccess) return fail(nullptr, IX_ERR_CUDA, "cudaMalloc failed");
     cudaEvent_t a, b;
@@ -2945,9 +2952,28 @@ int ix_md_set_constraints(ix_ctx* ctx, int num_constraints, const int32_t* pairs
         if ((int)consOf[c].size() > kMaxClusterConstraints)
             return fail(ctx, IX_ERR_INVALID, "a cluster of %zu constraints (the limit is %d)", consOf[c].size(),
                         kMaxClusterConstraints);
+        const size_t first = pair.size();
         for (int k : consOf[c]) {
             pair.push_back(make_int2(local[pairs[2 * k]], local[pairs[2 * k + 1]]));
             dist2.push_back(distances[k] * distances[k]);
+        }
+        if (consOf[c].size() == 3 && particleStart[c + 1] - particleStart[c] == 3) {
+            // a rigid triangle: its constraints as (0,1), (0,2), (1,2) (a constraint's orientation does not change
+            // its solution), which the device solves with every index known at compile time
+            std::vector<std::pair<int2, double>> tri;
+            for (size_t q = first; q < pair.size(); q++) {
+                const int2 e = pair[q];
+                tri.push_back({make_int2(std::min(e.x, e.y), std::max(e.x, e.y)), dist2[q]});
+            }
+            std::sort(tri.begin(), tri.end(), [](const std::pair<int2, double>& a, const std::pair<int2, double>& b) {
+                return a.first.x != b.first.x ? a.first.x < b.first.x : a.first.y < b.first.y;
+            });
+            if (tri[0].first.x == 0 && tri[0].first.y == 1 && tri[1].first.x == 0 && tri[1].first.y == 2 &&
+                tri[2].first.x == 1 && tri[2].first.y == 2)
+                for (int q = 0; q < 3; q++) {
+                    pair[first + q] = tri[q].first;
+                    dist2[first + q] = tri[q].second;
+                }
         }
         consStart.push_back((int)pair.size());
     }

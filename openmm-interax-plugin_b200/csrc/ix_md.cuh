@@ -106,32 +106,55 @@ __device__ __forceinline__ bool refreshSlot(const ListBuffers& L, int i, const d
     return (float)(dx * dx + dy * dy + dz * dz) > maxMove2;
 }
 
-// One cluster of kConstrainedDrift; returns whether one of its particles moved more than the list allows.
+// A rigid triangle (a 3-site water): 3 particles and the constraints (0,1), (0,2), (1,2) in this order, which the host
+// arranges.  Its solves take every index at compile time, so the cluster stays in registers.
+__device__ __forceinline__ int2 triPair(int q) { return make_int2(q == 2 ? 1 : 0, q == 0 ? 1 : 2); }
+
+__device__ __forceinline__ bool isTriangle(const ConstraintClusters& K, int c0, int np, int nc) {
+    if (np != 3 || nc != 3) return false;
+    const int2 a = K.pair[c0], b = K.pair[c0 + 1], c = K.pair[c0 + 2];
+    return a.x == 0 && a.y == 1 && b.x == 0 && b.y == 2 && c.x == 1 && c.y == 2;
+}
+
+// Solve the 3 x 3 system a x = b by the adjugate (Cramer's rule); false for a singular matrix.
+__device__ __forceinline__ bool solve3(const double (&a)[3][3], double (&b)[3]) {
+    const double i00 = a[1][1] * a[2][2] - a[1][2] * a[2][1], i01 = a[0][2] * a[2][1] - a[0][1] * a[2][2],
+                 i02 = a[0][1] * a[1][2] - a[0][2] * a[1][1];
+    const double i10 = a[1][2] * a[2][0] - a[1][0] * a[2][2], i11 = a[0][0] * a[2][2] - a[0][2] * a[2][0],
+                 i12 = a[0][2] * a[1][0] - a[0][0] * a[1][2];
+    const double i20 = a[1][0] * a[2][1] - a[1][1] * a[2][0], i21 = a[0][1] * a[2][0] - a[0][0] * a[2][1],
+                 i22 = a[0][0] * a[1][1] - a[0][1] * a[1][0];
+    const double det = a[0][0] * i00 + a[0][1] * i10 + a[0][2] * i20;
+    if (det == 0.0) return false;
+    const double inv = 1.0 / det;
+    const double x0 = (i00 * b[0] + i01 * b[1] + i02 * b[2]) * inv;
+    const double x1 = (i10 * b[0] + i11 * b[1] + i12 * b[2]) * inv;
+    const double x2 = (i20 * b[0] + i21 * b[1] + i22 * b[2]) * inv;
+    b[0] = x0;
+    b[1] = x1;
+    b[2] = x2;
+    return true;
+}
+
+// One cluster of kConstrainedDrift; returns whether one of its particles moved more than the list allows.  TRI: the
+// cluster is a rigid triangle (isTriangle).
+template <bool TRI>
 __device__ __forceinline__ bool constrainedDriftCluster(ConstraintClusters K, int c, double dt, const double* invMass,
                                                         const double* force, double* vel, double* pos,
                                                         const ListBuffers& L, bool refresh, float maxMove2) {
-    const int p0 = K.particleStart[c], np = K.particleStart[c + 1] - p0;
-    const int c0 = K.constraintStart[c], nc = K.constraintStart[c + 1] - c0;
+    constexpr int MP = TRI ? 3 : kMaxClusterParticles, MC = TRI ? 3 : kMaxClusterConstraints;
+    constexpr int kUnroll = TRI ? 3 : 1;   // the general cluster keeps its loops (and arrays in local memory)
+    const int p0 = K.particleStart[c], np = TRI ? 3 : K.particleStart[c + 1] - p0;
+    const int c0 = K.constraintStart[c], nc = TRI ? 3 : K.constraintStart[c + 1] - c0;
     const double h = 0.5 * dt;
     bool moved = false;
-    if (nc == 0) {
-        for (int k = 0; k < np; k++) {
-            const int i = K.particles[p0 + k];
-            double x[3];
-            for (int d = 0; d < 3; d++) {
-                const double v = vel[3 * i + d] + h * invMass[i] * force[3 * i + d];
-                vel[3 * i + d] = v;
-                x[d] = pos[3 * i + d] + dt * v;
-                pos[3 * i + d] = x[d];
-            }
-            if (refresh) moved |= refreshSlot(L, i, x, maxMove2);
-        }
-        return moved;
-    }
-    double old[kMaxClusterParticles][3], x[kMaxClusterParticles][3], w[kMaxClusterParticles];
-    for (int k = 0; k < np; k++) {
+    double old[MP][3], x[MP][3], w[MP];
+#pragma unroll kUnroll
+    for (int k = 0; k < MP; k++) {
+        if (k >= np) break;
         const int i = K.particles[p0 + k];
         w[k] = invMass[i];
+#pragma unroll kUnroll
         for (int d = 0; d < 3; d++) {
             old[k][d] = pos[3 * i + d];
             x[k][d] = old[k][d] + dt * (vel[3 * i + d] + h * w[k] * force[3 * i + d]);
@@ -139,18 +162,24 @@ __device__ __forceinline__ bool constrainedDriftCluster(ConstraintClusters K, in
     }
     // Newton on g_k(lambda) = d_k^2 - |s_k|^2 = 0, s_k the bond of constraint k, each particle moved along the
     // pre-drift bonds r_l: x_p += w_p lambda_l r_l, x_q -= w_q lambda_l r_l
-    int2 pair[kMaxClusterConstraints];
-    double r0[kMaxClusterConstraints][3], d2[kMaxClusterConstraints];
-    for (int q = 0; q < nc; q++) {
-        pair[q] = K.pair[c0 + q];
+    int2 pair[MC];
+    double r0[MC][3], d2[MC];
+#pragma unroll kUnroll
+    for (int q = 0; q < MC; q++) {
+        if (q >= nc) break;
+        pair[q] = TRI ? triPair(q) : K.pair[c0 + q];
         d2[q] = K.dist2[c0 + q];
+#pragma unroll kUnroll
         for (int d = 0; d < 3; d++) r0[q][d] = old[pair[q].x][d] - old[pair[q].y][d];
     }
     bool converged = false;
     for (int iteration = 0; iteration < 30; iteration++) {
-        double s[kMaxClusterConstraints][3], g[kMaxClusterConstraints];
+        double s[MC][3], g[MC];
         double worst = 0.0;
-        for (int k = 0; k < nc; k++) {
+#pragma unroll kUnroll
+        for (int k = 0; k < MC; k++) {
+            if (k >= nc) break;
+#pragma unroll kUnroll
             for (int d = 0; d < 3; d++) s[k][d] = x[pair[k].x][d] - x[pair[k].y][d];
             g[k] = d2[k] - (s[k][0] * s[k][0] + s[k][1] * s[k][1] + s[k][2] * s[k][2]);
             worst = fmax(worst, fabs(g[k]) / d2[k]);
@@ -159,28 +188,64 @@ __device__ __forceinline__ bool constrainedDriftCluster(ConstraintClusters K, in
             converged = true;
             break;
         }
-        double J[kMaxClusterConstraints][kMaxClusterConstraints];
-        for (int k = 0; k < nc; k++)
-            for (int l = 0; l < nc; l++) {
-                const double c = constraintCoupling(pair[k], pair[l], w);
-                J[k][l] = c == 0.0 ? 0.0 : 2.0 * c * (s[k][0] * r0[l][0] + s[k][1] * r0[l][1] + s[k][2] * r0[l][2]);
+        double J[MC][MC];
+#pragma unroll kUnroll
+        for (int k = 0; k < MC; k++) {
+            if (k >= nc) break;
+#pragma unroll kUnroll
+            for (int l = 0; l < MC; l++) {
+                if (l >= nc) break;
+                const double cp = constraintCoupling(pair[k], pair[l], w);
+                J[k][l] = cp == 0.0 ? 0.0 : 2.0 * cp * (s[k][0] * r0[l][0] + s[k][1] * r0[l][1] + s[k][2] * r0[l][2]);
             }
-        if (!solveSmall(J, g, nc)) break;
-        for (int l = 0; l < nc; l++)
+        }
+        bool solved;
+        if constexpr (TRI) solved = solve3(J, g);
+        else solved = solveSmall(J, g, nc);
+        if (!solved) break;
+#pragma unroll kUnroll
+        for (int l = 0; l < MC; l++) {
+            if (l >= nc) break;
+#pragma unroll kUnroll
             for (int d = 0; d < 3; d++) {
                 x[pair[l].x][d] += g[l] * w[pair[l].x] * r0[l][d];
                 x[pair[l].y][d] -= g[l] * w[pair[l].y] * r0[l][d];
             }
+        }
     }
     if (!converged) atomicOr(K.fail, 1);
     const double invDt = 1.0 / dt;
-    for (int k = 0; k < np; k++) {
+#pragma unroll kUnroll
+    for (int k = 0; k < MP; k++) {
+        if (k >= np) break;
         const int i = K.particles[p0 + k];
+#pragma unroll kUnroll
         for (int d = 0; d < 3; d++) {
             vel[3 * i + d] = (x[k][d] - old[k][d]) * invDt;
             pos[3 * i + d] = x[k][d];
         }
         if (refresh) moved |= refreshSlot(L, i, x[k], maxMove2);
+    }
+    return moved;
+}
+
+// A cluster without constraints (a single particle): half kick and drift.
+__device__ __forceinline__ bool freeDriftCluster(ConstraintClusters K, int c, double dt, const double* invMass,
+                                                 const double* force, double* vel, double* pos, const ListBuffers& L,
+                                                 bool refresh, float maxMove2) {
+    const int p0 = K.particleStart[c], np = K.particleStart[c + 1] - p0;
+    const double h = 0.5 * dt;
+    bool moved = false;
+    for (int k = 0; k < np; k++) {
+        const int i = K.particles[p0 + k];
+        double x[3];
+        for (int d = 0; d < 3; d++) {
+            const double v = vel[3 * i + d] + h * invMass[i] * force[3 * i + d];
+            vel[3 * i + d] = v;
+            x[d] = pos[3 * i + d] + dt * v;
+            pos[3 * i + d] = x[d];
+        }
+        if (refresh) moved |= refreshSlot(L, i, x, maxMove2);
     }
     return moved;
 }
@@ -194,22 +259,32 @@ __global__ void kConstrainedDrift(ConstraintClusters K, double dt, const double*
                                   double* vel, double* pos, ListBuffers L, bool refresh, float maxMove2) {
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
     bool moved = false;
-    if (c < K.num) moved = constrainedDriftCluster(K, c, dt, invMass, force, vel, pos, L, refresh, maxMove2);
+    if (c < K.num) {
+        const int c0 = K.constraintStart[c], nc = K.constraintStart[c + 1] - c0;
+        const int np = K.particleStart[c + 1] - K.particleStart[c];
+        if (nc == 0) moved = freeDriftCluster(K, c, dt, invMass, force, vel, pos, L, refresh, maxMove2);
+        else if (isTriangle(K, c0, np, nc))
+            moved = constrainedDriftCluster<true>(K, c, dt, invMass, force, vel, pos, L, refresh, maxMove2);
+        else moved = constrainedDriftCluster<false>(K, c, dt, invMass, force, vel, pos, L, refresh, maxMove2);
+    }
     if (refresh && __any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicOr(L.flag, 1);
 }
 
-// Velocities of each constrained cluster with the components along its bonds removed (no bond stretches), after the
-// second half kick: one linear solve of the cluster's multipliers and at most two refinements of the residual.
-__global__ void kConstrainVelocities(ConstraintClusters K, const double* invMass, const double* pos, double* vel) {
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= K.num) return;
-    const int p0 = K.particleStart[c], np = K.particleStart[c + 1] - p0;
-    const int c0 = K.constraintStart[c], nc = K.constraintStart[c + 1] - c0;
-    if (nc == 0) return;
-    double x[kMaxClusterParticles][3], v[kMaxClusterParticles][3], w[kMaxClusterParticles];
-    for (int k = 0; k < np; k++) {
+// The velocity stage of one constrained cluster (TRI: a rigid triangle, isTriangle).
+template <bool TRI>
+__device__ __forceinline__ void constrainClusterVelocities(ConstraintClusters K, int c, const double* invMass,
+                                                           const double* pos, double* vel) {
+    constexpr int MP = TRI ? 3 : kMaxClusterParticles, MC = TRI ? 3 : kMaxClusterConstraints;
+    constexpr int kUnroll = TRI ? 3 : 1;   // the general cluster keeps its loops (and arrays in local memory)
+    const int p0 = K.particleStart[c], np = TRI ? 3 : K.particleStart[c + 1] - p0;
+    const int c0 = K.constraintStart[c], nc = TRI ? 3 : K.constraintStart[c + 1] - c0;
+    double x[MP][3], v[MP][3], w[MP];
+#pragma unroll kUnroll
+    for (int k = 0; k < MP; k++) {
+        if (k >= np) break;
         const int i = K.particles[p0 + k];
         w[k] = invMass[i];
+#pragma unroll kUnroll
         for (int d = 0; d < 3; d++) {
             x[k][d] = pos[3 * i + d];
             v[k][d] = vel[3 * i + d];
@@ -217,19 +292,25 @@ __global__ void kConstrainVelocities(ConstraintClusters K, const double* invMass
     }
     // conditions r_k . (v_p - v_q) = 0 after v_i += sum_l a_{l,i} mu_l r_l: linear in mu, solved directly, then
     // once more on the residual (rounding)
-    int2 pair[kMaxClusterConstraints];
-    double r[kMaxClusterConstraints][3];
-    for (int q = 0; q < nc; q++) {
-        pair[q] = K.pair[c0 + q];
+    int2 pair[MC];
+    double r[MC][3];
+#pragma unroll kUnroll
+    for (int q = 0; q < MC; q++) {
+        if (q >= nc) break;
+        pair[q] = TRI ? triPair(q) : K.pair[c0 + q];
+#pragma unroll kUnroll
         for (int d = 0; d < 3; d++) r[q][d] = x[pair[q].x][d] - x[pair[q].y][d];
     }
     bool converged = false;
     for (int pass = 0; pass < 3; pass++) {
-        double rhs[kMaxClusterConstraints];
+        double rhs[MC];
         double worst = 0.0;
-        for (int k = 0; k < nc; k++) {
+#pragma unroll kUnroll
+        for (int k = 0; k < MC; k++) {
+            if (k >= nc) break;
             const double r2 = r[k][0] * r[k][0] + r[k][1] * r[k][1] + r[k][2] * r[k][2];
             double dot = 0.0;
+#pragma unroll kUnroll
             for (int d = 0; d < 3; d++) dot += r[k][d] * (v[pair[k].x][d] - v[pair[k].y][d]);
             rhs[k] = -dot;
             worst = fmax(worst, fabs(dot) / r2);    // stretching rate per ps
@@ -238,24 +319,51 @@ __global__ void kConstrainVelocities(ConstraintClusters K, const double* invMass
             converged = true;
             break;
         }
-        double M[kMaxClusterConstraints][kMaxClusterConstraints];
-        for (int k = 0; k < nc; k++)
-            for (int l = 0; l < nc; l++) {
-                const double c = constraintCoupling(pair[k], pair[l], w);
-                M[k][l] = c == 0.0 ? 0.0 : c * (r[k][0] * r[l][0] + r[k][1] * r[l][1] + r[k][2] * r[l][2]);
+        double M[MC][MC];
+#pragma unroll kUnroll
+        for (int k = 0; k < MC; k++) {
+            if (k >= nc) break;
+#pragma unroll kUnroll
+            for (int l = 0; l < MC; l++) {
+                if (l >= nc) break;
+                const double cp = constraintCoupling(pair[k], pair[l], w);
+                M[k][l] = cp == 0.0 ? 0.0 : cp * (r[k][0] * r[l][0] + r[k][1] * r[l][1] + r[k][2] * r[l][2]);
             }
-        if (!solveSmall(M, rhs, nc)) break;
-        for (int l = 0; l < nc; l++)
+        }
+        bool solved;
+        if constexpr (TRI) solved = solve3(M, rhs);
+        else solved = solveSmall(M, rhs, nc);
+        if (!solved) break;
+#pragma unroll kUnroll
+        for (int l = 0; l < MC; l++) {
+            if (l >= nc) break;
+#pragma unroll kUnroll
             for (int d = 0; d < 3; d++) {
                 v[pair[l].x][d] += rhs[l] * w[pair[l].x] * r[l][d];
                 v[pair[l].y][d] -= rhs[l] * w[pair[l].y] * r[l][d];
             }
+        }
     }
     if (!converged) atomicOr(K.fail, 1);
-    for (int k = 0; k < np; k++) {
+#pragma unroll kUnroll
+    for (int k = 0; k < MP; k++) {
+        if (k >= np) break;
         const int i = K.particles[p0 + k];
+#pragma unroll kUnroll
         for (int d = 0; d < 3; d++) vel[3 * i + d] = v[k][d];
     }
+}
+
+// Velocities of each constrained cluster with the components along its bonds removed (no bond stretches), after the
+// second half kick: one linear solve of the cluster's multipliers and at most two refinements of the residual.
+__global__ void kConstrainVelocities(ConstraintClusters K, const double* invMass, const double* pos, double* vel) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= K.num) return;
+    const int c0 = K.constraintStart[c], nc = K.constraintStart[c + 1] - c0;
+    if (nc == 0) return;
+    const int np = K.particleStart[c + 1] - K.particleStart[c];
+    if (isTriangle(K, c0, np, nc)) constrainClusterVelocities<true>(K, c, invMass, pos, vel);
+    else constrainClusterVelocities<false>(K, c, invMass, pos, vel);
 }
 
 }  // namespace ix

@@ -7,13 +7,16 @@
 //      float-float offsets from the i-block's center (the double-precision difference split into a float and its
 //      float remainder).  In large rectangular boxes each j particle is placed at its minimum image relative to the
 //      block center here, once, instead of per pair;
-//   2. queue: the tile's row masks (built with the list) give the candidate pairs; each lane writes its row's pairs
-//      to a per-warp queue at the row's offset (a warp prefix sum of the row counts), so that the expensive phase
-//      runs with every lane busy and no per-step candidate test;
-//   3. compute phase, in rounds of kPairRound queued pairs: each lane takes one pair, forms the displacement as
-//      (xj - xi) + (lo_j - lo_i) (the precision of the double difference, without double arithmetic), applies the
-//      exact cutoff test (borderline cases decided in double), evaluates the three terms in float and stores the
-//      pair force in shared memory;
+//   2. queue: the tile's row masks (built with the list, with the list's skin) give the candidate pairs.  The
+//      displacement of a pair is formed as (xj - xi) + (lo_j - lo_i) (the precision of the double difference, without
+//      double arithmetic) and tested against the exact cutoff (borderline cases decided in double).  Where the pairs
+//      are costly (per-particle parameters, soft core, switch or order-2 overlap), each lane first keeps the
+//      candidates of its row within the cutoff, so that the expensive phase runs with every lane on a pair that
+//      interacts; on the lean class-table path the compute phase tests each candidate instead.  The pairs of each row
+//      are written to a per-warp queue at the row's offset (a warp prefix sum of the row counts); the column masks
+//      are the transpose of the row masks;
+//   3. compute phase, in rounds of kPairRound queued pairs: each lane takes one pair, forms its displacement (the
+//      same operations), evaluates the three terms in float and stores the pair force in shared memory;
 //   4. gather: lane i sums the forces of its row (contiguous in the queue), lane j those of its column (located from
 //      the column mask and the row offsets), in a fixed order and without atomics; both go to the global 64-bit
 //      fixed-point force buffer (scale 2^32) after the tile.  Each tile's energies, summed per lane and then over
@@ -252,7 +255,8 @@ constexpr int kPairWarps = IX_TUNE_PAIR_WARPS;
 // 1: each tile's column lists (the queue positions of each column's pairs) are built once with the queue, and the
 // column forces of every round are read along them; 0: each round finds them from the row masks
 constexpr int kPairColumnLists = IX_TUNE_PAIR_COLUMN_LISTS;
-// 1: the class-table path without per-pair tests evaluates two queued pairs per lane at a time (computeQueuedPair2)
+// 1: the class-table path without per-pair tests evaluates two queued pairs per lane at a time in packed FP32
+// (computeQueuedPair2)
 constexpr int kPairIlp = IX_TUNE_PAIR_ILP;
 constexpr int kPairRound = IX_TUNE_PAIR_ROUND;   // queued pairs computed before their forces are gathered
 
@@ -265,7 +269,7 @@ struct PairWarpStorage {
     int jslot[32];               // sorted slot of each j particle, -1 for padding
     int rowStart[32];            // queue offset of each row
     unsigned rowMask[32];
-    unsigned short queue[1024];  // the tile's candidate pairs, row by row: (i << 5) | j
+    unsigned short queue[1024];  // the tile's pairs within the cutoff, row by row: (i << 5) | j
     float4 force[kPairRound];    // force on i of each pair of the current round (j receives the opposite)
     unsigned short colList[kPairColumnLists ? 1024 : 1];   // queue positions of each column's pairs, column by column
 };
@@ -301,34 +305,70 @@ __device__ __forceinline__ void flushForce(const float f[3], int s, int np, long
     if (f[2] != 0.0f) atomicAddFixed(F + 2 * np + s, toFixed(f[2]));
 }
 
-// One queued pair: displacement, exact cutoff test, the terms.  Returns the force on i (zero outside the cutoff).
-template <bool LEAN, bool TABLE, bool UNIFORM>
+// The displacement of j from i from their staged float-float offsets, with the per-pair minimum image where the
+// staging did not place j; r2 its squared length.
+__device__ __forceinline__ float pairDisplacement(const float4& hi_i, const float4& lo_i, const float4& hi_j,
+                                                  const float4& lo_j, bool perPairImage, const PairTermConfig& C,
+                                                  float& dx, float& dy, float& dz) {
+    float dxh = hi_j.x - hi_i.x, dyh = hi_j.y - hi_i.y, dzh = hi_j.z - hi_i.z;
+    float dxl = lo_j.x - lo_i.x, dyl = lo_j.y - lo_i.y, dzl = lo_j.z - lo_i.z;
+    if (perPairImage) minimumImageFF(dxh, dxl, dyh, dyl, dzh, dzl, C.boxff);
+    dx = dxh + dxl;
+    dy = dyh + dyl;
+    dz = dzh + dzl;
+    return fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+}
+
+// Whether a pair at squared float distance r2 is within the cutoff: the float distance, and within 1e-5 of the
+// cutoff the double-precision distance, as the reference decides.
+__device__ __forceinline__ bool withinCutoff(float r2, const float4& hi_i, const float4& lo_i, const float4& hi_j,
+                                             const float4& lo_j, bool perPairImage, const PairTermConfig& C) {
+    bool inside = r2 < C.cutoff2;
+    if (fabsf(r2 - C.cutoff2) < 1e-5f * C.cutoff2) {
+        double ddx = ((double)hi_j.x - (double)hi_i.x) + ((double)lo_j.x - (double)lo_i.x);
+        double ddy = ((double)hi_j.y - (double)hi_i.y) + ((double)lo_j.y - (double)lo_i.y);
+        double ddz = ((double)hi_j.z - (double)hi_i.z) + ((double)lo_j.z - (double)lo_i.z);
+        if (perPairImage) minimumImage(ddx, ddy, ddz, C.box);
+        const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz));
+        inside = sqrt(r2d) < C.cutoff;
+    }
+    return inside;
+}
+
+__device__ __forceinline__ bool pairInside(const float4& hi_i, const float4& lo_i, const float4& hi_j,
+                                           const float4& lo_j, bool perPairImage, const PairTermConfig& C) {
+    float dx, dy, dz;
+    const float r2 = pairDisplacement(hi_i, lo_i, hi_j, lo_j, perPairImage, C, dx, dy, dz);
+    return withinCutoff(r2, hi_i, lo_i, hi_j, lo_j, perPairImage, C);
+}
+
+// The 32 x 32 bit matrix whose row r is lane r's word, transposed (lane c receives bit r = bit c of lane r's word):
+// the off-diagonal blocks of 16, 8, 4, 2 and 1 exchanged between lane pairs.
+__device__ __forceinline__ unsigned transposeBits(unsigned x, int lane) {
+    const unsigned masks[5] = {0x0000ffffu, 0x00ff00ffu, 0x0f0f0f0fu, 0x33333333u, 0x55555555u};
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const int s = 16 >> k;
+        const unsigned m = masks[k];
+        const unsigned y = __shfl_xor_sync(0xffffffffu, x, s);
+        x = (lane & s) ? ((x & ~m) | ((y & ~m) >> s)) : ((x & m) | ((y & m) << s));
+    }
+    return x;
+}
+
+// One queued pair: displacement, the cutoff test (CHECK: the queue holds candidates; else the pairs were filtered
+// when queued), the terms.  Returns the force on i (zero outside the cutoff) and counts the pair if it interacts.
+template <bool LEAN, bool TABLE, bool UNIFORM, bool CHECK>
 __device__ __forceinline__ float4 computeQueuedPair(PairWarpStorage& S, int entry, int iBase, bool perPairImage,
                                                     const PairTermConfig& C, const ListBuffers& L,
                                                     const PairBuffers& P, const PairCoef* coef, float e[3],
                                                     unsigned& pairs) {
     const int i = entry >> 5, j = entry & 31;
-    const float4 hi_i = S.hi[0][i], hi_j = S.hi[1][j], lo_i = S.lo[0][i], lo_j = S.lo[1][j];
-    float dxh = hi_j.x - hi_i.x, dyh = hi_j.y - hi_i.y, dzh = hi_j.z - hi_i.z;
-    float dxl = lo_j.x - lo_i.x, dyl = lo_j.y - lo_i.y, dzl = lo_j.z - lo_i.z;
-    if (perPairImage) minimumImageFF(dxh, dxl, dyh, dyl, dzh, dzl, C.boxff);
-    const float dx = dxh + dxl, dy = dyh + dyl, dz = dzh + dzl;
-    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    bool inside = true;
-    if (C.useCutoff) {
-        inside = r2 < C.cutoff2;
-        if (fabsf(r2 - C.cutoff2) < 1e-5f * C.cutoff2) {
-            // decide as the reference does, on the double precision distance
-            double ddx = ((double)hi_j.x - (double)hi_i.x) + ((double)lo_j.x - (double)lo_i.x);
-            double ddy = ((double)hi_j.y - (double)hi_i.y) + ((double)lo_j.y - (double)lo_i.y);
-            double ddz = ((double)hi_j.z - (double)hi_i.z) + ((double)lo_j.z - (double)lo_i.z);
-            if (perPairImage) minimumImage(ddx, ddy, ddz, C.box);
-            const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz));
-            inside = sqrt(r2d) < C.cutoff;
-        }
-    }
+    float dx, dy, dz;
+    const float r2 = pairDisplacement(S.hi[0][i], S.lo[0][i], S.hi[1][j], S.lo[1][j], perPairImage, C, dx, dy, dz);
+    if (CHECK && C.useCutoff && !withinCutoff(r2, S.hi[0][i], S.lo[0][i], S.hi[1][j], S.lo[1][j], perPairImage, C))
+        return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     const int fi = S.flags[0][i], fj = S.flags[1][j];
-    if (!inside) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     float invR;
     const float r = sqrtRefined(r2, invR);
     float dEdR;
@@ -350,105 +390,90 @@ __device__ __forceinline__ float4 computeQueuedPair(PairWarpStorage& S, int entr
 }
 
 // Two queued pairs of the class-table path without per-pair tests (LEAN and UNIFORM: no soft core, switch, order-2
-// overlap, gate or scale), their arithmetic in one straight sequence so that each lane keeps two independent chains in
-// flight; a pair outside the cutoff is evaluated at a harmless distance and masked.  The results are those of
-// computeQueuedPair, operation for operation.  `two`: the second entry is a real pair.
+// overlap, gate or scale), evaluated in lockstep in packed FP32 (ix_f32x2.cuh): one instruction issues each operation
+// on both pairs.  A pair outside the cutoff is evaluated at its distance, where every term is finite, and masked.
+// `two`: the second entry is a real pair (else the first is evaluated twice and the copy masked).  Energies
+// accumulate per element in e2.
 __device__ __forceinline__ void computeQueuedPair2(PairWarpStorage& S, int entry0, int entry1, bool two,
                                                    bool perPairImage, const PairTermConfig& C, const PairBuffers& P,
-                                                   const PairCoef* coef, float e[3], unsigned& pairs,
+                                                   const PairCoef* coef, F2 (&e2)[3], unsigned& pairs,
                                                    float4& out0, float4& out1) {
-    const int entry[2] = {entry0, entry1};
-    float dx[2], dy[2], dz[2], r[2], invR[2];
+    const unsigned active = __activemask();
+    float dxs[2], dys[2], dzs[2], r2s[2];
     bool inside[2];
     const PairCoef* K[2];
 #pragma unroll
     for (int k = 0; k < 2; k++) {
-        const int i = entry[k] >> 5, j = entry[k] & 31;
-        const float4 hi_i = S.hi[0][i], hi_j = S.hi[1][j], lo_i = S.lo[0][i], lo_j = S.lo[1][j];
-        float dxh = hi_j.x - hi_i.x, dyh = hi_j.y - hi_i.y, dzh = hi_j.z - hi_i.z;
-        float dxl = lo_j.x - lo_i.x, dyl = lo_j.y - lo_i.y, dzl = lo_j.z - lo_i.z;
-        if (perPairImage) minimumImageFF(dxh, dxl, dyh, dyl, dzh, dzl, C.boxff);
-        dx[k] = dxh + dxl;
-        dy[k] = dyh + dyl;
-        dz[k] = dzh + dzl;
-        const float r2 = fmaf(dx[k], dx[k], fmaf(dy[k], dy[k], dz[k] * dz[k]));
-        bool in = k == 0 || two;
-        if (C.useCutoff) {
-            bool within = r2 < C.cutoff2;
-            if (fabsf(r2 - C.cutoff2) < 1e-5f * C.cutoff2) {
-                double ddx = ((double)hi_j.x - (double)hi_i.x) + ((double)lo_j.x - (double)lo_i.x);
-                double ddy = ((double)hi_j.y - (double)hi_i.y) + ((double)lo_j.y - (double)lo_i.y);
-                double ddz = ((double)hi_j.z - (double)hi_i.z) + ((double)lo_j.z - (double)lo_i.z);
-                if (perPairImage) minimumImage(ddx, ddy, ddz, C.box);
-                const double r2d = __dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz));
-                within = sqrt(r2d) < C.cutoff;
-            }
-            in = in && within;
-        }
+        const int entry = k ? entry1 : entry0;
+        const int i = entry >> 5, j = entry & 31;
+        const float r2 = pairDisplacement(S.hi[0][i], S.lo[0][i], S.hi[1][j], S.lo[1][j], perPairImage, C, dxs[k],
+                                          dys[k], dzs[k]);
+        const bool in = (k == 0 || two) &&
+                        (!C.useCutoff || withinCutoff(r2, S.hi[0][i], S.lo[0][i], S.hi[1][j], S.lo[1][j], perPairImage, C));
         inside[k] = in;
-        // a pair left out is evaluated at half the cutoff, where every term is finite, and its results dropped
-        r[k] = sqrtRefined(in ? r2 : 0.25f * C.cutoff2, invR[k]);
+        r2s[k] = r2;   // a pair left out is evaluated at its own (positive, finite) distance and masked
         const int fi = S.flags[0][i], fj = S.flags[1][j];
-        const int ci = (fi >> kClassShift) & 0xff, cj = (fj >> kClassShift) & 0xff;
-        K[k] = coef + ci * P.numClasses + cj;
+        K[k] = coef + ((fi >> kClassShift) & 0xff) * P.numClasses + ((fj >> kClassShift) & 0xff);
     }
-    float dTotal[2] = {0.0f, 0.0f};
-    float s8[2] = {0.0f, 0.0f}, ds8[2] = {0.0f, 0.0f};
+    F2 invR;
+    const F2 r = sqrtRefined2(f2(r2s[0], r2s[1]), invR);
+    const F2 mask = f2(inside[0] ? 1.0f : 0.0f, inside[1] ? 1.0f : 0.0f);
+    const F2 nmask = f2(inside[0] ? -1.0f : 0.0f, inside[1] ? -1.0f : 0.0f);
+    F2 nTotal = f2(0.0f);   // -dE/dr of all terms
     if (C.termMask & 1) {
-        const float4 kd[2] = {ldCoef(&K[0]->disp, C.coefShared), ldCoef(&K[1]->disp, C.coefShared)};
-        float E[2], D[2];
-        dispersionFromCoef2(r, invR, kd, E, D);
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            e[0] += inside[k] ? E[k] : 0.0f;
-            dTotal[k] += D[k];
-        }
+        const float4 a = ldCoef(&K[0]->disp, C.coefShared), b = ldCoef(&K[1]->disp, C.coefShared);
+        F2 nE, nD;
+        dispersionFromCoefP(r, invR, f2(a.x, b.x), f2(a.y, b.y), f2(a.z, b.z), f2(a.w, b.w), nE, nD);
+        e2[0] = fma2(nmask, nE, e2[0]);
+        nTotal = nTotal + nD;
     }
+    F2 s8 = f2(0.0f), ds8 = f2(0.0f);
     if (C.termMask & 2) {
-        const float4 a[2] = {ldCoef(&K[0]->ovA, C.coefShared), ldCoef(&K[1]->ovA, C.coefShared)};
-        const float4 b[2] = {ldCoef(&K[0]->ovB, C.coefShared), ldCoef(&K[1]->ovB, C.coefShared)};
-        const float4 c[2] = {ldCoef(&K[0]->ovC, C.coefShared), ldCoef(&K[1]->ovC, C.coefShared)};
-        const float k1[2] = {c[0].x, c[1].x}, k2[2] = {c[0].y, c[1].y};
-        overlapFromCoef2(r, a, b, k1, k2, s8, ds8);
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            e[1] += inside[k] ? c[k].z * s8[k] : 0.0f;
-            dTotal[k] = fmaf(1.0f, c[k].z * ds8[k], dTotal[k]);
-        }
+        const float4 a0 = ldCoef(&K[0]->ovA, C.coefShared), a1 = ldCoef(&K[1]->ovA, C.coefShared);
+        const float4 b0 = ldCoef(&K[0]->ovB, C.coefShared), b1 = ldCoef(&K[1]->ovB, C.coefShared);
+        const float4 c0 = ldCoef(&K[0]->ovC, C.coefShared), c1 = ldCoef(&K[1]->ovC, C.coefShared);
+        const float4 q0 = ldCoef(&K[0]->ovQ, C.coefShared), q1 = ldCoef(&K[1]->ovQ, C.coefShared);
+        const float4 u0 = ldCoef(&K[0]->ovR, C.coefShared), u1 = ldCoef(&K[1]->ovR, C.coefShared);
+        overlapFromCoefP(r, f2(a0.x, a1.x), f2(b0.x, b1.x), f2(b0.y, b1.y), f2(b0.z, b1.z), f2(b0.w, b1.w),
+                         f2(c0.x, c1.x), f2(c0.y, c1.y), f2(q0.x, q1.x), f2(q0.y, q1.y), f2(q0.z, q1.z),
+                         f2(q0.w, q1.w), f2(u0.x, u1.x), f2(u0.y, u1.y), active, s8, ds8);
+        const F2 amp = f2(c0.z, c1.z);
+        e2[1] = fma2(mask, amp * s8, e2[1]);
+        nTotal = fma2(amp * f2(-1.0f), ds8, nTotal);
     }
     if (C.termMask & 4) {
-        const float4 c[2] = {ldCoef(&K[0]->srC, C.coefShared), ldCoef(&K[1]->srC, C.coefShared)};
-        const float4 kl[2] = {ldCoef(&K[0]->srK, C.coefShared), ldCoef(&K[1]->srK, C.coefShared)};
+        const float4 c0 = ldCoef(&K[0]->srC, C.coefShared), c1 = ldCoef(&K[1]->srC, C.coefShared);
+        const float4 k0 = ldCoef(&K[0]->srK, C.coefShared), k1 = ldCoef(&K[1]->srK, C.coefShared);
         if (!(C.shareOverlap && (C.termMask & 2))) {
-            const float4 a[2] = {ldCoef(&K[0]->srA, C.coefShared), ldCoef(&K[1]->srA, C.coefShared)};
-            const float4 b[2] = {ldCoef(&K[0]->srB, C.coefShared), ldCoef(&K[1]->srB, C.coefShared)};
-            const float k1[2] = {c[0].x, c[1].x}, k2[2] = {c[0].y, c[1].y};
-            overlapFromCoef2(r, a, b, k1, k2, s8, ds8);
+            const float4 a0 = ldCoef(&K[0]->srA, C.coefShared), a1 = ldCoef(&K[1]->srA, C.coefShared);
+            const float4 b0 = ldCoef(&K[0]->srB, C.coefShared), b1 = ldCoef(&K[1]->srB, C.coefShared);
+            const float4 q0 = ldCoef(&K[0]->srQ, C.coefShared), q1 = ldCoef(&K[1]->srQ, C.coefShared);
+            const float4 u0 = ldCoef(&K[0]->srR, C.coefShared), u1 = ldCoef(&K[1]->srR, C.coefShared);
+            overlapFromCoefP(r, f2(a0.x, a1.x), f2(b0.x, b1.x), f2(b0.y, b1.y), f2(b0.z, b1.z), f2(b0.w, b1.w),
+                             f2(c0.x, c1.x), f2(c0.y, c1.y), f2(q0.x, q1.x), f2(q0.y, q1.y), f2(q0.z, q1.z),
+                             f2(q0.w, q1.w), f2(u0.x, u1.x), f2(u0.y, u1.y), active, s8, ds8);
         }
-#pragma unroll
-        for (int k = 0; k < 2; k++) {
-            const float st = c[k].z * s8[k];
-            const float E = fmaf(kl[k].y, st, kl[k].x) * st;
-            const float D = fmaf(2.0f * kl[k].y, st, kl[k].x) * c[k].z * ds8[k];
-            e[2] += inside[k] ? E : 0.0f;
-            dTotal[k] += D;
-        }
+        // (K_i+K_j)/2 St + (L_i+L_j)/2 St^2, St = (s_i+s_j)^3 8 pi S
+        const F2 norm = f2(c0.z, c1.z), kk = f2(k0.x, k1.x), ll = f2(k0.y, k1.y);
+        const F2 st = norm * s8;
+        e2[2] = fma2(mask, fma2(ll, st, kk) * st, e2[2]);
+        nTotal = fma2(fma2(ll * f2(-2.0f), st, kk * f2(-1.0f)) * norm, ds8, nTotal);
     }
-    float4 out[2];
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-        const float fs = inside[k] ? dTotal[k] * invR[k] : 0.0f;
-        out[k] = make_float4(dx[k] * fs, dy[k] * fs, dz[k] * fs, 0.0f);
-        pairs += inside[k];
-    }
-    out0 = out[0];
-    out1 = out[1];
+    const F2 fs = (nTotal * invR) * nmask;
+    const F2 fx = f2(dxs[0], dxs[1]) * fs, fy = f2(dys[0], dys[1]) * fs, fz = f2(dzs[0], dzs[1]) * fs;
+    out0 = make_float4(f2x(fx), f2x(fy), f2x(fz), 0.0f);
+    out1 = make_float4(f2y(fx), f2y(fy), f2y(fz), 0.0f);
+    pairs += (unsigned)inside[0] + (unsigned)inside[1];
 }
 
 template <bool LEAN, bool TABLE, bool UNIFORM = false>
 __global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPairTiles(ListBuffers L, PairBuffers P, PairTermConfig C) {
     __shared__ PairWarpStorage storage[kPairWarps];
     extern __shared__ float4 pairShared[];
+    // the candidates are filtered against the cutoff when queued, except on the class-table path without soft core,
+    // switch or order-2 overlap, whose pairs are cheap enough that the filter costs what it saves: there the compute
+    // phase tests each candidate
+    constexpr bool PREFILTER = !(LEAN && TABLE);
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
     PairWarpStorage& S = storage[warp];
@@ -480,7 +505,7 @@ __global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPai
         {
             const int jslot = L.tileJ[32 * t + lane];
             unsigned row = L.tileMask[64 * t + lane];
-            unsigned column = L.tileMask[64 * t + 32 + lane];
+            unsigned column = PREFILTER ? 0u : L.tileMask[64 * t + 32 + lane];
             __syncwarp();
             stageParticle(S, 0, lane, iBase + lane, cx, cy, cz, false, C, L, P);
             stageParticle(S, 1, lane, jslot, cx, cy, cz, shiftImage, C, L, P);
@@ -491,7 +516,20 @@ __global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPai
                 row &= ia ? ~jAlch : jAlch;
                 column &= ja ? ~iAlch : iAlch;
             }
-            // queue the tile's candidate pairs row by row
+            __syncwarp();
+            if (PREFILTER && C.useCutoff) {
+                // the row's candidates within the cutoff at the current positions
+                const float4 hi_i = S.hi[0][lane], lo_i = S.lo[0][lane];
+                unsigned kept = 0;
+                for (unsigned m = row; m; m &= m - 1) {
+                    const int j = __ffs(m) - 1;
+                    if (pairInside(hi_i, lo_i, S.hi[1][j], S.lo[1][j], perPairImage, C)) kept |= 1u << j;
+                }
+                row = kept;
+            }
+            // the filtered columns are the transpose of the filtered rows; unfiltered, the list holds them
+            if (PREFILTER) column = transposeBits(row, lane);
+            // queue the kept pairs row by row
             const int count = __popc(row);
             int start = count;
 #pragma unroll
@@ -526,6 +564,7 @@ __global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPai
                 __syncwarp();
             }
             float e[3] = {0.0f, 0.0f, 0.0f};
+            F2 e2[3] = {f2(0.0f), f2(0.0f), f2(0.0f)};   // the packed path's energies, per element
             float fj[3] = {0.0f, 0.0f, 0.0f};
             unsigned tilePairs = 0;
             for (int base = 0; base < total; base += kPairRound) {
@@ -536,16 +575,15 @@ __global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPai
                         const bool two = p + 32 < n;
                         float4 f0, f1;
                         computeQueuedPair2(S, S.queue[base + p], S.queue[base + (two ? p + 32 : p)], two,
-                                           perPairImage, C, P, coef, e, tilePairs, f0, f1);
+                                           perPairImage, C, P, coef, e2, tilePairs, f0, f1);
                         S.force[p] = f0;
                         if (two) S.force[p + 32] = f1;
                     }
                 }
                 else
                     for (int p = lane; p < n; p += 32)
-                        S.force[p] = computeQueuedPair<LEAN, TABLE, UNIFORM>(S, S.queue[base + p], iBase,
-                                                                              perPairImage, C, L, P, coef, e,
-                                                                              tilePairs);
+                        S.force[p] = computeQueuedPair<LEAN, TABLE, UNIFORM, !PREFILTER>(
+                            S, S.queue[base + p], iBase, perPairImage, C, L, P, coef, e, tilePairs);
                 __syncwarp();
                 // i side: this lane's row, contiguous in the queue
                 const int a = max(start, base), b = min(start + count, base + n);
@@ -584,6 +622,8 @@ __global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPai
                 __syncwarp();
             }
             pairs += tilePairs;
+            if (kPairIlp && LEAN && TABLE && UNIFORM)
+                for (int k = 0; k < 3; k++) e[k] = f2x(e2[k]) + f2y(e2[k]);
             flushForce(fj, jslot, L.np, P.forceFixed);
             // the tile's energies: a fixed reduction tree over the lanes, one slot per tile
             for (int k = 0; k < 3; k++) {

@@ -19,6 +19,7 @@
 #pragma once
 
 #include "ix_common.cuh"
+#include "ix_f32x2.cuh"
 #include "overlap_taylor_table.h"
 
 namespace ix {
@@ -142,6 +143,11 @@ struct PairCoef {
     float4 srB;     // as ovB
     float4 srC;     // as ovC .x .y; (s_i + s_j)^3 of the short-range widths; unused
     float4 srK;     // (K_i + K_j)/2, (L_i + L_j)/2, unused, unused
+    // the exponential rates of the packed path: q = log2(e)/width as float-float (qHi + qLo)
+    float4 ovQ;     // exchange overlap: -qa float part, qa float part, qa remainder, -qb float part
+    float4 ovR;     // qb float part, qb remainder, unused, unused
+    float4 srQ;     // short-range overlap, as ovQ
+    float4 srR;     // as ovR
 };
 
 // 8 pi S and its derivative from the coefficients (the cancellation-free form of overlapExact).
@@ -387,6 +393,110 @@ __device__ __forceinline__ void dispersionEnergy(float r, float invR, float4 pi,
     const float g = expX * dxdr;
     dEdR = -(e6 * fmaf(g, t[6], -6.0f * f6 * invR) + e8 * fmaf(g, t[8], -8.0f * f8 * invR) +
              e10 * fmaf(g, t[10], -10.0f * f10 * invR));
+}
+
+// ---------------------------------------------------------------------------------------------------------------------
+// Two pairs at once in packed FP32 (F2, ix_f32x2.cuh): the class-table forms above evaluated in lockstep on two pairs
+// of one lane.  Each returns what its scalar form returns, with the sign of some outputs folded away (noted per
+// function) so that no packed negation is needed.  Their rounding differs from the scalar forms only where a
+// product's rounding order differs; both agree with the FP64 oracle to the same bound.
+// ---------------------------------------------------------------------------------------------------------------------
+
+// dispersionFromCoef for two pairs: returns -energy (nE) and -dE/dr (nD).
+__device__ __forceinline__ void dispersionFromCoefP(F2 r, F2 invR, F2 c6, F2 c8, F2 c10, F2 dxdr, F2& nE, F2& nD) {
+    const F2 x = dxdr * r;
+    const F2 expX = expNeg2(x);
+    const F2 x2 = x * x;
+    const F2 x3 = x2 * x;
+    const F2 t6 = (x3 * x3) * f2(1.0f / 720.0f);
+    const F2 t7 = (t6 * x) * f2(1.0f / 7.0f);
+    const F2 t8 = (t7 * x) * f2(1.0f / 8.0f);
+    const F2 t9 = (t8 * x) * f2(1.0f / 9.0f);
+    const F2 t10 = (t9 * x) * f2(1.0f / 10.0f);
+    F2 s6 = fma2(x, f2(1.0f / 720.0f), f2(1.0f / 120.0f));
+    s6 = fma2(s6, x, f2(1.0f / 24.0f));
+    s6 = fma2(s6, x, f2(1.0f / 6.0f));
+    s6 = fma2(s6, x, f2(0.5f));
+    s6 = fma2(s6, x, f2(1.0f));
+    s6 = fma2(s6, x, f2(1.0f));
+    const F2 s8 = (s6 + t7) + t8;
+    const F2 s10 = (s8 + t9) + t10;
+    const F2 nExp = expX * f2(-1.0f);
+    F2 f6 = fma2(nExp, s6, f2(1.0f)), f8 = fma2(nExp, s8, f2(1.0f)), f10 = fma2(nExp, s10, f2(1.0f));
+    const float xa = f2x(x), xb = f2y(x);
+    if (xa < 5.5f || xb < 5.5f) {
+        // the series form where the closed form cancels (rare at interacting distances)
+        F2 term = t10, tail = f2(0.0f);
+#pragma unroll 1
+        for (int k = 11; k <= 28; k++) {
+            term = (term * x) * f2(__fdividef(1.0f, (float)k));
+            tail = tail + term;
+        }
+        const F2 tail8 = (tail + t10) + t9;
+        const F2 f10s = expX * tail, f8s = expX * tail8, f6s = expX * ((tail8 + t8) + t7);
+        f10 = sel2(xa < 5.5f, xb < 5.5f, f10s, f10);
+        f8 = sel2(xa < 4.5f, xb < 4.5f, f8s, f8);
+        f6 = sel2(xa < 3.5f, xb < 3.5f, f6s, f6);
+    }
+    const F2 invR2 = invR * invR;
+    const F2 e6 = ((c6 * invR2) * invR2) * invR2;
+    const F2 e8 = (((c8 * invR2) * invR2) * invR2) * invR2;
+    const F2 e10 = ((((c10 * invR2) * invR2) * invR2) * invR2) * invR2;
+    nE = fma2(f6, e6, fma2(f8, e8, f10 * e10));
+    const F2 g = expX * dxdr;
+    const F2 a6 = fma2(g, t6, (f6 * f2(-6.0f)) * invR);
+    const F2 a8 = fma2(g, t8, (f8 * f2(-8.0f)) * invR);
+    const F2 a10 = fma2(g, t10, (f10 * f2(-10.0f)) * invR);
+    nD = fma2(e10, a10, fma2(e8, a8, e6 * a6));
+}
+
+// overlapFromCoef for two pairs: 8 pi S and its derivative.  A, B, k1, k2 as overlapFromCoef (packed per element);
+// nqa, qa, qaLo and nqb, qb, qbLo the exponential rates (PairCoef ovQ/ovR).  `active`: the lanes of the warp that
+// call it together (they agree on which forms of the series/closed-form switch to evaluate).
+__device__ __forceinline__ void overlapFromCoefP(F2 r, F2 ia, F2 hab, F2 is3, F2 c2, F2 c3, F2 k1, F2 k2, F2 nqa,
+                                                 F2 qa, F2 qaLo, F2 nqb, F2 qb, F2 qbLo, unsigned active, F2& s8pi,
+                                                 F2& ds8pi) {
+    const F2 ea = expNegRate2(r, nqa, qa, qaLo);
+    const F2 d = r * hab;
+    const float da = f2x(d), db = f2y(d);
+    const bool seriesA = da < 2.0f, seriesB = db < 2.0f;
+    const bool anySeries = __any_sync(active, seriesA || seriesB);
+    const bool anyClosed = __any_sync(active, !seriesA || !seriesB);
+    F2 sP3 = f2(0.0f), sP4 = f2(0.0f), cP3 = f2(0.0f), cP4 = f2(0.0f);
+    if (anySeries) {
+        const F2 dd = f2(fminf(da, 2.0f), fminf(db, 2.0f));
+        F2 p4 = fma2(f2(1.0f / 1307674368000.0f), dd, f2(1.0f / 87178291200.0f));
+        p4 = fma2(p4, dd, f2(1.0f / 6227020800.0f));
+        p4 = fma2(p4, dd, f2(1.0f / 479001600.0f));
+        p4 = fma2(p4, dd, f2(1.0f / 39916800.0f));
+        p4 = fma2(p4, dd, f2(1.0f / 3628800.0f));
+        p4 = fma2(p4, dd, f2(1.0f / 362880.0f));
+        p4 = fma2(p4, dd, f2(1.0f / 40320.0f));
+        p4 = fma2(p4, dd, f2(1.0f / 5040.0f));
+        p4 = fma2(p4, dd, f2(1.0f / 720.0f));
+        p4 = fma2(p4, dd, f2(1.0f / 120.0f));
+        p4 = fma2(p4, dd, f2(1.0f / 24.0f));
+        sP3 = ea * fma2(dd, p4, f2(1.0f / 6.0f));
+        sP4 = ea * p4;
+    }
+    if (anyClosed) {
+        const F2 dd = f2(fmaxf(da, 2.0f), fmaxf(db, 2.0f));
+        const F2 eb = expNegRate2(r, nqb, qb, qbLo);
+        F2 id = rcpx2(dd);
+        id = fma2(id, fma2(dd * f2(-1.0f), id, f2(1.0f)), id);
+        cP3 = (eb - ea * fma2(dd, fma2(f2(0.5f), dd, f2(1.0f)), f2(1.0f))) * ((id * id) * id);
+        cP4 = fma2(ea, f2(-1.0f / 6.0f), cP3) * id;
+    }
+    const F2 eP3 = sel2(seriesA, seriesB, sP3, cP3), eP4 = sel2(seriesA, seriesB, sP4, cP4);
+    const F2 rk1 = r * k1;
+    const F2 br = (r * r) * (rk1 - k2);
+    const F2 dbr = r * fma2(f2(3.0f), rk1, k2 * f2(-2.0f));
+    const F2 poly = fma2(r, fma2(r, c3, c2), is3);
+    const F2 dpoly = fma2(r * f2(2.0f), c3, c2);
+    const F2 eg = fma2(eP3, br, ea * poly);
+    const F2 egp = fma2(eP3, dbr, fma2(fma2(f2(-3.0f), eP4, eP3) * hab, br, ea * dpoly));
+    s8pi = eg;
+    ds8pi = fma2(eg * f2(-1.0f), ia, egp);
 }
 
 }  // namespace ix

@@ -5,14 +5,14 @@
 namespace ix {
 
 constexpr int kProbeChains = 8;
-constexpr int kProbeIters = 4096;
+constexpr int kProbeIters = 16384;   // one wave of blocks that each run ~1 ms, so that the ramp and tail are negligible
 
 __global__ void kFmaPeak(float* sink, float seed) {
     float v[kProbeChains];
 #pragma unroll
     for (int c = 0; c < kProbeChains; c++) v[c] = seed + threadIdx.x * 1e-7f + c;
-    const float a = 0.999999f, b = 1e-7f;
-#pragma unroll 4
+    // the multiplier is a kernel argument's function, so that every FMA reads registers only
+    const float a = 1.0f - 1e-6f * seed, b = 1e-7f;
     for (int it = 0; it < kProbeIters; it++) {
 #pragma unroll
         for (int c = 0; c < kProbeChains; c++) v[c] = fmaf(v[c], a, b);

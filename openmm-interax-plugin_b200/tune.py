@@ -12,8 +12,10 @@ fresh process that loads that copy (IX_B200_LIBRARY) on the benchmark's shapes:
 
 The search is coordinate-wise: starting from the current values, each group of constants is varied over its
 candidates with the others fixed, and the best by the objective (the MD step time, plus the batched evaluation time
-for the groups that change it) is kept before the next group.  The chosen values and every measurement are written to
-tuning.json, which the build (build_lib.py) turns into compiler definitions.
+for the groups that change it) is kept before the next group if it beats the current values by more than MARGIN (the
+spread of repeated measurements of one build; a smaller gain is noise).  The chosen values and every measurement are
+written to tuning.json, which the build (build_lib.py) turns into compiler definitions.  `--reselect FILE` applies the
+selection again to the measurements recorded in FILE (no GPU).
 """
 import argparse
 import concurrent.futures
@@ -40,8 +42,8 @@ GROUPS = [
     ("pair tiles", [dict(IX_TUNE_PAIR_WARPS=w, IX_TUNE_PAIR_ROUND=r, IX_TUNE_PAIR_MIN_BLOCKS=b,
                          IX_TUNE_PAIR_COLUMN_LISTS=c, IX_TUNE_PAIR_ILP=i)
                     for w, r, b, c, i in ((4, 128, 8, 0, 0), (4, 64, 8, 0, 0), (4, 256, 6, 0, 0), (2, 128, 16, 0, 0),
-                                          (4, 64, 7, 1, 0), (4, 128, 6, 1, 0), (4, 128, 8, 0, 1), (4, 128, 6, 0, 1),
-                                          (4, 128, 6, 1, 1), (4, 64, 7, 1, 1))]),
+                                          (4, 128, 6, 1, 0), (4, 128, 5, 0, 1), (4, 128, 6, 0, 1), (4, 64, 5, 0, 1),
+                                          (2, 128, 10, 0, 1), (4, 256, 4, 0, 1))]),
     ("pair table", [dict(IX_TUNE_PAIR_SHARED_TABLE_BYTES=b) for b in (0, 1024, 2048)]),
     ("pair skin", [dict(IX_TUNE_PAIR_SKIN=s) for s in (0.06, 0.08, 0.1, 0.12)]),
     ("three-body", [dict(IX_TUNE_ATM_FAST=f, IX_TUNE_ATM_ROUND=r, IX_TUNE_ATM_MIN_BLOCKS=b)
@@ -154,10 +156,42 @@ def run_candidate(path, steps, clusters):
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
+# a candidate must beat the group's current values by this fraction of the objective to replace them
+MARGIN = 0.01
+
+
 def objective(m, with_clusters):
     if "error" in m or not (m["oracle_energy_error"] <= 1e-6 and m["oracle_force_error"] <= 1e-5):
         return float("inf")
     return m["md_step_ms"] + (m["clusters_ms"] if with_clusters else 0.0)
+
+
+def select(results, current, margin=MARGIN):
+    """The values kept after a group: `results` holds (objective, values) per candidate, one of them `current`."""
+    best = min(results, key=lambda r: r[0])
+    base = [r[0] for r in results if r[1] == current]
+    if base and not best[0] < (1.0 - margin) * base[0]:
+        return dict(current)
+    return dict(best[1])
+
+
+def reselect(path):
+    """Apply select() again to the measurements recorded in a tuning.json, group by group, and rewrite its choice."""
+    data = json.loads(Path(path).read_text())
+    current = dict(DEFAULTS)
+    groups = []
+    for entry in data["measurements"]:
+        if not groups or groups[-1][0] != entry["group"]:
+            groups.append((entry["group"], []))
+        groups[-1][1].append(entry)
+    for name, entries in groups:
+        clusters = "clusters_ms" in entries[0]["measured"]
+        results = [(objective(e["measured"], clusters), dict(current, **e["values"])) for e in entries]
+        current = select(results, current)
+    data["chosen"] = current
+    data["selection"] = f"best of each group if it beats the current values by more than {MARGIN:.0%}"
+    Path(path).write_text(json.dumps(data, indent=1) + "\n")
+    return current
 
 
 def main():
@@ -166,7 +200,12 @@ def main():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--measure", action="store_true", help=argparse.SUPPRESS)
     p.add_argument("--no-clusters", action="store_true", help=argparse.SUPPRESS)
+    p.add_argument("--reselect", metavar="FILE")
+    p.add_argument("--groups", help="comma-separated names of the groups to search (default: all)")
     args = p.parse_args()
+    if args.reselect:
+        print("chosen", reselect(args.reselect))
+        return
     if args.measure:
         print(json.dumps(measure(args.steps, clusters=not args.no_clusters)))
         return
@@ -176,7 +215,8 @@ def main():
     record = []
     workdir = tempfile.mkdtemp(prefix="ix_tune_")
     t0 = time.time()
-    for name, options in GROUPS:
+    groups = GROUPS if not args.groups else [g for g in GROUPS if g[0] in args.groups.split(",")]
+    for name, options in groups:
         # the batched workload has no pair list and no site lists to rebuild: the skins do not change it
         clusters = name not in ("pair skin", "site skin", "pair table")
         candidates = [dict(current, **o) for o in options]
@@ -184,14 +224,14 @@ def main():
         results = []
         for values in candidates:
             m = run_candidate(libs[_key(values)], args.steps, clusters)
-            results.append((objective(m, clusters), values, m))
+            results.append((objective(m, clusters), values))
             record.append({"group": name, "values": {k: values[k] for k in options[0]}, "measured": m})
             print(name, {k: values[k] for k in options[0]}, m, flush=True)
-        best = min(results, key=lambda r: r[0])
-        current = dict(best[1])
+        current = select(results, current)
     out = {"chosen": current, "device": torch.cuda.get_device_name(0), "steps": args.steps,
            "objective": "mean velocity-Verlet step of the 24,000-atom rigid-water box (ms), plus one batched "
                         "evaluation of the 4,096 clusters (ms) for the groups that change it",
+           "selection": f"best of each group if it beats the current values by more than {MARGIN:.0%}",
            "command": "python openmm-interax-plugin_b200/tune.py", "seconds": time.time() - t0,
            "measurements": record}
     Path(args.out).write_text(json.dumps(out, indent=1) + "\n")

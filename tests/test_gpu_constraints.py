@@ -89,3 +89,32 @@ def test_constraint_errors():
     system.addConstraint(0, 0, 0.1)
     with pytest.raises(OpenMMException, match="Illegal particle index"):
         Context(system)
+
+
+def test_general_clusters_beside_rigid_waters():
+    # waters 0 and 1 joined by an O-O constraint, waters 2 and 3 by an H-H one: clusters of 6 particles and 7
+    # constraints (the general solver) beside the rigid triangles of the other waters
+    system, pos = _rigid_box(seed=9)
+    for a, b in ((0, 3), (7, 10)):
+        system.addConstraint(a, b, float(np.linalg.norm(pos[a] - pos[b])))
+    ctx = Context(system)
+    ctx.setPositions(pos)
+    vel = W.initial_velocities(system, 300.0, seed=4)
+    energies = []
+    p, v = pos, vel
+    for chunk in range(4):
+        p, v, e = ctx.runVelocityVerlet(50, DT, v)
+        energies.append(e + _kinetic(system, v))
+        assert _bond_errors(system, p).max() < 1e-6
+        assert _bond_rates(system, p, v).max() < 1e-6
+    assert np.abs(np.array(energies) - energies[0]).max() < 0.02 * _kinetic(system, v)
+
+
+def test_too_large_cluster_is_rejected():
+    from interaxplugin import OpenMMException
+    system, pos, _ = W.water_box(27, 1.0, 0.45, seed=7, three_body=False, rigid=True)
+    # three waters joined into one cluster of 9 particles (the limit is 8)
+    system.addConstraint(0, 3, 0.3)
+    system.addConstraint(3, 6, 0.3)
+    with pytest.raises(OpenMMException, match="cluster of 9"):
+        Context(system)

@@ -52,3 +52,29 @@ def test_build_passes_the_tuned_values(tmp_path, monkeypatch):
     assert "arch=compute_100a,code=sm_100a" in " ".join(cmd)
     explicit = build_lib.compile_command(tmp_path / "lib.so", {"IX_TUNE_PAIR_ILP": 1})
     assert "-DIX_TUNE_PAIR_ILP=1" in explicit and not any("PAIR_ROUND" in a for a in explicit)
+
+
+def test_selection_keeps_the_current_values_within_the_margin(tmp_path):
+    cur = dict(tune.DEFAULTS)
+    other = dict(cur, IX_TUNE_PAIR_ROUND=64)
+    assert tune.select([(1.0, cur), (0.995, other)], cur) == cur             # 0.5%: noise
+    assert tune.select([(1.0, cur), (0.95, other)], cur) == other            # 5%: kept
+    assert tune.select([(float("inf"), cur), (0.95, other)], cur) == other   # the current values failed the oracle
+    record = {"chosen": {}, "measurements": [
+        {"group": "pair tiles", "values": {"IX_TUNE_PAIR_ROUND": 128},
+         "measured": {"md_step_ms": 0.30, "clusters_ms": 0.30, "oracle_energy_error": 1e-7,
+                      "oracle_force_error": 1e-6}},
+        {"group": "pair tiles", "values": {"IX_TUNE_PAIR_ROUND": 64},
+         "measured": {"md_step_ms": 0.25, "clusters_ms": 0.30, "oracle_energy_error": 1e-7,
+                      "oracle_force_error": 1e-6}},
+        {"group": "pair table", "values": {"IX_TUNE_PAIR_SHARED_TABLE_BYTES": 0},
+         "measured": {"md_step_ms": 0.25, "oracle_energy_error": 1e-7, "oracle_force_error": 1e-6}},
+        {"group": "pair table", "values": {"IX_TUNE_PAIR_SHARED_TABLE_BYTES": 1024},
+         "measured": {"md_step_ms": 0.249, "oracle_energy_error": 1e-7, "oracle_force_error": 1e-6}},
+        {"group": "pair table", "values": {"IX_TUNE_PAIR_SHARED_TABLE_BYTES": 2048},
+         "measured": {"md_step_ms": 0.20, "oracle_energy_error": 1e-3, "oracle_force_error": 1e-6}}]}
+    path = tmp_path / "tuning.json"
+    path.write_text(json.dumps(record))
+    chosen = tune.reselect(path)
+    assert chosen["IX_TUNE_PAIR_ROUND"] == 64 and chosen["IX_TUNE_PAIR_SHARED_TABLE_BYTES"] == 0
+    assert json.loads(path.read_text())["chosen"] == chosen
