@@ -14,16 +14,21 @@ second (the pair and triple counts come from the kernels, per step); ns/day foll
 --impl reference times the reference's own CPU implementation of the path (its CPU platform, restated, since the
 plugin cannot be built without OpenMM) on every host thread, one full evaluation of the same workload per step.
 """
-import argparse
-import ctypes
-import json
-import math
 import os
-import subprocess
-import sys
-import threading
-import time
-from pathlib import Path
+
+# Kernels of many CUDA streams run concurrently only as far as the device's hardware work queues keep them apart;
+# the default 8 queues make the served stream's requests wait behind one another's work.  Read when CUDA starts.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
+import argparse  # noqa: E402
+import ctypes  # noqa: E402
+import json  # noqa: E402
+import math  # noqa: E402
+import subprocess  # noqa: E402
+import sys  # noqa: E402
+import threading  # noqa: E402
+import time  # noqa: E402
+from pathlib import Path  # noqa: E402
 
 ROOT = Path(__file__).resolve().parent
 sys.path[:0] = [str(ROOT / "openmm-interax-plugin_b200"), str(ROOT / "oracle")]
@@ -39,6 +44,10 @@ F_TRIPLE = 151.0
 # DRAM bytes (read + write) of one pair-kernel launch on this workload, from one ncu capture of an MD-step launch
 # (dram__bytes_read.sum + dram__bytes_write.sum); the kernel is FP32-issue bound, the traffic is reported beside it
 PAIR_TRAFFIC_BYTES = 10082304
+# The same capture's hardware view: FMA-pipe busy fraction (sm__pipe_fma_cycles_active, pct of peak over active
+# cycles) and issue-slot use (sm__inst_issued), beside the algorithmic fraction
+PAIR_FMA_PIPE_ACTIVE = 0.340
+PAIR_ISSUE_ACTIVE = 0.740
 METRIC = "interactions/s"
 WORKLOAD = "water box 24,000 atoms (8,000 rigid 3-site waters, constrained, 6.208 nm periodic, cutoff 1.0 nm) + ATM " \
            "on 8,000 molecular sites (cutoff 0.6 nm); velocity-Verlet 1 fs with SHAKE/RATTLE"
@@ -450,6 +459,8 @@ def run_ours(args, rank, world):
                      "timing": "CUDA events around the kernel in a pass of the same steps with the three-body "
                                "chain serialised after the pair chain",
                      "traffic_gbs": PAIR_TRAFFIC_BYTES / (pair_ms * 1e-3) / 1e9,
+                     "hardware_ncu": {"fma_pipe_active": PAIR_FMA_PIPE_ACTIVE, "issue_active": PAIR_ISSUE_ACTIVE,
+                                      "source": "ncu capture of one MD-step launch (profiles/kPairTiles_24k.md)"},
                      "three_body_kernels_ms": atm_ms, "ops_per_triple": F_TRIPLE,
                      "three_body_achieved": triples_per_launch * F_TRIPLE / (atm_ms * 1e-3) / 1e12},
         "cpu_baseline": base,

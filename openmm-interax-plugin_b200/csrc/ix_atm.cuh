@@ -50,6 +50,8 @@ struct SiteCells {
     int* siteCell;               // numSites
 };
 constexpr int kSiteCellMax = 8192;   // cells the one-block sort holds in shared memory
+// sites up to this count are scattered and ordered in dynamic shared memory by the one-block sort (160 KB)
+constexpr int kSiteSortSharedMax = 40000;
 
 struct AtmBuffers {
     const int* siteOffsets;      // numSites + 1
@@ -209,11 +211,14 @@ __global__ void kSiteNeighbors(AtmBuffers A, AtmConfig C) {
 
 // The sites binned into the cell grid (rebuild only), in one block: each site's cell from its wrapped position, the
 // cell counts in shared memory, their scan, the scatter, and each cell's sites put in increasing order (so that the
-// lists built from the cells come out the same on every run).
-__global__ void __launch_bounds__(1024) kSiteCellSort(AtmBuffers A, AtmConfig C) {
+// lists built from the cells come out the same on every run).  With `sharedSites` (at most kSiteSortSharedMax sites,
+// the launch giving 4 bytes of dynamic shared memory per site) the scatter goes to shared memory and a warp per cell
+// writes each site at its rank among the cell's sites; else each cell is insertion-sorted in place in global memory.
+__global__ void __launch_bounds__(1024) kSiteCellSort(AtmBuffers A, AtmConfig C, int sharedSites) {
     if (*(volatile int*)A.flag == 0) return;
     __shared__ int count[kSiteCellMax];
     __shared__ int threadSum[1024];
+    extern __shared__ int scattered[];
     const SiteCells& G = A.cells;
     const int numCells = G.nc[0] * G.nc[1] * G.nc[2];
     const int t = threadIdx.x, T = blockDim.x;
@@ -251,8 +256,23 @@ __global__ void __launch_bounds__(1024) kSiteCellSort(AtmBuffers A, AtmConfig C)
     }
     if (t == T - 1) G.cellStart[numCells] = run;
     __syncthreads();
-    for (int s = t; s < C.numSites; s += T) G.cellSites[atomicAdd(&count[G.siteCell[s]], 1)] = s;
+    int* dst = sharedSites ? scattered : G.cellSites;
+    for (int s = t; s < C.numSites; s += T) dst[atomicAdd(&count[G.siteCell[s]], 1)] = s;
     __syncthreads();
+    if (sharedSites) {
+        // the sites are distinct, so each one's rank among its cell's sites is its place
+        const int warp = t >> 5, lane = t & 31;
+        for (int c = warp; c < numCells; c += T >> 5) {
+            const int start = G.cellStart[c], n = G.cellStart[c + 1] - start;
+            for (int e = lane; e < n; e += 32) {
+                const int x = scattered[start + e];
+                int rank = 0;
+                for (int f = 0; f < n; f++) rank += scattered[start + f] < x;
+                G.cellSites[start + rank] = x;
+            }
+        }
+        return;
+    }
     // insertion sort of each cell's sites (a few dozen at most)
     for (int c = t; c < numCells; c += T) {
         int* v = G.cellSites + G.cellStart[c];
@@ -270,43 +290,67 @@ __global__ void __launch_bounds__(1024) kSiteCellSort(AtmBuffers A, AtmConfig C)
 }
 
 // The list search over the cell grid (rebuild only): one warp per site A takes the sites B > A of other molecules
-// within the list cutoff from the 27 cells around A's cell, in cell order.  The counts and flags are those of
-// kSiteNeighbors.
-__global__ void kSiteNeighborsCells(AtmBuffers A, AtmConfig C) {
+// within the list cutoff from the 27 cells around A's cell, in cell order.  The 27 cells' sites are taken as one
+// sequence (a prefix over the cell sizes), so the lanes stay busy across cell boundaries.  The counts and flags are
+// those of kSiteNeighbors.  Launched with 256-thread blocks.
+__global__ void __launch_bounds__(256) kSiteNeighborsCells(AtmBuffers A, AtmConfig C) {
     if (*(volatile int*)A.flag == 0) return;
+    __shared__ int cellFirst[8][32], cellEnd[8][32];   // per warp: each cell's first site and its end in the sequence
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (warp >= C.numSites) return;
     const int a = warp;
     const int molA = A.molecule[a];
     const SiteCells& G = A.cells;
     const int cell = G.siteCell[a];
     const int cx = cell % G.nc[0], cy = (cell / G.nc[0]) % G.nc[1], cz = cell / (G.nc[0] * G.nc[1]);
+    // lane k < 27 takes the cell (dx, dy, dz) = (k % 3, k / 3 % 3, k / 9) - 1, the order of three nested loops
+    int first = 0, n = 0;
+    if (lane < 27) {
+        const int x = (cx + lane % 3 - 1 + G.nc[0]) % G.nc[0], y = (cy + lane / 3 % 3 - 1 + G.nc[1]) % G.nc[1],
+                  z = (cz + lane / 9 - 1 + G.nc[2]) % G.nc[2];
+        const int c = (z * G.nc[1] + y) * G.nc[0] + x;
+        first = G.cellStart[c];
+        n = G.cellStart[c + 1] - first;
+    }
+    int end = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, end, o);
+        if (lane >= o) end += v;
+    }
+    const int total = __shfl_sync(0xffffffffu, end, 31);
+    cellFirst[w][lane] = first;
+    cellEnd[w][lane] = end;
+    __syncwarp();
     int count = 0;
-    for (int dz = -1; dz <= 1; dz++)
-        for (int dy = -1; dy <= 1; dy++)
-            for (int dx = -1; dx <= 1; dx++) {
-                const int x = (cx + dx + G.nc[0]) % G.nc[0], y = (cy + dy + G.nc[1]) % G.nc[1],
-                          z = (cz + dz + G.nc[2]) % G.nc[2];
-                const int c = (z * G.nc[1] + y) * G.nc[0] + x;
-                const int end = G.cellStart[c + 1];
-                for (int k0 = G.cellStart[c]; k0 < end; k0 += 32) {
-                    const int k = k0 + lane;
-                    const int b = k < end ? G.cellSites[k] : -1;
-                    bool near = false;
-                    if (b > a && A.molecule[b] != molA) {
-                        double d[3];
-                        siteDelta(A, C, a, b, d);
-                        near = (float)(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) < C.listCutoff2;
-                    }
-                    const unsigned bal = __ballot_sync(0xffffffffu, near);
-                    if (near) {
-                        const int slot = count + __popc(bal & laneMaskLt());
-                        if (slot < A.cap) A.nbr[(size_t)a * A.cap + slot] = b;
-                    }
-                    count += __popc(bal);
-                }
+    for (int k0 = 0; k0 < total; k0 += 32) {
+        const int k = k0 + lane;
+        int b = -1;
+        if (k < total) {
+            // the cell holding entry k: the first whose end exceeds k (binary search over the 27 ends)
+            int lo = 0, hi = 26;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (cellEnd[w][mid] > k) hi = mid;
+                else lo = mid + 1;
             }
+            const int before = lo ? cellEnd[w][lo - 1] : 0;
+            b = G.cellSites[cellFirst[w][lo] + (k - before)];
+        }
+        bool near = false;
+        if (b > a && A.molecule[b] != molA) {
+            double d[3];
+            siteDelta(A, C, a, b, d);
+            near = (float)(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) < C.listCutoff2;
+        }
+        const unsigned bal = __ballot_sync(0xffffffffu, near);
+        if (near) {
+            const int slot = count + __popc(bal & laneMaskLt());
+            if (slot < A.cap) A.nbr[(size_t)a * A.cap + slot] = b;
+        }
+        count += __popc(bal);
+    }
     if (lane == 0) {
         A.nbrCount[a] = count;
         if (count > A.cap) atomicOr(A.flag + 1, 1);

@@ -123,6 +123,16 @@ struct ix_batch {
     int* dStep = nullptr;                // steps taken so far (device counter)
     cudaGraphExec_t stepGraph = nullptr;
     double stepDt = 0.0;
+    // deferUploads: a build's uploads are held on the host (pendingBytes, one entry per upload) until
+    // flushBatchUploads copies them asynchronously on the batch's stream from pinned staging, so that the server's
+    // worker does not wait for the copy engine; otherwise each upload is a synchronous copy
+    struct PendingUpload {
+        void* dst;
+        size_t offset, bytes;
+    };
+    bool deferUploads = false;
+    std::vector<char> pendingBytes;
+    std::vector<PendingUpload> pending;
 };
 
 namespace {
@@ -166,10 +176,34 @@ int batchAlloc(ix_batch* b, const std::string& name, size_t count, T** out) {
     return IX_OK;
 }
 
+// Host bytes to the device: held for flushBatchUploads when the batch defers its uploads, else copied synchronously.
+inline int batchCopyIn(ix_batch* b, void* dst, const void* src, size_t bytes) {
+    if (!bytes) return IX_OK;
+    if (b->deferUploads) {
+        const size_t offset = (b->pendingBytes.size() + 15) / 16 * 16;
+        b->pendingBytes.resize(offset + bytes);
+        std::memcpy(b->pendingBytes.data() + offset, src, bytes);
+        b->pending.push_back({dst, offset, bytes});
+        return IX_OK;
+    }
+    IX_BCUDA(b, cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice));
+    return IX_OK;
+}
+
 template <class T>
 int batchUpload(ix_batch* b, const std::string& name, const std::vector<T>& v, T** out) {
     IX_TRY(batchAlloc(b, name, v.size(), out));
-    if (!v.empty()) IX_BCUDA(b, cudaMemcpy(*out, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return batchCopyIn(b, *out, v.data(), v.size() * sizeof(T));
+}
+
+// Issue the held uploads of a build on the batch's stream from `pinned` (pinned host memory of at least
+// pendingBytes.size() bytes that stays valid until the stream has run them).
+int flushBatchUploads(ix_batch* b, char* pinned) {
+    if (!b->pendingBytes.empty()) std::memcpy(pinned, b->pendingBytes.data(), b->pendingBytes.size());
+    for (const auto& u : b->pending)
+        IX_BCUDA(b, cudaMemcpyAsync(u.dst, pinned + u.offset, u.bytes, cudaMemcpyHostToDevice, b->stream));
+    b->pending.clear();
+    b->pendingBytes.clear();
     return IX_OK;
 }
 
@@ -256,33 +290,63 @@ int buildBatchPairs(ix_batch* b, const std::vector<int>& blockStart, int nb) {
             p3[slot] = q3[s][k];
             flags[slot] = qf[s][k];
         }
-    // tiles and masks: every pair of a system, j after i, not excluded, gated on for some term
+    // tiles and masks: every pair of a system, j after i, not excluded, gated on for some term.  The rows start from
+    // the real j slots after i (every pair gated on when all of the system's particles carry the same gate bits, the
+    // usual case; else each pair is tested), then each exclusion clears its bit, then the columns are the transpose.
     std::vector<int> tileJ, tileI, tileStart(S + 1, 0);
     std::vector<unsigned> masks;
     for (int s = 0; s < S; s++) {
         tileStart[s] = (int)tileI.size();
         const ix_ctx* c = sys[s];
         const int b0 = blockStart[s], b1 = blockStart[s + 1];
+        int gates = -1;
+        bool uniformGates = true;
+        for (int k = 0; k < c->n && uniformGates; k++) {
+            const int g = flags[32 * b0 + k] & kFlagGates;
+            if (gates < 0) gates = g;
+            uniformGates = g == gates && g != 0;
+        }
+        const size_t first = tileI.size();
         for (int I = b0; I < b1; I++)
             for (int J = I; J < b1; J++) {
-                unsigned row[32] = {}, col[32] = {};
-                for (int k = 0; k < 32; k++) tileJ.push_back(sortedAtom[32 * J + k] >= 0 ? 32 * J + k : -1);
+                unsigned real = 0;
+                for (int k = 0; k < 32; k++) {
+                    const bool r = sortedAtom[32 * J + k] >= 0;
+                    tileJ.push_back(r ? 32 * J + k : -1);
+                    real |= (unsigned)r << k;
+                }
+                unsigned row[32];
                 for (int i = 0; i < 32; i++) {
                     const int si = 32 * I + i;
+                    row[i] = 0;
                     if (sortedAtom[si] < 0) continue;
-                    for (int k = 0; k < 32; k++) {
-                        const int sj = 32 * J + k;
-                        if (sj <= si || sortedAtom[sj] < 0 || !(flags[si] & flags[sj] & kFlagGates)) continue;
-                        const std::pair<int, int> e{si - 32 * b0, sj - 32 * b0};   // local indices, i < j
-                        if (std::binary_search(c->exclusions.begin(), c->exclusions.end(), e)) continue;
-                        row[i] |= 1u << k;
-                        col[k] |= 1u << i;
-                    }
+                    unsigned m = real & (J > I ? 0xffffffffu : (i == 31 ? 0u : 0xffffffffu << (i + 1)));
+                    if (!uniformGates)
+                        for (unsigned q = m; q; q &= q - 1) {
+                            const int k = __builtin_ctz(q);
+                            if (!(flags[si] & flags[32 * J + k] & kFlagGates)) m &= ~(1u << k);
+                        }
+                    row[i] = m;
                 }
                 tileI.push_back(I);
                 masks.insert(masks.end(), row, row + 32);
-                masks.insert(masks.end(), col, col + 32);
+                masks.insert(masks.end(), 32, 0u);
             }
+        // the tile of blocks (I, J), J >= I, of this system: tiles are numbered I-major from b0
+        const int nbs = b1 - b0;
+        auto tileOf = [&](int I, int J) {
+            const int i = I - b0;
+            return first + (size_t)(i * nbs - i * (i - 1) / 2) + (size_t)(J - I);
+        };
+        for (const auto& e : c->exclusions) {   // local indices, first < second
+            const int si = 32 * b0 + e.first, sj = 32 * b0 + e.second;
+            masks[64 * tileOf(si / 32, sj / 32) + (si & 31)] &= ~(1u << (sj & 31));
+        }
+        for (size_t t = first; t < tileI.size(); t++) {
+            unsigned* m = &masks[64 * t];
+            for (int i = 0; i < 32; i++)
+                for (unsigned q = m[i]; q; q &= q - 1) m[32 + __builtin_ctz(q)] |= 1u << i;
+        }
     }
     tileStart[S] = (int)tileI.size();
     b->numTiles = (int)tileI.size();
@@ -594,8 +658,8 @@ int batchMdSetup(ix_batch* b, const double* masses, const double* velocities, co
     IX_TRY(batchUpload(b, "stopStep", stop, &b->dStopStep));
     IX_TRY(batchUpload(b, "step", std::vector<int>{0}, &b->dStep));
     IX_TRY(batchAlloc(b, "velocities", 3 * (size_t)n, &b->dVel));
-    if (velocities)
-        IX_BCUDA(b, cudaMemcpy(b->dVel, velocities, 3 * (size_t)n * sizeof(double), cudaMemcpyHostToDevice));
+    if (velocities) IX_TRY(batchCopyIn(b, b->dVel, velocities, 3 * (size_t)n * sizeof(double)));
+    else if (b->deferUploads) IX_BCUDA(b, cudaMemsetAsync(b->dVel, 0, 3 * (size_t)n * sizeof(double), b->stream));
     else IX_BCUDA(b, cudaMemset(b->dVel, 0, 3 * (size_t)n * sizeof(double)));
     if (b->stepGraph && (oldVel != b->dVel || oldInv != b->dInvMass || oldStop != b->dStopStep || oldStep != b->dStep)) {
         cudaGraphExecDestroy(b->stepGraph);

@@ -967,6 +967,9 @@ static int allocateAtm(ix_ctx* ctx) {
         IX_TRY(deviceAlloc(ctx, "siteCellStart", kSiteCellMax + 1, &A.cells.cellStart));
         IX_TRY(deviceAlloc(ctx, "siteCellSites", ns, &A.cells.cellSites));
         IX_TRY(deviceAlloc(ctx, "siteCell", ns, &A.cells.siteCell));
+        // the one-block cell sort scatters up to kSiteSortSharedMax sites in dynamic shared memory (on this device)
+        IX_CUDA(ctx, cudaFuncSetAttribute(kSiteCellSort, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          kSiteSortSharedMax * (int)sizeof(int)));
     }
     {
         // the sites of each particle, so that the finishing kernel gives each particle its share of its sites' forces
@@ -1431,7 +1434,8 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         // launches cost less than a conditional graph node); the long-list flag is recomputed with the lists
         kClearFlagIf<<<1, 1, 0, sa>>>(A.flag + 2, A.flag);
         if (A.cells.nc[0]) {
-            kSiteCellSort<<<1, 1024, 0, sa>>>(A, C);
+            const int sharedSites = C.numSites <= kSiteSortSharedMax;
+            kSiteCellSort<<<1, 1024, sharedSites ? C.numSites * sizeof(int) : 0, sa>>>(A, C, sharedSites);
             kSiteNeighborsCells<<<(C.numSites * 32 + tpb - 1) / tpb, tpb, 0, sa>>>(A, C);
             ctx->launches += 1;
         }

@@ -564,7 +564,9 @@ bool cohortCompatible(const ServerRequest* r, const ServerRequest* r0) {
 // Enqueue a cohort's whole run on its batch's stream: the first evaluation, then every step up to the longest
 // request; after the last step of each group of requests (members are ordered by steps) their final state is copied
 // into the pinned staging and an event marks them done.
-int enqueueCohortRun(ServerShard* H, ServerUnit* u) {
+// The members' starting state (positions, velocities, masses and step counts) for the cohort's batch, held with the
+// build's uploads (the batch defers them).
+int stageCohortState(ServerUnit* u) {
     ix_batch* b = u->batch;
     const int nm = (int)u->members.size(), np = b->numParticles;
     std::vector<double> pos(3 * (size_t)np), vel(3 * (size_t)np, 0.0), mass((size_t)np, 1.0);
@@ -578,8 +580,12 @@ int enqueueCohortRun(ServerShard* H, ServerUnit* u) {
         steps[k] = r->steps;
     }
     IX_TRY(batchMdSetup(b, mass.data(), vel.data(), steps.data()));
-    IX_BCUDA(b, cudaMemcpyAsync(b->dPos, pos.data(), pos.size() * sizeof(double), cudaMemcpyHostToDevice, b->stream));
-    IX_BCUDA(b, cudaStreamSynchronize(b->stream));   // the host vectors go out of scope
+    return batchCopyIn(b, b->dPos, pos.data(), pos.size() * sizeof(double));
+}
+
+int enqueueCohortRun(ServerShard* H, ServerUnit* u) {
+    ix_batch* b = u->batch;
+    const int nm = (int)u->members.size(), np = b->numParticles;
     IX_BCUDA(b, cudaGraphLaunch(b->graph, b->stream));
     double* st = reinterpret_cast<double*>(u->staging);
     const size_t n3 = 3 * (size_t)np;
@@ -635,12 +641,18 @@ void launchCohort(ix_server* S, ServerShard* H, std::vector<ServerRequest*>& mem
     }
     {
         PhaseTimer t(H->workerSec[2]);
+        // the build's uploads go out asynchronously from the unit's pinned staging, after its results area
+        b->deferUploads = true;
         if (rc == IX_OK) rc = buildBatch(b);
+        if (rc == IX_OK) rc = stageCohortState(u);
         if (rc == IX_OK) {
             const size_t np = (size_t)b->numParticles;
-            u->staging = S->pinned.alloc((9 * np + 4 * members.size()) * sizeof(double));
+            const size_t results = (9 * np + 4 * members.size()) * sizeof(double);
+            u->staging = S->pinned.alloc(results + b->pendingBytes.size());
             if (!u->staging) rc = batchFail(b, IX_ERR_MEMORY, "pinned host staging could not be allocated");
+            else rc = flushBatchUploads(b, u->staging + results);
         }
+        b->deferUploads = false;
     }
     if (rc == IX_OK) {
         PhaseTimer t(H->workerSec[3]);

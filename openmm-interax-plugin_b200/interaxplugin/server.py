@@ -4,6 +4,11 @@ The scheduling runs in the library's native worker thread: admission by a device
 (periodic systems as contexts on their own streams, small non-periodic systems gathered into batched cohorts), and
 results unpacked from pinned staging as each request's last step completes.  This class only describes requests and
 collects results.
+
+The requests run on many CUDA streams at once; their kernels overlap on the device only as far as its hardware work
+queues keep the streams apart.  Set CUDA_DEVICE_MAX_CONNECTIONS=32 in the environment before CUDA starts in the
+process (the default 8 queues leave a small request waiting behind other requests' work: on the 20,000-request
+stream, p50 latency 172 ms with 8 queues, 6 ms with 32).
 """
 import ctypes
 
