@@ -764,7 +764,7 @@ def run_served(args, rank, world, num_requests=20000, budget=120e9, plain_sample
     def stream(requests, arrivals):
         """Submit `requests` at their arrival times (seconds from now), collect every result; returns the wall
         seconds and the latencies from the scheduled arrivals."""
-        lag, done = {}, {}
+        lag, done, order = {}, {}, []
         t0 = time.perf_counter()
         for i, ((system, pos, vel), n) in enumerate(requests):
             due = t0 + arrivals[i]
@@ -775,6 +775,7 @@ def run_served(args, rank, world, num_requests=20000, budget=120e9, plain_sample
                     time.sleep(1e-3)
             rid = srv.submit(system, pos, vel, steps=n, dt=0.001)
             lag[rid] = time.perf_counter() - due
+            order.append(rid)
         while len(done) < len(requests):
             got = srv.wait(60.0)
             if not got:
@@ -785,7 +786,7 @@ def run_served(args, rank, world, num_requests=20000, budget=120e9, plain_sample
         failed = [r for r in done.values() if r.status != 0]
         if failed:
             raise RuntimeError(f"{len(failed)} requests failed: {failed[0].error}")
-        return wall, np.array([done[rid].latency + max(lag[rid], 0.0) for rid in done])
+        return wall, np.array([done[rid].latency + max(lag[rid], 0.0) for rid in order])   # in request order
 
     if world > 1:
         import torch.distributed as dist
@@ -796,6 +797,8 @@ def run_served(args, rank, world, num_requests=20000, budget=120e9, plain_sample
     # latency: Poisson arrivals at a rate below the capacity, on the first `latency_requests` of the same stream
     m = min(args.latency_requests, num_requests)
     wall_p, lat = stream(reqs[:m], np.cumsum(rng.exponential(1.0 / args.rate, m)))
+    box_ids = {id(b[0]) for b in boxes}
+    box_mask = np.array([id(t[0]) in box_ids for t, _ in reqs[:m]])
     stats = srv.stats()
     srv.close()
     wall = rank_max(wall, world)
@@ -832,6 +835,10 @@ def run_served(args, rank, world, num_requests=20000, budget=120e9, plain_sample
                        "p50": 1000 * float(np.percentile(lat, 50)), "p99": 1000 * float(np.percentile(lat, 99)),
                        "mean": 1000 * float(lat.mean()), "max": 1000 * float(lat.max()),
                        "requests_per_s": m / wall_p},
+        "latency_by_kind_ms": {
+            kind: {"requests": int(sel.sum()), "p50": 1000 * float(np.percentile(lat[sel], 50)),
+                   "p99": 1000 * float(np.percentile(lat[sel], 99))}
+            for kind, sel in (("periodic boxes", box_mask), ("clusters", ~box_mask)) if sel.any()},
         "latency_at_saturation_ms": {"p50": 1000 * float(np.percentile(sat_lat, 50)),
                                      "p99": 1000 * float(np.percentile(sat_lat, 99))},
         "requests_per_s": all_requests / wall,

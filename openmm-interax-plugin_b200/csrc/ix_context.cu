@@ -1485,8 +1485,11 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
             kListTiles<0><<<L.nb, kListThreads, 0, s>>>(L, ctx->G);
             kScanTiles<<<1, 1024, 0, s>>>(L);
             kListTiles<1><<<L.nb, kListThreads, 0, s>>>(L, ctx->G);
-            kTileMasks<<<ctx->numSMs * 8, kListThreads, 0, s>>>(L, ctx->G);
-            kTileOrder<<<ctx->numSMs, 256, 0, s>>>(L);
+            // grids no larger than the tiles need, so that a small system's launches leave the other SMs to the
+            // kernels of other streams
+            kTileMasks<<<std::min(ctx->numSMs * 8, std::max(1, (L.tileCap + kListWarps - 1) / kListWarps)), kListThreads,
+                         0, s>>>(L, ctx->G);
+            kTileOrder<<<std::min(ctx->numSMs, std::max(1, (L.tileCap + 255) / 256)), 256, 0, s>>>(L);
             kClearFlag<<<1, 1, 0, s>>>(L.flag);
             ctx->launches += ctx->G.periodic ? 14 : 15;
             return IX_OK;
@@ -1503,7 +1506,9 @@ static int launchEvaluation(ix_ctx* ctx, unsigned terms, double* outForces, doub
         bool table = ctx->P.coef != nullptr;
         for (int t = 1; t < 3; t++)
             if ((terms >> t) & 1u) table = table && C.overlapMethod[t] == 0;
-        const int grid = lean ? ctx->pairGridBlocksLean : ctx->pairGridBlocks;
+        // a persistent grid, but no more warps than tiles (a small system leaves the other SMs to other streams)
+        const int grid = std::min(lean ? ctx->pairGridBlocksLean : ctx->pairGridBlocks,
+                                  std::max(1, (L.tileCap + kPairWarps - 1) / kPairWarps));
         // every pair of every selected term evaluated unscaled: no per-pair gate or scale tests
         bool uniform = lean;
         for (int t = 0; t < 3; t++)

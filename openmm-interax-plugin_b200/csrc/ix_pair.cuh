@@ -260,12 +260,14 @@ constexpr int kPairColumnLists = IX_TUNE_PAIR_COLUMN_LISTS;
 constexpr int kPairIlp = IX_TUNE_PAIR_ILP;
 constexpr int kPairRound = IX_TUNE_PAIR_ROUND;   // queued pairs computed before their forces are gathered
 
-// Per-warp shared memory of the pair kernel (about 6.8 KB, so that eight 4-warp blocks fit on an SM).  Parameters
-// are not staged: the compute phase reads them through the read-only cache by sorted slot.
+// Per-warp shared memory of the pair kernel (about 6.6 KB, so that eight 4-warp blocks fit on an SM).  Parameters
+// are not staged: the compute phase reads them through the read-only cache by sorted slot.  The w lanes carry what
+// each pair reads besides the displacement, so that the two loads per particle bring it along: hi.w the particle's
+// flags, lo.w its class-table offset (class x number of classes for an i particle, its class for a j particle), as
+// integer bits.
 struct PairWarpStorage {
     float4 hi[2][32];            // position offsets from the i-block center (float part); side 0 = i, 1 = j
     float4 lo[2][32];            // their float remainders
-    int flags[2][32];
     int jslot[32];               // sorted slot of each j particle, -1 for padding
     int rowStart[32];            // queue offset of each row
     unsigned rowMask[32];
@@ -286,14 +288,14 @@ __device__ __forceinline__ void stageParticle(PairWarpStorage& S, int side, int 
             z -= C.box.c[2] * rint(z * C.box.inv[2]);
         }
         const float xh = (float)x, yh = (float)y, zh = (float)z;
-        S.hi[side][lane] = make_float4(xh, yh, zh, 0.0f);
-        S.lo[side][lane] = make_float4((float)(x - xh), (float)(y - yh), (float)(z - zh), 0.0f);
-        S.flags[side][lane] = P.flags[s];
+        const int f = P.flags[s];
+        const int cls = ((f >> kClassShift) & 0xff) * (side == 0 ? P.numClasses : 1);
+        S.hi[side][lane] = make_float4(xh, yh, zh, __int_as_float(f));
+        S.lo[side][lane] = make_float4((float)(x - xh), (float)(y - yh), (float)(z - zh), __int_as_float(cls));
     }
     else {
-        S.flags[side][lane] = 0;
-        S.hi[side][lane] = make_float4(1e30f, 1e30f, 1e30f, 0.0f);
-        S.lo[side][lane] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        S.hi[side][lane] = make_float4(1e30f, 1e30f, 1e30f, __int_as_float(0));
+        S.lo[side][lane] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(0));
     }
     if (side == 1) S.jslot[lane] = s;
 }
@@ -364,17 +366,18 @@ __device__ __forceinline__ float4 computeQueuedPair(PairWarpStorage& S, int entr
                                                     const PairBuffers& P, const PairCoef* coef, float e[3],
                                                     unsigned& pairs) {
     const int i = entry >> 5, j = entry & 31;
+    const float4 hi_i = S.hi[0][i], lo_i = S.lo[0][i], hi_j = S.hi[1][j], lo_j = S.lo[1][j];
     float dx, dy, dz;
-    const float r2 = pairDisplacement(S.hi[0][i], S.lo[0][i], S.hi[1][j], S.lo[1][j], perPairImage, C, dx, dy, dz);
-    if (CHECK && C.useCutoff && !withinCutoff(r2, S.hi[0][i], S.lo[0][i], S.hi[1][j], S.lo[1][j], perPairImage, C))
+    const float r2 = pairDisplacement(hi_i, lo_i, hi_j, lo_j, perPairImage, C, dx, dy, dz);
+    if (CHECK && C.useCutoff && !withinCutoff(r2, hi_i, lo_i, hi_j, lo_j, perPairImage, C))
         return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    const int fi = S.flags[0][i], fj = S.flags[1][j];
+    const int fi = __float_as_int(hi_i.w), fj = __float_as_int(hi_j.w);
     float invR;
     const float r = sqrtRefined(r2, invR);
     float dEdR;
     if (TABLE) {
-        const int ci = (fi >> kClassShift) & 0xff, cj = (fj >> kClassShift) & 0xff;
-        dEdR = pairTermsTable<LEAN, UNIFORM>(C, r, invR, coef + ci * P.numClasses + cj, fi, fj, e);
+        const PairCoef* K = coef + (__float_as_int(lo_i.w) + __float_as_int(lo_j.w));
+        dEdR = pairTermsTable<LEAN, UNIFORM>(C, r, invR, K, fi, fj, e);
     }
     else {
         const int si = iBase + i, sj = S.jslot[j];
@@ -406,14 +409,12 @@ __device__ __forceinline__ void computeQueuedPair2(PairWarpStorage& S, int entry
     for (int k = 0; k < 2; k++) {
         const int entry = k ? entry1 : entry0;
         const int i = entry >> 5, j = entry & 31;
-        const float r2 = pairDisplacement(S.hi[0][i], S.lo[0][i], S.hi[1][j], S.lo[1][j], perPairImage, C, dxs[k],
-                                          dys[k], dzs[k]);
-        const bool in = (k == 0 || two) &&
-                        (!C.useCutoff || withinCutoff(r2, S.hi[0][i], S.lo[0][i], S.hi[1][j], S.lo[1][j], perPairImage, C));
+        const float4 hi_i = S.hi[0][i], lo_i = S.lo[0][i], hi_j = S.hi[1][j], lo_j = S.lo[1][j];
+        const float r2 = pairDisplacement(hi_i, lo_i, hi_j, lo_j, perPairImage, C, dxs[k], dys[k], dzs[k]);
+        const bool in = (k == 0 || two) && (!C.useCutoff || withinCutoff(r2, hi_i, lo_i, hi_j, lo_j, perPairImage, C));
         inside[k] = in;
         r2s[k] = r2;   // a pair left out is evaluated at its own (positive, finite) distance and masked
-        const int fi = S.flags[0][i], fj = S.flags[1][j];
-        K[k] = coef + ((fi >> kClassShift) & 0xff) * P.numClasses + ((fj >> kClassShift) & 0xff);
+        K[k] = coef + (__float_as_int(lo_i.w) + __float_as_int(lo_j.w));
     }
     F2 invR;
     const F2 r = sqrtRefined2(f2(r2s[0], r2s[1]), invR);
@@ -511,7 +512,8 @@ __global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPai
             stageParticle(S, 1, lane, jslot, cx, cy, cz, shiftImage, C, L, P);
             if (C.alchOnlyBit) {
                 // keep the pairs with exactly one alchemical particle
-                const bool ia = (S.flags[0][lane] & C.alchOnlyBit) != 0, ja = (S.flags[1][lane] & C.alchOnlyBit) != 0;
+                const bool ia = (__float_as_int(S.hi[0][lane].w) & C.alchOnlyBit) != 0;
+                const bool ja = (__float_as_int(S.hi[1][lane].w) & C.alchOnlyBit) != 0;
                 const unsigned iAlch = __ballot_sync(0xffffffffu, ia), jAlch = __ballot_sync(0xffffffffu, ja);
                 row &= ia ? ~jAlch : jAlch;
                 column &= ja ? ~iAlch : iAlch;

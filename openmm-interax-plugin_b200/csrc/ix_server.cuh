@@ -556,9 +556,15 @@ void launchContext(ix_server* S, ServerShard* H, ServerRequest* r) {
     S->stats.admitted++;
 }
 
-// Whether a small request can join a cohort started by r0: the same force settings, parameters and step size.
+// Whether a small request can join a cohort started by r0: the same force settings, parameters and step size, and a
+// size within a factor of kCohortSizeBand of r0's.  A cohort advances all its members step by step, so a small
+// request beside a large one (whose all-pairs and all-triples cost grows as n^2 and n^3) would wait for the large
+// one's steps.
+constexpr int kCohortSizeBand = 2;
 bool cohortCompatible(const ServerRequest* r, const ServerRequest* r0) {
-    return r->dt == r0->dt && r->sys->parameters == r0->sys->parameters && sameBatchSettings(r->sys, r0->sys);
+    const int a = std::min(r->sys->n, r0->sys->n), b = std::max(r->sys->n, r0->sys->n);
+    return b <= kCohortSizeBand * a && r->dt == r0->dt && r->sys->parameters == r0->sys->parameters &&
+           sameBatchSettings(r->sys, r0->sys);
 }
 
 // Enqueue a cohort's whole run on its batch's stream: the first evaluation, then every step up to the longest
