@@ -42,12 +42,12 @@ import numpy as np  # noqa: E402
 F_PAIR = 612.4
 F_TRIPLE = 151.0
 # DRAM bytes (read + write) of one pair-kernel launch on this workload, from one ncu capture of an MD-step launch
-# (dram__bytes_read.sum + dram__bytes_write.sum); the kernel is FP32-issue bound, the traffic is reported beside it
-PAIR_TRAFFIC_BYTES = 10082304
+# (dram__bytes.sum.per_second x gpu__time_duration.sum); the kernel is FP32-issue bound, the traffic is reported beside it
+PAIR_TRAFFIC_BYTES = 10162432
 # The same capture's hardware view: FMA-pipe busy fraction (sm__pipe_fma_cycles_active, pct of peak over active
 # cycles) and issue-slot use (sm__inst_issued), beside the algorithmic fraction
-PAIR_FMA_PIPE_ACTIVE = 0.340
-PAIR_ISSUE_ACTIVE = 0.740
+PAIR_FMA_PIPE_ACTIVE = 0.355
+PAIR_ISSUE_ACTIVE = 0.747
 METRIC = "interactions/s"
 WORKLOAD = "water box 24,000 atoms (8,000 rigid 3-site waters, constrained, 6.208 nm periodic, cutoff 1.0 nm) + ATM " \
            "on 8,000 molecular sites (cutoff 0.6 nm); velocity-Verlet 1 fs with SHAKE/RATTLE"
