@@ -67,7 +67,7 @@ def parse():
     # served stream: Poisson arrival rate (requests/s) of its latency phase and the server's running-request limit
     p.add_argument("--rate", type=float, default=100.0)
     p.add_argument("--latency-requests", type=int, default=4000)
-    p.add_argument("--max-running", type=int, default=256)
+    p.add_argument("--max-running", type=int, default=512)
     p.add_argument("--requests", type=int, default=20000)
     p.add_argument("--server-threads", type=int, default=1)
     p.add_argument("--cohort-window", type=float, default=200e-6)

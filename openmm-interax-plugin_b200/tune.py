@@ -47,7 +47,8 @@ GROUPS = [
     ("pair table", [dict(IX_TUNE_PAIR_SHARED_TABLE_BYTES=b) for b in (0, 1024, 2048)]),
     ("pair skin", [dict(IX_TUNE_PAIR_SKIN=s) for s in (0.06, 0.08, 0.1, 0.12)]),
     ("three-body", [dict(IX_TUNE_ATM_FAST=f, IX_TUNE_ATM_ROUND=r, IX_TUNE_ATM_MIN_BLOCKS=b)
-                    for f, r, b in ((64, 64, 7), (64, 64, 8), (64, 64, 10), (32, 32, 12), (64, 32, 8), (64, 128, 7))]),
+                    for f, r, b in ((64, 64, 7), (64, 64, 8), (64, 64, 10), (32, 32, 12), (64, 32, 8), (64, 128, 7),
+                                    (64, 128, 8), (64, 256, 5))]),
     ("site skin", [dict(IX_TUNE_SITE_SKIN=s) for s in (0.05, 0.1, 0.15)]),
 ]
 
