@@ -650,12 +650,17 @@ struct AtmWarpStorage {
 constexpr int kAtmWarps = 4;
 constexpr int kAtmMaxStaged = 256;
 constexpr int kAtmChunk = kAtmMaxStaged / 2;
+// Each long-list site is taken by this many warps, each evaluating every kAtmWideParts-th group of 32 of its pairs:
+// a site near the start of a large cluster has tens of thousands of (B, C) pairs, which one warp would take alone.
+constexpr int kAtmWideParts = 8;
 
-// Sites whose lists are longer than kAtmFast.  Up to kAtmMaxStaged neighbors within the cutoff are staged at once and
-// their pairs enumerated by a flat triangular index; a longer list is taken in chunks of kAtmChunk, each pair of
-// chunks (I <= J) staged side by side, so any length is handled.  The forces on B and C accumulate in shared memory
-// and are flushed to the fixed-point site forces after each staging.  Energies go to energyPartials[partialsOffset +
-// warp].
+// Sites whose lists are longer than kAtmFast, in units (site, part) of kAtmWideParts parts per site.  A unit stages up
+// to kAtmMaxStaged neighbors within the cutoff at once and evaluates its part of their pairs, enumerated by a flat
+// triangular index; a longer list is taken in chunks of kAtmChunk, each pair of chunks (I <= J) staged side by side,
+// so any length is handled.  The forces on B and C accumulate in shared memory and are flushed to the fixed-point
+// site forces after each staging (integer sums: the split changes no result's dependence on the order).  Energies go
+// to energyPartials[partialsOffset + warp]: with a grid of one warp per unit, one slot per unit (unit = site x
+// kAtmWideParts + part).
 // `gate` (may be null): the kernel returns at once unless *gate is set (a list longer than kAtmFast exists).
 __global__ void __launch_bounds__(32 * kAtmWarps) kTriplesWide(AtmBuffers A, AtmConfig C, int partialsOffset,
                                                                const int* gate) {
@@ -665,7 +670,9 @@ __global__ void __launch_bounds__(32 * kAtmWarps) kTriplesWide(AtmBuffers A, Atm
     const int lane = threadIdx.x & 31;
     double eAcc = 0.0;
     unsigned long long triples = 0;
-    for (int a = blockIdx.x * kAtmWarps + (threadIdx.x >> 5); a < C.numSites; a += gridDim.x * kAtmWarps) {
+    const int units = C.numSites * kAtmWideParts;
+    for (int u = blockIdx.x * kAtmWarps + (threadIdx.x >> 5); u < units; u += gridDim.x * kAtmWarps) {
+        const int a = u / kAtmWideParts, part = u % kAtmWideParts;
         const int n = A.nbrCount[a];
         if (n <= kAtmFast && n <= A.cap) continue;     // the fast kernel takes this site
         const float4 pa = A.siteParams[a];
@@ -708,7 +715,7 @@ __global__ void __launch_bounds__(32 * kAtmWarps) kTriplesWide(AtmBuffers A, Atm
         };
         auto triangle = [&](int m) {
             const int numPairs = m * (m - 1) / 2;
-            for (int p = lane; p < numPairs; p += 32) {
+            for (int p = lane + 32 * part; p < numPairs; p += 32 * kAtmWideParts) {
                 // p = c (c - 1)/2 + b with b < c
                 int c = (int)((1.0f + sqrtf(1.0f + 8.0f * (float)p)) * 0.5f);
                 while (c * (c - 1) / 2 > p) c--;
@@ -744,7 +751,8 @@ __global__ void __launch_bounds__(32 * kAtmWarps) kTriplesWide(AtmBuffers A, Atm
                     __syncwarp();
                     if (J == I) triangle(cI);
                     else
-                        for (int p = lane; p < cI * cJ; p += 32) pair(p / cJ, kAtmChunk + p % cJ);
+                        for (int p = lane + 32 * part; p < cI * cJ; p += 32 * kAtmWideParts)
+                            pair(p / cJ, kAtmChunk + p % cJ);
                     __syncwarp();
                     flush(0, cI);
                     if (J != I) flush(kAtmChunk, kAtmChunk + cJ);

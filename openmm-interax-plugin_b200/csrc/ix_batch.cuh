@@ -32,10 +32,11 @@ __global__ void kBatchPositions(ListBuffers L) {
 }
 
 // Per-system energies (4 per system: dispersion, exchange, short range, three-body) from the tile slots and the site
-// slots of the two triple kernels, in a fixed order; one thread per system.  Thread 0 also publishes the interaction
+// slots of the two triple kernels (wideParts per site of the wide kernel's, 0 when it does not run), in a fixed
+// order; one thread per system.  Thread 0 also publishes the interaction
 // counts and resets the pair kernel's tile counter.
 __global__ void kBatchEnergies(int numSystems, const int* tileStart, const double* tileEnergy, const int* siteStart,
-                               const double* siteFast, const double* siteWide, double* out,
+                               const double* siteFast, const double* siteWide, int wideParts, double* out,
                                unsigned long long* counts, int* taskCounter) {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s == 0) {
@@ -49,7 +50,10 @@ __global__ void kBatchEnergies(int numSystems, const int* tileStart, const doubl
     double e[4] = {0.0, 0.0, 0.0, 0.0};
     for (int t = tileStart[s]; t < tileStart[s + 1]; t++)
         for (int k = 0; k < 3; k++) e[k] += tileEnergy[3 * t + k];
-    for (int a = siteStart[s]; a < siteStart[s + 1]; a++) e[3] += siteFast[a] + siteWide[a];
+    for (int a = siteStart[s]; a < siteStart[s + 1]; a++) {
+        e[3] += siteFast[a];
+        for (int w = 0; w < wideParts; w++) e[3] += siteWide[(size_t)a * kAtmWideParts + w];
+    }
     for (int k = 0; k < 4; k++) out[4 * s + k] = e[k];
 }
 
@@ -485,10 +489,12 @@ int buildBatchSites(ix_batch* b) {
     IX_TRY(batchUpload(b, "atmParticleForce", std::vector<long long>(3 * (size_t)b->numParticles, 0),
                        &A.particleForce));
     A.numParticles = b->numParticles;
-    // one warp per site in both triple kernels, so that each site's energy has its own slot
+    // one warp per site in the fast kernel and one per (site, part) unit in the wide one, so that each site's energy
+    // has its own slots
     b->atmFastBlocks = (ns + kAtmFastWarps - 1) / kAtmFastWarps;
-    b->atmWideBlocks = *std::max_element(count.begin(), count.end()) > kAtmFast ? (ns + kAtmWarps - 1) / kAtmWarps : 0;
-    const size_t slots = (size_t)b->atmFastBlocks * kAtmFastWarps + (size_t)(ns + kAtmWarps - 1) / kAtmWarps * kAtmWarps;
+    const int wideBlocks = (int)(((size_t)ns * kAtmWideParts + kAtmWarps - 1) / kAtmWarps);
+    b->atmWideBlocks = *std::max_element(count.begin(), count.end()) > kAtmFast ? wideBlocks : 0;
+    const size_t slots = (size_t)b->atmFastBlocks * kAtmFastWarps + (size_t)wideBlocks * kAtmWarps;
     IX_TRY(batchUpload(b, "sitePartials", std::vector<double>(slots, 0.0), &b->sitePartials));
     A.energyPartials = b->sitePartials;
     A.tripleCount = b->dCounts + 1;
@@ -538,8 +544,10 @@ int enqueueBatch(ix_batch* b) {
         fast = b->tileEnergy;   // no sites: the site ranges are empty and never read
         wide = b->tileEnergy;
     }
+    // the wide kernel's slots hold energies only when it runs (a list longer than the fast kernel's)
     kBatchEnergies<<<(S + tpb - 1) / tpb, tpb, 0, st>>>(S, b->tileStart, b->tileEnergy, b->siteStart, fast, wide,
-                                                       b->dEnergies, b->dCounts, L.taskCounter);
+                                                       b->atmWideBlocks > 0 ? kAtmWideParts : 0, b->dEnergies,
+                                                       b->dCounts, L.taskCounter);
     IX_BCUDA(b, cudaGetLastError());
     return IX_OK;
 }

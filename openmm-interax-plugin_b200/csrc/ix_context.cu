@@ -1003,9 +1003,10 @@ static int allocateAtm(ix_ctx* ctx) {
     IX_TRY(deviceAlloc(ctx, "nbr", (size_t)ns * A.cap, &A.nbr));
     A.flag = ctx->dFlags + 4;
     A.numParticles = ctx->n;
-    // fast kernel: one warp per site; wide kernel (long lists): a grid that scans every site
+    // fast kernel: one warp per site; wide kernel (long lists): one wave of blocks over every (site, part) unit
     ctx->atmFastBlocks = std::max(1, (ns + kAtmFastWarps - 1) / kAtmFastWarps);
-    ctx->atmGridBlocks = std::max(1, std::min((ns + kAtmWarps - 1) / kAtmWarps, ctx->numSMs * 2));
+    ctx->atmGridBlocks = std::max(1, (int)std::min<long long>(((long long)ns * kAtmWideParts + kAtmWarps - 1) / kAtmWarps,
+                                                              (long long)ctx->numSMs * 4));
     IX_TRY(deviceAlloc(ctx, "atmPartials", atmPartialCount(ctx), &ctx->dAtmPartials));
     A.energyPartials = ctx->dAtmPartials;
     A.tripleCount = ctx->dCounts + 1;
