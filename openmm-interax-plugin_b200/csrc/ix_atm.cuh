@@ -48,6 +48,8 @@ struct SiteCells {
     int* cellStart;              // numCells + 1
     int* cellSites;              // the sites by cell, each cell's in increasing order
     int* siteCell;               // numSites
+    float4* wrapped;             // numSites: each site's position wrapped into the box (float), w its molecule (int
+                                 // bits), written by the cell sort for the list search
 };
 constexpr int kSiteCellMax = 8192;   // cells the one-block sort holds in shared memory
 // sites up to this count are scattered and ordered in dynamic shared memory by the one-block sort (160 KB)
@@ -231,6 +233,7 @@ __global__ void __launch_bounds__(1024) kSiteCellSort(AtmBuffers A, AtmConfig C,
         const int cz = min(max((int)(p.z * G.cellsPerNm[2]), 0), G.nc[2] - 1);
         const int cell = (cz * G.nc[1] + cy) * G.nc[0] + cx;
         G.siteCell[s] = cell;
+        G.wrapped[s] = make_float4(p.x, p.y, p.z, __int_as_float(A.molecule[s]));
         atomicAdd(&count[cell], 1);
     }
     __syncthreads();
@@ -291,7 +294,10 @@ __global__ void __launch_bounds__(1024) kSiteCellSort(AtmBuffers A, AtmConfig C,
 
 // The list search over the cell grid (rebuild only): one warp per site A takes the sites B > A of other molecules
 // within the list cutoff from the 27 cells around A's cell, in cell order.  The 27 cells' sites are taken as one
-// sequence (a prefix over the cell sizes), so the lanes stay busy across cell boundaries.  The counts and flags are
+// sequence (a prefix over the cell sizes), so the lanes stay busy across cell boundaries.  The distance test uses the
+// float wrapped positions of the cell sort with a margin of 1e-4 of the squared list cutoff, far above their rounding
+// (a few 1e-6): the list may hold a pair at the very edge of the list cutoff that the double-precision distance would
+// leave out, never the reverse, and the triple kernels test the cutoff itself in double.  The counts and flags are
 // those of kSiteNeighbors.  Launched with 256-thread blocks.
 __global__ void __launch_bounds__(256) kSiteNeighborsCells(AtmBuffers A, AtmConfig C) {
     if (*(volatile int*)A.flag == 0) return;
@@ -300,8 +306,10 @@ __global__ void __launch_bounds__(256) kSiteNeighborsCells(AtmBuffers A, AtmConf
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (warp >= C.numSites) return;
     const int a = warp;
-    const int molA = A.molecule[a];
     const SiteCells& G = A.cells;
+    const float4 pa = G.wrapped[a];
+    const int molA = __float_as_int(pa.w);
+    const float cut2 = C.listCutoff2 * (1.0f + 1e-4f);
     const int cell = G.siteCell[a];
     const int cx = cell % G.nc[0], cy = (cell / G.nc[0]) % G.nc[1], cz = cell / (G.nc[0] * G.nc[1]);
     // lane k < 27 takes the cell (dx, dy, dz) = (k % 3, k / 3 % 3, k / 9) - 1, the order of three nested loops
@@ -339,10 +347,13 @@ __global__ void __launch_bounds__(256) kSiteNeighborsCells(AtmBuffers A, AtmConf
             b = G.cellSites[cellFirst[w][lo] + (k - before)];
         }
         bool near = false;
-        if (b > a && A.molecule[b] != molA) {
-            double d[3];
-            siteDelta(A, C, a, b, d);
-            near = (float)(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]) < C.listCutoff2;
+        if (b > a) {
+            const float4 pb = G.wrapped[b];
+            float dx = pb.x - pa.x, dy = pb.y - pa.y, dz = pb.z - pa.z;
+            dx -= C.boxf.a[0] * rintf(dx * C.boxf.inv[0]);
+            dy -= C.boxf.b[1] * rintf(dy * C.boxf.inv[1]);
+            dz -= C.boxf.c[2] * rintf(dz * C.boxf.inv[2]);
+            near = __float_as_int(pb.w) != molA && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) < cut2;
         }
         const unsigned bal = __ballot_sync(0xffffffffu, near);
         if (near) {

@@ -967,6 +967,7 @@ static int allocateAtm(ix_ctx* ctx) {
         IX_TRY(deviceAlloc(ctx, "siteCellStart", kSiteCellMax + 1, &A.cells.cellStart));
         IX_TRY(deviceAlloc(ctx, "siteCellSites", ns, &A.cells.cellSites));
         IX_TRY(deviceAlloc(ctx, "siteCell", ns, &A.cells.siteCell));
+        IX_TRY(deviceAlloc(ctx, "siteWrapped", ns, &A.cells.wrapped));
         // the one-block cell sort scatters up to kSiteSortSharedMax sites in dynamic shared memory (on this device)
         IX_CUDA(ctx, cudaFuncSetAttribute(kSiteCellSort, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           kSiteSortSharedMax * (int)sizeof(int)));
