@@ -78,6 +78,7 @@ struct AtmBuffers {
 
 constexpr int kAtmFast = IX_TUNE_ATM_FAST;     // neighbor lists up to this length take the fast triple kernel
 constexpr int kAtmRound = IX_TUNE_ATM_ROUND;   // (B, C) pairs evaluated before their forces are gathered
+constexpr int kAtmAccum = IX_TUNE_ATM_ACCUM;   // 1: B and C forces as fixed-point shared-memory sums (no rounds)
 constexpr int kAtmFastWarps = 4;
 
 // The flat triangular index p = c (c - 1) / 2 + b of the pairs b < c < kAtmFast, decoded: b | c << 8.
@@ -544,8 +545,9 @@ struct AtmFastStorage {
     float4 pos[kAtmFast];        // displacement from A; w holds the molecule (int bits)
     float4 params[kAtmFast];
     int site[kAtmFast];
-    float4 fb[kAtmRound];        // force on B of each pair of the current round
-    float4 fc[kAtmRound];        // force on C
+    float4 fb[kAtmAccum ? 1 : kAtmRound];   // force on B of each pair of the current round
+    float4 fc[kAtmAccum ? 1 : kAtmRound];   // force on C
+    unsigned long long acc[kAtmAccum ? 3 : 1][kAtmAccum ? kAtmFast : 1];   // fixed-point force sums per neighbor
 };
 
 __global__ void __launch_bounds__(32 * kAtmFastWarps, IX_TUNE_ATM_MIN_BLOCKS) kTriplesFast(AtmBuffers A, AtmConfig C) {
@@ -574,6 +576,40 @@ __global__ void __launch_bounds__(32 * kAtmFastWarps, IX_TUNE_ATM_MIN_BLOCKS) kT
         float eSite = 0.0f;
         int next0 = lane + 1, next1 = lane + 33;    // next C of the pairs (k, C) each lane gathers as B
         const int numPairs = m * (m - 1) / 2;
+        if constexpr (kAtmAccum) {
+            // each triple's B and C forces go to the neighbors' fixed-point sums (integer adds: the order of the
+            // lanes does not change them), flushed once per site
+            for (int k = lane; k < m; k += 32) S.acc[0][k] = S.acc[1][k] = S.acc[2][k] = 0ull;
+            __syncwarp();
+            for (int q = lane; q < numPairs; q += 32) {
+                const unsigned bc = __ldg(kTrianglePairs.bc + q);
+                const int b = bc & 0xff, c = bc >> 8;
+                const float4 xb = S.pos[b], xc = S.pos[c];
+                if (__float_as_int(xb.w) == __float_as_int(xc.w)) continue;
+                float e;
+                float3 fA, fB, fC;
+                if (!atmTriple(C, pa, S.params[b], S.params[c], xb.x, xb.y, xb.z, xc.x, xc.y, xc.z, e, fA, fB, fC))
+                    continue;
+                fa[0] += fA.x;
+                fa[1] += fA.y;
+                fa[2] += fA.z;
+                eSite += e;
+                triples++;
+                atomicAdd(&S.acc[0][b], (unsigned long long)toFixed(fB.x));
+                atomicAdd(&S.acc[1][b], (unsigned long long)toFixed(fB.y));
+                atomicAdd(&S.acc[2][b], (unsigned long long)toFixed(fB.z));
+                atomicAdd(&S.acc[0][c], (unsigned long long)toFixed(fC.x));
+                atomicAdd(&S.acc[1][c], (unsigned long long)toFixed(fC.y));
+                atomicAdd(&S.acc[2][c], (unsigned long long)toFixed(fC.z));
+            }
+            __syncwarp();
+            for (int k = lane; k < m; k += 32) {
+                const int b = S.site[k];
+                for (int d = 0; d < 3; d++)
+                    if (S.acc[d][k]) atomicAddFixed(A.siteForce + d * C.numSites + b, (long long)S.acc[d][k]);
+            }
+        }
+        else
         for (int base = 0; base < numPairs; base += kAtmRound) {
             const int count = min(kAtmRound, numPairs - base);
             for (int q = lane; q < count; q += 32) {
@@ -630,8 +666,10 @@ __global__ void __launch_bounds__(32 * kAtmFastWarps, IX_TUNE_ATM_MIN_BLOCKS) kT
             if (f[1] != 0.0f) atomicAddFixed(A.siteForce + C.numSites + b, toFixed(f[1]));
             if (f[2] != 0.0f) atomicAddFixed(A.siteForce + 2 * C.numSites + b, toFixed(f[2]));
         };
-        flush(lane, f0);
-        flush(lane + 32, f1);
+        if constexpr (!kAtmAccum) {
+            flush(lane, f0);
+            flush(lane + 32, f1);
+        }
         for (int o = 16; o > 0; o >>= 1) {
             fa[0] += __shfl_xor_sync(0xffffffffu, fa[0], o);
             fa[1] += __shfl_xor_sync(0xffffffffu, fa[1], o);

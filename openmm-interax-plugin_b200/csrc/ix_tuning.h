@@ -45,3 +45,8 @@
 #ifndef IX_TUNE_ATM_MIN_BLOCKS
 #define IX_TUNE_ATM_MIN_BLOCKS 7
 #endif
+// three-body: 1 = the fast kernel adds each triple's B and C forces to per-neighbor 64-bit fixed-point sums in shared
+// memory (integer atomics, no rounds); 0 = it stores them per round and gathers them per neighbor
+#ifndef IX_TUNE_ATM_ACCUM
+#define IX_TUNE_ATM_ACCUM 0
+#endif

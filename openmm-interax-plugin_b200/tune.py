@@ -35,7 +35,8 @@ import build_lib  # noqa: E402
 DEFAULTS = {"IX_TUNE_PAIR_WARPS": 4, "IX_TUNE_PAIR_ROUND": 128, "IX_TUNE_PAIR_MIN_BLOCKS": 8,
             "IX_TUNE_PAIR_COLUMN_LISTS": 0, "IX_TUNE_PAIR_ILP": 0, "IX_TUNE_PAIR_SHARED_TABLE_BYTES": 0,
             "IX_TUNE_PAIR_SKIN": 0.1,
-            "IX_TUNE_SITE_SKIN": 0.1, "IX_TUNE_ATM_FAST": 64, "IX_TUNE_ATM_ROUND": 64, "IX_TUNE_ATM_MIN_BLOCKS": 7}
+            "IX_TUNE_SITE_SKIN": 0.1, "IX_TUNE_ATM_FAST": 64, "IX_TUNE_ATM_ROUND": 64, "IX_TUNE_ATM_MIN_BLOCKS": 7,
+            "IX_TUNE_ATM_ACCUM": 0}
 
 # groups of constants searched together, each with its candidate values (dicts of the group's macros)
 GROUPS = [
@@ -46,9 +47,10 @@ GROUPS = [
                                           (2, 128, 10, 0, 1), (4, 256, 4, 0, 1))]),
     ("pair table", [dict(IX_TUNE_PAIR_SHARED_TABLE_BYTES=b) for b in (0, 1024, 2048)]),
     ("pair skin", [dict(IX_TUNE_PAIR_SKIN=s) for s in (0.06, 0.08, 0.1, 0.12)]),
-    ("three-body", [dict(IX_TUNE_ATM_FAST=f, IX_TUNE_ATM_ROUND=r, IX_TUNE_ATM_MIN_BLOCKS=b)
-                    for f, r, b in ((64, 64, 7), (64, 64, 8), (64, 64, 10), (32, 32, 12), (64, 32, 8), (64, 128, 7),
-                                    (64, 128, 8), (64, 256, 5))]),
+    ("three-body", [dict(IX_TUNE_ATM_FAST=f, IX_TUNE_ATM_ROUND=r, IX_TUNE_ATM_MIN_BLOCKS=b, IX_TUNE_ATM_ACCUM=acc)
+                    for f, r, b, acc in ((64, 64, 7, 0), (64, 64, 8, 0), (64, 64, 10, 0), (32, 32, 12, 0),
+                                         (64, 32, 8, 0), (64, 128, 7, 0), (64, 128, 8, 0), (64, 256, 5, 0),
+                                         (64, 128, 7, 1))]),
     ("site skin", [dict(IX_TUNE_SITE_SKIN=s) for s in (0.05, 0.1, 0.15)]),
 ]
 

@@ -42,7 +42,9 @@ def test_candidates_respect_the_kernels_limits():
             assert per_warp * v["IX_TUNE_PAIR_WARPS"] <= 48 * 1024
             # the fast triple kernel's 4 warps: staged neighbors (two float4 and an int each) and a round's B and C
             # forces, within 48 KB of static shared memory, and the blocks per SM it asks for within 228 KB
-            atm_block = 4 * (2 * 16 * v["IX_TUNE_ATM_FAST"] + 4 * v["IX_TUNE_ATM_FAST"] + 2 * 16 * v["IX_TUNE_ATM_ROUND"])
+            rounds = 1 if v["IX_TUNE_ATM_ACCUM"] else v["IX_TUNE_ATM_ROUND"]
+            sums = 3 * 8 * v["IX_TUNE_ATM_FAST"] if v["IX_TUNE_ATM_ACCUM"] else 8
+            atm_block = 4 * (2 * 16 * v["IX_TUNE_ATM_FAST"] + 4 * v["IX_TUNE_ATM_FAST"] + 2 * 16 * rounds + sums)
             assert atm_block <= 48 * 1024
             assert (atm_block + 1024) * v["IX_TUNE_ATM_MIN_BLOCKS"] <= 228 * 1024
             assert 0.0 < v["IX_TUNE_PAIR_SKIN"] < 0.5 and 0.0 < v["IX_TUNE_SITE_SKIN"] < 0.5
