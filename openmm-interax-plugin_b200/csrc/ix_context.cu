@@ -588,7 +588,8 @@ static void overlapCoefficients(double w1, double w2, float4& A, float4& B, floa
 // Particles with identical parameters of all pair forces form a class; with at most kMaxClasses classes the kernel
 // reads the coefficients of a pair from a class-pair table instead of recomputing them (see PairCoef).  Sets the
 // class in bits 8..15 of each particle's flags.
-constexpr int kMaxClasses = 16;
+constexpr int kMaxClasses = IX_TUNE_PAIR_MAX_CLASSES;
+static_assert(kMaxClasses >= 1 && kMaxClasses <= 256, "a particle's class is 8 bits of its flags");
 
 // The class-pair table of one or more systems that share their pair forces' layout (a context, or the systems of a
 // batch): flags[s][i] |= class << kClassShift.  Returns the number of classes, 0 when there are more than kMaxClasses

@@ -27,6 +27,11 @@
 #ifndef IX_TUNE_PAIR_SHARED_TABLE_BYTES
 #define IX_TUNE_PAIR_SHARED_TABLE_BYTES 0
 #endif
+// pair kernel: the most parameter classes (particles with identical pair parameters) for which it reads each pair's
+// coefficients from a class-pair table (at most 256: the class is 8 bits of the flags); above, per-particle parameters
+#ifndef IX_TUNE_PAIR_MAX_CLASSES
+#define IX_TUNE_PAIR_MAX_CLASSES 16
+#endif
 // pair list: skin (nm) of the list cutoff; the list is rebuilt when a particle has moved by half of it
 #ifndef IX_TUNE_PAIR_SKIN
 #define IX_TUNE_PAIR_SKIN 0.1f

@@ -34,6 +34,7 @@ import build_lib  # noqa: E402
 
 DEFAULTS = {"IX_TUNE_PAIR_WARPS": 4, "IX_TUNE_PAIR_ROUND": 128, "IX_TUNE_PAIR_MIN_BLOCKS": 8,
             "IX_TUNE_PAIR_COLUMN_LISTS": 0, "IX_TUNE_PAIR_ILP": 0, "IX_TUNE_PAIR_SHARED_TABLE_BYTES": 0,
+            "IX_TUNE_PAIR_MAX_CLASSES": 16,
             "IX_TUNE_PAIR_SKIN": 0.1,
             "IX_TUNE_SITE_SKIN": 0.1, "IX_TUNE_ATM_FAST": 64, "IX_TUNE_ATM_ROUND": 64, "IX_TUNE_ATM_MIN_BLOCKS": 7,
             "IX_TUNE_ATM_ACCUM": 0}
