@@ -69,7 +69,7 @@ def parse():
     p.add_argument("--latency-requests", type=int, default=4000)
     p.add_argument("--max-running", type=int, default=512)
     p.add_argument("--requests", type=int, default=20000)
-    p.add_argument("--server-threads", type=int, default=1)
+    p.add_argument("--server-threads", type=int, default=3)
     p.add_argument("--cohort-window", type=float, default=200e-6)
     return p.parse_args()
 
