@@ -10,6 +10,12 @@ fresh process that loads that copy (IX_B200_LIBRARY) on the benchmark's shapes:
   and the pair kernel's and the three-body kernels' own times (CUDA events, the chains serialised);
 * the 4,096 water clusters of the batched workload: the time of one batched evaluation.
 
+A candidate counts only if it computes what the shipped build computes.  Before the search, the shipped (in-tree)
+library relaxes the box once and records its energy and forces at that frame, and the clusters' batched energies and
+forces, in a fresh process of its own.  Each candidate evaluates the same frame and clusters, and its results must
+agree with the recorded ones to within half the accuracy bar (1e-6 relative energy, 1e-5 relative RMS force) that the
+tests hold the shipped build to against the FP64 oracle; every candidate's MD run then starts from that frame.
+
 The search is coordinate-wise: starting from the current values, each group of constants is varied over its
 candidates with the others fixed, and the best by the objective (the MD step time, plus the batched evaluation time
 for the groups that change it) is kept before the next group if it beats the current values by more than MARGIN (the
@@ -77,32 +83,75 @@ def compile_candidates(candidates, workdir, jobs=4):
     return out
 
 
-def measure(steps, clusters=True):
-    """Timings of the library named by IX_B200_LIBRARY (run in a fresh process)."""
+# a candidate's energy (relative) and forces (relative RMS) against the shipped build's: half the accuracy bar, so
+# that a candidate within it stays within the bar against the FP64 oracle too
+AGREEMENT_ENERGY = 5e-7
+AGREEMENT_FORCE = 5e-6
+
+
+def _box_system():
+    from interaxplugin import workloads as W
+    cfg = W.CONFIGS["24k"]
+    return W.water_box(cfg["num_waters"], cfg["box_length"], cfg["cutoff"], seed=1,
+                       three_body_cutoff=cfg["three_body_cutoff"], rigid=True)
+
+
+def force_error(f, ref):
+    """Relative RMS difference of two force arrays."""
+    import numpy as np
+    f, ref = np.asarray(f, dtype=np.float64), np.asarray(ref, dtype=np.float64)
+    return float(np.sqrt(((f - ref) ** 2).mean() / (ref ** 2).mean()))
+
+
+def batch_energy_error(energies, ref):
+    """The largest difference of a cluster's total energy, relative to the sum of its terms' magnitudes (a cluster's
+    terms can cancel to a small total)."""
+    import numpy as np
+    energies, ref = np.asarray(energies, dtype=np.float64), np.asarray(ref, dtype=np.float64)
+    scale = np.maximum(np.abs(ref).sum(1), 1e-300)
+    return float((np.abs(energies.sum(1) - ref.sum(1)) / scale).max())
+
+
+def reference_frame(path):
+    """With the library this process loads (the shipped in-tree build): relax the 24k box once and record the frame
+    with its energy and forces, and the 4,096 clusters' batched energies and forces, in `path` (.npz)."""
+    import numpy as np
+
+    sys.path.insert(0, str(PKG.parent))
+    import bench  # the benchmark's relaxation
+    from interaxplugin import BatchContext, Context
+    from interaxplugin import workloads as W
+
+    system, pos, _ = _box_system()
+    ctx = Context(system)
+    pos = bench.relax(ctx, system, pos, iterations=30)
+    st = ctx.getState()
+    systems, positions = W.cluster_set(4096, seed=1)
+    energies, forces = BatchContext(systems).compute(positions)
+    np.savez(path, pos=pos, energy=st.getPotentialEnergy(), forces=st.getForces(), batch_energies=energies,
+             batch_forces=np.concatenate(forces))
+
+
+def measure(steps, frame, clusters=True):
+    """Agreement with the shipped build at the recorded frame (`frame`, from reference_frame) and timings of the
+    library named by IX_B200_LIBRARY (run in a fresh process)."""
     import ctypes
 
     import numpy as np
     import torch
 
-    sys.path.insert(0, str(PKG.parent))
-    import bench  # the benchmark's relaxation
     from interaxplugin import BatchContext, Context, _capi
     from interaxplugin import workloads as W
 
-    cfg = W.CONFIGS["24k"]
-    system, pos, box = W.water_box(cfg["num_waters"], cfg["box_length"], cfg["cutoff"], seed=1,
-                                   three_body_cutoff=cfg["three_body_cutoff"], rigid=True)
+    ref = np.load(frame)
+    system, _, _ = _box_system()
     ctx = Context(system)
     L = _capi.lib()
-    pos = bench.relax(ctx, system, pos, iterations=30)
-    # the candidate must give the oracle's result (the target bar) to count at all
-    sys.path.insert(0, str(PKG.parent / "oracle"))
-    import pyoracle
+    pos = ref["pos"]
+    ctx.setPositions(pos)
     st = ctx.getState()
-    e_or, f_or = pyoracle.evaluate(system, pos, box)
-    f = st.getForces()
-    err_e = abs(st.getPotentialEnergy() - e_or) / abs(e_or)
-    err_f = float(np.sqrt(((f - f_or) ** 2).mean() / (f_or ** 2).mean()))
+    err_e = abs(st.getPotentialEnergy() - float(ref["energy"])) / abs(float(ref["energy"]))
+    err_f = force_error(st.getForces(), ref["forces"])
     vel = np.ascontiguousarray(W.initial_velocities(system, 300.0, seed=0))
     masses = np.array([system.getParticleMass(i) for i in range(system.getNumParticles())])
     ctx._check(L.ix_md_set_masses(ctx._ctx, _capi.ptr(masses)))
@@ -126,11 +175,13 @@ def measure(steps, clusters=True):
         pair.append(p.value)
         atm.append(t.value)
     out = {"md_step_ms": step_ms, "pair_kernel_ms": float(np.median(pair)), "three_body_ms": float(np.median(atm)),
-           "oracle_energy_error": err_e, "oracle_force_error": err_f}
+           "energy_error": err_e, "force_error": err_f}
     if clusters:
         systems, positions = W.cluster_set(4096, seed=1)
         batch = BatchContext(systems)
-        batch.compute(positions)
+        energies, forces = batch.compute(positions)
+        out["clusters_energy_error"] = batch_energy_error(energies, ref["batch_energies"])
+        out["clusters_force_error"] = force_error(np.concatenate(forces), ref["batch_forces"])
         dpos = torch.from_numpy(np.ascontiguousarray(np.concatenate(positions))).cuda()
         dfor = torch.empty_like(dpos)
         den = torch.empty((4096, 4), dtype=torch.float64, device="cuda")
@@ -149,9 +200,18 @@ def measure(steps, clusters=True):
     return out
 
 
-def run_candidate(path, steps, clusters):
+def record_reference_frame(path):
+    """reference_frame(path) in a fresh process with the in-tree library (no IX_B200_LIBRARY)."""
+    env = {k: v for k, v in os.environ.items() if k != "IX_B200_LIBRARY"}
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--reference-frame", str(path)]
+    r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
+    if r.returncode != 0:
+        raise RuntimeError("recording the shipped build's reference frame failed:\n" + r.stderr[-2000:])
+
+
+def run_candidate(path, steps, frame, clusters):
     env = dict(os.environ, IX_B200_LIBRARY=str(path))
-    cmd = [sys.executable, str(Path(__file__).resolve()), "--measure", "--steps", str(steps)]
+    cmd = [sys.executable, str(Path(__file__).resolve()), "--measure", "--steps", str(steps), "--frame", str(frame)]
     if not clusters:
         cmd.append("--no-clusters")
     r = subprocess.run(cmd, env=env, capture_output=True, text=True, timeout=900)
@@ -164,8 +224,20 @@ def run_candidate(path, steps, clusters):
 MARGIN = 0.01
 
 
+def agrees(m):
+    """Whether a measurement's results meet the bar: agreement with the shipped build (energy_error, force_error and,
+    with the clusters, clusters_*), or, in measurements recorded by an earlier form of the tuner, the error against
+    the FP64 oracle (oracle_*, against the full bar)."""
+    if "oracle_energy_error" in m:
+        return m["oracle_energy_error"] <= 1e-6 and m["oracle_force_error"] <= 1e-5
+    ok = m["energy_error"] <= AGREEMENT_ENERGY and m["force_error"] <= AGREEMENT_FORCE
+    if "clusters_energy_error" in m:
+        ok = ok and m["clusters_energy_error"] <= AGREEMENT_ENERGY and m["clusters_force_error"] <= AGREEMENT_FORCE
+    return ok
+
+
 def objective(m, with_clusters):
-    if "error" in m or not (m["oracle_energy_error"] <= 1e-6 and m["oracle_force_error"] <= 1e-5):
+    if "error" in m or not agrees(m):
         return float("inf")
     return m["md_step_ms"] + (m["clusters_ms"] if with_clusters else 0.0)
 
@@ -203,6 +275,8 @@ def main():
     p.add_argument("--out", default=str(build_lib.TUNING))
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--measure", action="store_true", help=argparse.SUPPRESS)
+    p.add_argument("--frame", help=argparse.SUPPRESS)
+    p.add_argument("--reference-frame", metavar="NPZ", help=argparse.SUPPRESS)
     p.add_argument("--no-clusters", action="store_true", help=argparse.SUPPRESS)
     p.add_argument("--reselect", metavar="FILE")
     p.add_argument("--groups", help="comma-separated names of the groups to search (default: all)")
@@ -210,8 +284,11 @@ def main():
     if args.reselect:
         print("chosen", reselect(args.reselect))
         return
+    if args.reference_frame:
+        reference_frame(args.reference_frame)
+        return
     if args.measure:
-        print(json.dumps(measure(args.steps, clusters=not args.no_clusters)))
+        print(json.dumps(measure(args.steps, args.frame, clusters=not args.no_clusters)))
         return
     import torch
     current = dict(DEFAULTS)
@@ -219,6 +296,8 @@ def main():
     record = []
     workdir = tempfile.mkdtemp(prefix="ix_tune_")
     t0 = time.time()
+    frame = Path(workdir) / "reference_frame.npz"
+    record_reference_frame(frame)
     groups = GROUPS if not args.groups else [g for g in GROUPS if g[0] in args.groups.split(",")]
     for name, options in groups:
         # the batched workload has no pair list and no site lists to rebuild: the skins do not change it
@@ -227,7 +306,7 @@ def main():
         libs = compile_candidates(candidates, workdir)
         results = []
         for values in candidates:
-            m = run_candidate(libs[_key(values)], args.steps, clusters)
+            m = run_candidate(libs[_key(values)], args.steps, frame, clusters)
             results.append((objective(m, clusters), values))
             record.append({"group": name, "values": {k: values[k] for k in options[0]}, "measured": m})
             print(name, {k: values[k] for k in options[0]}, m, flush=True)

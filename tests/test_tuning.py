@@ -66,7 +66,7 @@ def test_selection_keeps_the_current_values_within_the_margin(tmp_path):
     other = dict(cur, IX_TUNE_PAIR_ROUND=64)
     assert tune.select([(1.0, cur), (0.995, other)], cur) == cur             # 0.5%: noise
     assert tune.select([(1.0, cur), (0.95, other)], cur) == other            # 5%: kept
-    assert tune.select([(float("inf"), cur), (0.95, other)], cur) == other   # the current values failed the oracle
+    assert tune.select([(float("inf"), cur), (0.95, other)], cur) == other   # the current values failed the check
     record = {"chosen": {}, "measurements": [
         {"group": "pair tiles", "values": {"IX_TUNE_PAIR_ROUND": 128},
          "measured": {"md_step_ms": 0.30, "clusters_ms": 0.30, "oracle_energy_error": 1e-7,
@@ -85,3 +85,27 @@ def test_selection_keeps_the_current_values_within_the_margin(tmp_path):
     chosen = tune.reselect(path)
     assert chosen["IX_TUNE_PAIR_ROUND"] == 64 and chosen["IX_TUNE_PAIR_SHARED_TABLE_BYTES"] == 0
     assert json.loads(path.read_text())["chosen"] == chosen
+
+
+def test_candidates_are_checked_against_the_shipped_build():
+    base = {"md_step_ms": 0.2, "energy_error": 1e-7, "force_error": 1e-6}
+    assert tune.agrees(base)
+    assert not tune.agrees(dict(base, energy_error=6e-7))       # half the 1e-6 energy bar
+    assert not tune.agrees(dict(base, force_error=6e-6))        # half the 1e-5 force bar
+    with_clusters = dict(base, clusters_energy_error=1e-7, clusters_force_error=1e-6)
+    assert tune.agrees(with_clusters)
+    assert not tune.agrees(dict(with_clusters, clusters_energy_error=1e-6))
+    assert tune.objective(dict(with_clusters, clusters_ms=0.3), True) == 0.2 + 0.3
+    assert tune.objective(dict(base, force_error=1e-4), False) == float("inf")
+    # measurements recorded against the FP64 oracle keep the full bar
+    assert tune.agrees({"oracle_energy_error": 9e-7, "oracle_force_error": 9e-6})
+    # the error measures: relative RMS forces, and per cluster the total energy on the scale of its terms
+    import numpy as np
+    ref = np.ones((4, 3))
+    assert abs(tune.force_error(ref * (1 + 1e-6), ref) - 1e-6) < 1e-12
+    e_ref = np.array([[10.0, -10.0, 1.0, 0.0], [5.0, 0.0, 0.0, 0.0]])
+    e = e_ref.copy()
+    e[0, 2] += 2.1e-6                                        # 1e-7 of the first cluster's 21 kJ/mol of terms
+    assert abs(tune.batch_energy_error(e, e_ref) - 1e-7) < 1e-12
+    # the tuner runs the library only: the oracle is the tests' checker
+    assert "pyoracle" not in (PKG / "tune.py").read_text()
