@@ -1,0 +1,187 @@
+"""Pin the FP64 oracle's Axilrod-Teller-Muto term to the reference's own three-body tests (no GPU).
+
+* testTriple (tests/TestInteraxThreeBodyForce.h:185-222): one triple against its energy written out with the law of
+  cosines, three identical sites against C9 = 3/4 alpha C6, and the scale factor.
+* computeReferenceEnergy and computeReferenceForces (tests/TestInteraxThreeBodyForce.h:71-129 and the finite
+  differences after them): the energy as a loop over all triples of sites with the cosines of the angles at the
+  vertices, distinct molecules, the cutoff on all three sides, periodic minimum images, Tang-Toennies and centroid
+  damping and the alchemical factor; the forces as central differences of that energy.  Restated here in Python.
+"""
+import itertools
+import math
+
+import numpy as np
+import pytest
+
+import pyoracle
+from interaxplugin import InteraxThreeBodyForce, System
+
+# the three site types of testTriple: alpha (nm^3), frequency (kJ/mol), width (nm)
+SITE_TYPES = [(0.004087456746801944, 911.0681141195369, 0.03), (0.0016246535729804365, 1262.664320774599, 0.025),
+              (0.008817709933796472, 747.5256543931184, 0.035)]
+TRIPLE = np.array([[0.1, -0.2, 0.05], [0.45, 0.1, -0.1], [-0.05, 0.3, 0.2]])
+
+
+def c9_of(a, b, c):
+    """C9 of three sites from their (alpha, frequency) (InteraxThreeBodyForceImpl.h:69-72)."""
+    (aa, wa), (ab, wb), (ac, wc) = a, b, c
+    return 1.5 * aa * ab * ac * wa * wb * wc * (wa + wb + wc) / ((wa + wb) * (wb + wc) * (wc + wa))
+
+
+def single_sites(types, box=None):
+    system = System()
+    force = InteraxThreeBodyForce()
+    for i, (a, w, s) in enumerate(types):
+        system.addParticle(1.0)
+        force.addSite([i], a, w, s)
+    system.addForce(force)
+    return system, force
+
+
+def test_triple_against_the_law_of_cosines():
+    system, force = single_sites(SITE_TYPES)
+    p = TRIPLE
+    rab, rac, rbc = (np.linalg.norm(p[1] - p[0]), np.linalg.norm(p[2] - p[0]), np.linalg.norm(p[2] - p[1]))
+    cos_a = (rab ** 2 + rac ** 2 - rbc ** 2) / (2 * rab * rac)
+    cos_b = (rab ** 2 + rbc ** 2 - rac ** 2) / (2 * rab * rbc)
+    cos_c = (rac ** 2 + rbc ** 2 - rab ** 2) / (2 * rac * rbc)
+    geometry = (1 + 3 * cos_a * cos_b * cos_c) / (rab * rac * rbc) ** 3
+    expected = c9_of(*[t[:2] for t in SITE_TYPES]) * geometry
+    e, _ = pyoracle.evaluate(system, p, np.eye(3) * 10.0)
+    assert e == pytest.approx(expected, rel=1e-12)
+    # three identical sites: the C6 of a site is 3/4 alpha^2 w, and C9 = 3/4 alpha C6
+    a, w, _ = SITE_TYPES[0]
+    system, force = single_sites([SITE_TYPES[0]] * 3)
+    c6 = 0.75 * a * a * w
+    e, _ = pyoracle.evaluate(system, p, np.eye(3) * 10.0)
+    assert e == pytest.approx(0.75 * a * c6 * geometry, rel=1e-12)
+    # the scale factor multiplies every triple
+    force.setScaleFactor(0.7)
+    e_scaled, _ = pyoracle.evaluate(system, p, np.eye(3) * 10.0)
+    assert e_scaled == pytest.approx(0.7 * e, rel=1e-12)
+
+
+def tang_toennies(n, x):
+    """f_n(x) = 1 - exp(-x) sum_{k<=n} x^k/k!, summed as its tail exp(-x) sum_{k>n} x^k/k! below x = n + 1, where the
+    closed form cancels."""
+    term, partial = 1.0, 1.0
+    for k in range(1, n + 1):
+        term *= x / k
+        partial += term
+    if x >= n + 1:
+        return 1.0 - math.exp(-x) * partial
+    tail = 0.0
+    for k in range(n + 1, 400):
+        term *= x / k
+        tail += term
+        if term < 1e-30 * tail:
+            break
+    return math.exp(-x) * tail
+
+
+def brute_force_energy(sites, positions, box_length, cutoff, scale, tt_scale, radius, lam):
+    """The ATM energy as a loop over all triples of sites (the reference test's computeReferenceEnergy).  `sites`:
+    (particles, alpha, frequency, width, molecule, alchemical) per site; a negative molecule is the site's own."""
+    centre = [np.mean([positions[p] for p in s[0]], axis=0) for s in sites]
+    molecule = [s[4] if s[4] >= 0 else -1 - i for i, s in enumerate(sites)]
+
+    def delta(i, j):
+        d = centre[j] - centre[i]
+        return d - box_length * np.floor(d / box_length + 0.5)
+
+    def damping(i, j, r):
+        f = 1.0
+        if tt_scale:
+            f *= tang_toennies(3, tt_scale * 2 * r / (sites[i][3] + sites[j][3]))
+        if radius > 0:
+            f *= 1 - math.exp(-(r / radius) ** 6)
+        return f
+
+    energy = 0.0
+    for i, j, k in itertools.combinations(range(len(sites)), 3):
+        if molecule[i] == molecule[j] or molecule[i] == molecule[k] or molecule[j] == molecule[k]:
+            continue
+        a, b, c = delta(i, j), delta(i, k), delta(j, k)
+        ra, rb, rc = np.linalg.norm(a), np.linalg.norm(b), np.linalg.norm(c)
+        if ra >= cutoff or rb >= cutoff or rc >= cutoff:
+            continue
+        # the angle at each vertex lies between the vectors to its two neighbours
+        cos_a, cos_b, cos_c = a @ b / (ra * rb), -(a @ c) / (ra * rc), b @ c / (rb * rc)
+        c9 = scale * c9_of(sites[i][1:3], sites[j][1:3], sites[k][1:3])
+        e = c9 * (1 + 3 * cos_a * cos_b * cos_c) / (ra * rb * rc) ** 3
+        e *= damping(i, j, ra) * damping(i, k, rb) * damping(j, k, rc)
+        if sites[i][5] or sites[j][5] or sites[k][5]:
+            e *= lam
+        energy += e
+    return energy
+
+
+# damping scale and centroid radius where both dampings are of order one at the sites' distances (0.3-0.6 nm)
+@pytest.mark.parametrize("tt_scale, radius", [(0.0, 0.0), (0.3, 0.0), (0.0, 0.4), (0.3, 0.4)])
+def test_against_the_all_triples_loop(tt_scale, radius):
+    rng = np.random.default_rng(7)
+    box_length, cutoff, scale, lam = 1.3, 0.6, 0.8, 0.6
+    # 13 particles: 8 single-particle sites and 2 centroid sites of 2 and 3 particles; two sites share molecule 5, two
+    # share molecule 2, two are alchemical
+    layout = [[0], [1], [2], [3], [4], [5], [6], [7], [8, 9], [10, 11, 12]]
+    molecules = [5, 5, -1, 2, -1, -1, 2, -1, -1, -1]
+    alchemical = [False, False, True, False, False, False, False, True, False, False]
+    for attempt in range(100):
+        # one site per cell of a jittered 3 x 3 x 3 grid cut to 10 sites, its particles within 0.05 nm of the site
+        cells = rng.permutation(27)[:10]
+        pos = np.zeros((13, 3))
+        for s, parts in enumerate(layout):
+            grid = np.array([cells[s] % 3, (cells[s] // 3) % 3, cells[s] // 9], dtype=float)
+            site = (grid + 0.5 + rng.uniform(-0.2, 0.2, 3)) * box_length / 3
+            for p in parts:
+                pos[p] = site + rng.uniform(-0.05, 0.05, 3)
+        # no side within 2e-3 nm of the cutoff, so that the central differences do not straddle it
+        centres = np.array([pos[parts].mean(0) for parts in layout])
+        d = centres[:, None] - centres[None]
+        d -= box_length * np.floor(d / box_length + 0.5)
+        r = np.linalg.norm(d, axis=-1)
+        if np.all(np.abs(r - cutoff) > 2e-3):
+            break
+    system = System()
+    force = InteraxThreeBodyForce()
+    for _ in range(13):
+        system.addParticle(1.0)
+    sites = []
+    for s, parts in enumerate(layout):
+        a, w, width = SITE_TYPES[s % 3]
+        force.addSite(parts, a, w, width, molecules[s], alchemical[s])
+        sites.append((parts, a, w, width, molecules[s], alchemical[s]))
+    force.setCutoffDistance(cutoff)
+    force.setUsesPeriodicBoundaryConditions(True)
+    force.setScaleFactor(scale)
+    if tt_scale:
+        force.setDampingMethod(InteraxThreeBodyForce.TangToennies)
+        force.setDampingScale(tt_scale)
+    force.setCentroidDampingRadius(radius)
+    system.addForce(force)
+    box = np.eye(3) * box_length
+    e, f = pyoracle.evaluate(system, pos, box, parameters={force.getAlchemicalParameterName(): lam})
+
+    def energy(x):
+        return brute_force_energy(sites, x, box_length, cutoff, scale, tt_scale, radius, lam)
+
+    expected = energy(pos)
+    # the case exercises the alchemical factor (some triples hold an alchemical site) and the damping
+    assert expected != 0.0
+    assert brute_force_energy(sites, pos, box_length, cutoff, scale, tt_scale, radius, 1.0) != expected
+    if tt_scale or radius:
+        undamped = brute_force_energy(sites, pos, box_length, cutoff, scale, 0.0, 0.0, lam)
+        assert abs(expected - undamped) > 1e-2 * abs(undamped)
+    assert e == pytest.approx(expected, rel=1e-10)
+    # forces: five-point central differences of the loop's energy
+    h = 1e-5
+    fd = np.zeros_like(pos)
+    for p in range(len(pos)):
+        for k in range(3):
+            def shifted(t):
+                x = pos.copy()
+                x[p, k] += t
+                return energy(x)
+            fd[p, k] = -(shifted(-2 * h) - 8 * shifted(-h) + 8 * shifted(h) - shifted(2 * h)) / (12 * h)
+    rms = math.sqrt((fd ** 2).mean())
+    assert np.abs(f - fd).max() <= 1e-6 * rms
