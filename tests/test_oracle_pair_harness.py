@@ -88,7 +88,16 @@ def switching(r, start, cutoff):
     return 1 - 10 * x ** 3 + 15 * x ** 4 - 6 * x ** 5
 
 
-def harness(force, model, positions, box_length, lam):
+def minimum_image(d, box):
+    """The shortest periodic image of d in a box whose rows are its (reduced) edge vectors: d reduced along c, b and a,
+    then the nearest of it and its 26 neighbouring images."""
+    for k in (2, 1, 0):
+        d = d - box[k] * round(d[k] / box[k][k])
+    images = [d + i * box[0] + j * box[1] + k * box[2] for i in (-1, 0, 1) for j in (-1, 0, 1) for k in (-1, 0, 1)]
+    return min(images, key=lambda v: v @ v)
+
+
+def harness(force, model, positions, box, lam):
     """Energy, forces and the sum of |pair energies| before switching (the error scale) of a pair force, by the loop
     over all pairs."""
     n = force.getNumParticles()
@@ -105,7 +114,7 @@ def harness(force, model, positions, box_length, lam):
                 continue
             d = positions[j] - positions[i]
             if periodic:
-                d = d - box_length * np.floor(d / box_length + 0.5)
+                d = minimum_image(d, box)
             r = mpmath.sqrt(sum(mpmath.mpf(float(v)) ** 2 for v in d))
             base = model(force.getParticleParameters(i)[:-1], force.getParticleParameters(j)[:-1])
             if base is None:
@@ -175,9 +184,16 @@ MODELS = {"dispersion": lambda p, q: dispersion_pair(p, q, 0.8), "exchange": exc
           "short_range": short_range_pair}
 
 
+# a triclinic box in reduced form (each edge's components along the earlier edges within half of them); its
+# perpendicular widths (1.452, 1.461, 1.5 nm) stay above twice the 0.7 nm cutoff, so each pair has one image within it
+TRICLINIC = np.array([[1.55, 0.0, 0.0], [0.4, 1.5, 0.0], [-0.3, 0.35, 1.5]])
+
+
 @pytest.mark.parametrize("kind", ["dispersion", "exchange", "short_range"])
-@pytest.mark.parametrize("method, lam", [(InteraxPairForce.CutoffPeriodic, 0.6), (InteraxPairForce.NoCutoff, 0.3)])
-def test_pair_force_against_the_harness(kind, method, lam):
+@pytest.mark.parametrize("method, lam, triclinic", [(InteraxPairForce.CutoffPeriodic, 0.6, False),
+                                                    (InteraxPairForce.CutoffPeriodic, 0.6, True),
+                                                    (InteraxPairForce.NoCutoff, 0.3, False)])
+def test_pair_force_against_the_harness(kind, method, lam, triclinic):
     mp.dps = 40
     rng = np.random.default_rng(5)
     box_length = 1.5
@@ -188,9 +204,9 @@ def test_pair_force_against_the_harness(kind, method, lam):
     pos += rng.uniform(-0.08, 0.08, pos.shape)
     pos = np.vstack([pos, pos[0] + [0.12, 0.0, 0.0], pos[5] + [0.0, 0.15, 0.0]])
     system, force = build(kind, method, rng)
-    box = np.eye(3) * box_length
+    box = TRICLINIC if triclinic else np.eye(3) * box_length
     e, f = pyoracle.evaluate(system, pos, box, parameters={force.getAlchemicalParameterName(): lam})
-    expected, forces, scale = harness(force, MODELS[kind], pos, box_length, lam)
+    expected, forces, scale = harness(force, MODELS[kind], pos, box, lam)
     # both in double or better: the oracle agrees to ~1e-13 of the error scale, where the soft core alone moves the
     # energy by a few per cent and a change of lambda by 1e-4 moves it by 1e-5
     assert abs(e - expected) <= 1e-11 * scale, (e, expected, scale)
