@@ -1,0 +1,46 @@
+"""The B200 kernels against the reference's pair-test harness itself (tests/TestInteraxPairForce.h:59-148, restated in
+40-digit arithmetic in test_oracle_pair_harness.py), with the three pair forces in one System, so that they run in
+one fused pass: exclusions, a lone pair, equal, nearly equal and distinct widths, alchemical particles in and out of
+the soft core, switching, rectangular and triclinic periodic boxes, and no cutoff.
+
+Each force group is held to the reference's single-precision bar for its pair tests (energy 2e-5 of the sum of |pair
+energies|, force 2e-4 of the largest force, tests/TestInteraxPairForce.h:727-730); the fused total to this build's
+target (1e-6 of the sum of |pair energies|, 1e-5 relative RMS force) against the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+import test_oracle_pair_harness as H
+from interaxplugin import Context, InteraxPairForce, System
+from parity import compare, gpu_state, max_force_error
+
+pytestmark = pytest.mark.gpu
+
+KINDS = ["dispersion", "exchange", "short_range"]
+
+
+@pytest.mark.parametrize("method, lam, triclinic", [(InteraxPairForce.CutoffPeriodic, 0.6, False),
+                                                    (InteraxPairForce.CutoffPeriodic, 0.6, True),
+                                                    (InteraxPairForce.NoCutoff, 0.3, False)])
+def test_fused_pair_forces_against_the_harness(method, lam, triclinic):
+    H.mp.dps = 40
+    rng = np.random.default_rng(11)
+    pos = H.harness_positions(rng)
+    system = System()
+    for _ in range(len(pos)):
+        system.addParticle(1.0)
+    forces = []
+    for group, kind in enumerate(KINDS):
+        _, force = H.build(kind, method, rng)
+        force.setForceGroup(group)
+        system.addForce(force)
+        forces.append(force)
+    box = H.TRICLINIC if triclinic else np.eye(3) * H.BOX_LENGTH
+    params = {"lambda_sterics": lam}
+    ctx = Context(system)
+    for group, (kind, force) in enumerate(zip(KINDS, forces)):
+        e, f, _ = gpu_state(system, pos, box, params, groups=1 << group, context=ctx)
+        expected, f_ref, scale = H.harness(force, H.MODELS[kind], pos, box, lam)
+        assert abs(e - expected) <= 2e-5 * scale, (kind, e, expected, scale)
+        assert max_force_error(f, f_ref) <= 2e-4, kind
+    compare(system, pos, box, params, scale="abs", context=ctx)

@@ -184,6 +184,18 @@ MODELS = {"dispersion": lambda p, q: dispersion_pair(p, q, 0.8), "exchange": exc
           "short_range": short_range_pair}
 
 
+BOX_LENGTH = 1.5
+
+
+def harness_positions(rng):
+    """12 particles on a jittered 3 x 2 x 2 lattice of the rectangular box, and two more 0.12 and 0.15 nm from
+    particles 0 and 5; the first of those is alchemical, so its pair with particle 0 is in the soft core."""
+    grid = np.array([[x, y, z] for x in range(3) for y in range(2) for z in range(2)], dtype=float)
+    pos = (grid + 0.5) * np.array([BOX_LENGTH / 3, BOX_LENGTH / 2, BOX_LENGTH / 2])
+    pos += rng.uniform(-0.08, 0.08, pos.shape)
+    return np.vstack([pos, pos[0] + [0.12, 0.0, 0.0], pos[5] + [0.0, 0.15, 0.0]])
+
+
 # a triclinic box in reduced form (each edge's components along the earlier edges within half of them); its
 # perpendicular widths (1.452, 1.461, 1.5 nm) stay above twice the 0.7 nm cutoff, so each pair has one image within it
 TRICLINIC = np.array([[1.55, 0.0, 0.0], [0.4, 1.5, 0.0], [-0.3, 0.35, 1.5]])
@@ -196,15 +208,9 @@ TRICLINIC = np.array([[1.55, 0.0, 0.0], [0.4, 1.5, 0.0], [-0.3, 0.35, 1.5]])
 def test_pair_force_against_the_harness(kind, method, lam, triclinic):
     mp.dps = 40
     rng = np.random.default_rng(5)
-    box_length = 1.5
-    # 12 particles on a jittered 3 x 2 x 2 lattice of the box, and two more 0.12 and 0.15 nm from particles 0 and 5;
-    # the first of those is alchemical, so its pair with particle 0 is in the soft core
-    grid = np.array([[x, y, z] for x in range(3) for y in range(2) for z in range(2)], dtype=float)
-    pos = (grid + 0.5) * np.array([box_length / 3, box_length / 2, box_length / 2])
-    pos += rng.uniform(-0.08, 0.08, pos.shape)
-    pos = np.vstack([pos, pos[0] + [0.12, 0.0, 0.0], pos[5] + [0.0, 0.15, 0.0]])
+    pos = harness_positions(rng)
     system, force = build(kind, method, rng)
-    box = TRICLINIC if triclinic else np.eye(3) * box_length
+    box = TRICLINIC if triclinic else np.eye(3) * BOX_LENGTH
     e, f = pyoracle.evaluate(system, pos, box, parameters={force.getAlchemicalParameterName(): lam})
     expected, forces, scale = harness(force, MODELS[kind], pos, box, lam)
     # both in double or better: the oracle agrees to ~1e-13 of the error scale, where the soft core alone moves the
