@@ -116,11 +116,14 @@ def brute_force_energy(sites, positions, box_length, cutoff, scale, tt_scale, ra
     return energy
 
 
+BOX_LENGTH, CUTOFF, SCALE, LAMBDA = 1.3, 0.6, 0.8, 0.6
 # damping scale and centroid radius where both dampings are of order one at the sites' distances (0.3-0.6 nm)
-@pytest.mark.parametrize("tt_scale, radius", [(0.0, 0.0), (0.3, 0.0), (0.0, 0.4), (0.3, 0.4)])
-def test_against_the_all_triples_loop(tt_scale, radius):
-    rng = np.random.default_rng(7)
-    box_length, cutoff, scale, lam = 1.3, 0.6, 0.8, 0.6
+DAMPING_CASES = [(0.0, 0.0), (0.3, 0.0), (0.0, 0.4), (0.3, 0.4)]
+
+
+def loop_case(tt_scale, radius, rng):
+    """A periodic case of every option: the System, its force, the sites as the loop takes them, and positions."""
+    box_length, cutoff = BOX_LENGTH, CUTOFF
     # 13 particles: 8 single-particle sites and 2 centroid sites of 2 and 3 particles; two sites share molecule 5, two
     # share molecule 2, two are alchemical
     layout = [[0], [1], [2], [3], [4], [5], [6], [7], [8, 9], [10, 11, 12]]
@@ -153,27 +156,20 @@ def test_against_the_all_triples_loop(tt_scale, radius):
         sites.append((parts, a, w, width, molecules[s], alchemical[s]))
     force.setCutoffDistance(cutoff)
     force.setUsesPeriodicBoundaryConditions(True)
-    force.setScaleFactor(scale)
+    force.setScaleFactor(SCALE)
     if tt_scale:
         force.setDampingMethod(InteraxThreeBodyForce.TangToennies)
         force.setDampingScale(tt_scale)
     force.setCentroidDampingRadius(radius)
     system.addForce(force)
-    box = np.eye(3) * box_length
-    e, f = pyoracle.evaluate(system, pos, box, parameters={force.getAlchemicalParameterName(): lam})
+    return system, force, sites, pos
 
+
+def loop_energy_and_forces(sites, pos, tt_scale, radius, lam=LAMBDA):
+    """The loop's energy, and the forces as five-point central differences of it."""
     def energy(x):
-        return brute_force_energy(sites, x, box_length, cutoff, scale, tt_scale, radius, lam)
+        return brute_force_energy(sites, x, BOX_LENGTH, CUTOFF, SCALE, tt_scale, radius, lam)
 
-    expected = energy(pos)
-    # the case exercises the alchemical factor (some triples hold an alchemical site) and the damping
-    assert expected != 0.0
-    assert brute_force_energy(sites, pos, box_length, cutoff, scale, tt_scale, radius, 1.0) != expected
-    if tt_scale or radius:
-        undamped = brute_force_energy(sites, pos, box_length, cutoff, scale, 0.0, 0.0, lam)
-        assert abs(expected - undamped) > 1e-2 * abs(undamped)
-    assert e == pytest.approx(expected, rel=1e-10)
-    # forces: five-point central differences of the loop's energy
     h = 1e-5
     fd = np.zeros_like(pos)
     for p in range(len(pos)):
@@ -183,5 +179,21 @@ def test_against_the_all_triples_loop(tt_scale, radius):
                 x[p, k] += t
                 return energy(x)
             fd[p, k] = -(shifted(-2 * h) - 8 * shifted(-h) + 8 * shifted(h) - shifted(2 * h)) / (12 * h)
+    return energy(pos), fd
+
+
+@pytest.mark.parametrize("tt_scale, radius", DAMPING_CASES)
+def test_against_the_all_triples_loop(tt_scale, radius):
+    system, force, sites, pos = loop_case(tt_scale, radius, np.random.default_rng(7))
+    box = np.eye(3) * BOX_LENGTH
+    e, f = pyoracle.evaluate(system, pos, box, parameters={force.getAlchemicalParameterName(): LAMBDA})
+    expected, fd = loop_energy_and_forces(sites, pos, tt_scale, radius)
+    # the case exercises the alchemical factor (some triples hold an alchemical site) and the damping
+    assert expected != 0.0
+    assert brute_force_energy(sites, pos, BOX_LENGTH, CUTOFF, SCALE, tt_scale, radius, 1.0) != expected
+    if tt_scale or radius:
+        undamped = brute_force_energy(sites, pos, BOX_LENGTH, CUTOFF, SCALE, 0.0, 0.0, LAMBDA)
+        assert abs(expected - undamped) > 1e-2 * abs(undamped)
+    assert e == pytest.approx(expected, rel=1e-10)
     rms = math.sqrt((fd ** 2).mean())
     assert np.abs(f - fd).max() <= 1e-6 * rms
