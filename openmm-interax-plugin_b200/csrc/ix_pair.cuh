@@ -255,6 +255,9 @@ constexpr int kPairWarps = IX_TUNE_PAIR_WARPS;
 // 1: each tile's column lists (the queue positions of each column's pairs) are built once with the queue, and the
 // column forces of every round are read along them; 0: each round finds them from the row masks
 constexpr int kPairColumnLists = IX_TUNE_PAIR_COLUMN_LISTS;
+// 1: the column masks are always the transpose of the row masks, formed in registers (the tile list's column words
+// are not read); 0: only where the rows are filtered when queued
+constexpr bool kPairColumnTranspose = IX_TUNE_PAIR_COLUMN_TRANSPOSE != 0;
 // 1: the class-table path without per-pair tests evaluates two queued pairs per lane at a time in packed FP32
 // (computeQueuedPair2)
 constexpr int kPairIlp = IX_TUNE_PAIR_ILP;
@@ -506,7 +509,7 @@ __global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPai
         {
             const int jslot = L.tileJ[32 * t + lane];
             unsigned row = L.tileMask[64 * t + lane];
-            unsigned column = PREFILTER ? 0u : L.tileMask[64 * t + 32 + lane];
+            unsigned column = (PREFILTER || kPairColumnTranspose) ? 0u : L.tileMask[64 * t + 32 + lane];
             __syncwarp();
             stageParticle(S, 0, lane, iBase + lane, cx, cy, cz, false, C, L, P);
             stageParticle(S, 1, lane, jslot, cx, cy, cz, shiftImage, C, L, P);
@@ -529,8 +532,9 @@ __global__ void __launch_bounds__(32 * kPairWarps, IX_TUNE_PAIR_MIN_BLOCKS) kPai
                 }
                 row = kept;
             }
-            // the filtered columns are the transpose of the filtered rows; unfiltered, the list holds them
-            if (PREFILTER) column = transposeBits(row, lane);
+            // the filtered columns are the transpose of the filtered rows; unfiltered, the list holds them (or, with
+            // kPairColumnTranspose, they are formed here the same way)
+            if (PREFILTER || kPairColumnTranspose) column = transposeBits(row, lane);
             // queue the kept pairs row by row
             const int count = __popc(row);
             int start = count;

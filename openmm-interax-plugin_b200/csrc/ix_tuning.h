@@ -19,6 +19,12 @@
 #ifndef IX_TUNE_PAIR_COLUMN_LISTS
 #define IX_TUNE_PAIR_COLUMN_LISTS 0
 #endif
+// pair kernel: 1 = each tile's column masks formed in registers as the transpose of its row masks on every path;
+// 0 = loaded from the tile list where the candidates are not filtered against the cutoff when queued (the list holds
+// both, the columns the exact transpose of the rows)
+#ifndef IX_TUNE_PAIR_COLUMN_TRANSPOSE
+#define IX_TUNE_PAIR_COLUMN_TRANSPOSE 0
+#endif
 // pair kernel: 1 = two queued pairs per lane at a time on the class-table path without per-pair tests
 #ifndef IX_TUNE_PAIR_ILP
 #define IX_TUNE_PAIR_ILP 0

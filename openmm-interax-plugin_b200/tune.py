@@ -39,7 +39,8 @@ sys.path.insert(0, str(PKG))
 import build_lib  # noqa: E402
 
 DEFAULTS = {"IX_TUNE_PAIR_WARPS": 4, "IX_TUNE_PAIR_ROUND": 128, "IX_TUNE_PAIR_MIN_BLOCKS": 8,
-            "IX_TUNE_PAIR_COLUMN_LISTS": 0, "IX_TUNE_PAIR_ILP": 0, "IX_TUNE_PAIR_SHARED_TABLE_BYTES": 0,
+            "IX_TUNE_PAIR_COLUMN_LISTS": 0, "IX_TUNE_PAIR_COLUMN_TRANSPOSE": 0, "IX_TUNE_PAIR_ILP": 0,
+            "IX_TUNE_PAIR_SHARED_TABLE_BYTES": 0,
             "IX_TUNE_PAIR_MAX_CLASSES": 16,
             "IX_TUNE_PAIR_SKIN": 0.1,
             "IX_TUNE_SITE_SKIN": 0.1, "IX_TUNE_ATM_FAST": 64, "IX_TUNE_ATM_ROUND": 64, "IX_TUNE_ATM_MIN_BLOCKS": 7,
@@ -53,6 +54,7 @@ GROUPS = [
                                           (4, 128, 6, 1, 0), (4, 128, 5, 0, 1), (4, 128, 6, 0, 1), (4, 64, 5, 0, 1),
                                           (2, 128, 10, 0, 1), (4, 256, 4, 0, 1))]),
     ("pair table", [dict(IX_TUNE_PAIR_SHARED_TABLE_BYTES=b) for b in (0, 1024, 2048)]),
+    ("pair columns", [dict(IX_TUNE_PAIR_COLUMN_TRANSPOSE=v) for v in (0, 1)]),
     ("pair skin", [dict(IX_TUNE_PAIR_SKIN=s) for s in (0.06, 0.08, 0.1, 0.12)]),
     ("three-body", [dict(IX_TUNE_ATM_FAST=f, IX_TUNE_ATM_ROUND=r, IX_TUNE_ATM_MIN_BLOCKS=b, IX_TUNE_ATM_ACCUM=acc)
                     for f, r, b, acc in ((64, 64, 7, 0), (64, 64, 8, 0), (64, 64, 10, 0), (32, 32, 12, 0),
