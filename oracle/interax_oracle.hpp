@@ -9,6 +9,12 @@
 //
 // The math is templated over the value type so that tests can run it with an operation-counting type, which is how
 // the algorithmic work per pair and per triple is fixed (see ox_count_* in interax_oracle.cpp).
+//
+// Parity is pinned: tests/test_oracle_golden.py checks it against the reference's golden export values (per-term
+// energies and forces of two InteraxFF systems) and its known answers; tests/test_oracle_pair_harness.py and
+// tests/test_oracle_three_body.py against independent restatements of the reference's pair-test harness (in 40-digit
+// arithmetic) and of its three-body all-triples loop, with every option; tests/test_long_range_correction.py against
+// high-precision quadrature.
 #pragma once
 
 #include <algorithm>
